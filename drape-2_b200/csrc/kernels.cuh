@@ -1,0 +1,977 @@
+// Device data layout and kernels of one implicit-Euler substep (predict / contact setup, contact activation,
+// owner-computes term assembly, persistent PCG + line search, finish), plus statistics.
+//
+// Reference algorithm: CpuSolver::Impl::substep (libs/sim/src/cpu_solver.cpp:230-314) in the displacement form of the
+// reference's 32-bit GPU path (u = x - xStart, term positions relative to the term's first vertex;
+// libs/sim/kernels/kernels.h:30-448). Per Newton iteration this file runs three launches instead of the reference's
+// ~40 + 13 per CG iteration dispatches with host round trips (gpu_solver_core.cpp:325-407):
+//   k_activate   contact activation (kernels.h:85-99)
+//   k_assemble   gradient, 3x3 block Hessian, block-Jacobi inverse and contact release, computed by the owner of each
+//                block row from its incident terms (replaces term kernels + gather, kernels.h:104-231)
+//   k_solve      one cooperative persistent launch: PCG (kernels.h:237-347), contact force, FP64 Newton slope, FP64
+//                line search and step application (cpu_solver.cpp:264-283) with device-side decisions.
+#pragma once
+
+#include <cooperative_groups.h>
+#include <cstdint>
+
+#include "device_math.cuh"
+
+namespace dcu {
+
+constexpr int kWarp = 32;
+constexpr int kAssembleWarps = 8;   // warps per k_assemble block
+constexpr int kRowLanes = 8;        // lanes per block row in the SpMV
+constexpr int kSolveThreads = 512;  // k_solve block size
+constexpr uint32_t kPinnedBit = 0x80000000u;
+constexpr int kPartialStride = 4;   // doubles per block in the partials array
+
+struct Particle {
+  float mass;
+  uint32_t fabric, garment, pinned;
+};
+
+struct Fabric {
+  float k[3];       // stretch warp, weft, bias
+  float limit[2];   // strain limits
+  float thickness, friction, damping;
+};
+
+struct Stretch {
+  uint32_t v[3];
+  uint32_t fabric;
+  float4 d;  // dmInv (0,0), (1,0), (0,1), (1,1)
+  float area;
+  float pad[3];
+};
+
+struct Hinge {
+  uint32_t v[4];
+  float K, rest;
+  float pad[2];
+};
+
+struct Seam {
+  uint32_t a, b, garment;
+  float startGap;
+};
+
+struct Contact {
+  float4 normal;  // xyz: plane normal, w: offset = r - phi(xStart)
+  float force, frictionLambda;
+  uint32_t nearBody, active;
+};
+
+struct Garment {
+  int32_t phase;  // 0 Assembling, 1 Settling
+  int32_t pad;
+  double assemblyTime;
+};
+
+// Device control block: the PCG / Newton scalars every block of k_solve recomputes identically, plus counters.
+struct Control {
+  int newtonDone;   // this substep's Newton loop has stopped (slope >= 0 or max move < 1e-9)
+  int error;        // 1: a grid barrier gave up waiting; 2: a row exceeded the assembly capacity
+  unsigned int barrierCount, barrierGeneration;
+  long long cgIterations, newtonIterations, lineSearchHalvings, substeps;
+  double lastAlpha, lastSlope, lastE0, lastMaxMove;
+  int lastCg;
+  int pad;
+};
+
+struct Params {
+  float h, invH2;
+  float gravity[3];
+  float limitScale, seamStiffness, closingSpeed, frictionSlip, collisionOffset, dampingScale, assemblyExtraDamping;
+  float contactReach, contactSnap;
+  double hD, cgTolerance;
+  int maxCg;
+  uint32_t n, nStretch, nHinge, nSeam, nBlocks, nGarments, slotsPadded;
+  unsigned long long barrierLimitNs;
+};
+
+struct Dev {
+  Params P;
+  FieldInfo field;
+  double fieldOrigin[3], fieldCell;
+  const float* fieldValues;
+  const Particle* particle;
+  const Fabric* fabric;
+  Garment* garment;
+  const Stretch* stretch;
+  const Hinge* hinge;
+  const Seam* seam;
+  const uint32_t* rowStart;
+  const uint32_t* colIndex;  // bit 31: the column's particle is pinned
+  const uint32_t* incStart;
+  const uint32_t* incEntry;
+  const uint32_t* incLocal;
+  float4 *x, *v, *xStart, *yRel, *u, *grad, *step, *r, *z, *p0, *p1, *ap, *apFull, *resid;
+  const float4* fExt;
+  const float4* pinPos;
+  float* blocks;   // 9 planes of slotsPadded floats, component 3*row+col
+  float4* precond; // 3 float4 (rows) per particle
+  Contact* contact;
+  double* partials;
+  Control* ctl;
+};
+
+// ---------------------------------------------------------------------------------------------------------------
+// Grid barrier with a bounded wait (cooperative launch guarantees co-residency; the bound turns a lost block into an
+// error status instead of a hang).
+
+__device__ __forceinline__ unsigned long long globalTimerNs() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ inline bool gridBarrier(Control* ctl, unsigned long long limitNs) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int* gen = &ctl->barrierGeneration;
+    volatile int* err = &ctl->error;
+    const unsigned int g0 = *gen;
+    __threadfence();
+    const unsigned int arrived = atomicAdd(&ctl->barrierCount, 1u) + 1u;
+    ok = 1;
+    if (arrived == gridDim.x) {
+      atomicExch(&ctl->barrierCount, 0u);
+      __threadfence();
+      atomicAdd(&ctl->barrierGeneration, 1u);
+    } else {
+      const unsigned long long start = globalTimerNs();
+      unsigned int spins = 0;
+      while (*gen == g0) {
+        if (*err != 0) {
+          ok = 0;
+          break;
+        }
+        if ((++spins & 63u) == 0 && globalTimerNs() - start > limitNs) {
+          atomicExch(&ctl->error, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+// Block-wide FP64 sum of up to kPartialStride values; thread 0 gets the result. Fixed tree shape -> deterministic.
+template <int K>
+__device__ inline void blockSum(double (&v)[K], double* out) {
+  __shared__ double red[K][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k) red[k][w] = v[k];
+  __syncthreads();
+  if (w == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      double s = lane < nw ? red[k][lane] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+      if (lane == 0) out[k] = s;
+    }
+  }
+}
+
+// Sums column k of the per-block partials over the grid, identically in every block; result broadcast to all threads.
+template <int K>
+__device__ inline void gridTotals(const double* partials, double (&out)[K]) {
+  __shared__ double res[K];
+  double v[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) v[k] = 0.0;
+  for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] += __ldcg(partials + b * kPartialStride + k);
+  blockSum<K>(v, res);
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < K; ++k) out[k] = res[k];
+  __syncthreads();
+}
+
+__device__ inline double gridMax(const double* partials, int k) {
+  __shared__ double red[32];
+  __shared__ double res;
+  double v = 0.0;
+  for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x) v = fmax(v, __ldcg(partials + b * kPartialStride + k));
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    double s = lane < nw ? red[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s = fmax(s, __shfl_down_sync(0xffffffffu, s, o));
+    if (lane == 0) res = s;
+  }
+  __syncthreads();
+  const double out = res;
+  __syncthreads();
+  return out;
+}
+
+__device__ __forceinline__ float3 filterContact(const Contact& c, float3 v) {
+  if (c.active == 0u) return v;
+  const float3 n = xyz(c.normal);
+  return v - n * dot(n, v);
+}
+
+__device__ __forceinline__ float contactRadius(const Params& P, const Fabric& f) {
+  return __fadd_rn(P.collisionOffset, __fmul_rn(0.5f, f.thickness));
+}
+
+__device__ __forceinline__ float3 ld3(const float4* p, uint32_t i) { return xyz(p[i]); }
+
+__device__ __forceinline__ float seamTarget(const Dev& D, const Seam& s) {
+  const Garment g = D.garment[s.garment];
+  if (g.phase != 0) return 0.0f;
+  return fmaxf(0.0f, s.startGap - D.P.closingSpeed * static_cast<float>(g.assemblyTime));
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Substep setup: predict (kernels.h:34-51) and contact setup (kernels.h:55-82).
+
+__device__ inline void contactSetupOne(const Dev& D, uint32_t i, float3 xs, Contact& c) {
+  const float lastForce = c.force;
+  c.nearBody = 0u;
+  c.active = 0u;
+  c.frictionLambda = 0.0f;
+  c.force = 0.0f;
+  const Particle pa = D.particle[i];
+  if (D.field.present && pa.pinned == 0u) {
+    const float radius = contactRadius(D.P, D.fabric[pa.fabric]);
+    const float phi = fieldSample(D.fieldValues, D.field, xs);
+    if (phi < __fadd_rn(radius, D.P.contactReach)) {
+      const float3 normal = fieldGradient(D.fieldValues, D.field, xs);
+      if (!isZero(normal)) {
+        c.nearBody = 1u;
+        c.normal = f4(normal, __fsub_rn(radius, phi));
+        c.frictionLambda = lastForce;
+      }
+    }
+  }
+}
+
+__global__ void k_begin(Dev D) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    D.ctl->newtonDone = 0;
+    D.ctl->substeps += 1;
+  }
+  const float h = D.P.h;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < D.P.n; i += gridDim.x * blockDim.x) {
+    const float4 x4 = D.x[i];
+    D.xStart[i] = x4;
+    const Particle pa = D.particle[i];
+    if (pa.pinned != 0u) {
+      D.yRel[i] = make_float4(0, 0, 0, 0);
+      D.u[i] = make_float4(0, 0, 0, 0);
+    } else {
+      const float3 vel = ld3(D.v, i);
+      const float3 g = D.garment[pa.garment].phase == 1 ? mk(D.P.gravity[0], D.P.gravity[1], D.P.gravity[2]) : mk(0, 0, 0);
+      const float3 acc = g + div(ld3(D.fExt, i), pa.mass);
+      D.yRel[i] = f4(vel * h + acc * (h * h));
+      D.u[i] = f4(vel * h);
+    }
+    Contact c = D.contact[i];
+    contactSetupOne(D, i, xyz(x4), c);
+    D.contact[i] = c;
+  }
+}
+
+// Contact candidates for given positions (test entry point; same code as k_begin).
+__global__ void k_contact_candidates(Dev D, const float4* xs, Contact* out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < D.P.n; i += gridDim.x * blockDim.x) {
+    Contact c{};
+    contactSetupOne(D, i, xyz(xs[i]), c);
+    out[i] = c;
+  }
+}
+
+// Holds near particles on their plane for this Newton iteration, projecting any below it (kernels.h:85-99).
+__global__ void k_activate(Dev D) {
+  if (D.ctl->newtonDone) return;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < D.P.n; i += gridDim.x * blockDim.x) {
+    Contact c = D.contact[i];
+    if (c.nearBody == 0u) continue;
+    const float3 n = xyz(c.normal);
+    float3 ui = ld3(D.u, i);
+    const float gap = c.normal.w - dot(n, ui);
+    if (gap > -D.P.contactSnap) c.active = 1u;
+    if (c.active != 0u && gap > 0.0f) {
+      ui += n * gap;
+      D.u[i] = f4(ui);
+    }
+    D.contact[i].active = c.active;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Owner-computes assembly: one warp per block row i. Each lane evaluates one incident term (kind, id, local vertex a)
+// for vertex a only (its gradient and Hessian row), stages the N blocks in shared memory with their row-local slot,
+// and the lane owning each slot sums the staged blocks in incidence-list order, after the particle's own inertia and
+// friction term: the reference's fixed gather order (gpu_solver_core.cpp:184-224), with no atomics.
+
+struct AssembleShared {
+  float blk[kAssembleWarps][kWarp][4][9];
+  uint8_t tgt[kAssembleWarps][kWarp][4];
+  float g[kAssembleWarps][kWarp][3];
+};
+
+__device__ inline float3 relPos(const Dev& D, uint32_t v0, uint32_t vk) {
+  return (ld3(D.xStart, vk) - ld3(D.xStart, v0)) + ld3(D.u, vk);
+}
+
+__device__ inline StretchIn stretchIn(const Dev& D, const Stretch& t) {
+  const Fabric f = D.fabric[t.fabric];
+  StretchIn s;
+  s.d = t.d;
+  s.area = t.area;
+  s.k[0] = f.k[0];
+  s.k[1] = f.k[1];
+  s.k[2] = f.k[2];
+  s.limit[0] = f.limit[0];
+  s.limit[1] = f.limit[1];
+  s.limitScale = D.P.limitScale;
+  return s;
+}
+
+// Evaluates incidence entry `code` for its vertex a: gradient g, Hessian row H[0..N-1]; returns N.
+__device__ inline int evalEntry(const Dev& D, uint32_t code, float3& g, M3 H[4]) {
+  const uint32_t kind = code >> 30, term = (code >> 2) & 0x0FFFFFFFu, a = code & 3u;
+  if (kind == 0) {
+    const Stretch t = D.stretch[term];
+    float3 x[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) x[k] = relPos(D, t.v[0], t.v[k]);
+    stretchRow(stretchIn(D, t), x, static_cast<int>(a), g, H);
+    return 3;
+  }
+  if (kind == 1) {
+    const Hinge t = D.hinge[term];
+    float3 x[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) x[k] = relPos(D, t.v[0], t.v[k]);
+    hingeRow(t.K, t.rest, x, static_cast<int>(a), g, H);
+    return 4;
+  }
+  const Seam s = D.seam[term];
+  const float3 x0 = ld3(D.u, s.a);
+  const float3 x1 = relPos(D, s.a, s.b);
+  seamRow(D.P.seamStiffness, seamTarget(D, s), x0, x1, static_cast<int>(a), g, H);
+  return 2;
+}
+
+__global__ void __launch_bounds__(kAssembleWarps * kWarp) k_assemble(Dev D) {
+  if (D.ctl->newtonDone) return;
+  __shared__ AssembleShared sh;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint32_t warpsTotal = gridDim.x * kAssembleWarps;
+  for (uint32_t i = blockIdx.x * kAssembleWarps + w; i < D.P.n; i += warpsTotal) {
+    const uint32_t rs = D.rowStart[i], L = D.rowStart[i + 1] - rs;
+    const Particle pa = D.particle[i];
+    const Contact c = D.contact[i];
+    // The particle's own term: inertia 1/2 (m/h^2)|u - yRel|^2 and friction (kernels.h:104-129).
+    float3 gOwn = mk(0, 0, 0);
+    M3 hOwn;
+    zero(hOwn);
+    if (pa.pinned == 0u) {
+      const float k = pa.mass * D.P.invH2;
+      gOwn = (ld3(D.u, i) - ld3(D.yRel, i)) * k;
+      hOwn.m[0] = hOwn.m[4] = hOwn.m[8] = k;
+    }
+    if (c.frictionLambda > 0.0f)
+      frictionRow(ld3(D.u, i), xyz(c.normal), D.fabric[pa.fabric].friction * c.frictionLambda,
+                  D.P.frictionSlip * D.P.h, gOwn, hOwn);
+    // Slot accumulators: lane owns row-local slots lane and lane + 32.
+    float acc0[9], acc1[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) acc0[k] = acc1[k] = 0.0f;
+    uint32_t diagLocal = 0;
+    for (uint32_t s = 0; s < L; ++s)
+      if ((D.colIndex[rs + s] & ~kPinnedBit) == i) diagLocal = s;
+    if (diagLocal == static_cast<uint32_t>(lane))
+#pragma unroll
+      for (int k = 0; k < 9; ++k) acc0[k] = hOwn.m[k];
+    if (diagLocal == static_cast<uint32_t>(lane) + 32u)
+#pragma unroll
+      for (int k = 0; k < 9; ++k) acc1[k] = hOwn.m[k];
+    float3 gAcc = gOwn;
+    const uint32_t es = D.incStart[i], ee = D.incStart[i + 1];
+    for (uint32_t base = es; base < ee; base += kWarp) {
+      const uint32_t cnt = min(static_cast<uint32_t>(kWarp), ee - base);
+      if (static_cast<uint32_t>(lane) < cnt) {
+        const uint32_t code = D.incEntry[base + lane];
+        const uint32_t local = D.incLocal[base + lane];
+        float3 g;
+        M3 H[4];
+        const int N = evalEntry(D, code, g, H);
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          sh.tgt[w][lane][b] = b < N ? static_cast<uint8_t>((local >> (8 * b)) & 0xFFu) : 0xFFu;
+          if (b < N)
+#pragma unroll
+            for (int k = 0; k < 9; ++k) sh.blk[w][lane][b][k] = H[b].m[k];
+        }
+        sh.g[w][lane][0] = g.x;
+        sh.g[w][lane][1] = g.y;
+        sh.g[w][lane][2] = g.z;
+      }
+      __syncwarp();
+      for (uint32_t e = 0; e < cnt; ++e) {
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const uint32_t t = sh.tgt[w][e][b];
+          if (t == static_cast<uint32_t>(lane)) {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) acc0[k] += sh.blk[w][e][b][k];
+          } else if (t == static_cast<uint32_t>(lane) + 32u) {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) acc1[k] += sh.blk[w][e][b][k];
+          }
+        }
+        gAcc += mk(sh.g[w][e][0], sh.g[w][e][1], sh.g[w][e][2]);
+      }
+      __syncwarp();
+    }
+    // Blocks out (coalesced planes).
+    const uint32_t SP = D.P.slotsPadded;
+    if (static_cast<uint32_t>(lane) < L)
+#pragma unroll
+      for (int k = 0; k < 9; ++k) D.blocks[k * SP + rs + lane] = acc0[k];
+    if (static_cast<uint32_t>(lane) + 32u < L)
+#pragma unroll
+      for (int k = 0; k < 9; ++k) D.blocks[k * SP + rs + lane + 32] = acc1[k];
+    // Diagonal owner: block-Jacobi inverse (kernels.h:237-249).
+    const bool ownDiag0 = diagLocal == static_cast<uint32_t>(lane);
+    const bool ownDiag1 = diagLocal == static_cast<uint32_t>(lane) + 32u;
+    if (ownDiag0 || ownDiag1) {
+      M3 A;
+#pragma unroll
+      for (int k = 0; k < 9; ++k) A.m[k] = ownDiag0 ? acc0[k] : acc1[k];
+      M3 inv;
+      if (pa.pinned != 0u) {
+        zero(inv);
+      } else {
+        bool ok = false;
+        inv = invertSpd(A, ok);
+      }
+      D.precond[3 * i + 0] = make_float4(inv.m[0], inv.m[1], inv.m[2], 0.0f);
+      D.precond[3 * i + 1] = make_float4(inv.m[3], inv.m[4], inv.m[5], 0.0f);
+      D.precond[3 * i + 2] = make_float4(inv.m[6], inv.m[7], inv.m[8], 0.0f);
+    }
+    // Gradient (pinned rows zero) and contact release (kernels.h:204-231).
+    if (lane == 0) {
+      const float3 gi = pa.pinned != 0u ? mk(0, 0, 0) : gAcc;
+      D.grad[i] = f4(gi);
+      if (c.active != 0u && dot(gi, xyz(c.normal)) < 0.0f) D.contact[i].active = 0u;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Energy at u + alpha * step, in FP64, summed per thread over particles (inertia + friction) and terms.
+
+__device__ inline double energyPartial(const Dev& D, double alpha) {
+  double e = 0.0;
+  const uint32_t n = D.P.n, S = D.P.nStretch, H = D.P.nHinge, K = D.P.nSeam;
+  const uint32_t total = n + S + H + K;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  auto pos = [&](uint32_t v0, uint32_t vk) -> d3 {
+    const d3 rel = toD(ld3(D.xStart, vk)) - toD(ld3(D.xStart, v0));
+    return rel + (toD(ld3(D.u, vk)) + alpha * toD(ld3(D.step, vk)));
+  };
+  const double invH2 = 1.0 / (D.P.hD * D.P.hD);
+  for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += stride) {
+    if (idx < n) {
+      const uint32_t i = idx;
+      const Particle pa = D.particle[i];
+      const d3 ui = toD(ld3(D.u, i)) + alpha * toD(ld3(D.step, i));
+      if (pa.pinned == 0u) {
+        const d3 dd = ui - toD(ld3(D.yRel, i));
+        e += 0.5 * static_cast<double>(pa.mass) * invH2 * dotd(dd, dd);
+      }
+      const Contact c = D.contact[i];
+      if (c.frictionLambda > 0.0f)
+        e += frictionEnergy(ui, toD(xyz(c.normal)),
+                            static_cast<double>(D.fabric[pa.fabric].friction) * static_cast<double>(c.frictionLambda),
+                            static_cast<double>(D.P.frictionSlip) * D.P.hD);
+    } else if (idx < n + S) {
+      const Stretch t = D.stretch[idx - n];
+      d3 x[3];
+      for (int k = 0; k < 3; ++k) x[k] = pos(t.v[0], t.v[k]);
+      e += stretchEnergy(stretchIn(D, t), x);
+    } else if (idx < n + S + H) {
+      const Hinge t = D.hinge[idx - n - S];
+      d3 x[4];
+      for (int k = 0; k < 4; ++k) x[k] = pos(t.v[0], t.v[k]);
+      e += hingeEnergy(t.K, t.rest, x);
+    } else {
+      const Seam s = D.seam[idx - n - S - H];
+      e += seamEnergy(D.P.seamStiffness, seamTarget(D, s), pos(s.a, s.a), pos(s.a, s.b));
+    }
+  }
+  return e;
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Persistent solve: PCG with FP64 dot products, then the Newton line search. Every block computes the same scalars
+// from the same partials, so all blocks take the same branches; two grid barriers per CG iteration (the direction
+// update p = z + beta p is folded into the next SpMV, which rebuilds each neighbour's p from z and the previous p).
+
+// Contact-filtered block-Jacobi PCG (cpu_solver.cpp:169-213): writes step, resid; returns the iteration count, or -1
+// when a grid barrier gave up.
+__device__ inline int pcgSolve(const Dev& D) {
+  Control* ctl = D.ctl;
+  const unsigned long long lim = D.P.barrierLimitNs;
+  const uint32_t n = D.P.n;
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  __shared__ double red[kPartialStride];
+
+  // CG init (kernels.h:252-268): step = 0, resid = -grad, r = filter(resid), z = filter(M r).
+  {
+    double v[2] = {0.0, 0.0};
+    for (uint32_t i = tid; i < n; i += stride) {
+      const Contact c = D.contact[i];
+      const float3 res = -ld3(D.grad, i);
+      const float3 ri = filterContact(c, res);
+      const M3 M = {{D.precond[3 * i].x, D.precond[3 * i].y, D.precond[3 * i].z, D.precond[3 * i + 1].x,
+                     D.precond[3 * i + 1].y, D.precond[3 * i + 1].z, D.precond[3 * i + 2].x, D.precond[3 * i + 2].y,
+                     D.precond[3 * i + 2].z}};
+      const float3 zi = filterContact(c, mul(M, ri));
+      D.step[i] = make_float4(0, 0, 0, 0);
+      D.resid[i] = f4(res);
+      D.r[i] = f4(ri);
+      D.z[i] = f4(zi);
+      v[0] += static_cast<double>(ri.x) * zi.x + static_cast<double>(ri.y) * zi.y + static_cast<double>(ri.z) * zi.z;
+      v[1] += static_cast<double>(ri.x) * ri.x + static_cast<double>(ri.y) * ri.y + static_cast<double>(ri.z) * ri.z;
+    }
+    blockSum<2>(v, red);
+    if (threadIdx.x == 0) {
+      D.partials[blockIdx.x * kPartialStride + 0] = red[0];
+      D.partials[blockIdx.x * kPartialStride + 1] = red[1];
+    }
+  }
+  if (!gridBarrier(ctl, lim)) return -1;
+  double tot[2];
+  gridTotals<2>(D.partials, tot);
+  double rz = tot[0];
+  const double r0 = sqrt(tot[1]);
+  bool done = !(r0 > 0.0);
+  double beta = 0.0;
+  float4* pPrev = D.p0;
+  float4* pCur = D.p1;
+  int it = 0;
+  const int maxCg = D.P.maxCg;
+  const uint32_t SP = D.P.slotsPadded;
+  const uint32_t groupsTotal = stride / kRowLanes;
+  const uint32_t gid = tid / kRowLanes;
+  const int sub = threadIdx.x & (kRowLanes - 1);
+  const unsigned groupMask = 0xFFu << ((threadIdx.x & 31) & ~(kRowLanes - 1));
+  while (!done && it < maxCg) {
+    // SpMV with the direction update folded in: p_j = z_j + beta * pPrev_j.
+    double vpap = 0.0;
+    const float fb = static_cast<float>(beta);
+    const bool first = it == 0;
+    for (uint32_t i0 = gid * 1u; i0 < n + 0u; i0 += groupsTotal) {
+      const uint32_t i = i0;
+      const uint32_t rs = D.rowStart[i], re = D.rowStart[i + 1];
+      float3 acc = mk(0, 0, 0);
+      const bool rowPinned = D.particle[i].pinned != 0u;
+      if (!rowPinned) {
+        for (uint32_t s = rs + sub; s < re; s += kRowLanes) {
+          const uint32_t col = __ldg(D.colIndex + s);
+          if (col & kPinnedBit) continue;
+          const uint32_t j = col;
+          const float3 zj = ld3(D.z, j);
+          const float3 pj = first ? zj : zj + ld3(pPrev, j) * fb;
+          const float a0 = D.blocks[0 * SP + s], a1 = D.blocks[1 * SP + s], a2 = D.blocks[2 * SP + s];
+          const float a3 = D.blocks[3 * SP + s], a4 = D.blocks[4 * SP + s], a5 = D.blocks[5 * SP + s];
+          const float a6 = D.blocks[6 * SP + s], a7 = D.blocks[7 * SP + s], a8 = D.blocks[8 * SP + s];
+          acc.x += a0 * pj.x + a1 * pj.y + a2 * pj.z;
+          acc.y += a3 * pj.x + a4 * pj.y + a5 * pj.z;
+          acc.z += a6 * pj.x + a7 * pj.y + a8 * pj.z;
+        }
+      }
+#pragma unroll
+      for (int o = kRowLanes / 2; o > 0; o >>= 1) {
+        acc.x += __shfl_xor_sync(groupMask, acc.x, o);
+        acc.y += __shfl_xor_sync(groupMask, acc.y, o);
+        acc.z += __shfl_xor_sync(groupMask, acc.z, o);
+      }
+      if (sub == 0) {
+        const float3 zi = ld3(D.z, i);
+        const float3 pi = first ? zi : zi + ld3(pPrev, i) * fb;
+        pCur[i] = f4(pi);
+        const float3 filtered = filterContact(D.contact[i], acc);
+        D.apFull[i] = f4(acc);
+        D.ap[i] = f4(filtered);
+        vpap += static_cast<double>(pi.x) * filtered.x + static_cast<double>(pi.y) * filtered.y +
+                static_cast<double>(pi.z) * filtered.z;
+      }
+    }
+    {
+      double v[1] = {vpap};
+      blockSum<1>(v, red);
+      if (threadIdx.x == 0) D.partials[blockIdx.x * kPartialStride] = red[0];
+    }
+    if (!gridBarrier(ctl, lim)) return -1;
+    double pAp[1];
+    gridTotals<1>(D.partials, pAp);
+    if (!(pAp[0] > 0.0)) break;
+    const double alpha = rz / pAp[0];
+    const float fa = static_cast<float>(alpha);
+    ++it;
+    // Update (kernels.h:304-315) fused with the preconditioner apply (kernels.h:324-332).
+    double v[2] = {0.0, 0.0};
+    for (uint32_t i = tid; i < n; i += stride) {
+      const Contact c = D.contact[i];
+      const float3 pi = ld3(pCur, i);
+      D.step[i] = f4(ld3(D.step, i) + pi * fa);
+      const float3 ri = ld3(D.r, i) - ld3(D.ap, i) * fa;
+      D.r[i] = f4(ri);
+      D.resid[i] = f4(ld3(D.resid, i) - ld3(D.apFull, i) * fa);
+      const M3 M = {{D.precond[3 * i].x, D.precond[3 * i].y, D.precond[3 * i].z, D.precond[3 * i + 1].x,
+                     D.precond[3 * i + 1].y, D.precond[3 * i + 1].z, D.precond[3 * i + 2].x, D.precond[3 * i + 2].y,
+                     D.precond[3 * i + 2].z}};
+      const float3 zi = filterContact(c, mul(M, ri));
+      D.z[i] = f4(zi);
+      v[0] += static_cast<double>(ri.x) * ri.x + static_cast<double>(ri.y) * ri.y + static_cast<double>(ri.z) * ri.z;
+      v[1] += static_cast<double>(ri.x) * zi.x + static_cast<double>(ri.y) * zi.y + static_cast<double>(ri.z) * zi.z;
+    }
+    blockSum<2>(v, red);
+    if (threadIdx.x == 0) {
+      D.partials[blockIdx.x * kPartialStride + 0] = red[0];
+      D.partials[blockIdx.x * kPartialStride + 1] = red[1];
+    }
+    if (!gridBarrier(ctl, lim)) return -1;
+    double t2[2];
+    gridTotals<2>(D.partials, t2);
+    if (sqrt(t2[0]) <= D.P.cgTolerance * r0) break;
+    beta = t2[1] / rz;
+    rz = t2[1];
+    float4* tmp = pPrev;
+    pPrev = pCur;
+    pCur = tmp;
+  }
+  return it;
+}
+
+__global__ void __launch_bounds__(kSolveThreads) k_solve(Dev D) {
+  Control* ctl = D.ctl;
+  if (ctl->newtonDone) return;
+  const unsigned long long lim = D.P.barrierLimitNs;
+  const uint32_t n = D.P.n;
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  __shared__ double red[kPartialStride];
+  const int it = pcgSolve(D);
+  if (it < 0) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    ctl->cgIterations += it;
+    ctl->newtonIterations += 1;
+    ctl->lastCg = it;
+  }
+
+  // Contact normal force from the residual (kernels.h:391-396), Newton slope grad . step and E(0), in FP64.
+  {
+    double v[2] = {0.0, 0.0};
+    for (uint32_t i = tid; i < n; i += stride) {
+      const Contact c = D.contact[i];
+      const float3 res = ld3(D.resid, i);
+      D.contact[i].force = c.active != 0u ? fmaxf(0.0f, -dot(res, xyz(c.normal))) : 0.0f;
+      const float3 g = ld3(D.grad, i), s = ld3(D.step, i);
+      v[0] += static_cast<double>(g.x) * s.x + static_cast<double>(g.y) * s.y + static_cast<double>(g.z) * s.z;
+    }
+    v[1] = energyPartial(D, 0.0);
+    blockSum<2>(v, red);
+    if (threadIdx.x == 0) {
+      D.partials[blockIdx.x * kPartialStride + 0] = red[0];
+      D.partials[blockIdx.x * kPartialStride + 1] = red[1];
+    }
+  }
+  if (!gridBarrier(ctl, lim)) return;
+  double se[2];
+  gridTotals<2>(D.partials, se);
+  const double slope = se[0], e0 = se[1];
+  if (!(slope < 0.0)) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      ctl->newtonDone = 1;
+      ctl->lastSlope = slope;
+    }
+    return;
+  }
+  // Backtracking line search, Armijo c = 1e-4, at most 20 halvings (cpu_solver.cpp:269-274).
+  double alpha = 1.0;
+  for (int ls = 0; ls < 20; ++ls) {
+    double v[1] = {energyPartial(D, alpha)};
+    blockSum<1>(v, red);
+    if (threadIdx.x == 0) D.partials[blockIdx.x * kPartialStride] = red[0];
+    if (!gridBarrier(ctl, lim)) return;
+    double e[1];
+    gridTotals<1>(D.partials, e);
+    if (e[0] <= e0 + 1e-4 * alpha * slope) break;
+    alpha *= 0.5;
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->lineSearchHalvings += 1;
+  }
+  // Apply the step; max move; the next Newton iteration's friction uses this solve's forces (kernels.h:407-414).
+  {
+    double mv = 0.0;
+    const float fa = static_cast<float>(alpha);
+    for (uint32_t i = tid; i < n; i += stride) {
+      const float3 d = ld3(D.step, i) * fa;
+      D.u[i] = f4(ld3(D.u, i) + d);
+      mv = fmax(mv, static_cast<double>(fmaxf(fabsf(d.x), fmaxf(fabsf(d.y), fabsf(d.z)))));
+      Contact c = D.contact[i];
+      D.contact[i].frictionLambda = c.active != 0u ? c.force : 0.0f;
+    }
+    __shared__ double mred[32];
+    for (int o = 16; o > 0; o >>= 1) mv = fmax(mv, __shfl_down_sync(0xffffffffu, mv, o));
+    if ((threadIdx.x & 31) == 0) mred[threadIdx.x >> 5] = mv;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double m = 0.0;
+      for (int k = 0; k < static_cast<int>((blockDim.x + 31) >> 5); ++k) m = fmax(m, mred[k]);
+      D.partials[blockIdx.x * kPartialStride + 2] = m;
+    }
+  }
+  if (!gridBarrier(ctl, lim)) return;
+  const double maxMove = gridMax(D.partials, 2);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    ctl->lastAlpha = alpha;
+    ctl->lastSlope = slope;
+    ctl->lastE0 = e0;
+    ctl->lastMaxMove = maxMove;
+    if (maxMove < 1e-9) ctl->newtonDone = 1;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Finish: x = xStart + u, post-solve push-out below the snap tolerance, pins, damped velocity (kernels.h:419-448,
+// cpu_solver.cpp:285-313); the assembly clock of Assembling garments advances by h.
+
+__global__ void k_finish(Dev D) {
+  const float h = D.P.h;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < D.P.n; i += gridDim.x * blockDim.x) {
+    const Particle pa = D.particle[i];
+    const Fabric fab = D.fabric[pa.fabric];
+    const float3 xs = ld3(D.xStart, i);
+    float3 xn = xs + ld3(D.u, i);
+    if (pa.pinned != 0u) {
+      xn = ld3(D.pinPos, i);
+    } else if (D.field.present) {
+      const float radius = contactRadius(D.P, fab);
+      if (fieldSample(D.fieldValues, D.field, xn) < radius - D.P.contactSnap) {
+        if (isZero(fieldGradient(D.fieldValues, D.field, xn))) {
+          xn = landOnBody(D.fieldValues, D.field, radius, xs, xn);
+        } else {
+          collideBody(D.fieldValues, D.field, radius, fab.friction, xs, xn);
+        }
+      }
+    }
+    float c = D.P.dampingScale * fab.damping;
+    if (D.garment[pa.garment].phase == 0) c += D.P.assemblyExtraDamping;
+    const float3 vel = div(xn - xs, h) * fmaxf(0.0f, 1.0f - c * h);
+    D.x[i] = f4(xn);
+    D.v[i] = f4(vel);
+  }
+}
+
+__global__ void k_advance_clock(Dev D) {
+  for (uint32_t g = threadIdx.x; g < D.P.nGarments; g += blockDim.x)
+    if (D.garment[g].phase == 0) D.garment[g].assemblyTime += D.P.hD;
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Statistics (sim_model.cpp:222-241) in FP64: per-block partials, the last block to finish combines them.
+
+struct StatsOut {
+  double kineticEnergy, sumV2, maxSeamGap, maxPenetration;
+  unsigned long long moving;
+  int nonFinite;
+  int pad;
+};
+
+__global__ void k_stats(Dev D, double* part, unsigned int* done, StatsOut* out) {
+  double ke = 0, v2s = 0, gap = 0, pen = 0;
+  unsigned long long moving = 0;
+  int bad = 0;
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  for (uint32_t i = tid; i < D.P.n; i += stride) {
+    const float3 x = ld3(D.x, i), v = ld3(D.v, i);
+    if (!isfinite(x.x) || !isfinite(x.y) || !isfinite(x.z) || !isfinite(v.x) || !isfinite(v.y) || !isfinite(v.z)) bad = 1;
+    if (D.field.present) {
+      const double phi = fieldSampleD(D.fieldValues, D.field, x.x, x.y, x.z, D.fieldOrigin[0], D.fieldOrigin[1],
+                                      D.fieldOrigin[2], D.fieldCell);
+      pen = fmax(pen, -phi);
+    }
+    const Particle pa = D.particle[i];
+    if (pa.pinned != 0u) continue;
+    const double vv = static_cast<double>(v.x) * v.x + static_cast<double>(v.y) * v.y + static_cast<double>(v.z) * v.z;
+    ke += 0.5 * static_cast<double>(pa.mass) * vv;
+    v2s += vv;
+    ++moving;
+  }
+  for (uint32_t k = tid; k < D.P.nSeam; k += stride) {
+    const Seam s = D.seam[k];
+    const float3 d = ld3(D.x, s.a) - ld3(D.x, s.b);
+    gap = fmax(gap, static_cast<double>(sqrtf(d.x * d.x + d.y * d.y + d.z * d.z)));
+  }
+  double sums[2] = {ke, v2s};
+  __shared__ double r2[2];
+  blockSum<2>(sums, r2);
+  __shared__ double mx[2][32];
+  __shared__ unsigned long long mv[32];
+  __shared__ int bd[32];
+  for (int o = 16; o > 0; o >>= 1) {
+    gap = fmax(gap, __shfl_down_sync(0xffffffffu, gap, o));
+    pen = fmax(pen, __shfl_down_sync(0xffffffffu, pen, o));
+    moving += __shfl_down_sync(0xffffffffu, moving, o);
+    bad |= __shfl_down_sync(0xffffffffu, bad, o);
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  if (lane == 0) {
+    mx[0][w] = gap;
+    mx[1][w] = pen;
+    mv[w] = moving;
+    bd[w] = bad;
+  }
+  __syncthreads();
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    double g = 0, p = 0;
+    unsigned long long m = 0;
+    int b = 0;
+    for (int k = 0; k < nw; ++k) {
+      g = fmax(g, mx[0][k]);
+      p = fmax(p, mx[1][k]);
+      m += mv[k];
+      b |= bd[k];
+    }
+    double* row = part + blockIdx.x * 8;
+    row[0] = r2[0];
+    row[1] = r2[1];
+    row[2] = g;
+    row[3] = p;
+    row[4] = static_cast<double>(m);
+    row[5] = b;
+    __threadfence();
+    last = atomicAdd(done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    StatsOut s{};
+    for (unsigned int b = 0; b < gridDim.x; ++b) {
+      const double* row = part + b * 8;
+      s.kineticEnergy += __ldcg(row + 0);
+      s.sumV2 += __ldcg(row + 1);
+      s.maxSeamGap = fmax(s.maxSeamGap, __ldcg(row + 2));
+      s.maxPenetration = fmax(s.maxPenetration, __ldcg(row + 3));
+      s.moving += static_cast<unsigned long long>(__ldcg(row + 4));
+      s.nonFinite |= __ldcg(row + 5) != 0.0;
+    }
+    *out = s;
+    *done = 0;
+  }
+}
+
+// PCG on a given system (test and measurement entry point): block-Jacobi inverse of each diagonal block, then the
+// same persistent PCG as k_solve.
+__global__ void k_pcg_precondition(Dev D, const uint32_t* __restrict__ diag) {
+  const uint32_t SP = D.P.slotsPadded;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < D.P.n; i += gridDim.x * blockDim.x) {
+    M3 A;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) A.m[k] = D.blocks[k * SP + diag[i]];
+    M3 inv;
+    if (D.particle[i].pinned != 0u) {
+      zero(inv);
+    } else {
+      bool ok = false;
+      inv = invertSpd(A, ok);
+    }
+    D.precond[3 * i + 0] = make_float4(inv.m[0], inv.m[1], inv.m[2], 0.0f);
+    D.precond[3 * i + 1] = make_float4(inv.m[3], inv.m[4], inv.m[5], 0.0f);
+    D.precond[3 * i + 2] = make_float4(inv.m[6], inv.m[7], inv.m[8], 0.0f);
+  }
+}
+
+__global__ void __launch_bounds__(kSolveThreads) k_pcg_only(Dev D) {
+  const int it = pcgSolve(D);
+  if (it >= 0 && blockIdx.x == 0 && threadIdx.x == 0) D.ctl->lastCg = it;
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Standalone block-CSR SpMV (8 lanes per row), y = A x over unpinned rows and columns.
+
+__global__ void k_spmv(uint32_t n, const uint32_t* __restrict__ rowStart, const uint32_t* __restrict__ colIndex,
+                       const float* __restrict__ blocks, uint32_t SP, const uint8_t* __restrict__ pinned,
+                       const float4* __restrict__ x, float4* __restrict__ y) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  const uint32_t gid = tid / kRowLanes, groups = stride / kRowLanes;
+  const int sub = threadIdx.x & (kRowLanes - 1);
+  const unsigned groupMask = 0xFFu << ((threadIdx.x & 31) & ~(kRowLanes - 1));
+  const uint32_t rounds = (n + groups - 1) / groups;
+  for (uint32_t r = 0; r < rounds; ++r) {
+    const uint32_t i = gid + r * groups;
+    float3 acc = mk(0, 0, 0);
+    if (i < n && !pinned[i]) {
+      const uint32_t rs = rowStart[i], re = rowStart[i + 1];
+      for (uint32_t s = rs + sub; s < re; s += kRowLanes) {
+        const uint32_t j = colIndex[s];
+        if (pinned[j]) continue;
+        const float3 pj = xyz(x[j]);
+        acc.x += blocks[0 * SP + s] * pj.x + blocks[1 * SP + s] * pj.y + blocks[2 * SP + s] * pj.z;
+        acc.y += blocks[3 * SP + s] * pj.x + blocks[4 * SP + s] * pj.y + blocks[5 * SP + s] * pj.z;
+        acc.z += blocks[6 * SP + s] * pj.x + blocks[7 * SP + s] * pj.y + blocks[8 * SP + s] * pj.z;
+      }
+    }
+#pragma unroll
+    for (int o = kRowLanes / 2; o > 0; o >>= 1) {
+      acc.x += __shfl_xor_sync(groupMask, acc.x, o);
+      acc.y += __shfl_xor_sync(groupMask, acc.y, o);
+      acc.z += __shfl_xor_sync(groupMask, acc.z, o);
+    }
+    if (sub == 0 && i < n) y[i] = f4(acc);
+  }
+}
+
+// A barrier that waits for one more block than the grid has: it can only end by its time limit. Used by the test of
+// the bounded wait; returns the error status in *out.
+__global__ void k_barrier_probe(Control* ctl, unsigned long long limitNs, int* out) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int* gen = &ctl->barrierGeneration;
+    const unsigned int g0 = *gen;
+    atomicAdd(&ctl->barrierCount, 1u);
+    const unsigned long long start = globalTimerNs();
+    ok = 1;
+    while (*gen == g0) {  // nobody releases: gridDim.x + 1 arrivals never happen
+      if (globalTimerNs() - start > limitNs) {
+        atomicExch(&ctl->error, 1);
+        ok = 0;
+        break;
+      }
+      __nanosleep(256);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && blockIdx.x == 0) *out = ok ? 0 : ctl->error;
+}
+
+}  // namespace dcu

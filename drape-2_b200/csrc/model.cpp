@@ -1,0 +1,361 @@
+// Host-side scene model of the CUDA solver (see model.hpp).
+#include "model.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <stdexcept>
+
+namespace drape_b200 {
+
+namespace {
+
+double norm3(double x, double y, double z) { return std::sqrt(x * x + y * y + z * z); }
+
+// FabricPhysical bending coefficients and edge stiffness (bending.cpp:7-18).
+void bendCoefficients(double bendWarp, double bendWeft, double& p, double& q) {
+  const double floor = 0.05 * std::min(bendWarp, bendWeft);
+  p = std::max((3.0 * bendWarp - bendWeft) / 2.0, floor);
+  q = std::max(bendWeft, floor);
+}
+
+double edgeStiffness(double p, double q, const double dir[2], const double grain[2]) {
+  const double dn = std::sqrt(dir[0] * dir[0] + dir[1] * dir[1]);
+  const double gn = std::sqrt(grain[0] * grain[0] + grain[1] * grain[1]);
+  const double d0 = dir[0] / dn, d1 = dir[1] / dn, u0 = grain[0] / gn, u1 = grain[1] / gn;
+  const double c = d0 * u0 + d1 * u1;
+  const double s = d0 * u1 - d1 * u0;
+  return p * s * s + q * c * c;
+}
+
+inline uint64_t edgeKey(uint32_t a, uint32_t b) {
+  const uint32_t lo = std::min(a, b), hi = std::max(a, b);
+  return (static_cast<uint64_t>(lo) << 32) | hi;
+}
+
+}  // namespace
+
+std::size_t Model::garmentIndex(const std::string& id) const {
+  for (std::size_t i = 0; i < garments.size(); ++i)
+    if (garments[i].id == id) return i;
+  throw std::out_of_range("unknown garment '" + id + "'");
+}
+
+double Model::hingeStiffness(std::size_t hgi) const {
+  double B = 0;
+  for (const auto& side : hingeSides[hgi]) {
+    const auto& f = fabrics[side.fabric];
+    double p, q;
+    bendCoefficients(f.bend_warp, f.bend_weft, p, q);
+    B += 0.5 * edgeStiffness(p, q, side.edgeDir, side.grain);
+  }
+  return B * hingeGeom[hgi];
+}
+
+void Model::updateMass(uint32_t i) { mass[i] = std::max(vertexArea[i] * fabrics[pFabric[i]].weight, 1e-12); }
+
+uint32_t Model::slot(uint32_t row, uint32_t col) const {
+  const auto begin = colIndex.begin() + rowStart[row];
+  const auto end = colIndex.begin() + rowStart[row + 1];
+  return static_cast<uint32_t>(std::lower_bound(begin, end, col) - colIndex.begin());
+}
+
+Model Model::build(const drape_scene_desc& scene) {
+  Model next;
+  next.settings = scene.settings;
+  if (scene.body) {
+    next.hasBody = true;
+    next.field = *scene.body;
+    const long long count = static_cast<long long>(std::max(0, scene.body->dims[0])) *
+                            std::max(0, scene.body->dims[1]) * std::max(0, scene.body->dims[2]);
+    if (scene.body->values && count > 0) {
+      if (scene.body->dims[0] < 2 || scene.body->dims[1] < 2 || scene.body->dims[2] < 2)
+        throw std::invalid_argument("collision field needs at least 2 samples per axis");
+      next.fieldValues.assign(scene.body->values, scene.body->values + count);
+    }
+    next.field.values = nullptr;
+  }
+  for (uint32_t gi0 = 0; gi0 < scene.garment_count; ++gi0) {
+    const drape_garment_desc& sg = scene.garments[gi0];
+    const std::string id = sg.id ? sg.id : "";
+    if (sg.vertex_count > 0 && (!sg.initial_positions || !sg.rest || !sg.vertex_area || !sg.vertex_piece))
+      throw std::invalid_argument("garment '" + id + "': one initial position per mesh vertex required");
+    if (sg.piece_count > 0 && !sg.piece_fabric)
+      throw std::invalid_argument("garment '" + id + "': one fabric per pattern piece required");
+    Garment g;
+    g.id = id;
+    g.offset = static_cast<uint32_t>(next.x.size());
+    g.count = sg.vertex_count;
+    g.fabricOffset = static_cast<uint32_t>(next.fabrics.size());
+    g.pieceCount = sg.piece_count;
+    const auto gi = static_cast<uint32_t>(next.garments.size());
+    const uint32_t off = g.offset;
+    next.fabrics.insert(next.fabrics.end(), sg.piece_fabric, sg.piece_fabric + sg.piece_count);
+    for (uint32_t v = 0; v < sg.vertex_count; ++v) {
+      if (sg.vertex_piece[v] >= sg.piece_count)
+        throw std::invalid_argument("garment '" + id + "': vertex piece out of range");
+      next.x.push_back({static_cast<float>(sg.initial_positions[3 * v]), static_cast<float>(sg.initial_positions[3 * v + 1]),
+                        static_cast<float>(sg.initial_positions[3 * v + 2])});
+      next.vertexArea.push_back(sg.vertex_area[v]);
+      next.pFabric.push_back(g.fabricOffset + sg.vertex_piece[v]);
+      next.pGarment.push_back(gi);
+    }
+    const uint32_t* T = sg.triangles;
+    for (uint32_t t = 0; t < sg.triangle_count; ++t)
+      for (int k = 0; k < 3; ++k)
+        if (T[3 * t + k] >= sg.vertex_count) throw std::invalid_argument("garment '" + id + "': triangle vertex out of range");
+    auto rest = [&](uint32_t v, int c) { return sg.rest[2 * v + c]; };
+    auto triArea = [&](uint32_t t) {
+      const uint32_t a = T[3 * t], b = T[3 * t + 1], c = T[3 * t + 2];
+      const double e0 = rest(b, 0) - rest(a, 0), e1 = rest(b, 1) - rest(a, 1);
+      const double f0 = rest(c, 0) - rest(a, 0), f1 = rest(c, 1) - rest(a, 1);
+      return 0.5 * std::abs(e0 * f1 - e1 * f0);
+    };
+    // Stretch terms: rest shape in the piece's grain frame, dmInv = Dm^-1, area = |det Dm| / 2 (sim_model.cpp:107-123).
+    for (uint32_t t = 0; t < sg.triangle_count; ++t) {
+      const uint32_t piece = sg.triangle_piece[t];
+      const double u0 = sg.piece_grain[2 * piece], u1 = sg.piece_grain[2 * piece + 1];
+      double r[3][2];
+      for (int k = 0; k < 3; ++k) {
+        const uint32_t v = T[3 * t + k];
+        r[k][0] = rest(v, 0) * u0 + rest(v, 1) * u1;
+        r[k][1] = rest(v, 0) * -u1 + rest(v, 1) * u0;
+      }
+      const double a = r[1][0] - r[0][0], b = r[2][0] - r[0][0], c = r[1][1] - r[0][1], d = r[2][1] - r[0][1];
+      const double det = a * d - c * b;
+      const double invdet = 1.0 / det;  // adjugate times 1 / det (the operation order of Eigen's 2x2 inverse)
+      Stretch st;
+      for (int k = 0; k < 3; ++k) st.v[k] = off + T[3 * t + k];
+      st.dmInv[0][0] = d * invdet;
+      st.dmInv[0][1] = -b * invdet;
+      st.dmInv[1][0] = -c * invdet;
+      st.dmInv[1][1] = a * invdet;
+      st.area = 0.5 * std::abs(det);
+      st.fabric = g.fabricOffset + piece;
+      next.stretch.push_back(st);
+    }
+    // Edge occurrences in insertion order (triangle t, then k = 0, 1, 2), stably sorted by (min, max): the same
+    // sequence a std::map<pair<min,max>, vector<tri>> iterates.
+    std::vector<std::pair<uint64_t, uint32_t>> occ;
+    occ.reserve(3 * sg.triangle_count);
+    for (uint32_t t = 0; t < sg.triangle_count; ++t)
+      for (int k = 0; k < 3; ++k) occ.push_back({edgeKey(T[3 * t + k], T[3 * t + (k + 1) % 3]), t});
+    std::stable_sort(occ.begin(), occ.end(),
+                     [](const std::pair<uint64_t, uint32_t>& p, const std::pair<uint64_t, uint32_t>& q) {
+                       return p.first < q.first;
+                     });
+    auto opposite = [&](uint32_t t, uint32_t e0, uint32_t e1) {
+      for (int k = 0; k < 3; ++k) {
+        const uint32_t v = T[3 * t + k];
+        if (v != e0 && v != e1) return v;
+      }
+      return e0;
+    };
+    for (std::size_t i = 0; i < occ.size();) {
+      std::size_t j = i;
+      while (j < occ.size() && occ[j].first == occ[i].first) ++j;
+      if (j - i == 2 && sg.triangle_piece[occ[i].second] == sg.triangle_piece[occ[i + 1].second]) {
+        const uint32_t e0 = static_cast<uint32_t>(occ[i].first >> 32), e1 = static_cast<uint32_t>(occ[i].first);
+        const uint32_t t0 = occ[i].second, t1 = occ[i + 1].second;
+        const uint32_t piece = sg.triangle_piece[t0];
+        Hinge hg;
+        hg.v = {off + opposite(t0, e0, e1), off + opposite(t1, e0, e1), off + e0, off + e1};
+        next.hinges.push_back(hg);
+        HingeSide side;
+        side.fabric = g.fabricOffset + piece;
+        side.edgeDir[0] = rest(e1, 0) - rest(e0, 0);
+        side.edgeDir[1] = rest(e1, 1) - rest(e0, 1);
+        side.grain[0] = sg.piece_grain[2 * piece];
+        side.grain[1] = sg.piece_grain[2 * piece + 1];
+        next.hingeSides.push_back({side, side});
+        next.hingeGeom.push_back((side.edgeDir[0] * side.edgeDir[0] + side.edgeDir[1] * side.edgeDir[1]) /
+                                 (triArea(t0) + triArea(t1)));
+      }
+      i = j;
+    }
+    // The triangle of a boundary edge (an edge with exactly one triangle), or -1.
+    auto triangleWithEdge = [&](uint32_t a, uint32_t b) -> int64_t {
+      const uint64_t key = edgeKey(a, b);
+      auto lo = std::lower_bound(occ.begin(), occ.end(), key,
+                                 [](const std::pair<uint64_t, uint32_t>& p, uint64_t k) { return p.first < k; });
+      if (lo == occ.end() || lo->first != key) return -1;
+      if (lo + 1 != occ.end() && (lo + 1)->first == key) return -1;
+      return lo->second;
+    };
+    const uint32_t* SP = sg.seam_pairs;
+    for (uint32_t k = 0; k < sg.seam_pair_count; ++k) {
+      const uint32_t a = SP[4 * k], b = SP[4 * k + 1], seam = SP[4 * k + 2];
+      if (a >= sg.vertex_count || b >= sg.vertex_count)
+        throw std::invalid_argument("garment '" + id + "': seam pair vertex out of range");
+      Seam spring;
+      spring.a = off + a;
+      spring.b = off + b;
+      spring.garment = gi;
+      const double* pa = sg.initial_positions + 3 * a;
+      const double* pb = sg.initial_positions + 3 * b;
+      spring.startGap = static_cast<float>(norm3(pa[0] - pb[0], pa[1] - pb[1], pa[2] - pb[2]));
+      next.seams.push_back(spring);
+      if (k + 1 >= sg.seam_pair_count || SP[4 * (k + 1) + 2] != seam) continue;
+      const uint32_t na = SP[4 * (k + 1)], nb = SP[4 * (k + 1) + 1];
+      const int64_t tA = triangleWithEdge(a, na), tB = triangleWithEdge(b, nb);
+      if (tA < 0 || tB < 0) continue;
+      const auto ta = static_cast<uint32_t>(tA), tb = static_cast<uint32_t>(tB);
+      const uint32_t pieceA = sg.triangle_piece[ta], pieceB = sg.triangle_piece[tb];
+      Hinge hg;
+      hg.v = {off + opposite(ta, a, na), off + opposite(tb, b, nb), off + a, off + na};
+      next.hinges.push_back(hg);
+      HingeSide sa, sb;
+      sa.fabric = g.fabricOffset + pieceA;
+      sa.edgeDir[0] = rest(na, 0) - rest(a, 0);
+      sa.edgeDir[1] = rest(na, 1) - rest(a, 1);
+      sa.grain[0] = sg.piece_grain[2 * pieceA];
+      sa.grain[1] = sg.piece_grain[2 * pieceA + 1];
+      sb.fabric = g.fabricOffset + pieceB;
+      sb.edgeDir[0] = rest(nb, 0) - rest(b, 0);
+      sb.edgeDir[1] = rest(nb, 1) - rest(b, 1);
+      sb.grain[0] = sg.piece_grain[2 * pieceB];
+      sb.grain[1] = sg.piece_grain[2 * pieceB + 1];
+      next.hingeSides.push_back({sa, sb});
+      next.hingeGeom.push_back((sa.edgeDir[0] * sa.edgeDir[0] + sa.edgeDir[1] * sa.edgeDir[1]) / (triArea(ta) + triArea(tb)));
+    }
+    next.garments.push_back(g);
+  }
+  const std::size_t n = next.x.size();
+  next.v.assign(n, Vec3f{});
+  next.fExt.assign(n, Vec3d{});
+  next.pinned.assign(n, 0);
+  next.mass.assign(n, 0.0);
+  for (uint32_t k = 0; k < scene.pin_count; ++k) {
+    const uint32_t p = scene.pin_particles[k];
+    if (p >= n) throw std::out_of_range("pin particle out of range");
+    const Vec3f pos{static_cast<float>(scene.pin_positions[3 * k]), static_cast<float>(scene.pin_positions[3 * k + 1]),
+                    static_cast<float>(scene.pin_positions[3 * k + 2])};
+    next.pinned[p] = 1;
+    next.pins.push_back({p, pos});
+    next.x[p] = pos;
+  }
+  for (uint32_t k = 0; k < scene.force_count; ++k) {
+    const uint32_t p = scene.force_particles[k];
+    if (p >= n) throw std::out_of_range("force particle out of range");
+    next.fExt[p].x += scene.forces[3 * k];
+    next.fExt[p].y += scene.forces[3 * k + 1];
+    next.fExt[p].z += scene.forces[3 * k + 2];
+  }
+  for (uint32_t i = 0; i < n; ++i) next.updateMass(i);
+  for (std::size_t h = 0; h < next.hinges.size(); ++h) next.hinges[h].K = next.hingeStiffness(h);
+  next.buildStructure();
+  next.buildIncidence();
+  return next;
+}
+
+void Model::buildStructure() {
+  const std::size_t n = x.size();
+  // Every coupled (row, col) pair as one 64-bit key; sorting and deduplicating gives the CSR rows directly.
+  std::vector<uint64_t> keys;
+  keys.reserve(n + 9 * stretch.size() + 16 * hinges.size() + 4 * seams.size());
+  for (uint32_t i = 0; i < n; ++i) keys.push_back((static_cast<uint64_t>(i) << 32) | i);
+  auto couple = [&](const uint32_t* vs, int m) {
+    for (int a = 0; a < m; ++a)
+      for (int b = 0; b < m; ++b) keys.push_back((static_cast<uint64_t>(vs[a]) << 32) | vs[b]);
+  };
+  for (const auto& t : stretch) couple(t.v.data(), 3);
+  for (const auto& h : hinges) couple(h.v.data(), 4);
+  for (const auto& s : seams) {
+    const uint32_t ab[2] = {s.a, s.b};
+    couple(ab, 2);
+  }
+  std::sort(keys.begin(), keys.end());
+  keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
+  rowStart.assign(n + 1, 0);
+  colIndex.resize(keys.size());
+  for (std::size_t k = 0; k < keys.size(); ++k) {
+    colIndex[k] = static_cast<uint32_t>(keys[k]);
+    ++rowStart[(keys[k] >> 32) + 1];
+  }
+  for (std::size_t i = 0; i < n; ++i) rowStart[i + 1] += rowStart[i];
+  diagSlot.resize(n);
+  for (uint32_t i = 0; i < n; ++i) diagSlot[i] = slot(i, i);
+  auto slotsFor = [&](const uint32_t* vs, int m, uint32_t* out) {
+    for (int a = 0; a < m; ++a)
+      for (int b = 0; b < m; ++b) out[a * m + b] = slot(vs[a], vs[b]);
+  };
+  stretchSlots.resize(stretch.size());
+  for (std::size_t k = 0; k < stretch.size(); ++k) slotsFor(stretch[k].v.data(), 3, stretchSlots[k].data());
+  hingeSlots.resize(hinges.size());
+  for (std::size_t k = 0; k < hinges.size(); ++k) slotsFor(hinges[k].v.data(), 4, hingeSlots[k].data());
+  seamSlots.resize(seams.size());
+  for (std::size_t k = 0; k < seams.size(); ++k) {
+    const uint32_t ab[2] = {seams[k].a, seams[k].b};
+    slotsFor(ab, 2, seamSlots[k].data());
+  }
+  contactForce.assign(n, 0.0);
+  maxRowSlots = 0;
+  for (std::size_t i = 0; i < n; ++i) maxRowSlots = std::max(maxRowSlots, rowStart[i + 1] - rowStart[i]);
+}
+
+void Model::buildIncidence() {
+  const std::size_t n = x.size();
+  incStart.assign(n + 1, 0);
+  for (const auto& t : stretch)
+    for (auto v : t.v) ++incStart[v + 1];
+  for (const auto& h : hinges)
+    for (auto v : h.v) ++incStart[v + 1];
+  for (const auto& s : seams) {
+    ++incStart[s.a + 1];
+    ++incStart[s.b + 1];
+  }
+  for (std::size_t i = 0; i < n; ++i) incStart[i + 1] += incStart[i];
+  incEntry.assign(incStart[n], 0);
+  incLocal.assign(incStart[n], 0);
+  std::vector<uint32_t> fill(incStart.begin(), incStart.end() - 1);
+  auto add = [&](uint32_t kind, uint32_t term, uint32_t a, uint32_t particle, const uint32_t* slots, int N) {
+    const uint32_t e = fill[particle]++;
+    incEntry[e] = (kind << 30) | (term << 2) | a;
+    uint32_t packed = 0;
+    for (int b = 0; b < N; ++b) packed |= (slots[a * N + b] - rowStart[particle]) << (8 * b);
+    incLocal[e] = packed;
+  };
+  if (stretch.size() >= (1u << 28) || hinges.size() >= (1u << 28) || seams.size() >= (1u << 28))
+    throw std::invalid_argument("too many terms for the incidence encoding");
+  if (maxRowSlots > kMaxRowSlots)
+    throw std::invalid_argument("a particle couples to " + std::to_string(maxRowSlots) + " particles; the CUDA solver supports " +
+                                std::to_string(kMaxRowSlots));
+  for (uint32_t t = 0; t < stretch.size(); ++t)
+    for (uint32_t a = 0; a < 3; ++a) add(0, t, a, stretch[t].v[a], stretchSlots[t].data(), 3);
+  for (uint32_t h = 0; h < hinges.size(); ++h)
+    for (uint32_t a = 0; a < 4; ++a) add(1, h, a, hinges[h].v[a], hingeSlots[h].data(), 4);
+  for (uint32_t k = 0; k < seams.size(); ++k) {
+    const uint32_t ab[2] = {seams[k].a, seams[k].b};
+    for (uint32_t a = 0; a < 2; ++a) add(2, k, a, ab[a], seamSlots[k].data(), 2);
+  }
+  maxRowEntries = 0;
+  for (std::size_t i = 0; i < n; ++i) maxRowEntries = std::max(maxRowEntries, incStart[i + 1] - incStart[i]);
+}
+
+void Model::updateFabric(const std::string& id, const drape_fabric* pieceFabric, uint32_t count) {
+  auto& g = garments[garmentIndex(id)];
+  if (count != g.pieceCount) throw std::invalid_argument("one fabric per pattern piece required");
+  std::copy(pieceFabric, pieceFabric + count, fabrics.begin() + g.fabricOffset);
+  for (uint32_t i = g.offset; i < g.offset + g.count; ++i) updateMass(i);
+  for (std::size_t h = 0; h < hinges.size(); ++h) {
+    const auto fi = hingeSides[h][0].fabric;
+    if (fi >= g.fabricOffset && fi < g.fabricOffset + g.pieceCount) hinges[h].K = hingeStiffness(h);
+  }
+}
+
+void Model::setPhase(const std::string& id, int phase) {
+  const auto gi = garmentIndex(id);
+  auto& g = garments[gi];
+  g.phase = phase;
+  if (phase == DRAPE_PHASE_ASSEMBLING) {
+    g.assemblyTime = 0;
+    for (auto& sp : seams) {
+      if (sp.garment != gi) continue;
+      // |x_a - x_b| on float positions, as the reference's Vec3f norm (sim_model.cpp:302).
+      const float dx = x[sp.a].x - x[sp.b].x, dy = x[sp.a].y - x[sp.b].y, dz = x[sp.a].z - x[sp.b].z;
+      sp.startGap = std::sqrt(dx * dx + dy * dy + dz * dz);
+    }
+  }
+}
+
+}  // namespace drape_b200

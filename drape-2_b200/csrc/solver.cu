@@ -1,0 +1,1225 @@
+// Host driver of the CUDA cloth solver and its C ABI (include/drape_cuda.h).
+//
+// The driver plays the role of the reference's GpuSolverCore (libs/sim/src/gpu/gpu_solver_core.cpp:41-407): it owns
+// the model (model.hpp), the device buffers and one CUDA stream, and issues per substep
+//   k_begin, then per Newton iteration k_activate, k_assemble, k_solve (cooperative), then k_finish, k_advance_clock.
+// Unlike the reference driver there is no host round trip inside a substep: energies, slope, line search and the
+// Newton stop test are decided on the device. The host synchronises once per step() to read the work counters and the
+// error status (the bounded grid barrier's timeout).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/drape_cuda.h"
+#include "kernels.cuh"
+#include "model.hpp"
+
+using drape_b200::Model;
+
+namespace {
+
+void check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw std::runtime_error(std::string("cuda: ") + what + ": " + cudaGetErrorString(e));
+}
+#define CK(x) check((x), #x)
+
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void alloc(size_t count) {
+    release();
+    n = count;
+    CK(cudaMalloc(&p, sizeof(T) * std::max<size_t>(count, 1)));
+    CK(cudaMemset(p, 0, sizeof(T) * std::max<size_t>(count, 1)));
+  }
+  void upload(const T* src, size_t count, cudaStream_t s) {
+    if (count > n) alloc(count);
+    if (count) CK(cudaMemcpyAsync(p, src, sizeof(T) * count, cudaMemcpyHostToDevice, s));
+  }
+  void upload(const std::vector<T>& v, cudaStream_t s) {
+    if (v.size() > n || !p) alloc(v.size());
+    if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s));
+  }
+};
+
+template <class T>
+struct HostPinned {
+  T* p = nullptr;
+  HostPinned() = default;
+  HostPinned(const HostPinned&) = delete;
+  HostPinned& operator=(const HostPinned&) = delete;
+  ~HostPinned() {
+    if (p) cudaFreeHost(p);
+  }
+  void alloc() {
+    if (!p) {
+      CK(cudaMallocHost(&p, sizeof(T)));
+      std::memset(static_cast<void*>(p), 0, sizeof(T));
+    }
+  }
+};
+
+float4 f4(drape_b200::Vec3f v) { return make_float4(v.x, v.y, v.z, 0.0f); }
+
+thread_local std::string g_lastError;
+
+}  // namespace
+
+struct drape_solver {
+  int device = 0;
+  int numSMs = 0;
+  cudaStream_t stream = nullptr;
+  std::string error;
+  Model m;
+  bool built = false;
+  int solveGrid = 0, pointGrid = 0, assembleGrid = 0, statsGrid = 0;
+  unsigned long long barrierLimitNs = 2000000000ull;  // 2 s
+  int failAfter = -1;
+
+  DBuf<dcu::Particle> particle;
+  DBuf<dcu::Fabric> fabric;
+  DBuf<dcu::Garment> garment;
+  DBuf<dcu::Stretch> stretch;
+  DBuf<dcu::Hinge> hinge;
+  DBuf<dcu::Seam> seam;
+  DBuf<uint32_t> rowStart, colIndex, incStart, incEntry, incLocal;
+  DBuf<float> fieldValues, blocks;
+  DBuf<float4> x, v, xStart, yRel, u, grad, step, r, z, p0, p1, ap, apFull, resid, fExt, pinPos, precond;
+  DBuf<dcu::Contact> contact;
+  DBuf<double> partials, statsPartials;
+  DBuf<dcu::Control> ctl;
+  DBuf<dcu::StatsOut> statsOut;
+  DBuf<unsigned int> statsDone;
+  HostPinned<dcu::Control> hCtl;
+  HostPinned<dcu::StatsOut> hStats;
+  dcu::Dev dev{};
+
+  // ---- setup ----
+
+  explicit drape_solver(int dev_) : device(dev_) {
+    int count = 0;
+    CK(cudaGetDeviceCount(&count));
+    if (device < 0 || device >= count) throw std::runtime_error("cuda: no device " + std::to_string(device));
+    CK(cudaSetDevice(device));
+    cudaDeviceProp prop{};
+    CK(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) throw std::runtime_error(std::string("cuda: device ") + prop.name + " is not sm_100");
+    if (!prop.cooperativeLaunch) throw std::runtime_error("cuda: device does not support cooperative launch");
+    numSMs = prop.multiProcessorCount;
+    CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    int perSM = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, dcu::k_solve, dcu::kSolveThreads, 0));
+    if (perSM < 1) throw std::runtime_error("cuda: the solve kernel does not fit on an SM");
+    solveGrid = numSMs * std::min(perSM, 2);
+    pointGrid = numSMs * 8;
+    statsGrid = numSMs * 2;
+    hCtl.alloc();
+    hStats.alloc();
+    ctl.alloc(1);
+    partials.alloc(static_cast<size_t>(solveGrid) * dcu::kPartialStride);
+    statsPartials.alloc(static_cast<size_t>(statsGrid) * 8);
+    statsOut.alloc(1);
+    statsDone.alloc(1);
+  }
+
+  ~drape_solver() {
+    if (stream) {
+      cudaSetDevice(device);
+      cudaStreamSynchronize(stream);
+      cudaStreamDestroy(stream);
+    }
+  }
+
+  void use() const { CK(cudaSetDevice(device)); }
+
+  std::vector<dcu::Particle> particleData() const {
+    std::vector<dcu::Particle> out(m.x.size());
+    for (size_t i = 0; i < out.size(); ++i)
+      out[i] = {static_cast<float>(m.mass[i]), m.pFabric[i], m.pGarment[i], m.pinned[i] ? 1u : 0u};
+    return out;
+  }
+  std::vector<dcu::Fabric> fabricData() const {
+    std::vector<dcu::Fabric> out;
+    for (const auto& f : m.fabrics) {
+      dcu::Fabric d{};
+      d.k[0] = static_cast<float>(f.stretch_warp);
+      d.k[1] = static_cast<float>(f.stretch_weft);
+      d.k[2] = static_cast<float>(f.stretch_bias);
+      d.limit[0] = static_cast<float>(f.strain_limit_warp);
+      d.limit[1] = static_cast<float>(f.strain_limit_weft);
+      d.thickness = static_cast<float>(f.thickness);
+      d.friction = static_cast<float>(f.friction);
+      d.damping = static_cast<float>(f.damping);
+      out.push_back(d);
+    }
+    if (out.empty()) out.push_back(dcu::Fabric{});
+    return out;
+  }
+  std::vector<dcu::Garment> garmentData() const {
+    std::vector<dcu::Garment> out;
+    for (const auto& g : m.garments) out.push_back({g.phase, 0, g.assemblyTime});
+    if (out.empty()) out.push_back(dcu::Garment{});
+    return out;
+  }
+  std::vector<dcu::Hinge> hingeData() const {
+    std::vector<dcu::Hinge> out;
+    for (const auto& h : m.hinges)
+      out.push_back({{h.v[0], h.v[1], h.v[2], h.v[3]}, static_cast<float>(h.K), static_cast<float>(h.restAngle), {0, 0}});
+    return out;
+  }
+  std::vector<dcu::Seam> seamData() const {
+    std::vector<dcu::Seam> out;
+    for (const auto& s : m.seams) out.push_back({s.a, s.b, s.garment, s.startGap});
+    return out;
+  }
+
+  void build(const drape_scene_desc& scene) {
+    use();
+    Model next = Model::build(scene);
+    built = false;
+    m = std::move(next);
+    const uint32_t n = static_cast<uint32_t>(m.x.size());
+    const uint32_t B = static_cast<uint32_t>(m.colIndex.size());
+    const uint32_t SP = (B + 31u) & ~31u;
+    cudaStream_t s = stream;
+    particle.upload(particleData(), s);
+    fabric.upload(fabricData(), s);
+    garment.upload(garmentData(), s);
+    {
+      std::vector<dcu::Stretch> st;
+      for (const auto& t : m.stretch) {
+        dcu::Stretch d{};
+        for (int k = 0; k < 3; ++k) d.v[k] = t.v[k];
+        d.fabric = t.fabric;
+        d.d = make_float4(static_cast<float>(t.dmInv[0][0]), static_cast<float>(t.dmInv[1][0]),
+                          static_cast<float>(t.dmInv[0][1]), static_cast<float>(t.dmInv[1][1]));
+        d.area = static_cast<float>(t.area);
+        st.push_back(d);
+      }
+      stretch.upload(st, s);
+    }
+    hinge.upload(hingeData(), s);
+    seam.upload(seamData(), s);
+    rowStart.upload(m.rowStart, s);
+    {
+      std::vector<uint32_t> cols(m.colIndex);
+      for (auto& c : cols)
+        if (m.pinned[c]) c |= dcu::kPinnedBit;
+      colIndex.upload(cols, s);
+    }
+    incStart.upload(m.incStart, s);
+    incEntry.upload(m.incEntry, s);
+    incLocal.upload(m.incLocal, s);
+    if (!m.fieldValues.empty()) {
+      fieldValues.upload(m.fieldValues, s);
+    } else {
+      fieldValues.alloc(1);
+    }
+    blocks.alloc(static_cast<size_t>(SP) * 9);
+    for (DBuf<float4>* b : {&x, &v, &xStart, &yRel, &u, &grad, &step, &r, &z, &p0, &p1, &ap, &apFull, &resid, &fExt, &pinPos})
+      b->alloc(n);
+    precond.alloc(static_cast<size_t>(n) * 3);
+    contact.alloc(n);
+    {
+      std::vector<float4> xs(n), vs(n), fe(n), pp(n);
+      for (uint32_t i = 0; i < n; ++i) {
+        xs[i] = f4(m.x[i]);
+        vs[i] = f4(m.v[i]);
+        fe[i] = make_float4(static_cast<float>(m.fExt[i].x), static_cast<float>(m.fExt[i].y),
+                            static_cast<float>(m.fExt[i].z), 0.0f);
+      }
+      for (const auto& [i, pos] : m.pins) pp[i] = f4(pos);
+      x.upload(xs, s);
+      v.upload(vs, s);
+      fExt.upload(fe, s);
+      pinPos.upload(pp, s);
+    }
+    dcu::Control c0{};
+    CK(cudaMemcpyAsync(ctl.p, &c0, sizeof(c0), cudaMemcpyHostToDevice, s));
+    // Launch view.
+    dcu::Dev d{};
+    auto& P = d.P;
+    P.gravity[0] = static_cast<float>(m.settings.gravity[0]);
+    P.gravity[1] = static_cast<float>(m.settings.gravity[1]);
+    P.gravity[2] = static_cast<float>(m.settings.gravity[2]);
+    P.limitScale = static_cast<float>(m.settings.strain_limit_stiffness_scale);
+    P.seamStiffness = static_cast<float>(m.settings.seam_stiffness);
+    P.closingSpeed = static_cast<float>(m.settings.assembly_closing_speed);
+    P.frictionSlip = static_cast<float>(m.settings.friction_slip_speed);
+    P.collisionOffset = static_cast<float>(m.settings.collision_offset);
+    P.dampingScale = static_cast<float>(m.settings.damping_scale);
+    P.assemblyExtraDamping = static_cast<float>(m.settings.assembly_extra_damping);
+    P.contactReach = static_cast<float>(drape_b200::kContactReach);
+    P.contactSnap = static_cast<float>(drape_b200::kContactSnap);
+    P.cgTolerance = m.settings.cg_tolerance;
+    P.maxCg = m.settings.max_cg_iterations;
+    P.n = n;
+    P.nStretch = static_cast<uint32_t>(m.stretch.size());
+    P.nHinge = static_cast<uint32_t>(m.hinges.size());
+    P.nSeam = static_cast<uint32_t>(m.seams.size());
+    P.nBlocks = B;
+    P.nGarments = static_cast<uint32_t>(m.garments.size());
+    P.slotsPadded = SP;
+    P.barrierLimitNs = barrierLimitNs;
+    d.field.present = !m.fieldValues.empty() ? 1 : 0;
+    d.field.ox = static_cast<float>(m.field.origin[0]);
+    d.field.oy = static_cast<float>(m.field.origin[1]);
+    d.field.oz = static_cast<float>(m.field.origin[2]);
+    d.field.cell = static_cast<float>(m.field.cell_size);
+    d.field.band = static_cast<float>(m.hasBody ? m.field.band : 0.02);
+    for (int a = 0; a < 3; ++a) d.field.dims[a] = m.field.dims[a];
+    for (int a = 0; a < 3; ++a) d.fieldOrigin[a] = m.field.origin[a];
+    d.fieldCell = m.field.cell_size;
+    d.fieldValues = fieldValues.p;
+    d.particle = particle.p;
+    d.fabric = fabric.p;
+    d.garment = garment.p;
+    d.stretch = stretch.p;
+    d.hinge = hinge.p;
+    d.seam = seam.p;
+    d.rowStart = rowStart.p;
+    d.colIndex = colIndex.p;
+    d.incStart = incStart.p;
+    d.incEntry = incEntry.p;
+    d.incLocal = incLocal.p;
+    d.x = x.p;
+    d.v = v.p;
+    d.xStart = xStart.p;
+    d.yRel = yRel.p;
+    d.u = u.p;
+    d.grad = grad.p;
+    d.step = step.p;
+    d.r = r.p;
+    d.z = z.p;
+    d.p0 = p0.p;
+    d.p1 = p1.p;
+    d.ap = ap.p;
+    d.apFull = apFull.p;
+    d.resid = resid.p;
+    d.fExt = fExt.p;
+    d.pinPos = pinPos.p;
+    d.blocks = blocks.p;
+    d.precond = precond.p;
+    d.contact = contact.p;
+    d.partials = partials.p;
+    d.ctl = ctl.p;
+    dev = d;
+    assembleGrid = static_cast<int>(std::max<uint32_t>(1, std::min<uint32_t>((n + dcu::kAssembleWarps - 1) / dcu::kAssembleWarps,
+                                                                           static_cast<uint32_t>(numSMs) * 16)));
+    CK(cudaStreamSynchronize(s));
+    built = true;
+  }
+
+  void requireBuilt() const {
+    if (!built) throw std::logic_error("not built");
+  }
+
+  // ---- model <-> device ----
+
+  // Device -> model: positions, velocities and contact forces (the state the device advances).
+  void syncToModel() {
+    use();
+    const size_t n = m.x.size();
+    std::vector<float4> xs(n), vs(n);
+    std::vector<dcu::Contact> cs(n);
+    if (n) {
+      CK(cudaMemcpyAsync(xs.data(), x.p, sizeof(float4) * n, cudaMemcpyDeviceToHost, stream));
+      CK(cudaMemcpyAsync(vs.data(), v.p, sizeof(float4) * n, cudaMemcpyDeviceToHost, stream));
+      CK(cudaMemcpyAsync(cs.data(), contact.p, sizeof(dcu::Contact) * n, cudaMemcpyDeviceToHost, stream));
+      CK(cudaStreamSynchronize(stream));
+    }
+    for (size_t i = 0; i < n; ++i) {
+      m.x[i] = {xs[i].x, xs[i].y, xs[i].z};
+      m.v[i] = {vs[i].x, vs[i].y, vs[i].z};
+      m.contactForce[i] = cs[i].force;
+    }
+  }
+
+  // Model -> device: everything the model may have changed (restore, setPhase, updateFabric).
+  void syncFromModel() {
+    use();
+    const size_t n = m.x.size();
+    std::vector<float4> xs(n), vs(n);
+    std::vector<dcu::Contact> cs(n);
+    if (n) {
+      CK(cudaMemcpyAsync(cs.data(), contact.p, sizeof(dcu::Contact) * n, cudaMemcpyDeviceToHost, stream));
+      CK(cudaStreamSynchronize(stream));
+    }
+    for (size_t i = 0; i < n; ++i) {
+      xs[i] = f4(m.x[i]);
+      vs[i] = f4(m.v[i]);
+      cs[i].force = static_cast<float>(m.contactForce[i]);
+    }
+    x.upload(xs, stream);
+    v.upload(vs, stream);
+    contact.upload(cs, stream);
+    particle.upload(particleData(), stream);
+    fabric.upload(fabricData(), stream);
+    garment.upload(garmentData(), stream);
+    hinge.upload(hingeData(), stream);
+    seam.upload(seamData(), stream);
+    CK(cudaStreamSynchronize(stream));
+  }
+
+  // ---- stepping ----
+
+  void resetControlAfterError() {
+    dcu::Control c{};
+    CK(cudaMemcpy(&c, ctl.p, sizeof(c), cudaMemcpyDeviceToHost));
+    c.error = 0;
+    c.barrierCount = 0;
+    CK(cudaMemcpy(ctl.p, &c, sizeof(c), cudaMemcpyHostToDevice));
+  }
+
+  void launchSolve(const dcu::Dev& d) {
+    void* args[] = {const_cast<dcu::Dev*>(&d)};
+    CK(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(dcu::k_solve), dim3(solveGrid), dim3(dcu::kSolveThreads),
+                                   args, 0, stream));
+  }
+
+  void enqueueSubstep(double h, int iterations) {
+    dcu::Dev d = dev;
+    d.P.h = static_cast<float>(h);
+    d.P.invH2 = static_cast<float>(1.0 / (h * h));
+    d.P.hD = h;
+    d.P.barrierLimitNs = barrierLimitNs;
+    const uint32_t n = d.P.n;
+    const int pg = static_cast<int>(std::min<uint32_t>((n + 255) / 256, static_cast<uint32_t>(pointGrid)));
+    dcu::k_begin<<<std::max(pg, 1), 256, 0, stream>>>(d);
+    CK(cudaGetLastError());
+    for (int it = 0; it < iterations; ++it) {
+      dcu::k_activate<<<std::max(pg, 1), 256, 0, stream>>>(d);
+      dcu::k_assemble<<<assembleGrid, dcu::kAssembleWarps * dcu::kWarp, 0, stream>>>(d);
+      CK(cudaGetLastError());
+      launchSolve(d);
+    }
+    dcu::k_finish<<<std::max(pg, 1), 256, 0, stream>>>(d);
+    dcu::k_advance_clock<<<1, 32, 0, stream>>>(d);
+    CK(cudaGetLastError());
+    for (auto& g : m.garments)
+      if (g.phase == DRAPE_PHASE_ASSEMBLING) g.assemblyTime += h;
+  }
+
+  void readControl() {
+    CK(cudaMemcpyAsync(hCtl.p, ctl.p, sizeof(dcu::Control), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    if (hCtl.p->error != 0) {
+      const int e = hCtl.p->error;
+      resetControlAfterError();
+      throw std::runtime_error(e == 1 ? "cuda: a grid barrier timed out (the step was abandoned)"
+                                      : "cuda: device error status " + std::to_string(e));
+    }
+  }
+
+  void advance(double dt, int substeps, int iterations) {
+    requireBuilt();
+    use();
+    if (failAfter == 0) throw std::runtime_error("cuda: injected device failure");
+    if (failAfter > 0) --failAfter;
+    if (m.x.empty()) return;
+    const int sub = std::max(1, substeps);
+    const double h = dt / sub;
+    const int its = std::max(1, iterations);
+    for (int k = 0; k < sub; ++k) enqueueSubstep(h, its);
+    readControl();
+  }
+
+  drape_stats stats() {
+    requireBuilt();
+    use();
+    drape_stats st{};
+    if (m.x.empty()) return st;
+    dcu::k_stats<<<statsGrid, 256, 0, stream>>>(dev, statsPartials.p, statsDone.p, statsOut.p);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(hStats.p, statsOut.p, sizeof(dcu::StatsOut), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    const dcu::StatsOut& s = *hStats.p;
+    st.has_non_finite = s.nonFinite;
+    st.kinetic_energy = s.kineticEnergy;
+    st.rms_speed = s.moving ? std::sqrt(s.sumV2 / static_cast<double>(s.moving)) : 0.0;
+    st.max_seam_gap = s.maxSeamGap;
+    st.max_body_penetration = m.hasBody ? s.maxPenetration : 0.0;
+    return st;
+  }
+
+  drape_counters counters() {
+    use();
+    CK(cudaMemcpyAsync(hCtl.p, ctl.p, sizeof(dcu::Control), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    drape_counters c{};
+    c.substeps = hCtl.p->substeps;
+    c.newton_iterations = hCtl.p->newtonIterations;
+    c.cg_iterations = hCtl.p->cgIterations;
+    c.line_search_halvings = hCtl.p->lineSearchHalvings;
+    return c;
+  }
+
+  void resetCounters() {
+    use();
+    CK(cudaMemcpyAsync(hCtl.p, ctl.p, sizeof(dcu::Control), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    dcu::Control c = *hCtl.p;
+    c.substeps = c.newtonIterations = c.cgIterations = c.lineSearchHalvings = 0;
+    *hCtl.p = c;
+    CK(cudaMemcpyAsync(ctl.p, hCtl.p, sizeof(dcu::Control), cudaMemcpyHostToDevice, stream));
+    CK(cudaStreamSynchronize(stream));
+  }
+
+  void readVec(const DBuf<float4>& b, float* out, size_t count) {
+    requireBuilt();
+    use();
+    if (count != m.x.size()) throw std::invalid_argument("readPositions: span size must equal particleCount()");
+    std::vector<float4> tmp(count);
+    if (count) {
+      CK(cudaMemcpyAsync(tmp.data(), b.p, sizeof(float4) * count, cudaMemcpyDeviceToHost, stream));
+      CK(cudaStreamSynchronize(stream));
+    }
+    for (size_t i = 0; i < count; ++i) {
+      out[3 * i] = tmp[i].x;
+      out[3 * i + 1] = tmp[i].y;
+      out[3 * i + 2] = tmp[i].z;
+    }
+  }
+
+  // ---- device-side snapshots for the drape runner ----
+
+  struct DeviceSnapshot {
+    DBuf<float4> x, v;
+    DBuf<dcu::Contact> contact;
+    std::vector<int> phases;
+    std::vector<double> assemblyTime;
+    std::vector<float> seamStartGap;
+  };
+
+  void saveTo(DeviceSnapshot& s) {
+    const size_t n = m.x.size();
+    if (s.x.n != n) {
+      s.x.alloc(n);
+      s.v.alloc(n);
+      s.contact.alloc(n);
+    }
+    if (n) {
+      CK(cudaMemcpyAsync(s.x.p, x.p, sizeof(float4) * n, cudaMemcpyDeviceToDevice, stream));
+      CK(cudaMemcpyAsync(s.v.p, v.p, sizeof(float4) * n, cudaMemcpyDeviceToDevice, stream));
+      CK(cudaMemcpyAsync(s.contact.p, contact.p, sizeof(dcu::Contact) * n, cudaMemcpyDeviceToDevice, stream));
+    }
+    s.phases.clear();
+    s.assemblyTime.clear();
+    for (const auto& g : m.garments) {
+      s.phases.push_back(g.phase);
+      s.assemblyTime.push_back(g.assemblyTime);
+    }
+    s.seamStartGap.clear();
+    for (const auto& sp : m.seams) s.seamStartGap.push_back(sp.startGap);
+  }
+
+  void restoreFrom(const DeviceSnapshot& s) {
+    const size_t n = m.x.size();
+    if (n) {
+      CK(cudaMemcpyAsync(x.p, s.x.p, sizeof(float4) * n, cudaMemcpyDeviceToDevice, stream));
+      CK(cudaMemcpyAsync(v.p, s.v.p, sizeof(float4) * n, cudaMemcpyDeviceToDevice, stream));
+      CK(cudaMemcpyAsync(contact.p, s.contact.p, sizeof(dcu::Contact) * n, cudaMemcpyDeviceToDevice, stream));
+    }
+    for (size_t g = 0; g < m.garments.size(); ++g) {
+      m.garments[g].phase = s.phases[g];
+      m.garments[g].assemblyTime = s.assemblyTime[g];
+    }
+    for (size_t k = 0; k < m.seams.size(); ++k) m.seams[k].startGap = s.seamStartGap[k];
+    garment.upload(garmentData(), stream);
+    seam.upload(seamData(), stream);
+    CK(cudaStreamSynchronize(stream));
+  }
+
+  // Phase change without a full host round trip: seam start gaps need the current positions.
+  void setPhase(const std::string& id, int phase) {
+    requireBuilt();
+    if (phase == DRAPE_PHASE_ASSEMBLING) {
+      syncToModel();
+      m.setPhase(id, phase);
+      syncFromModel();
+    } else {
+      m.setPhase(id, phase);
+      use();
+      garment.upload(garmentData(), stream);
+      CK(cudaStreamSynchronize(stream));
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------------------------------------------
+// The drape runner (DrapeSession, libs/sim/src/drape_session.cpp:12-95) over the device solver, with its snapshots
+// kept in device memory.
+
+namespace {
+
+constexpr double kTimeEps = 1e-9;
+
+drape_drape_options defaultOptions() {
+  drape_drape_options o{};
+  o.substeps = 1;
+  o.iterations = 2;
+  o.frame_dt = 1.0 / 60.0;
+  o.max_assembly_seconds = 3.0;
+  o.seam_gap_done = 0.001;
+  o.settle_rms_speed = 0.002;
+  o.settle_hold_frames = 60;
+  o.max_sim_seconds = 20.0;
+  o.snapshot_every = 30;
+  o.max_retries = 3;
+  o.energy_rise_frames = 60;
+  return o;
+}
+
+drape_drape_result drapeToRest(drape_solver& s, const std::vector<std::string>& garments, const drape_drape_options& o) {
+  drape_drape_result result{};
+  auto setAll = [&](int phase) {
+    for (const auto& g : garments) s.setPhase(g, phase);
+  };
+  setAll(DRAPE_PHASE_ASSEMBLING);
+  struct Saved {
+    drape_solver::DeviceSnapshot snap;
+    double time = 0;
+    int phase = DRAPE_PHASE_ASSEMBLING;
+    double phaseTime = 0;
+  } saved;
+  s.saveTo(saved.snap);
+  int state = DRAPE_STATE_ASSEMBLING, phase = DRAPE_PHASE_ASSEMBLING;
+  double time = 0, phaseTime = 0, lastEnergy = INFINITY;
+  int substeps = o.substeps, stillFrames = 0, riseFrames = 0, keptFrames = 0;
+  auto resetCounters = [&] {
+    stillFrames = 0;
+    riseFrames = 0;
+    lastEnergy = INFINITY;
+  };
+  auto finished = [&] {
+    return state == DRAPE_STATE_SETTLED || state == DRAPE_STATE_FAILED || state == DRAPE_STATE_TIMED_OUT;
+  };
+  while (!finished()) {
+    if (time >= o.max_sim_seconds - kTimeEps) {
+      result.simulated_seconds = time;
+      state = DRAPE_STATE_TIMED_OUT;
+      break;
+    }
+    s.advance(o.frame_dt, substeps, o.iterations);
+    ++result.frames_run;
+    ++keptFrames;
+    time += o.frame_dt;
+    phaseTime += o.frame_dt;
+    const drape_stats st = s.stats();
+    riseFrames = st.kinetic_energy > lastEnergy ? riseFrames + 1 : 0;
+    lastEnergy = st.kinetic_energy;
+    if (st.has_non_finite || riseFrames >= o.energy_rise_frames) {
+      ++result.retries;
+      if (result.retries > o.max_retries) {
+        result.retries = o.max_retries;
+        result.failed = 1;
+        result.simulated_seconds = time;
+        state = DRAPE_STATE_FAILED;
+        break;
+      }
+      s.restoreFrom(saved.snap);
+      time = saved.time;
+      phase = saved.phase;
+      phaseTime = saved.phaseTime;
+      keptFrames = static_cast<int>(saved.time / o.frame_dt + 0.5);
+      substeps *= 2;
+      resetCounters();
+      state = phase == DRAPE_PHASE_ASSEMBLING ? DRAPE_STATE_ASSEMBLING : DRAPE_STATE_SETTLING;
+      continue;
+    }
+    if (phase == DRAPE_PHASE_ASSEMBLING) {
+      if (st.max_seam_gap < o.seam_gap_done || phaseTime >= o.max_assembly_seconds - kTimeEps) {
+        result.assembly_end_seam_gap = st.max_seam_gap;
+        result.assembly_seconds = time;
+        phase = DRAPE_PHASE_SETTLING;
+        setAll(phase);
+        phaseTime = 0;
+        resetCounters();
+      }
+    } else {
+      stillFrames = st.rms_speed < o.settle_rms_speed ? stillFrames + 1 : 0;
+      if (stillFrames >= o.settle_hold_frames) {
+        result.settled = 1;
+        result.simulated_seconds = time;
+        state = DRAPE_STATE_SETTLED;
+        break;
+      }
+    }
+    if (keptFrames % o.snapshot_every == 0) {
+      s.saveTo(saved.snap);
+      saved.time = time;
+      saved.phase = phase;
+      saved.phaseTime = phaseTime;
+    }
+    if (time >= o.max_sim_seconds - kTimeEps) {
+      result.simulated_seconds = time;
+      state = DRAPE_STATE_TIMED_OUT;
+      break;
+    }
+    state = phase == DRAPE_PHASE_ASSEMBLING ? DRAPE_STATE_ASSEMBLING : DRAPE_STATE_SETTLING;
+  }
+  return result;
+}
+
+template <class F>
+int guarded(const drape_solver* cs, F&& f) {
+  auto* s = const_cast<drape_solver*>(cs);
+  try {
+    f();
+    return DRAPE_OK;
+  } catch (const std::invalid_argument& e) {
+    (s ? s->error : g_lastError) = e.what();
+    return DRAPE_INVALID;
+  } catch (const std::out_of_range& e) {
+    (s ? s->error : g_lastError) = e.what();
+    return DRAPE_OUT_OF_RANGE;
+  } catch (const std::logic_error& e) {
+    (s ? s->error : g_lastError) = e.what();
+    return DRAPE_NOT_BUILT;
+  } catch (const std::exception& e) {
+    (s ? s->error : g_lastError) = e.what();
+    return DRAPE_DEVICE_ERROR;
+  }
+}
+
+void need(const drape_solver* s) {
+  if (!s) throw std::invalid_argument("null solver handle");
+}
+
+void copyStructure(const Model& m, uint32_t* row_start, uint32_t* col_index, uint32_t* diag_slot,
+                   uint32_t* stretch_slots, uint32_t* hinge_slots, uint32_t* seam_slots, uint32_t* stretch_v,
+                   uint32_t* hinge_v, uint32_t* seam_ab) {
+  if (row_start) std::copy(m.rowStart.begin(), m.rowStart.end(), row_start);
+  if (col_index) std::copy(m.colIndex.begin(), m.colIndex.end(), col_index);
+  if (diag_slot) std::copy(m.diagSlot.begin(), m.diagSlot.end(), diag_slot);
+  for (size_t t = 0; t < m.stretch.size(); ++t) {
+    if (stretch_slots) std::copy(m.stretchSlots[t].begin(), m.stretchSlots[t].end(), stretch_slots + 9 * t);
+    if (stretch_v) std::copy(m.stretch[t].v.begin(), m.stretch[t].v.end(), stretch_v + 3 * t);
+  }
+  for (size_t h = 0; h < m.hinges.size(); ++h) {
+    if (hinge_slots) std::copy(m.hingeSlots[h].begin(), m.hingeSlots[h].end(), hinge_slots + 16 * h);
+    if (hinge_v) std::copy(m.hinges[h].v.begin(), m.hinges[h].v.end(), hinge_v + 4 * h);
+  }
+  for (size_t k = 0; k < m.seams.size(); ++k) {
+    if (seam_slots) std::copy(m.seamSlots[k].begin(), m.seamSlots[k].end(), seam_slots + 4 * k);
+    if (seam_ab) {
+      seam_ab[2 * k] = m.seams[k].a;
+      seam_ab[2 * k + 1] = m.seams[k].b;
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int drape_cuda_version(void) { return 100; }
+
+int drape_cuda_is_available(void) {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return 0;
+  }
+  for (int d = 0; d < count; ++d) {
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, d) == cudaSuccess && prop.major == 10) {
+      cudaFuncAttributes attr{};
+      if (cudaFuncGetAttributes(&attr, dcu::k_solve) == cudaSuccess) return 1;
+      cudaGetLastError();
+    }
+  }
+  return 0;
+}
+
+int drape_cuda_create(int device, drape_solver** out) {
+  return guarded(nullptr, [&] {
+    if (!out) throw std::invalid_argument("null output pointer");
+    *out = nullptr;
+    *out = new drape_solver(device);
+  });
+}
+
+void drape_cuda_destroy(drape_solver* s) { delete s; }
+
+const char* drape_cuda_last_error(const drape_solver* s) { return s ? s->error.c_str() : g_lastError.c_str(); }
+
+int drape_cuda_build(drape_solver* s, const drape_scene_desc* scene) {
+  return guarded(s, [&] {
+    need(s);
+    if (!scene) throw std::invalid_argument("null scene");
+    s->build(*scene);
+  });
+}
+
+int drape_cuda_update_fabric(drape_solver* s, const char* garment, const drape_fabric* piece_fabric, uint32_t count) {
+  return guarded(s, [&] {
+    need(s);
+    s->requireBuilt();
+    s->syncToModel();
+    s->m.updateFabric(garment ? garment : "", piece_fabric, count);
+    s->syncFromModel();
+  });
+}
+
+int drape_cuda_set_phase(drape_solver* s, const char* garment, int phase) {
+  return guarded(s, [&] {
+    need(s);
+    if (phase != DRAPE_PHASE_ASSEMBLING && phase != DRAPE_PHASE_SETTLING) throw std::invalid_argument("unknown phase");
+    s->setPhase(garment ? garment : "", phase);
+  });
+}
+
+int drape_cuda_step(drape_solver* s, double dt, int substeps, int iterations) {
+  return guarded(s, [&] {
+    need(s);
+    s->advance(dt, substeps, iterations);
+  });
+}
+
+int drape_cuda_read_positions(const drape_solver* s, float* out, size_t count) {
+  return guarded(s, [&] {
+    need(s);
+    const_cast<drape_solver*>(s)->readVec(s->x, out, count);
+  });
+}
+
+int drape_cuda_read_velocities(const drape_solver* s, float* out, size_t count) {
+  return guarded(s, [&] {
+    need(s);
+    const_cast<drape_solver*>(s)->readVec(s->v, out, count);
+  });
+}
+
+int drape_cuda_stats(drape_solver* s, drape_stats* out) {
+  return guarded(s, [&] {
+    need(s);
+    *out = s->stats();
+  });
+}
+
+int drape_cuda_snapshot_sizes(const drape_solver* s, uint32_t* particles, uint32_t* garments, uint32_t* seams) {
+  return guarded(s, [&] {
+    need(s);
+    s->requireBuilt();
+    *particles = static_cast<uint32_t>(s->m.x.size());
+    *garments = static_cast<uint32_t>(s->m.garments.size());
+    *seams = static_cast<uint32_t>(s->m.seams.size());
+  });
+}
+
+int drape_cuda_snapshot(const drape_solver* cs, float* positions, float* velocities, int32_t* phases,
+                        double* assembly_time, float* seam_start_gap, double* contact_force) {
+  return guarded(cs, [&] {
+    need(cs);
+    auto* s = const_cast<drape_solver*>(cs);
+    s->requireBuilt();
+    s->syncToModel();
+    const auto& m = s->m;
+    for (size_t i = 0; i < m.x.size(); ++i) {
+      positions[3 * i] = m.x[i].x;
+      positions[3 * i + 1] = m.x[i].y;
+      positions[3 * i + 2] = m.x[i].z;
+      velocities[3 * i] = m.v[i].x;
+      velocities[3 * i + 1] = m.v[i].y;
+      velocities[3 * i + 2] = m.v[i].z;
+      contact_force[i] = m.contactForce[i];
+    }
+    for (size_t g = 0; g < m.garments.size(); ++g) {
+      phases[g] = m.garments[g].phase;
+      assembly_time[g] = m.garments[g].assemblyTime;
+    }
+    for (size_t k = 0; k < m.seams.size(); ++k) seam_start_gap[k] = m.seams[k].startGap;
+  });
+}
+
+int drape_cuda_restore(drape_solver* s, const float* positions, const float* velocities, uint32_t particles,
+                       const int32_t* phases, const double* assembly_time, uint32_t garments,
+                       const float* seam_start_gap, uint32_t seams, const double* contact_force,
+                       uint32_t contact_count) {
+  return guarded(s, [&] {
+    need(s);
+    s->requireBuilt();
+    auto& m = s->m;
+    if (particles != m.x.size() || garments != m.garments.size())
+      throw std::invalid_argument("snapshot does not match this scene");
+    for (size_t i = 0; i < particles; ++i) {
+      m.x[i] = {positions[3 * i], positions[3 * i + 1], positions[3 * i + 2]};
+      m.v[i] = {velocities[3 * i], velocities[3 * i + 1], velocities[3 * i + 2]};
+    }
+    if (contact_count == m.contactForce.size()) {
+      for (size_t i = 0; i < contact_count; ++i) m.contactForce[i] = contact_force[i];
+    } else {
+      std::fill(m.contactForce.begin(), m.contactForce.end(), 0.0);
+    }
+    for (size_t g = 0; g < garments; ++g) {
+      m.garments[g].phase = phases[g] == 0 ? DRAPE_PHASE_ASSEMBLING : DRAPE_PHASE_SETTLING;
+      m.garments[g].assemblyTime = assembly_time[g];
+    }
+    if (seams == m.seams.size())
+      for (size_t k = 0; k < seams; ++k) m.seams[k].startGap = seam_start_gap[k];
+    s->syncFromModel();
+  });
+}
+
+int drape_cuda_range(const drape_solver* s, const char* garment, uint32_t* offset, uint32_t* count) {
+  return guarded(s, [&] {
+    need(s);
+    s->requireBuilt();
+    const auto& g = s->m.garments[s->m.garmentIndex(garment ? garment : "")];
+    *offset = g.offset;
+    *count = g.count;
+  });
+}
+
+int drape_cuda_particle_count(const drape_solver* s, size_t* out) {
+  return guarded(s, [&] {
+    need(s);
+    *out = s->built ? s->m.x.size() : 0;
+  });
+}
+
+int drape_cuda_drape_to_rest(drape_solver* s, const char* const* garments, uint32_t garment_count,
+                             const drape_drape_options* options, drape_drape_result* out) {
+  return guarded(s, [&] {
+    need(s);
+    s->requireBuilt();
+    std::vector<std::string> ids;
+    for (uint32_t k = 0; k < garment_count; ++k) ids.emplace_back(garments[k] ? garments[k] : "");
+    for (const auto& id : ids) s->m.garmentIndex(id);
+    *out = drapeToRest(*s, ids, options ? *options : defaultOptions());
+  });
+}
+
+int drape_cuda_counters(const drape_solver* s, drape_counters* out) {
+  return guarded(s, [&] {
+    need(s);
+    *out = const_cast<drape_solver*>(s)->counters();
+  });
+}
+
+int drape_cuda_reset_counters(drape_solver* s) {
+  return guarded(s, [&] {
+    need(s);
+    s->resetCounters();
+  });
+}
+
+int drape_cuda_structure_sizes(const drape_solver* s, uint32_t sizes[5]) {
+  return guarded(s, [&] {
+    need(s);
+    s->requireBuilt();
+    sizes[0] = static_cast<uint32_t>(s->m.x.size());
+    sizes[1] = static_cast<uint32_t>(s->m.colIndex.size());
+    sizes[2] = static_cast<uint32_t>(s->m.stretch.size());
+    sizes[3] = static_cast<uint32_t>(s->m.hinges.size());
+    sizes[4] = static_cast<uint32_t>(s->m.seams.size());
+  });
+}
+
+int drape_cuda_structure(const drape_solver* s, uint32_t* row_start, uint32_t* col_index, uint32_t* diag_slot,
+                         uint32_t* stretch_slots, uint32_t* hinge_slots, uint32_t* seam_slots, uint32_t* stretch_v,
+                         uint32_t* hinge_v, uint32_t* seam_ab) {
+  return guarded(s, [&] {
+    need(s);
+    s->requireBuilt();
+    copyStructure(s->m, row_start, col_index, diag_slot, stretch_slots, hinge_slots, seam_slots, stretch_v, hinge_v,
+                  seam_ab);
+  });
+}
+
+struct drape_model {
+  Model m;
+};
+
+int drape_model_build(const drape_scene_desc* scene, drape_model** out) {
+  return guarded(nullptr, [&] {
+    if (!scene || !out) throw std::invalid_argument("null argument");
+    *out = nullptr;
+    auto* dm = new drape_model;
+    try {
+      dm->m = Model::build(*scene);
+    } catch (...) {
+      delete dm;
+      throw;
+    }
+    *out = dm;
+  });
+}
+
+void drape_model_destroy(drape_model* m) { delete m; }
+
+const char* drape_model_last_error(void) { return g_lastError.c_str(); }
+
+int drape_model_structure_sizes(const drape_model* dm, uint32_t sizes[5]) {
+  return guarded(nullptr, [&] {
+    if (!dm) throw std::invalid_argument("null model");
+    sizes[0] = static_cast<uint32_t>(dm->m.x.size());
+    sizes[1] = static_cast<uint32_t>(dm->m.colIndex.size());
+    sizes[2] = static_cast<uint32_t>(dm->m.stretch.size());
+    sizes[3] = static_cast<uint32_t>(dm->m.hinges.size());
+    sizes[4] = static_cast<uint32_t>(dm->m.seams.size());
+  });
+}
+
+int drape_model_structure(const drape_model* dm, uint32_t* row_start, uint32_t* col_index, uint32_t* diag_slot,
+                          uint32_t* stretch_slots, uint32_t* hinge_slots, uint32_t* seam_slots, uint32_t* stretch_v,
+                          uint32_t* hinge_v, uint32_t* seam_ab) {
+  return guarded(nullptr, [&] {
+    if (!dm) throw std::invalid_argument("null model");
+    copyStructure(dm->m, row_start, col_index, diag_slot, stretch_slots, hinge_slots, seam_slots, stretch_v, hinge_v,
+                  seam_ab);
+  });
+}
+
+int drape_cuda_contact_candidates(drape_solver* s, const float* x_start, uint8_t* near_flag, float* normal,
+                                  float* offset) {
+  return guarded(s, [&] {
+    need(s);
+    s->requireBuilt();
+    s->use();
+    const size_t n = s->m.x.size();
+    if (!n) return;
+    std::vector<float4> xs(n);
+    for (size_t i = 0; i < n; ++i) xs[i] = make_float4(x_start[3 * i], x_start[3 * i + 1], x_start[3 * i + 2], 0.0f);
+    DBuf<float4> dx;
+    DBuf<dcu::Contact> dc;
+    dx.upload(xs, s->stream);
+    dc.alloc(n);
+    dcu::k_contact_candidates<<<std::max<int>(1, static_cast<int>((n + 255) / 256)), 256, 0, s->stream>>>(s->dev, dx.p, dc.p);
+    CK(cudaGetLastError());
+    std::vector<dcu::Contact> cs(n);
+    CK(cudaMemcpyAsync(cs.data(), dc.p, sizeof(dcu::Contact) * n, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    for (size_t i = 0; i < n; ++i) {
+      near_flag[i] = cs[i].nearBody ? 1 : 0;
+      normal[3 * i] = cs[i].normal.x;
+      normal[3 * i + 1] = cs[i].normal.y;
+      normal[3 * i + 2] = cs[i].normal.z;
+      offset[i] = cs[i].normal.w;
+    }
+  });
+}
+
+int drape_cuda_capture_system(drape_solver* s, double h, float* blocks, float* grad, uint8_t* active) {
+  return guarded(s, [&] {
+    need(s);
+    s->requireBuilt();
+    s->use();
+    const size_t n = s->m.x.size();
+    if (!n) return;
+    // Run the substep prologue on scratch copies of the mutable state so the solver state is not changed.
+    DBuf<float4> xs0, u0, ys0, xst0;
+    DBuf<dcu::Contact> c0;
+    xs0.alloc(n);
+    c0.alloc(n);
+    u0.alloc(n);
+    ys0.alloc(n);
+    xst0.alloc(n);
+    CK(cudaMemcpyAsync(c0.p, s->contact.p, sizeof(dcu::Contact) * n, cudaMemcpyDeviceToDevice, s->stream));
+    dcu::Control ctlSave{};
+    CK(cudaMemcpyAsync(&ctlSave, s->ctl.p, sizeof(ctlSave), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    dcu::Dev d = s->dev;
+    d.P.h = static_cast<float>(h);
+    d.P.invH2 = static_cast<float>(1.0 / (h * h));
+    d.P.hD = h;
+    d.contact = c0.p;
+    d.u = u0.p;
+    d.yRel = ys0.p;
+    d.xStart = xst0.p;
+    const int pg = std::max<int>(1, static_cast<int>((n + 255) / 256));
+    dcu::k_begin<<<pg, 256, 0, s->stream>>>(d);
+    dcu::k_activate<<<pg, 256, 0, s->stream>>>(d);
+    dcu::k_assemble<<<s->assembleGrid, dcu::kAssembleWarps * dcu::kWarp, 0, s->stream>>>(d);
+    CK(cudaGetLastError());
+    const size_t B = s->m.colIndex.size(), SP = s->dev.P.slotsPadded;
+    std::vector<float> planes(9 * SP);
+    std::vector<float4> g(n);
+    std::vector<dcu::Contact> cs(n);
+    CK(cudaMemcpyAsync(planes.data(), s->blocks.p, sizeof(float) * 9 * SP, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaMemcpyAsync(g.data(), s->grad.p, sizeof(float4) * n, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaMemcpyAsync(cs.data(), c0.p, sizeof(dcu::Contact) * n, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaMemcpyAsync(s->ctl.p, &ctlSave, sizeof(ctlSave), cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    for (size_t k = 0; k < B; ++k)
+      for (int c = 0; c < 9; ++c) blocks[9 * k + c] = planes[c * SP + k];
+    for (size_t i = 0; i < n; ++i) {
+      grad[3 * i] = g[i].x;
+      grad[3 * i + 1] = g[i].y;
+      grad[3 * i + 2] = g[i].z;
+      active[i] = cs[i].active ? 1 : 0;
+    }
+  });
+}
+
+int drape_cuda_pcg(uint32_t n, const uint32_t* row_start, const uint32_t* col_index, const float* blocks,
+                   const uint8_t* pinned, const uint8_t* active, const float* normals, const float* grad,
+                   int max_iterations, double tolerance, float* step, float* resid, int* iterations) {
+  return guarded(nullptr, [&] {
+    if (!row_start || !col_index || !blocks || !pinned || !grad || !step || !resid || !iterations)
+      throw std::invalid_argument("null argument");
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    drape_solver s(dev);
+    const uint32_t B = row_start[n];
+    const uint32_t SP = (B + 31u) & ~31u;
+    std::vector<uint32_t> cols(col_index, col_index + B);
+    for (auto& c : cols) {
+      if (c >= n) throw std::invalid_argument("column index out of range");
+      if (pinned[c]) c |= dcu::kPinnedBit;
+    }
+    std::vector<float> planes(9 * static_cast<size_t>(SP), 0.0f);
+    for (size_t k = 0; k < B; ++k)
+      for (int c = 0; c < 9; ++c) planes[c * SP + k] = blocks[9 * k + c];
+    std::vector<dcu::Particle> parts(n);
+    std::vector<dcu::Contact> cs(n);
+    std::vector<float4> g(n), pre(3 * static_cast<size_t>(n));
+    for (uint32_t i = 0; i < n; ++i) {
+      parts[i] = {1.0f, 0, 0, pinned[i] ? 1u : 0u};
+      cs[i].active = active && active[i] ? 1u : 0u;
+      cs[i].nearBody = cs[i].active;
+      if (normals) cs[i].normal = make_float4(normals[3 * i], normals[3 * i + 1], normals[3 * i + 2], 0.0f);
+      g[i] = make_float4(grad[3 * i], grad[3 * i + 1], grad[3 * i + 2], 0.0f);
+      // Block-Jacobi inverse of the diagonal block, computed on the host here exactly as k_assemble does on the device
+      // is not required: this entry point builds the preconditioner with the same device routine below.
+    }
+    cudaStream_t st = s.stream;
+    DBuf<dcu::Particle> dpart;
+    DBuf<uint32_t> drs, dci;
+    DBuf<float> dbl;
+    DBuf<float4> dg, dstep, dr, dz, dp0, dp1, dap, dapf, dres, dpre;
+    DBuf<dcu::Contact> dcs;
+    dpart.upload(parts, st);
+    drs.upload(std::vector<uint32_t>(row_start, row_start + n + 1), st);
+    dci.upload(cols, st);
+    dbl.upload(planes, st);
+    dg.upload(g, st);
+    dcs.upload(cs, st);
+    for (DBuf<float4>* b : {&dstep, &dr, &dz, &dp0, &dp1, &dap, &dapf, &dres}) b->alloc(n);
+    dpre.alloc(3 * static_cast<size_t>(n));
+    dcu::Dev d{};
+    d.P.n = n;
+    d.P.nBlocks = B;
+    d.P.slotsPadded = SP;
+    d.P.maxCg = max_iterations;
+    d.P.cgTolerance = tolerance;
+    d.P.barrierLimitNs = s.barrierLimitNs;
+    d.P.h = 1.0f;
+    d.P.hD = 1.0;
+    d.particle = dpart.p;
+    d.rowStart = drs.p;
+    d.colIndex = dci.p;
+    d.blocks = dbl.p;
+    d.grad = dg.p;
+    d.contact = dcs.p;
+    d.step = dstep.p;
+    d.r = dr.p;
+    d.z = dz.p;
+    d.p0 = dp0.p;
+    d.p1 = dp1.p;
+    d.ap = dap.p;
+    d.apFull = dapf.p;
+    d.resid = dres.p;
+    d.precond = dpre.p;
+    d.partials = s.partials.p;
+    d.ctl = s.ctl.p;
+    // Preconditioner: diagonal block inverses with the device routine, then the persistent PCG alone (no line search:
+    // the energy terms are absent, so k_solve stops after the contact-force phase with slope computed on zero terms).
+    std::vector<uint32_t> diag(n, B);
+    for (uint32_t i = 0; i < n; ++i)
+      for (uint32_t k = row_start[i]; k < row_start[i + 1]; ++k)
+        if (col_index[k] == i) diag[i] = k;
+    for (uint32_t i = 0; i < n; ++i)
+      if (diag[i] == B) throw std::invalid_argument("row without a diagonal block");
+    DBuf<uint32_t> ddiag;
+    ddiag.upload(diag, st);
+    dcu::k_pcg_precondition<<<std::max<int>(1, static_cast<int>((n + 255) / 256)), 256, 0, st>>>(d, ddiag.p);
+    CK(cudaGetLastError());
+    void* args[] = {&d};
+    CK(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(dcu::k_pcg_only), dim3(s.solveGrid),
+                                   dim3(dcu::kSolveThreads), args, 0, st));
+    std::vector<float4> hs(n), hr(n);
+    dcu::Control c{};
+    CK(cudaMemcpyAsync(hs.data(), dstep.p, sizeof(float4) * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hr.data(), dres.p, sizeof(float4) * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&c, s.ctl.p, sizeof(c), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (c.error) throw std::runtime_error("cuda: a grid barrier timed out");
+    for (uint32_t i = 0; i < n; ++i) {
+      step[3 * i] = hs[i].x;
+      step[3 * i + 1] = hs[i].y;
+      step[3 * i + 2] = hs[i].z;
+      resid[3 * i] = hr[i].x;
+      resid[3 * i + 1] = hr[i].y;
+      resid[3 * i + 2] = hr[i].z;
+    }
+    *iterations = c.lastCg;
+  });
+}
+
+int drape_cuda_spmv_device(uint32_t n, const uint32_t* d_row_start, const uint32_t* d_col_index, const float* d_blocks,
+                           uint32_t slots_padded, const uint8_t* d_pinned, const void* d_x, void* d_y, void* stream) {
+  return guarded(nullptr, [&] {
+    if (!n) return;
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    int sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const uint32_t groups = (n + 0u);
+    const uint32_t threads = 256;
+    const uint32_t blocksNeeded = (groups * dcu::kRowLanes + threads - 1) / threads;
+    const uint32_t grid = std::min<uint32_t>(blocksNeeded, static_cast<uint32_t>(sms) * 8);
+    dcu::k_spmv<<<grid, threads, 0, static_cast<cudaStream_t>(stream)>>>(
+        n, d_row_start, d_col_index, d_blocks, slots_padded, d_pinned, static_cast<const float4*>(d_x),
+        static_cast<float4*>(d_y));
+    CK(cudaGetLastError());
+  });
+}
+
+int drape_cuda_set_barrier_limit(drape_solver* s, uint64_t nanoseconds) {
+  return guarded(s, [&] {
+    need(s);
+    s->barrierLimitNs = nanoseconds ? nanoseconds : 2000000000ull;
+  });
+}
+
+int drape_cuda_test_barrier_timeout(int device, int blocks, uint64_t nanoseconds, int* status) {
+  return guarded(nullptr, [&] {
+    if (!status || blocks < 1 || blocks > 1024) throw std::invalid_argument("bad argument");
+    if (nanoseconds == 0 || nanoseconds > 1000000000ull) throw std::invalid_argument("limit must be in (0, 1 s]");
+    CK(cudaSetDevice(device));
+    DBuf<dcu::Control> c;
+    DBuf<int> out;
+    c.alloc(1);
+    out.alloc(1);
+    dcu::k_barrier_probe<<<blocks, 32>>>(c.p, nanoseconds, out.p);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    CK(cudaMemcpy(status, out.p, sizeof(int), cudaMemcpyDeviceToHost));
+  });
+}
+
+int drape_cuda_inject_failure(drape_solver* s, int steps) {
+  return guarded(s, [&] {
+    need(s);
+    s->failAfter = steps;
+  });
+}
+
+}  // extern "C"

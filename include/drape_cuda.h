@@ -1,0 +1,167 @@
+/*
+ * C ABI of the B200 cloth-solver hot path (libdrape_cuda.so).
+ *
+ * One opaque handle is one solver: the reference's drape::sim::Solver (libs/sim/include/drape/sim/solver.hpp:85-98)
+ * with its state on one GPU. A reference-side CudaSolver forwards each Solver method to the
+ * entry point named beside it, and registers itself as a SolverBackend in makeSolver / isAvailable / backendName
+ * (libs/sim/include/drape/sim/solver_factory.hpp:12-20, libs/sim/src/solver_factory.cpp:16-61), so the GPU/CPU switch
+ * (libs/session/include/drape/session/sim_controller.hpp:25) can select it.
+ *
+ * Every call returns an int status. The wrapper maps them to the reference's exception types:
+ *   DRAPE_OK              0
+ *   DRAPE_INVALID        -1  std::invalid_argument  (inconsistent scene, size mismatch: sim_model.cpp:81-86,
+ *                                                   cpu_solver.cpp:340-343, sim_model.cpp:342-344)
+ *   DRAPE_OUT_OF_RANGE   -2  std::out_of_range      (unknown garment id, pin/force particle out of range:
+ *                                                   solver.hpp:96, sim_model.cpp:184, :190)
+ *   DRAPE_DEVICE_ERROR   -3  std::runtime_error     ("cuda: <cause>", the backend-prefixed device failure of
+ *                                                   metal_device.cpp:136 / solver_factory.cpp:57)
+ *   DRAPE_NOT_BUILT      -4  std::runtime_error     (a call that needs a scene before build)
+ * drape_cuda_last_error() returns the message of the last failing call on that handle (thread-local for NULL).
+ *
+ * Threading: one handle is driven by one host thread at a time (as the reference's sim thread drives its Solver,
+ * sim_controller.cpp:57-98). Distinct handles are independent.
+ */
+#ifndef DRAPE_CUDA_H
+#define DRAPE_CUDA_H
+
+#include "drape_scene.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  DRAPE_OK = 0,
+  DRAPE_INVALID = -1,
+  DRAPE_OUT_OF_RANGE = -2,
+  DRAPE_DEVICE_ERROR = -3,
+  DRAPE_NOT_BUILT = -4
+};
+
+typedef struct drape_solver drape_solver;
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+int drape_cuda_version(void);
+
+/* isAvailable(SolverBackend) (solver_factory.cpp:25-47): 1 when a CUDA device of compute capability 10.0 is present
+   and this library's kernels load on it, else 0. */
+int drape_cuda_is_available(void);
+
+/* makeSolver (solver_factory.cpp:49-61): creates a solver on CUDA device `device`. Fails with DRAPE_DEVICE_ERROR
+   ("cuda: ...") when the device is missing or is not sm_100. */
+int drape_cuda_create(int device, drape_solver** out);
+void drape_cuda_destroy(drape_solver* s);
+const char* drape_cuda_last_error(const drape_solver* s);
+
+/* Solver::build (solver.hpp:88): copies everything from the scene (the body field's samples too); a rebuild
+   replaces all state. The block-CSR pattern, slot maps and term lists are built once here on the host in the
+   reference's order (sim_model.cpp:41-175), then uploaded. */
+int drape_cuda_build(drape_solver* s, const drape_scene_desc* scene);
+
+/* Solver::updateFabric (solver.hpp:89): `count` must equal the garment's piece count. */
+int drape_cuda_update_fabric(drape_solver* s, const char* garment, const drape_fabric* piece_fabric, uint32_t count);
+
+/* Solver::setPhase (solver.hpp:90): DRAPE_PHASE_ASSEMBLING or DRAPE_PHASE_SETTLING. Entering Assembling resets the
+   garment's assembly clock and re-measures its seams' start gaps (sim_model.cpp:295-305). */
+int drape_cuda_set_phase(drape_solver* s, const char* garment, int phase);
+
+/* Solver::step (solver.hpp:91; StepInput solver.hpp:57-61): max(1, substeps) implicit-Euler substeps of dt/substeps,
+   each minimised by max(1, iterations) Newton iterations. Returns after the work has completed on the device. */
+int drape_cuda_step(drape_solver* s, double dt, int substeps, int iterations);
+
+/* Solver::readPositions (solver.hpp:92): 3 floats per particle; count must equal the particle count. */
+int drape_cuda_read_positions(const drape_solver* s, float* out, size_t count);
+/* Velocities, 3 floats per particle (part of Solver::snapshot). */
+int drape_cuda_read_velocities(const drape_solver* s, float* out, size_t count);
+
+/* Solver::stats (solver.hpp:93; SimModel::stats sim_model.cpp:222-241), reduced on the device in FP64. */
+int drape_cuda_stats(drape_solver* s, drape_stats* out);
+
+/* Solver::snapshot / restore (solver.hpp:94-95; Snapshot solver.hpp:76-83; sim_model.cpp:243-274).
+   positions, velocities: 3 floats per particle; phases, assembly_time: per garment; seam_start_gap: per seam spring;
+   contact_force: per particle. drape_cuda_snapshot_sizes gives the counts. restore throws invalid_argument when the
+   particle or garment count does not match; a contact-force or seam array of another size is ignored (forces reset
+   to zero, start gaps kept), as the reference does. */
+int drape_cuda_snapshot_sizes(const drape_solver* s, uint32_t* particles, uint32_t* garments, uint32_t* seams);
+int drape_cuda_snapshot(const drape_solver* s, float* positions, float* velocities, int32_t* phases,
+                        double* assembly_time, float* seam_start_gap, double* contact_force);
+int drape_cuda_restore(drape_solver* s, const float* positions, const float* velocities, uint32_t particles,
+                       const int32_t* phases, const double* assembly_time, uint32_t garments,
+                       const float* seam_start_gap, uint32_t seams, const double* contact_force,
+                       uint32_t contact_count);
+
+/* Solver::range / particleCount (solver.hpp:96-97). */
+int drape_cuda_range(const drape_solver* s, const char* garment, uint32_t* offset, uint32_t* count);
+int drape_cuda_particle_count(const drape_solver* s, size_t* out);
+
+/* drapeToRest (libs/sim/include/drape/sim/drape_runner.hpp:40, libs/sim/src/drape_session.cpp:32-95): runs the
+   Assembling -> Settling -> Settled frame loop with the stability guard, snapshots (kept on the device) and retries,
+   for the listed garments. options may be NULL for the defaults of DrapeOptions. */
+int drape_cuda_drape_to_rest(drape_solver* s, const char* const* garments, uint32_t garment_count,
+                             const drape_drape_options* options, drape_drape_result* out);
+
+/* Work counters (Newton, PCG, line-search halvings) since the last reset. */
+int drape_cuda_counters(const drape_solver* s, drape_counters* out);
+int drape_cuda_reset_counters(drape_solver* s);
+
+/* Block-CSR structure and term lists as built (the bit-exact artefacts of sim_model.cpp:41-175). sizes: [0] particles,
+   [1] block slots, [2] stretch terms, [3] hinges, [4] seam springs. Pointers may be NULL. */
+int drape_cuda_structure_sizes(const drape_solver* s, uint32_t sizes[5]);
+int drape_cuda_structure(const drape_solver* s, uint32_t* row_start, uint32_t* col_index, uint32_t* diag_slot,
+                         uint32_t* stretch_slots, uint32_t* hinge_slots, uint32_t* seam_slots, uint32_t* stretch_v,
+                         uint32_t* hinge_v, uint32_t* seam_ab);
+
+/* The same structure built on the host alone, without a device (for callers and tests that check the integer
+   artefacts on machines without a GPU). */
+typedef struct drape_model drape_model;
+int drape_model_build(const drape_scene_desc* scene, drape_model** out);
+void drape_model_destroy(drape_model* m);
+const char* drape_model_last_error(void);
+int drape_model_structure_sizes(const drape_model* m, uint32_t sizes[5]);
+int drape_model_structure(const drape_model* m, uint32_t* row_start, uint32_t* col_index, uint32_t* diag_slot,
+                          uint32_t* stretch_slots, uint32_t* hinge_slots, uint32_t* seam_slots, uint32_t* stretch_v,
+                          uint32_t* hinge_v, uint32_t* seam_ab);
+
+/* Contact candidates (kernels.h:55-82 / cpu_solver.cpp:247-263) for given substep-start positions (3 floats per
+   particle), computed by the device's contact-setup code path: near flag, normal (3 floats), plane offset. The solver
+   state is not changed. */
+int drape_cuda_contact_candidates(drape_solver* s, const float* x_start, uint8_t* near_flag, float* normal,
+                                  float* offset);
+
+/* The first Newton system of the next substep of length h (predict, contact setup and activation, term evaluation
+   and assembly: cpu_solver.cpp:230-265 / gpu_solver_core.cpp:333-343), computed on the device without changing the
+   solver state: blocks (9 floats per slot, row-major), gradient (3 floats per particle), contact-active flags. */
+int drape_cuda_capture_system(drape_solver* s, double h, float* blocks, float* grad, uint8_t* active);
+
+/* Contact-filtered block-Jacobi PCG (cpu_solver.cpp:169-213, kernels.h:237-347) on a system given in host memory,
+   solved by the device's persistent PCG kernel: blocks 9 floats per slot (row-major), grad and normals 3 floats per
+   particle. Returns the step, the unfiltered residual and the iteration count. */
+int drape_cuda_pcg(uint32_t n, const uint32_t* row_start, const uint32_t* col_index, const float* blocks,
+                   const uint8_t* pinned, const uint8_t* active, const float* normals, const float* grad,
+                   int max_iterations, double tolerance, float* step, float* resid, int* iterations);
+
+/* Block-CSR SpMV on device buffers (the PCG's inner product, kernels.h:272-289 without the contact filter):
+   y = A x over rows and columns whose pinned flag is 0. Blocks are 9 planes of `slots_padded` floats (plane k holds
+   component k = 3 * row + col of every slot); x and y are float4 per particle. Runs on `stream` (a cudaStream_t, or
+   NULL for the legacy default stream) and does not synchronise. Used to measure the SpMV on its own. */
+int drape_cuda_spmv_device(uint32_t n, const uint32_t* d_row_start, const uint32_t* d_col_index,
+                           const float* d_blocks, uint32_t slots_padded, const uint8_t* d_pinned, const void* d_x,
+                           void* d_y, void* stream);
+
+/* The bounded wait of the device grid barrier, in nanoseconds (0 restores the default of 2 s). A kernel whose barrier
+   waits longer sets the handle's error status and returns instead of hanging; the step then fails with
+   DRAPE_DEVICE_ERROR and the solver stays usable. */
+int drape_cuda_set_barrier_limit(drape_solver* s, uint64_t nanoseconds);
+/* Test hook: runs a grid barrier that can only end by its time limit (it waits for one more block than it has) on
+   `blocks` blocks with the given limit, and returns the status the blocks read back in *status (0: released, which
+   cannot happen; 1: timed out). Exercises the bounded wait without a device fault. */
+int drape_cuda_test_barrier_timeout(int device, int blocks, uint64_t nanoseconds, int* status);
+/* Test hook: make the next step fail with DRAPE_DEVICE_ERROR after `steps` more successful steps (-1: never), to
+   exercise the caller's GPU -> CPU fallback (sim_controller.cpp:155-176) without a device fault. */
+int drape_cuda_inject_failure(drape_solver* s, int steps);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DRAPE_CUDA_H */
