@@ -73,11 +73,13 @@ struct Control {
   int newtonDone;   // this substep's Newton loop has stopped (slope >= 0 or max move < 1e-9)
   int error;        // 1: a grid barrier gave up waiting; 2: a row exceeded the assembly capacity
   unsigned int barrierCount, barrierGeneration;
-  long long cgIterations, newtonIterations, lineSearchHalvings, substeps;
+  long long cgIterations, newtonIterations, lineSearchHalvings, substeps, energyEvaluations;
   double lastAlpha, lastSlope, lastE0, lastMaxMove;
   int lastCg;
   int pad;
 };
+
+constexpr unsigned int kCgLogCapacity = 1u << 16;  // PCG iterations per Newton iteration, ring buffer
 
 struct Params {
   float h, invH2;
@@ -114,6 +116,7 @@ struct Dev {
   Contact* contact;
   double* partials;
   Control* ctl;
+  int* cgLog;  // kCgLogCapacity entries
 };
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -681,9 +684,11 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(Dev D) {
   const int it = pcgSolve(D);
   if (it < 0) return;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (D.cgLog) D.cgLog[static_cast<unsigned long long>(ctl->newtonIterations) % kCgLogCapacity] = it;
     ctl->cgIterations += it;
     ctl->newtonIterations += 1;
     ctl->lastCg = it;
+    ctl->energyEvaluations += 1;  // E(0) below
   }
 
   // Contact normal force from the residual (kernels.h:391-396), Newton slope grad . step and E(0), in FP64.
@@ -717,6 +722,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(Dev D) {
   // Backtracking line search, Armijo c = 1e-4, at most 20 halvings (cpu_solver.cpp:269-274).
   double alpha = 1.0;
   for (int ls = 0; ls < 20; ++ls) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->energyEvaluations += 1;
     double v[1] = {energyPartial(D, alpha)};
     blockSum<1>(v, red);
     if (threadIdx.x == 0) D.partials[blockIdx.x * kPartialStride] = red[0];

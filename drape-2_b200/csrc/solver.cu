@@ -28,6 +28,15 @@ void check(cudaError_t e, const char* what) {
 }
 #define CK(x) check((x), #x)
 
+// Host -> device byte counter of the solver whose public call is running on this thread (see CountTransfers).
+thread_local uint64_t* g_h2d = nullptr;
+
+struct CountTransfers {
+  uint64_t* prev;
+  explicit CountTransfers(uint64_t* c) : prev(g_h2d) { g_h2d = c; }
+  ~CountTransfers() { g_h2d = prev; }
+};
+
 template <class T>
 struct DBuf {
   T* p = nullptr;
@@ -48,13 +57,11 @@ struct DBuf {
     CK(cudaMemset(p, 0, sizeof(T) * std::max<size_t>(count, 1)));
   }
   void upload(const T* src, size_t count, cudaStream_t s) {
-    if (count > n) alloc(count);
+    if (count > n || !p) alloc(count);
     if (count) CK(cudaMemcpyAsync(p, src, sizeof(T) * count, cudaMemcpyHostToDevice, s));
+    if (g_h2d) *g_h2d += sizeof(T) * count;
   }
-  void upload(const std::vector<T>& v, cudaStream_t s) {
-    if (v.size() > n || !p) alloc(v.size());
-    if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice, s));
-  }
+  void upload(const std::vector<T>& v, cudaStream_t s) { upload(v.data(), v.size(), s); }
 };
 
 template <class T>
@@ -107,7 +114,55 @@ struct drape_solver {
   DBuf<unsigned int> statsDone;
   HostPinned<dcu::Control> hCtl;
   HostPinned<dcu::StatsOut> hStats;
+  DBuf<int> cgLog;
   dcu::Dev dev{};
+  uint64_t h2dBytes = 0, d2hBytes = 0;
+
+  // Kernel timing (drape_cuda_profile): event pairs recorded around launches, folded in after each synchronisation.
+  struct Pending {
+    cudaEvent_t a, b;
+    int kind;
+  };
+  bool profiling = false;
+  std::vector<cudaEvent_t> eventPool;
+  std::vector<Pending> pending;
+  drape_profile prof{};
+
+  cudaEvent_t takeEvent() {
+    if (eventPool.empty()) {
+      cudaEvent_t e;
+      CK(cudaEventCreate(&e));
+      return e;
+    }
+    cudaEvent_t e = eventPool.back();
+    eventPool.pop_back();
+    return e;
+  }
+  // Records a start event when profiling; returns it (or nullptr).
+  cudaEvent_t profStart() {
+    if (!profiling) return nullptr;
+    cudaEvent_t a = takeEvent();
+    CK(cudaEventRecord(a, stream));
+    return a;
+  }
+  void profStop(cudaEvent_t a, int kind) {
+    if (!a) return;
+    cudaEvent_t b = takeEvent();
+    CK(cudaEventRecord(b, stream));
+    pending.push_back({a, b, kind});
+  }
+  // After the stream has been synchronised.
+  void collectProfile() {
+    for (const auto& p : pending) {
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, p.a, p.b));
+      prof.launches[p.kind] += 1;
+      prof.milliseconds[p.kind] += ms;
+      eventPool.push_back(p.a);
+      eventPool.push_back(p.b);
+    }
+    pending.clear();
+  }
 
   // ---- setup ----
 
@@ -135,12 +190,18 @@ struct drape_solver {
     statsPartials.alloc(static_cast<size_t>(statsGrid) * 8);
     statsOut.alloc(1);
     statsDone.alloc(1);
+    cgLog.alloc(dcu::kCgLogCapacity);
   }
 
   ~drape_solver() {
     if (stream) {
       cudaSetDevice(device);
       cudaStreamSynchronize(stream);
+      for (const auto& p : pending) {
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+      }
+      for (auto e : eventPool) cudaEventDestroy(e);
       cudaStreamDestroy(stream);
     }
   }
@@ -318,6 +379,7 @@ struct drape_solver {
     d.contact = contact.p;
     d.partials = partials.p;
     d.ctl = ctl.p;
+    d.cgLog = cgLog.p;
     dev = d;
     assembleGrid = static_cast<int>(std::max<uint32_t>(1, std::min<uint32_t>((n + dcu::kAssembleWarps - 1) / dcu::kAssembleWarps,
                                                                            static_cast<uint32_t>(numSMs) * 16)));
@@ -342,6 +404,7 @@ struct drape_solver {
       CK(cudaMemcpyAsync(vs.data(), v.p, sizeof(float4) * n, cudaMemcpyDeviceToHost, stream));
       CK(cudaMemcpyAsync(cs.data(), contact.p, sizeof(dcu::Contact) * n, cudaMemcpyDeviceToHost, stream));
       CK(cudaStreamSynchronize(stream));
+      d2hBytes += (2 * sizeof(float4) + sizeof(dcu::Contact)) * n;
     }
     for (size_t i = 0; i < n; ++i) {
       m.x[i] = {xs[i].x, xs[i].y, xs[i].z};
@@ -399,18 +462,28 @@ struct drape_solver {
     d.P.hD = h;
     d.P.barrierLimitNs = barrierLimitNs;
     const uint32_t n = d.P.n;
-    const int pg = static_cast<int>(std::min<uint32_t>((n + 255) / 256, static_cast<uint32_t>(pointGrid)));
-    dcu::k_begin<<<std::max(pg, 1), 256, 0, stream>>>(d);
+    const int pg = std::max(1, static_cast<int>(std::min<uint32_t>((n + 255) / 256, static_cast<uint32_t>(pointGrid))));
+    cudaEvent_t e = profStart();
+    dcu::k_begin<<<pg, 256, 0, stream>>>(d);
     CK(cudaGetLastError());
+    profStop(e, 0);
     for (int it = 0; it < iterations; ++it) {
-      dcu::k_activate<<<std::max(pg, 1), 256, 0, stream>>>(d);
+      e = profStart();
+      dcu::k_activate<<<pg, 256, 0, stream>>>(d);
+      profStop(e, 1);
+      e = profStart();
       dcu::k_assemble<<<assembleGrid, dcu::kAssembleWarps * dcu::kWarp, 0, stream>>>(d);
       CK(cudaGetLastError());
+      profStop(e, 2);
+      e = profStart();
       launchSolve(d);
+      profStop(e, 3);
     }
-    dcu::k_finish<<<std::max(pg, 1), 256, 0, stream>>>(d);
+    e = profStart();
+    dcu::k_finish<<<pg, 256, 0, stream>>>(d);
     dcu::k_advance_clock<<<1, 32, 0, stream>>>(d);
     CK(cudaGetLastError());
+    profStop(e, 4);
     for (auto& g : m.garments)
       if (g.phase == DRAPE_PHASE_ASSEMBLING) g.assemblyTime += h;
   }
@@ -418,6 +491,8 @@ struct drape_solver {
   void readControl() {
     CK(cudaMemcpyAsync(hCtl.p, ctl.p, sizeof(dcu::Control), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
+    d2hBytes += sizeof(dcu::Control);
+    collectProfile();
     if (hCtl.p->error != 0) {
       const int e = hCtl.p->error;
       resetControlAfterError();
@@ -444,10 +519,14 @@ struct drape_solver {
     use();
     drape_stats st{};
     if (m.x.empty()) return st;
+    cudaEvent_t e = profStart();
     dcu::k_stats<<<statsGrid, 256, 0, stream>>>(dev, statsPartials.p, statsDone.p, statsOut.p);
     CK(cudaGetLastError());
+    profStop(e, 5);
     CK(cudaMemcpyAsync(hStats.p, statsOut.p, sizeof(dcu::StatsOut), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
+    d2hBytes += sizeof(dcu::StatsOut);
+    collectProfile();
     const dcu::StatsOut& s = *hStats.p;
     st.has_non_finite = s.nonFinite;
     st.kinetic_energy = s.kineticEnergy;
@@ -474,7 +553,7 @@ struct drape_solver {
     CK(cudaMemcpyAsync(hCtl.p, ctl.p, sizeof(dcu::Control), cudaMemcpyDeviceToHost, stream));
     CK(cudaStreamSynchronize(stream));
     dcu::Control c = *hCtl.p;
-    c.substeps = c.newtonIterations = c.cgIterations = c.lineSearchHalvings = 0;
+    c.substeps = c.newtonIterations = c.cgIterations = c.lineSearchHalvings = c.energyEvaluations = 0;
     *hCtl.p = c;
     CK(cudaMemcpyAsync(ctl.p, hCtl.p, sizeof(dcu::Control), cudaMemcpyHostToDevice, stream));
     CK(cudaStreamSynchronize(stream));
@@ -488,6 +567,7 @@ struct drape_solver {
     if (count) {
       CK(cudaMemcpyAsync(tmp.data(), b.p, sizeof(float4) * count, cudaMemcpyDeviceToHost, stream));
       CK(cudaStreamSynchronize(stream));
+      d2hBytes += sizeof(float4) * count;
     }
     for (size_t i = 0; i < count; ++i) {
       out[3 * i] = tmp[i].x;
@@ -679,6 +759,7 @@ drape_drape_result drapeToRest(drape_solver& s, const std::vector<std::string>& 
 template <class F>
 int guarded(const drape_solver* cs, F&& f) {
   auto* s = const_cast<drape_solver*>(cs);
+  CountTransfers count(s ? &s->h2dBytes : nullptr);
   try {
     f();
     return DRAPE_OK;
@@ -917,6 +998,67 @@ int drape_cuda_reset_counters(drape_solver* s) {
   return guarded(s, [&] {
     need(s);
     s->resetCounters();
+  });
+}
+
+int drape_cuda_cg_history(const drape_solver* cs, int32_t* out, size_t capacity, size_t* count) {
+  return guarded(cs, [&] {
+    need(cs);
+    auto* s = const_cast<drape_solver*>(cs);
+    const drape_counters c = s->counters();
+    const size_t total = static_cast<size_t>(c.newton_iterations);
+    const size_t kept = std::min<size_t>(total, dcu::kCgLogCapacity);
+    const size_t take = std::min(kept, capacity);
+    std::vector<int> all(dcu::kCgLogCapacity);
+    CK(cudaMemcpy(all.data(), s->cgLog.p, sizeof(int) * all.size(), cudaMemcpyDeviceToHost));
+    const size_t first = total - kept;  // oldest kept index
+    for (size_t k = 0; k < take; ++k) out[k] = all[(first + k) % dcu::kCgLogCapacity];
+    *count = take;
+  });
+}
+
+int drape_cuda_stream(const drape_solver* s, void** stream) {
+  return guarded(s, [&] {
+    need(s);
+    *stream = static_cast<void*>(s->stream);
+  });
+}
+
+int drape_cuda_profile(drape_solver* s, int enable) {
+  return guarded(s, [&] {
+    need(s);
+    s->use();
+    CK(cudaStreamSynchronize(s->stream));
+    s->collectProfile();
+    s->profiling = enable != 0;
+    if (s->profiling) {
+      s->prof = drape_profile{};
+      const drape_counters c = s->counters();
+      s->prof.cg_iterations = -c.cg_iterations;  // made relative in drape_cuda_profile_read
+      s->prof.energy_evaluations = -s->hCtl.p->energyEvaluations;
+    }
+  });
+}
+
+int drape_cuda_profile_read(const drape_solver* cs, drape_profile* out) {
+  return guarded(cs, [&] {
+    need(cs);
+    auto* s = const_cast<drape_solver*>(cs);
+    s->use();
+    CK(cudaStreamSynchronize(s->stream));
+    s->collectProfile();
+    const drape_counters c = s->counters();
+    *out = s->prof;
+    out->cg_iterations += c.cg_iterations;
+    out->energy_evaluations += s->hCtl.p->energyEvaluations;
+  });
+}
+
+int drape_cuda_transfer_bytes(const drape_solver* s, uint64_t* h2d, uint64_t* d2h) {
+  return guarded(s, [&] {
+    need(s);
+    *h2d = s->h2dBytes;
+    *d2h = s->d2hBytes;
   });
 }
 

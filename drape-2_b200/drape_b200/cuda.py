@@ -80,8 +80,21 @@ def load(build_if_missing: bool = True):
     L.drape_cuda_set_barrier_limit.argtypes = [C.c_void_p, C.c_uint64]
     L.drape_cuda_test_barrier_timeout.argtypes = [C.c_int, C.c_int, C.c_uint64, _P(C.c_int)]
     L.drape_cuda_inject_failure.argtypes = [C.c_void_p, C.c_int]
+    L.drape_cuda_cg_history.argtypes = [C.c_void_p, _P(_i32), C.c_size_t, _P(C.c_size_t)]
+    L.drape_cuda_stream.argtypes = [C.c_void_p, _P(C.c_void_p)]
+    L.drape_cuda_profile.argtypes = [C.c_void_p, C.c_int]
+    L.drape_cuda_profile_read.argtypes = [C.c_void_p, _P(drape_profile)]
+    L.drape_cuda_transfer_bytes.argtypes = [C.c_void_p, _P(C.c_uint64), _P(C.c_uint64)]
     _lib = L
     return L
+
+
+KERNEL_NAMES = ("k_begin", "k_activate", "k_assemble", "k_solve", "k_finish", "k_stats")
+
+
+class drape_profile(C.Structure):
+    _fields_ = [("launches", C.c_int64 * 6), ("milliseconds", C.c_double * 6), ("cg_iterations", C.c_int64),
+                ("energy_evaluations", C.c_int64)]
 
 
 def _raise(code: int, msg) -> None:
@@ -247,6 +260,32 @@ class CudaSolver:
         blocks, grad, active = np.zeros((B, 3, 3), np.float32), np.zeros((n, 3), np.float32), np.zeros(n, np.uint8)
         self._check(self.L.drape_cuda_capture_system(self.h, h, _p(blocks, _f), _p(grad, _f), _p(active, _u8)))
         return dict(blocks=blocks, grad=grad, active=active, **st)
+
+    def cg_history(self, capacity: int = 1 << 16) -> np.ndarray:
+        out = np.zeros(capacity, np.int32)
+        cnt = C.c_size_t()
+        self._check(self.L.drape_cuda_cg_history(self.h, _p(out, _i32), capacity, C.byref(cnt)))
+        return out[:cnt.value]
+
+    def stream_handle(self) -> int:
+        p = C.c_void_p()
+        self._check(self.L.drape_cuda_stream(self.h, C.byref(p)))
+        return p.value or 0
+
+    def profile(self, enable: bool) -> None:
+        self._check(self.L.drape_cuda_profile(self.h, 1 if enable else 0))
+
+    def profile_read(self) -> dict:
+        p = drape_profile()
+        self._check(self.L.drape_cuda_profile_read(self.h, C.byref(p)))
+        return dict(launches={k: int(p.launches[i]) for i, k in enumerate(KERNEL_NAMES)},
+                    milliseconds={k: float(p.milliseconds[i]) for i, k in enumerate(KERNEL_NAMES)},
+                    cg_iterations=int(p.cg_iterations), energy_evaluations=int(p.energy_evaluations))
+
+    def transfer_bytes(self):
+        a, b = C.c_uint64(), C.c_uint64()
+        self._check(self.L.drape_cuda_transfer_bytes(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def set_barrier_limit(self, nanoseconds: int) -> None:
         self._check(self.L.drape_cuda_set_barrier_limit(self.h, int(nanoseconds)))

@@ -145,12 +145,12 @@ class Fabric:
         return drape_fabric(*[float(getattr(self, f[0])) for f in drape_fabric._fields_])
 
 
-def test_jersey() -> Fabric:
+def jersey_fabric() -> Fabric:
     """The reference's jersey test fabric (libs/core/src/test_fabrics.cpp:5)."""
     return Fabric(400, 200, 100, 0.5, 0.8, 2e-6, 1.5e-6, 0.160, 0.0006, 0.3, 0.3)
 
 
-def test_stiff() -> Fabric:
+def stiff_fabric() -> Fabric:
     """libs/core/src/test_fabrics.cpp:7."""
     return Fabric(20000, 20000, 5000, 0.02, 0.02, 100e-6, 100e-6, 0.450, 0.0008, 0.3, 1.0)
 

@@ -22,7 +22,7 @@ from typing import List, Optional, Sequence
 
 import numpy as np
 
-from .scene import Fabric, Field, Garment, Scene, Settings, test_jersey
+from .scene import Fabric, Field, Garment, Scene, Settings, jersey_fabric
 
 
 # ---------------------------------------------------------------------------------------------------------------
@@ -152,33 +152,34 @@ def sphere_field(radius=0.15, center=(0.0, 0.0, 0.0), cell=0.004, pad=0.05, band
     return sampled_field(sphere_sdf(center, radius), lo, cell, (n, n, n), band)
 
 
-TORSO_BOTTOM = (0.0, 0.0, 0.0)
-TORSO_TOP = (0.0, 0.6, 0.0)
+TORSO_HALF = 0.3        # torso capsule: segment of 0.6 m along z, centred at the origin
 TORSO_RADIUS = 0.15
 ARM_RADIUS = 0.05
-ARM_ROOT_Y = 0.5
 ARM_LENGTH = 0.45
 
 
 def capsule_union_sdf(torso_radius=TORSO_RADIUS, arm_radius=ARM_RADIUS):
-    """Torso capsule (axis y from 0 to 0.6 m, r = 0.15 m) and two arm capsules (r = 0.05 m) leaving the torso at
-    y = 0.5 m and pointing 45 degrees below horizontal along +-x."""
+    """The capsule-union body, lying down: a torso capsule (r = 0.15 m, h = 0.6 m) along z through the origin, and two
+    arm capsules (r = 0.05 m, 0.45 m long) leaving the torso's end points outward along +-z and 45 degrees below
+    horizontal. A garment wrapped around the torso hangs from its top; the arms stand under the garment's open
+    ends."""
     c, s = math.cos(math.radians(45.0)), math.sin(math.radians(45.0))
-    parts = [capsule_sdf(TORSO_BOTTOM, TORSO_TOP, torso_radius)]
+    parts = [capsule_sdf((0.0, 0.0, -TORSO_HALF), (0.0, 0.0, TORSO_HALF), torso_radius)]
     for sign in (1.0, -1.0):
-        root = (sign * 0.10, ARM_ROOT_Y, 0.0)
-        tip = (sign * (0.10 + ARM_LENGTH * c), ARM_ROOT_Y - ARM_LENGTH * s, 0.0)
+        root = (0.0, 0.0, sign * TORSO_HALF)
+        tip = (0.0, -ARM_LENGTH * s, sign * (TORSO_HALF + ARM_LENGTH * c))
         parts.append(capsule_sdf(root, tip, arm_radius))
     return union(*parts)
 
 
-def capsule_union_field(n: int = 128, cell: float = 0.004, band: float = 0.02, torso_radius=TORSO_RADIUS,
+def capsule_union_field(n: int = 128, cell: float = 0.006, band: float = 0.02, torso_radius=TORSO_RADIUS,
                         arm_radius=ARM_RADIUS) -> Field:
-    """The capsule union sampled on an n^3 grid. n * cell is about 0.51 m, less than the 0.9 m torso, so the grid is
-    placed over the part the garment touches: x, z centred on the torso axis, y from -0.05 m (the arms cross the tube
-    at about y = 0.39 m). Outside the grid the field is +band (no contact), as in collision_field.cpp:15."""
+    """The capsule union sampled on an n^3 grid centred on the torso (y shifted down by a quarter span, where the
+    garment hangs). The grid must hold the 0.7 m garment: a 128^3 grid at the workload's nominal 4 mm spans only
+    0.508 m, so the sample count is kept and the spacing widened (6 mm for 128^3, 3 mm for 256^3). Outside the grid
+    the field is +band (no contact), as in collision_field.cpp:15."""
     span = (n - 1) * cell
-    origin = (-0.5 * span, -0.05, -0.5 * span)
+    origin = (-0.5 * span, 0.16 - span, -0.5 * span)  # top of the grid 1 cm above the torso's top line
     return sampled_field(capsule_union_sdf(torso_radius, arm_radius), origin, cell, (n, n, n), band)
 
 
@@ -204,19 +205,20 @@ def sheet_on_sphere(n: int = 40, size: float = 0.5, height: float = 0.3, jitter:
 
 def tube_fabric(friction: float = 0.4) -> Fabric:
     """Tube fabric: the jersey test fabric with friction mu = 0.4."""
-    f = test_jersey()
+    f = jersey_fabric()
     f.friction = friction
     return f
 
 
-def seamed_tube(nx: int = 63, ny: int = 80, width: float = 0.55, height: float = 0.7, radius: float = 0.21,
-                top: float = 0.44, friction: float = 0.4, field: Optional[Field] = None, field_n: int = 128,
-                field_cell: float = 0.004, torso_radius=TORSO_RADIUS, arm_radius=ARM_RADIUS,
+def seamed_tube(nx: int = 63, ny: int = 80, width: float = 0.55, height: float = 0.7, radius: float = 0.20,
+                friction: float = 0.4, field: Optional[Field] = None, field_n: int = 128,
+                field_cell: float = 0.006, torso_radius=TORSO_RADIUS, arm_radius=ARM_RADIUS,
                 settings: Optional[Settings] = None, gid: str = "tube") -> Scene:
-    """Two panels (front, back) wrapped on a cylinder of the given radius around the torso axis, sewn along both side
-    edges. The panel placement follows the reference's cylinder placement (libs/garment/src/placement.cpp:35-41):
-    theta = centre + x / R, axial = y. At R = 0.21 m the side gaps are ~0.11 m, wider than the arms (0.10 m), so
-    the arms pass through the open seams; assembly closes the seams around them."""
+    """Two panels (upper, lower) wrapped on a cylinder of the given radius around the torso's axis (z), sewn along
+    both side edges (the 0.7 m edges, which run along the axis). The placement follows the reference's cylinder
+    placement (libs/garment/src/placement.cpp:35-41): theta = centre + x / R, axial = y. At R = 0.2 m the open seams
+    leave ~8 cm gaps at the sides; Assembling closes them into a 1.1 m-round sleeve, looser than the torso, which then
+    hangs from the torso's top under gravity."""
     rest1, tris1, va1, b1 = grid_piece(width, height, nx, ny)
     V = rest1.shape[0]
     rest = np.concatenate([rest1, rest1])
@@ -242,8 +244,8 @@ def seamed_tube(nx: int = 63, ny: int = 80, width: float = 0.55, height: float =
         sl = slice(piece * V, (piece + 1) * V)
         theta = centre + (rest[sl, 0] - width / 2) / radius
         x[sl, 0] = radius * np.sin(theta)
-        x[sl, 1] = top - height + rest[sl, 1]
-        x[sl, 2] = radius * np.cos(theta)
+        x[sl, 1] = radius * np.cos(theta)
+        x[sl, 2] = rest[sl, 1] - height / 2
     fab = tube_fabric(friction)
     g = Garment(gid, rest, vpiece, varea, tris, tpiece, np.array([[0.0, 1.0], [0.0, 1.0]]), [fab, fab], pairs, x,
                 boundary)
@@ -253,11 +255,11 @@ def seamed_tube(nx: int = 63, ny: int = 80, width: float = 0.55, height: float =
 
 
 def tube_10k(**kw) -> Scene:
-    return seamed_tube(63, 80, field_n=128, field_cell=0.004, **kw)
+    return seamed_tube(63, 80, field_n=128, field_cell=0.006, **kw)
 
 
 def tube_60k(**kw) -> Scene:
-    return seamed_tube(154, 195, field_n=256, field_cell=0.002, **kw)
+    return seamed_tube(154, 195, field_n=256, field_cell=0.003, **kw)
 
 
 def tube_variant(seed: int, n_particles: int, field_n: int = 128) -> Scene:
@@ -270,8 +272,8 @@ def tube_variant(seed: int, n_particles: int, field_n: int = 128) -> Scene:
     per_panel = n_particles / 2
     nx = max(4, int(round(math.sqrt(per_panel * w / h))))
     ny = max(4, int(round(per_panel / nx)))
-    radius = tr + 0.06
-    cell = 0.51 / (field_n - 1)
+    radius = tr + 0.05
+    cell = 0.762 / (field_n - 1)
     return seamed_tube(nx, ny, width=w, height=h, radius=radius, field_n=field_n, field_cell=cell, torso_radius=tr,
                        arm_radius=ar, gid=f"tube{seed}")
 
@@ -283,7 +285,7 @@ def strip_scene(grain=(1.0, 0.0), fabric: Optional[Fabric] = None, h: float = 0.
     """Strip 0.2 x 0.05 m pinned at x = 0 and pulled along +x with 0.5 N in total at x = 0.2, no gravity
     (libs/sim/tests/test_cpu_solver.cpp:30-53)."""
     if fabric is None:
-        fabric = test_jersey()
+        fabric = jersey_fabric()
         fabric.damping = 1.0
     g = flat_garment("strip", 0.2, 0.05, h, fabric, grain=grain)
     scene = Scene([g], settings=Settings(gravity=(0.0, 0.0, 0.0)))
@@ -312,7 +314,7 @@ def measured_strain(x: np.ndarray, rest: np.ndarray) -> float:
 def hanging_sheet() -> Scene:
     """0.5 x 0.5 m jersey sheet (h = 1 cm) in the XY plane pinned at its two top corners
     (libs/sim/tests/sim_test_utils.hpp:52-80)."""
-    g = piece_garment("sheet", 0.5, 0.5, 51, 51, test_jersey())
+    g = piece_garment("sheet", 0.5, 0.5, 51, 51, jersey_fabric())
     g.initial_positions = np.stack([g.rest[:, 0], 0.5 + g.rest[:, 1], np.zeros(g.vertex_count)], axis=1)
     scene = Scene([g])
     for corner in ((0.0, 0.5), (0.5, 0.5)):
@@ -323,7 +325,7 @@ def hanging_sheet() -> Scene:
 
 def centred_sheet(size: float, h: float, height: float, fabric: Optional[Fabric] = None) -> Garment:
     """libs/sim/tests/sphere_scene.hpp:24-27."""
-    return flat_garment("sheet", size, size, h, fabric or test_jersey(), (-size / 2, height, -size / 2))
+    return flat_garment("sheet", size, size, h, fabric or jersey_fabric(), (-size / 2, height, -size / 2))
 
 
 K_CONTACT = 0.003 + 0.0006 / 2  # collision offset + half the jersey thickness (sphere_scene.hpp:21)
@@ -332,7 +334,7 @@ K_CONTACT = 0.003 + 0.0006 / 2  # collision offset + half the jersey thickness (
 def sewn_pair(w=0.05, hgt=0.05, gap=0.1, h=0.01, fabric: Optional[Fabric] = None) -> Garment:
     """Two w x hgt squares in the XZ plane, the second shifted by gap beyond the first's right edge, sewn
     first.right <-> second.left (libs/sim/tests/test_seams.cpp:12-29)."""
-    fabric = fabric or test_jersey()
+    fabric = fabric or jersey_fabric()
     nx = int(round(w / h)) + 1
     ny = int(round(hgt / h)) + 1
     rest1, tris1, va1, b1 = grid_piece(w, hgt, nx, ny)
@@ -368,7 +370,7 @@ def slope_scene(friction: float, angle_deg: float = 20.0):
     lo = np.array([-0.1, -0.1, -0.1])
     n = int(math.ceil(0.2 / cell)) + 1
     field = sampled_field(sdf, lo, cell, (n, n, n), 0.02)
-    f = test_jersey()
+    f = jersey_fabric()
     f.friction = friction
     g = flat_garment("patch", 0.02, 0.02, 0.01, f)
     r = g.rest - 0.01

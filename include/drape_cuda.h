@@ -104,6 +104,29 @@ int drape_cuda_drape_to_rest(drape_solver* s, const char* const* garments, uint3
 int drape_cuda_counters(const drape_solver* s, drape_counters* out);
 int drape_cuda_reset_counters(drape_solver* s);
 
+/* PCG iterations of each Newton iteration since the last reset, oldest first (at most `capacity`; *count gets the
+   number written). */
+int drape_cuda_cg_history(const drape_solver* s, int32_t* out, size_t capacity, size_t* count);
+
+/* The CUDA stream (a cudaStream_t) all of this solver's work runs on, for callers that time it with events. */
+int drape_cuda_stream(const drape_solver* s, void** stream);
+
+/* Kernel timing: with profiling on, every launch is bracketed by CUDA events on the solver's stream and its device
+   time accumulated per kernel: [0] begin (predict + contact setup), [1] activate, [2] assemble, [3] solve
+   (persistent PCG + line search), [4] finish, [5] stats. */
+enum { DRAPE_KERNEL_COUNT = 6 };
+typedef struct drape_profile {
+  int64_t launches[DRAPE_KERNEL_COUNT];
+  double milliseconds[DRAPE_KERNEL_COUNT];
+  int64_t cg_iterations;        /* PCG iterations inside the profiled solve launches */
+  int64_t energy_evaluations;   /* FP64 energy passes (E(0) and every line-search trial) */
+} drape_profile;
+int drape_cuda_profile(drape_solver* s, int enable); /* enabling also clears the accumulated figures */
+int drape_cuda_profile_read(const drape_solver* s, drape_profile* out);
+
+/* Bytes copied host -> device and device -> host by this solver since creation. */
+int drape_cuda_transfer_bytes(const drape_solver* s, uint64_t* h2d, uint64_t* d2h);
+
 /* Block-CSR structure and term lists as built (the bit-exact artefacts of sim_model.cpp:41-175). sizes: [0] particles,
    [1] block slots, [2] stretch terms, [3] hinges, [4] seam springs. Pointers may be NULL. */
 int drape_cuda_structure_sizes(const drape_solver* s, uint32_t sizes[5]);
