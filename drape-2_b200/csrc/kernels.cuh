@@ -12,7 +12,7 @@
 //                line search and step application (cpu_solver.cpp:264-283) with device-side decisions.
 #pragma once
 
-#include <cooperative_groups.h>
+#include <cuda/atomic>
 #include <cstdint>
 
 #include "device_math.cuh"
@@ -21,10 +21,11 @@ namespace dcu {
 
 constexpr int kWarp = 32;
 constexpr int kAssembleWarps = 8;   // warps per k_assemble block
-constexpr int kRowLanes = 8;        // lanes per block row in the SpMV
-constexpr int kSolveThreads = 512;  // k_solve block size
+constexpr int kRowLanes = 4;        // lanes per block row in the SpMV
+constexpr int kSolveThreads = 1024; // k_solve block size (one block per SM)
 constexpr uint32_t kPinnedBit = 0x80000000u;
 constexpr int kPartialStride = 4;   // doubles per block in the partials array
+constexpr uint32_t kMaxRowSlots = 64;  // block slots per row the assembly kernel accumulates (checked at build)
 
 struct Particle {
   float mass;
@@ -72,7 +73,7 @@ struct Garment {
 struct Control {
   int newtonDone;   // this substep's Newton loop has stopped (slope >= 0 or max move < 1e-9)
   int error;        // 1: a grid barrier gave up waiting; 2: a row exceeded the assembly capacity
-  unsigned int barrierCount, barrierGeneration;
+  unsigned long long barrierArrivals;
   long long cgIterations, newtonIterations, lineSearchHalvings, substeps, energyEvaluations;
   double lastAlpha, lastSlope, lastE0, lastMaxMove;
   int lastCg;
@@ -105,6 +106,7 @@ struct Dev {
   const Seam* seam;
   const uint32_t* rowStart;
   const uint32_t* colIndex;  // bit 31: the column's particle is pinned
+  const uint32_t* diagSlot;
   const uint32_t* incStart;
   const uint32_t* incEntry;
   const uint32_t* incLocal;
@@ -120,8 +122,16 @@ struct Dev {
 };
 
 // ---------------------------------------------------------------------------------------------------------------
-// Grid barrier with a bounded wait (cooperative launch guarantees co-residency; the bound turns a lost block into an
-// error status instead of a hang).
+// Grid-wide synchronisation for the cooperative persistent kernels (cooperative launch guarantees co-residency).
+//
+// Arrivals only ever increase: a launch's k-th barrier completes when the counter reaches base + k * gridDim.x, base
+// being the counter at the launch's start rounded down to a multiple of gridDim.x (no barrier can complete before
+// every block has arrived, so a block that reads the counter late still rounds to the same base). Thread 0 adds its
+// block's arrival with release semantics after publishing the block's partial sums and polls with acquire loads; a
+// time limit turns a lost block into an error status and a return instead of a hang.
+//
+// Reductions alternate between two halves of the partials array, so a block that has already passed a barrier and
+// publishes its next partial cannot overwrite values a slower block is still summing.
 
 __device__ __forceinline__ unsigned long long globalTimerNs() {
   unsigned long long t;
@@ -129,43 +139,56 @@ __device__ __forceinline__ unsigned long long globalTimerNs() {
   return t;
 }
 
-__device__ inline bool gridBarrier(Control* ctl, unsigned long long limitNs) {
-  __shared__ int ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    volatile unsigned int* gen = &ctl->barrierGeneration;
-    volatile int* err = &ctl->error;
-    const unsigned int g0 = *gen;
-    __threadfence();
-    const unsigned int arrived = atomicAdd(&ctl->barrierCount, 1u) + 1u;
-    ok = 1;
-    if (arrived == gridDim.x) {
-      atomicExch(&ctl->barrierCount, 0u);
-      __threadfence();
-      atomicAdd(&ctl->barrierGeneration, 1u);
-    } else {
-      const unsigned long long start = globalTimerNs();
-      unsigned int spins = 0;
-      while (*gen == g0) {
-        if (*err != 0) {
-          ok = 0;
-          break;
-        }
-        if ((++spins & 63u) == 0 && globalTimerNs() - start > limitNs) {
-          atomicExch(&ctl->error, 1);
-          ok = 0;
-          break;
-        }
-        __nanosleep(64);
-      }
-    }
-    __threadfence();
-  }
-  __syncthreads();
-  return ok != 0;
-}
+struct GridSync {
+  Control* ctl;
+  unsigned long long target, limitNs;
+  unsigned int parity;
 
-// Block-wide FP64 sum of up to kPartialStride values; thread 0 gets the result. Fixed tree shape -> deterministic.
+  __device__ void init(Control* c, unsigned long long lim) {
+    __shared__ unsigned long long base;
+    if (threadIdx.x == 0) {
+      cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> a(c->barrierArrivals);
+      const unsigned long long now = a.load(cuda::memory_order_relaxed);
+      base = now - now % gridDim.x;
+    }
+    __syncthreads();
+    ctl = c;
+    target = base;
+    limitNs = lim;
+    parity = 0;
+  }
+
+  __device__ bool sync() {
+    __shared__ int ok;
+    target += gridDim.x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> a(ctl->barrierArrivals);
+      a.fetch_add(1ull, cuda::memory_order_release);
+      int good = 1;
+      unsigned int spins = 0;
+      const unsigned long long start = globalTimerNs();
+      while (a.load(cuda::memory_order_acquire) < target) {
+        if ((++spins & 31u) == 0) {
+          if (*reinterpret_cast<volatile int*>(&ctl->error) != 0) {
+            good = 0;
+            break;
+          }
+          if (globalTimerNs() - start > limitNs) {
+            atomicExch(&ctl->error, 1);
+            good = 0;
+            break;
+          }
+        }
+      }
+      ok = good;
+    }
+    __syncthreads();
+    return ok != 0;
+  }
+};
+
+// Block-wide FP64 sums; thread 0 gets the result. Fixed tree shape, so deterministic.
 template <int K>
 __device__ inline void blockSum(double (&v)[K], double* out) {
   __shared__ double red[K][32];
@@ -190,42 +213,73 @@ __device__ inline void blockSum(double (&v)[K], double* out) {
   }
 }
 
-// Sums column k of the per-block partials over the grid, identically in every block; result broadcast to all threads.
-template <int K>
-__device__ inline void gridTotals(const double* partials, double (&out)[K]) {
+// Grid-wide FP64 sums (or maxima): every block publishes its block total, passes the barrier, then warp 0 of every
+// block combines all blocks' totals in the same fixed order, so every block obtains bit-identical results and takes
+// the same branches. Returns false when the barrier gave up.
+template <int K, bool Max = false>
+__device__ inline bool gridReduce(const Dev& D, GridSync& gs, double (&v)[K], double (&out)[K]) {
   __shared__ double res[K];
-  double v[K];
+  double* half = D.partials + static_cast<size_t>(gs.parity) * gridDim.x * kPartialStride;
+  gs.parity ^= 1u;
+  if (Max) {
+    __shared__ double mred[K][32];
 #pragma unroll
-  for (int k = 0; k < K; ++k) v[k] = 0.0;
-  for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+    for (int k = 0; k < K; ++k)
 #pragma unroll
-    for (int k = 0; k < K; ++k) v[k] += __ldcg(partials + b * kPartialStride + k);
-  blockSum<K>(v, res);
+      for (int o = 16; o > 0; o >>= 1) v[k] = fmax(v[k], __shfl_down_sync(0xffffffffu, v[k], o));
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0)
+#pragma unroll
+      for (int k = 0; k < K; ++k) mred[k][threadIdx.x >> 5] = v[k];
+    __syncthreads();
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        double m = mred[k][0];
+        for (int w = 1; w < static_cast<int>((blockDim.x + 31) >> 5); ++w) m = fmax(m, mred[k][w]);
+        half[blockIdx.x * kPartialStride + k] = m;
+      }
+  } else {
+    double blk[K];
+    blockSum<K>(v, blk);
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int k = 0; k < K; ++k) half[blockIdx.x * kPartialStride + k] = blk[k];
+  }
+  if (!gs.sync()) return false;
+  if (threadIdx.x < 32) {
+    double s[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) s[k] = Max ? -INFINITY : 0.0;
+    for (unsigned int b = threadIdx.x; b < gridDim.x; b += 32)
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const double x = __ldcg(half + b * kPartialStride + k);
+        s[k] = Max ? fmax(s[k], x) : s[k] + x;
+      }
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double y = __shfl_xor_sync(0xffffffffu, s[k], o);
+        s[k] = Max ? fmax(s[k], y) : s[k] + y;
+      }
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int k = 0; k < K; ++k) res[k] = s[k];
+  }
   __syncthreads();
 #pragma unroll
   for (int k = 0; k < K; ++k) out[k] = res[k];
-  __syncthreads();
+  return true;
 }
 
-__device__ inline double gridMax(const double* partials, int k) {
-  __shared__ double red[32];
-  __shared__ double res;
-  double v = 0.0;
-  for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x) v = fmax(v, __ldcg(partials + b * kPartialStride + k));
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-  __syncthreads();
-  if (lane == 0) red[w] = v;
-  __syncthreads();
-  if (w == 0) {
-    double s = lane < nw ? red[lane] : 0.0;
-    for (int o = 16; o > 0; o >>= 1) s = fmax(s, __shfl_down_sync(0xffffffffu, s, o));
-    if (lane == 0) res = s;
-  }
-  __syncthreads();
-  const double out = res;
-  __syncthreads();
-  return out;
+// This block's contiguous share of [0, n): the persistent kernels give each block one range of rows, so the
+// neighbour gathers of the SpMV mostly hit rows the same block (hence the same SM's L1) just touched.
+__device__ __forceinline__ void blockRange(uint32_t n, uint32_t& r0, uint32_t& r1) {
+  const uint32_t per = (n + gridDim.x - 1) / gridDim.x;
+  r0 = min(n, blockIdx.x * per);
+  r1 = min(n, r0 + per);
 }
 
 __device__ __forceinline__ float3 filterContact(const Contact& c, float3 v) {
@@ -325,15 +379,18 @@ __global__ void k_activate(Dev D) {
 
 // ---------------------------------------------------------------------------------------------------------------
 // Owner-computes assembly: one warp per block row i. Each lane evaluates one incident term (kind, id, local vertex a)
-// for vertex a only (its gradient and Hessian row), stages the N blocks in shared memory with their row-local slot,
-// and the lane owning each slot sums the staged blocks in incidence-list order, after the particle's own inertia and
-// friction term: the reference's fixed gather order (gpu_solver_core.cpp:184-224), with no atomics.
+// for vertex a only (its gradient and Hessian row) and stages the N blocks in shared memory with their row-local
+// slots. The warp then adds the staged blocks into the row's slot accumulators one entry at a time, in incidence-list
+// order, after the particle's own inertia and friction term: the reference's fixed gather order
+// (gpu_solver_core.cpp:184-224), deterministic and without atomics.
 
-struct AssembleShared {
-  float blk[kAssembleWarps][kWarp][4][9];
-  uint8_t tgt[kAssembleWarps][kWarp][4];
-  float g[kAssembleWarps][kWarp][3];
+struct AssembleWarp {
+  float blk[kWarp][4][9];        // staged Hessian-row blocks of up to 32 entries
+  float g[kWarp][3];             // staged gradient of vertex a
+  uint8_t tgt[kWarp][4];         // row-local slot of each staged block (0xFF: none)
+  float acc[kMaxRowSlots][9];    // the row's block accumulators
 };
+constexpr size_t kAssembleSmem = sizeof(AssembleWarp) * kAssembleWarps;
 
 __device__ inline float3 relPos(const Dev& D, uint32_t v0, uint32_t vk) {
   return (ld3(D.xStart, vk) - ld3(D.xStart, v0)) + ld3(D.u, vk);
@@ -381,11 +438,14 @@ __device__ inline int evalEntry(const Dev& D, uint32_t code, float3& g, M3 H[4])
 
 __global__ void __launch_bounds__(kAssembleWarps * kWarp) k_assemble(Dev D) {
   if (D.ctl->newtonDone) return;
-  __shared__ AssembleShared sh;
+  extern __shared__ __align__(16) unsigned char assembleSmem[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  AssembleWarp& sh = reinterpret_cast<AssembleWarp*>(assembleSmem)[w];
   const uint32_t warpsTotal = gridDim.x * kAssembleWarps;
+  const uint32_t SP = D.P.slotsPadded;
   for (uint32_t i = blockIdx.x * kAssembleWarps + w; i < D.P.n; i += warpsTotal) {
     const uint32_t rs = D.rowStart[i], L = D.rowStart[i + 1] - rs;
+    const uint32_t diagLocal = D.diagSlot[i] - rs;
     const Particle pa = D.particle[i];
     const Contact c = D.contact[i];
     // The particle's own term: inertia 1/2 (m/h^2)|u - yRel|^2 and friction (kernels.h:104-129).
@@ -400,23 +460,21 @@ __global__ void __launch_bounds__(kAssembleWarps * kWarp) k_assemble(Dev D) {
     if (c.frictionLambda > 0.0f)
       frictionRow(ld3(D.u, i), xyz(c.normal), D.fabric[pa.fabric].friction * c.frictionLambda,
                   D.P.frictionSlip * D.P.h, gOwn, hOwn);
-    // Slot accumulators: lane owns row-local slots lane and lane + 32.
-    float acc0[9], acc1[9];
+    for (uint32_t k = lane; k < 9u * L; k += kWarp) (&sh.acc[0][0])[k] = 0.0f;
+    __syncwarp();
+    if (lane < 9) {
+      float own = 0.0f;
 #pragma unroll
-    for (int k = 0; k < 9; ++k) acc0[k] = acc1[k] = 0.0f;
-    uint32_t diagLocal = 0;
-    for (uint32_t s = 0; s < L; ++s)
-      if ((D.colIndex[rs + s] & ~kPinnedBit) == i) diagLocal = s;
-    if (diagLocal == static_cast<uint32_t>(lane))
-#pragma unroll
-      for (int k = 0; k < 9; ++k) acc0[k] = hOwn.m[k];
-    if (diagLocal == static_cast<uint32_t>(lane) + 32u)
-#pragma unroll
-      for (int k = 0; k < 9; ++k) acc1[k] = hOwn.m[k];
-    float3 gAcc = gOwn;
+      for (int k = 0; k < 9; ++k)
+        if (k == lane) own = hOwn.m[k];
+      sh.acc[diagLocal][lane] = own;
+    }
+    // Lanes 27..29 accumulate the gradient components, starting with the own term.
+    float gAcc = lane == 27 ? gOwn.x : (lane == 28 ? gOwn.y : (lane == 29 ? gOwn.z : 0.0f));
     const uint32_t es = D.incStart[i], ee = D.incStart[i + 1];
     for (uint32_t base = es; base < ee; base += kWarp) {
       const uint32_t cnt = min(static_cast<uint32_t>(kWarp), ee - base);
+      __syncwarp();
       if (static_cast<uint32_t>(lane) < cnt) {
         const uint32_t code = D.incEntry[base + lane];
         const uint32_t local = D.incLocal[base + lane];
@@ -425,64 +483,62 @@ __global__ void __launch_bounds__(kAssembleWarps * kWarp) k_assemble(Dev D) {
         const int N = evalEntry(D, code, g, H);
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
-          sh.tgt[w][lane][b] = b < N ? static_cast<uint8_t>((local >> (8 * b)) & 0xFFu) : 0xFFu;
+          sh.tgt[lane][b] = b < N ? static_cast<uint8_t>((local >> (8 * b)) & 0xFFu) : 0xFFu;
           if (b < N)
 #pragma unroll
-            for (int k = 0; k < 9; ++k) sh.blk[w][lane][b][k] = H[b].m[k];
+            for (int k = 0; k < 9; ++k) sh.blk[lane][b][k] = H[b].m[k];
         }
-        sh.g[w][lane][0] = g.x;
-        sh.g[w][lane][1] = g.y;
-        sh.g[w][lane][2] = g.z;
+        sh.g[lane][0] = g.x;
+        sh.g[lane][1] = g.y;
+        sh.g[lane][2] = g.z;
       }
       __syncwarp();
+      // Entry by entry: lanes 0..26 add blocks 0..2 (block lane / 9, component lane % 9), lanes 0..8 then block 3;
+      // the N slots of one entry are distinct, so no two lanes of one step touch the same accumulator.
+      const int b0 = lane / 9, comp = lane - 9 * (lane / 9);
       for (uint32_t e = 0; e < cnt; ++e) {
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-          const uint32_t t = sh.tgt[w][e][b];
-          if (t == static_cast<uint32_t>(lane)) {
-#pragma unroll
-            for (int k = 0; k < 9; ++k) acc0[k] += sh.blk[w][e][b][k];
-          } else if (t == static_cast<uint32_t>(lane) + 32u) {
-#pragma unroll
-            for (int k = 0; k < 9; ++k) acc1[k] += sh.blk[w][e][b][k];
-          }
+        if (lane < 27) {
+          const uint32_t t = sh.tgt[e][b0];
+          if (t != 0xFFu) sh.acc[t][comp] += sh.blk[e][b0][comp];
+        } else if (lane < 30) {
+          gAcc += sh.g[e][lane - 27];
         }
-        gAcc += mk(sh.g[w][e][0], sh.g[w][e][1], sh.g[w][e][2]);
+        if (lane < 9) {
+          const uint32_t t = sh.tgt[e][3];
+          if (t != 0xFFu) sh.acc[t][lane] += sh.blk[e][3][lane];
+        }
+        __syncwarp();
       }
-      __syncwarp();
     }
+    __syncwarp();
     // Blocks out (coalesced planes).
-    const uint32_t SP = D.P.slotsPadded;
-    if (static_cast<uint32_t>(lane) < L)
+    for (uint32_t k = lane; k < L; k += kWarp)
 #pragma unroll
-      for (int k = 0; k < 9; ++k) D.blocks[k * SP + rs + lane] = acc0[k];
-    if (static_cast<uint32_t>(lane) + 32u < L)
-#pragma unroll
-      for (int k = 0; k < 9; ++k) D.blocks[k * SP + rs + lane + 32] = acc1[k];
-    // Diagonal owner: block-Jacobi inverse (kernels.h:237-249).
-    const bool ownDiag0 = diagLocal == static_cast<uint32_t>(lane);
-    const bool ownDiag1 = diagLocal == static_cast<uint32_t>(lane) + 32u;
-    if (ownDiag0 || ownDiag1) {
-      M3 A;
-#pragma unroll
-      for (int k = 0; k < 9; ++k) A.m[k] = ownDiag0 ? acc0[k] : acc1[k];
+      for (int cc = 0; cc < 9; ++cc) D.blocks[cc * SP + rs + k] = sh.acc[k][cc];
+    const float gx = __shfl_sync(0xffffffffu, gAcc, 27);
+    const float gy = __shfl_sync(0xffffffffu, gAcc, 28);
+    const float gz = __shfl_sync(0xffffffffu, gAcc, 29);
+    if (lane == 0) {
+      // Block-Jacobi inverse of the diagonal block (kernels.h:237-249); zero for pinned particles.
       M3 inv;
       if (pa.pinned != 0u) {
         zero(inv);
       } else {
+        M3 A;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) A.m[k] = sh.acc[diagLocal][k];
         bool ok = false;
         inv = invertSpd(A, ok);
       }
       D.precond[3 * i + 0] = make_float4(inv.m[0], inv.m[1], inv.m[2], 0.0f);
       D.precond[3 * i + 1] = make_float4(inv.m[3], inv.m[4], inv.m[5], 0.0f);
       D.precond[3 * i + 2] = make_float4(inv.m[6], inv.m[7], inv.m[8], 0.0f);
-    }
-    // Gradient (pinned rows zero) and contact release (kernels.h:204-231).
-    if (lane == 0) {
-      const float3 gi = pa.pinned != 0u ? mk(0, 0, 0) : gAcc;
+      // Gradient (pinned rows zero) and contact release (kernels.h:204-231).
+      const float3 gi = pa.pinned != 0u ? mk(0, 0, 0) : mk(gx, gy, gz);
       D.grad[i] = f4(gi);
       if (c.active != 0u && dot(gi, xyz(c.normal)) < 0.0f) D.contact[i].active = 0u;
     }
+    __syncwarp();
   }
 }
 
@@ -533,45 +589,43 @@ __device__ inline double energyPartial(const Dev& D, double alpha) {
 
 // ---------------------------------------------------------------------------------------------------------------
 // Persistent solve: PCG with FP64 dot products, then the Newton line search. Every block computes the same scalars
-// from the same partials, so all blocks take the same branches; two grid barriers per CG iteration (the direction
+// from the same partials, so all blocks take the same branches; two grid reductions per CG iteration (the direction
 // update p = z + beta p is folded into the next SpMV, which rebuilds each neighbour's p from z and the previous p).
+
+__device__ __forceinline__ M3 loadPrecond(const Dev& D, uint32_t i) {
+  const float4 a = D.precond[3 * i], b = D.precond[3 * i + 1], c = D.precond[3 * i + 2];
+  return M3{{a.x, a.y, a.z, b.x, b.y, b.z, c.x, c.y, c.z}};
+}
+
+__device__ __forceinline__ double dotd3(float3 a, float3 b) {
+  return static_cast<double>(a.x) * b.x + static_cast<double>(a.y) * b.y + static_cast<double>(a.z) * b.z;
+}
 
 // Contact-filtered block-Jacobi PCG (cpu_solver.cpp:169-213): writes step, resid; returns the iteration count, or -1
 // when a grid barrier gave up.
-__device__ inline int pcgSolve(const Dev& D) {
-  Control* ctl = D.ctl;
-  const unsigned long long lim = D.P.barrierLimitNs;
+__device__ inline int pcgSolve(const Dev& D, GridSync& gs) {
   const uint32_t n = D.P.n;
-  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
-  __shared__ double red[kPartialStride];
+  uint32_t r0i, r1i;
+  blockRange(n, r0i, r1i);
 
   // CG init (kernels.h:252-268): step = 0, resid = -grad, r = filter(resid), z = filter(M r).
+  double tot[2];
   {
     double v[2] = {0.0, 0.0};
-    for (uint32_t i = tid; i < n; i += stride) {
+    for (uint32_t i = r0i + threadIdx.x; i < r1i; i += blockDim.x) {
       const Contact c = D.contact[i];
       const float3 res = -ld3(D.grad, i);
       const float3 ri = filterContact(c, res);
-      const M3 M = {{D.precond[3 * i].x, D.precond[3 * i].y, D.precond[3 * i].z, D.precond[3 * i + 1].x,
-                     D.precond[3 * i + 1].y, D.precond[3 * i + 1].z, D.precond[3 * i + 2].x, D.precond[3 * i + 2].y,
-                     D.precond[3 * i + 2].z}};
-      const float3 zi = filterContact(c, mul(M, ri));
+      const float3 zi = filterContact(c, mul(loadPrecond(D, i), ri));
       D.step[i] = make_float4(0, 0, 0, 0);
       D.resid[i] = f4(res);
       D.r[i] = f4(ri);
       D.z[i] = f4(zi);
-      v[0] += static_cast<double>(ri.x) * zi.x + static_cast<double>(ri.y) * zi.y + static_cast<double>(ri.z) * zi.z;
-      v[1] += static_cast<double>(ri.x) * ri.x + static_cast<double>(ri.y) * ri.y + static_cast<double>(ri.z) * ri.z;
+      v[0] += dotd3(ri, zi);
+      v[1] += dotd3(ri, ri);
     }
-    blockSum<2>(v, red);
-    if (threadIdx.x == 0) {
-      D.partials[blockIdx.x * kPartialStride + 0] = red[0];
-      D.partials[blockIdx.x * kPartialStride + 1] = red[1];
-    }
+    if (!gridReduce<2>(D, gs, v, tot)) return -1;
   }
-  if (!gridBarrier(ctl, lim)) return -1;
-  double tot[2];
-  gridTotals<2>(D.partials, tot);
   double rz = tot[0];
   const double r0 = sqrt(tot[1]);
   bool done = !(r0 > 0.0);
@@ -581,30 +635,27 @@ __device__ inline int pcgSolve(const Dev& D) {
   int it = 0;
   const int maxCg = D.P.maxCg;
   const uint32_t SP = D.P.slotsPadded;
-  const uint32_t groupsTotal = stride / kRowLanes;
-  const uint32_t gid = tid / kRowLanes;
+  const uint32_t groups = blockDim.x / kRowLanes;
   const int sub = threadIdx.x & (kRowLanes - 1);
-  const unsigned groupMask = 0xFFu << ((threadIdx.x & 31) & ~(kRowLanes - 1));
+  const unsigned groupMask = ((1u << kRowLanes) - 1u) << ((threadIdx.x & 31) & ~(kRowLanes - 1));
   while (!done && it < maxCg) {
     // SpMV with the direction update folded in: p_j = z_j + beta * pPrev_j.
-    double vpap = 0.0;
+    double vpap[1] = {0.0};
     const float fb = static_cast<float>(beta);
     const bool first = it == 0;
-    for (uint32_t i0 = gid * 1u; i0 < n + 0u; i0 += groupsTotal) {
-      const uint32_t i = i0;
-      const uint32_t rs = D.rowStart[i], re = D.rowStart[i + 1];
+    for (uint32_t i = r0i + threadIdx.x / kRowLanes; i < r1i; i += groups) {
+      const uint32_t rs = __ldg(D.rowStart + i), re = __ldg(D.rowStart + i + 1);
       float3 acc = mk(0, 0, 0);
-      const bool rowPinned = D.particle[i].pinned != 0u;
-      if (!rowPinned) {
+      if (D.particle[i].pinned == 0u) {
         for (uint32_t s = rs + sub; s < re; s += kRowLanes) {
           const uint32_t col = __ldg(D.colIndex + s);
           if (col & kPinnedBit) continue;
-          const uint32_t j = col;
-          const float3 zj = ld3(D.z, j);
-          const float3 pj = first ? zj : zj + ld3(pPrev, j) * fb;
-          const float a0 = D.blocks[0 * SP + s], a1 = D.blocks[1 * SP + s], a2 = D.blocks[2 * SP + s];
-          const float a3 = D.blocks[3 * SP + s], a4 = D.blocks[4 * SP + s], a5 = D.blocks[5 * SP + s];
-          const float a6 = D.blocks[6 * SP + s], a7 = D.blocks[7 * SP + s], a8 = D.blocks[8 * SP + s];
+          const float3 zj = ld3(D.z, col);
+          const float3 pj = first ? zj : zj + ld3(pPrev, col) * fb;
+          const float* b = D.blocks + s;
+          const float a0 = __ldg(b), a1 = __ldg(b + SP), a2 = __ldg(b + 2 * SP);
+          const float a3 = __ldg(b + 3 * SP), a4 = __ldg(b + 4 * SP), a5 = __ldg(b + 5 * SP);
+          const float a6 = __ldg(b + 6 * SP), a7 = __ldg(b + 7 * SP), a8 = __ldg(b + 8 * SP);
           acc.x += a0 * pj.x + a1 * pj.y + a2 * pj.z;
           acc.y += a3 * pj.x + a4 * pj.y + a5 * pj.z;
           acc.z += a6 * pj.x + a7 * pj.y + a8 * pj.z;
@@ -623,47 +674,31 @@ __device__ inline int pcgSolve(const Dev& D) {
         const float3 filtered = filterContact(D.contact[i], acc);
         D.apFull[i] = f4(acc);
         D.ap[i] = f4(filtered);
-        vpap += static_cast<double>(pi.x) * filtered.x + static_cast<double>(pi.y) * filtered.y +
-                static_cast<double>(pi.z) * filtered.z;
+        vpap[0] += dotd3(pi, filtered);
       }
     }
-    {
-      double v[1] = {vpap};
-      blockSum<1>(v, red);
-      if (threadIdx.x == 0) D.partials[blockIdx.x * kPartialStride] = red[0];
-    }
-    if (!gridBarrier(ctl, lim)) return -1;
     double pAp[1];
-    gridTotals<1>(D.partials, pAp);
+    if (!gridReduce<1>(D, gs, vpap, pAp)) return -1;
     if (!(pAp[0] > 0.0)) break;
     const double alpha = rz / pAp[0];
     const float fa = static_cast<float>(alpha);
     ++it;
     // Update (kernels.h:304-315) fused with the preconditioner apply (kernels.h:324-332).
     double v[2] = {0.0, 0.0};
-    for (uint32_t i = tid; i < n; i += stride) {
+    for (uint32_t i = r0i + threadIdx.x; i < r1i; i += blockDim.x) {
       const Contact c = D.contact[i];
       const float3 pi = ld3(pCur, i);
       D.step[i] = f4(ld3(D.step, i) + pi * fa);
       const float3 ri = ld3(D.r, i) - ld3(D.ap, i) * fa;
       D.r[i] = f4(ri);
       D.resid[i] = f4(ld3(D.resid, i) - ld3(D.apFull, i) * fa);
-      const M3 M = {{D.precond[3 * i].x, D.precond[3 * i].y, D.precond[3 * i].z, D.precond[3 * i + 1].x,
-                     D.precond[3 * i + 1].y, D.precond[3 * i + 1].z, D.precond[3 * i + 2].x, D.precond[3 * i + 2].y,
-                     D.precond[3 * i + 2].z}};
-      const float3 zi = filterContact(c, mul(M, ri));
+      const float3 zi = filterContact(c, mul(loadPrecond(D, i), ri));
       D.z[i] = f4(zi);
-      v[0] += static_cast<double>(ri.x) * ri.x + static_cast<double>(ri.y) * ri.y + static_cast<double>(ri.z) * ri.z;
-      v[1] += static_cast<double>(ri.x) * zi.x + static_cast<double>(ri.y) * zi.y + static_cast<double>(ri.z) * zi.z;
+      v[0] += dotd3(ri, ri);
+      v[1] += dotd3(ri, zi);
     }
-    blockSum<2>(v, red);
-    if (threadIdx.x == 0) {
-      D.partials[blockIdx.x * kPartialStride + 0] = red[0];
-      D.partials[blockIdx.x * kPartialStride + 1] = red[1];
-    }
-    if (!gridBarrier(ctl, lim)) return -1;
     double t2[2];
-    gridTotals<2>(D.partials, t2);
+    if (!gridReduce<2>(D, gs, v, t2)) return -1;
     if (sqrt(t2[0]) <= D.P.cgTolerance * r0) break;
     beta = t2[1] / rz;
     rz = t2[1];
@@ -674,14 +709,15 @@ __device__ inline int pcgSolve(const Dev& D) {
   return it;
 }
 
-__global__ void __launch_bounds__(kSolveThreads) k_solve(Dev D) {
+__global__ void __launch_bounds__(kSolveThreads, 1) k_solve(Dev D) {
   Control* ctl = D.ctl;
   if (ctl->newtonDone) return;
-  const unsigned long long lim = D.P.barrierLimitNs;
+  GridSync gs;
+  gs.init(ctl, D.P.barrierLimitNs);
   const uint32_t n = D.P.n;
-  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
-  __shared__ double red[kPartialStride];
-  const int it = pcgSolve(D);
+  uint32_t r0i, r1i;
+  blockRange(n, r0i, r1i);
+  const int it = pcgSolve(D, gs);
   if (it < 0) return;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     if (D.cgLog) D.cgLog[static_cast<unsigned long long>(ctl->newtonIterations) % kCgLogCapacity] = it;
@@ -692,25 +728,18 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(Dev D) {
   }
 
   // Contact normal force from the residual (kernels.h:391-396), Newton slope grad . step and E(0), in FP64.
+  double se[2];
   {
     double v[2] = {0.0, 0.0};
-    for (uint32_t i = tid; i < n; i += stride) {
+    for (uint32_t i = r0i + threadIdx.x; i < r1i; i += blockDim.x) {
       const Contact c = D.contact[i];
       const float3 res = ld3(D.resid, i);
       D.contact[i].force = c.active != 0u ? fmaxf(0.0f, -dot(res, xyz(c.normal))) : 0.0f;
-      const float3 g = ld3(D.grad, i), s = ld3(D.step, i);
-      v[0] += static_cast<double>(g.x) * s.x + static_cast<double>(g.y) * s.y + static_cast<double>(g.z) * s.z;
+      v[0] += dotd3(ld3(D.grad, i), ld3(D.step, i));
     }
     v[1] = energyPartial(D, 0.0);
-    blockSum<2>(v, red);
-    if (threadIdx.x == 0) {
-      D.partials[blockIdx.x * kPartialStride + 0] = red[0];
-      D.partials[blockIdx.x * kPartialStride + 1] = red[1];
-    }
+    if (!gridReduce<2>(D, gs, v, se)) return;
   }
-  if (!gridBarrier(ctl, lim)) return;
-  double se[2];
-  gridTotals<2>(D.partials, se);
   const double slope = se[0], e0 = se[1];
   if (!(slope < 0.0)) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -724,44 +753,30 @@ __global__ void __launch_bounds__(kSolveThreads) k_solve(Dev D) {
   for (int ls = 0; ls < 20; ++ls) {
     if (blockIdx.x == 0 && threadIdx.x == 0) ctl->energyEvaluations += 1;
     double v[1] = {energyPartial(D, alpha)};
-    blockSum<1>(v, red);
-    if (threadIdx.x == 0) D.partials[blockIdx.x * kPartialStride] = red[0];
-    if (!gridBarrier(ctl, lim)) return;
     double e[1];
-    gridTotals<1>(D.partials, e);
+    if (!gridReduce<1>(D, gs, v, e)) return;
     if (e[0] <= e0 + 1e-4 * alpha * slope) break;
     alpha *= 0.5;
     if (blockIdx.x == 0 && threadIdx.x == 0) ctl->lineSearchHalvings += 1;
   }
   // Apply the step; max move; the next Newton iteration's friction uses this solve's forces (kernels.h:407-414).
-  {
-    double mv = 0.0;
-    const float fa = static_cast<float>(alpha);
-    for (uint32_t i = tid; i < n; i += stride) {
-      const float3 d = ld3(D.step, i) * fa;
-      D.u[i] = f4(ld3(D.u, i) + d);
-      mv = fmax(mv, static_cast<double>(fmaxf(fabsf(d.x), fmaxf(fabsf(d.y), fabsf(d.z)))));
-      Contact c = D.contact[i];
-      D.contact[i].frictionLambda = c.active != 0u ? c.force : 0.0f;
-    }
-    __shared__ double mred[32];
-    for (int o = 16; o > 0; o >>= 1) mv = fmax(mv, __shfl_down_sync(0xffffffffu, mv, o));
-    if ((threadIdx.x & 31) == 0) mred[threadIdx.x >> 5] = mv;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double m = 0.0;
-      for (int k = 0; k < static_cast<int>((blockDim.x + 31) >> 5); ++k) m = fmax(m, mred[k]);
-      D.partials[blockIdx.x * kPartialStride + 2] = m;
-    }
+  double mv[1] = {0.0};
+  const float fa = static_cast<float>(alpha);
+  for (uint32_t i = r0i + threadIdx.x; i < r1i; i += blockDim.x) {
+    const float3 d = ld3(D.step, i) * fa;
+    D.u[i] = f4(ld3(D.u, i) + d);
+    mv[0] = fmax(mv[0], static_cast<double>(fmaxf(fabsf(d.x), fmaxf(fabsf(d.y), fabsf(d.z)))));
+    const Contact c = D.contact[i];
+    D.contact[i].frictionLambda = c.active != 0u ? c.force : 0.0f;
   }
-  if (!gridBarrier(ctl, lim)) return;
-  const double maxMove = gridMax(D.partials, 2);
+  double maxMove[1];
+  if (!gridReduce<1, true>(D, gs, mv, maxMove)) return;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     ctl->lastAlpha = alpha;
     ctl->lastSlope = slope;
     ctl->lastE0 = e0;
-    ctl->lastMaxMove = maxMove;
-    if (maxMove < 1e-9) ctl->newtonDone = 1;
+    ctl->lastMaxMove = maxMove[0];
+    if (maxMove[0] < 1e-9) ctl->newtonDone = 1;
   }
 }
 
@@ -916,13 +931,15 @@ __global__ void k_pcg_precondition(Dev D, const uint32_t* __restrict__ diag) {
   }
 }
 
-__global__ void __launch_bounds__(kSolveThreads) k_pcg_only(Dev D) {
-  const int it = pcgSolve(D);
+__global__ void __launch_bounds__(kSolveThreads, 1) k_pcg_only(Dev D) {
+  GridSync gs;
+  gs.init(D.ctl, D.P.barrierLimitNs);
+  const int it = pcgSolve(D, gs);
   if (it >= 0 && blockIdx.x == 0 && threadIdx.x == 0) D.ctl->lastCg = it;
 }
 
 // ---------------------------------------------------------------------------------------------------------------
-// Standalone block-CSR SpMV (8 lanes per row), y = A x over unpinned rows and columns.
+// Standalone block-CSR SpMV (kRowLanes lanes per row), y = A x over unpinned rows and columns.
 
 __global__ void k_spmv(uint32_t n, const uint32_t* __restrict__ rowStart, const uint32_t* __restrict__ colIndex,
                        const float* __restrict__ blocks, uint32_t SP, const uint8_t* __restrict__ pinned,
@@ -930,7 +947,7 @@ __global__ void k_spmv(uint32_t n, const uint32_t* __restrict__ rowStart, const 
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
   const uint32_t gid = tid / kRowLanes, groups = stride / kRowLanes;
   const int sub = threadIdx.x & (kRowLanes - 1);
-  const unsigned groupMask = 0xFFu << ((threadIdx.x & 31) & ~(kRowLanes - 1));
+  const unsigned groupMask = ((1u << kRowLanes) - 1u) << ((threadIdx.x & 31) & ~(kRowLanes - 1));
   const uint32_t rounds = (n + groups - 1) / groups;
   for (uint32_t r = 0; r < rounds; ++r) {
     const uint32_t i = gid + r * groups;
@@ -957,27 +974,13 @@ __global__ void k_spmv(uint32_t n, const uint32_t* __restrict__ rowStart, const 
 }
 
 // A barrier that waits for one more block than the grid has: it can only end by its time limit. Used by the test of
-// the bounded wait; returns the error status in *out.
+// the bounded wait; returns the status the blocks read back in *out (1: gave up).
 __global__ void k_barrier_probe(Control* ctl, unsigned long long limitNs, int* out) {
-  __shared__ int ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    volatile unsigned int* gen = &ctl->barrierGeneration;
-    const unsigned int g0 = *gen;
-    atomicAdd(&ctl->barrierCount, 1u);
-    const unsigned long long start = globalTimerNs();
-    ok = 1;
-    while (*gen == g0) {  // nobody releases: gridDim.x + 1 arrivals never happen
-      if (globalTimerNs() - start > limitNs) {
-        atomicExch(&ctl->error, 1);
-        ok = 0;
-        break;
-      }
-      __nanosleep(256);
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x == 0 && blockIdx.x == 0) *out = ok ? 0 : ctl->error;
+  GridSync gs;
+  gs.init(ctl, limitNs);
+  gs.target += 1;  // one arrival that never comes
+  const bool released = gs.sync();
+  if (threadIdx.x == 0 && blockIdx.x == 0) *out = released ? 0 : ctl->error;
 }
 
 }  // namespace dcu

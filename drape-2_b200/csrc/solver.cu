@@ -104,7 +104,7 @@ struct drape_solver {
   DBuf<dcu::Stretch> stretch;
   DBuf<dcu::Hinge> hinge;
   DBuf<dcu::Seam> seam;
-  DBuf<uint32_t> rowStart, colIndex, incStart, incEntry, incLocal;
+  DBuf<uint32_t> rowStart, colIndex, diagSlot, incStart, incEntry, incLocal;
   DBuf<float> fieldValues, blocks;
   DBuf<float4> x, v, xStart, yRel, u, grad, step, r, z, p0, p1, ap, apFull, resid, fExt, pinPos, precond;
   DBuf<dcu::Contact> contact;
@@ -177,16 +177,18 @@ struct drape_solver {
     if (!prop.cooperativeLaunch) throw std::runtime_error("cuda: device does not support cooperative launch");
     numSMs = prop.multiProcessorCount;
     CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    CK(cudaFuncSetAttribute(dcu::k_assemble, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            static_cast<int>(dcu::kAssembleSmem)));
     int perSM = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, dcu::k_solve, dcu::kSolveThreads, 0));
     if (perSM < 1) throw std::runtime_error("cuda: the solve kernel does not fit on an SM");
-    solveGrid = numSMs * std::min(perSM, 2);
+    solveGrid = numSMs;  // one 1024-thread block per SM: fewest barrier arrivals
     pointGrid = numSMs * 8;
     statsGrid = numSMs * 2;
     hCtl.alloc();
     hStats.alloc();
     ctl.alloc(1);
-    partials.alloc(static_cast<size_t>(solveGrid) * dcu::kPartialStride);
+    partials.alloc(2 * static_cast<size_t>(solveGrid) * dcu::kPartialStride);  // two halves, alternating
     statsPartials.alloc(static_cast<size_t>(statsGrid) * 8);
     statsOut.alloc(1);
     statsDone.alloc(1);
@@ -283,6 +285,7 @@ struct drape_solver {
         if (m.pinned[c]) c |= dcu::kPinnedBit;
       colIndex.upload(cols, s);
     }
+    diagSlot.upload(m.diagSlot, s);
     incStart.upload(m.incStart, s);
     incEntry.upload(m.incEntry, s);
     incLocal.upload(m.incLocal, s);
@@ -355,6 +358,7 @@ struct drape_solver {
     d.seam = seam.p;
     d.rowStart = rowStart.p;
     d.colIndex = colIndex.p;
+    d.diagSlot = diagSlot.p;
     d.incStart = incStart.p;
     d.incEntry = incEntry.p;
     d.incLocal = incLocal.p;
@@ -445,7 +449,7 @@ struct drape_solver {
     dcu::Control c{};
     CK(cudaMemcpy(&c, ctl.p, sizeof(c), cudaMemcpyDeviceToHost));
     c.error = 0;
-    c.barrierCount = 0;
+    c.barrierArrivals = 0;
     CK(cudaMemcpy(ctl.p, &c, sizeof(c), cudaMemcpyHostToDevice));
   }
 
@@ -472,7 +476,7 @@ struct drape_solver {
       dcu::k_activate<<<pg, 256, 0, stream>>>(d);
       profStop(e, 1);
       e = profStart();
-      dcu::k_assemble<<<assembleGrid, dcu::kAssembleWarps * dcu::kWarp, 0, stream>>>(d);
+      dcu::k_assemble<<<assembleGrid, dcu::kAssembleWarps * dcu::kWarp, dcu::kAssembleSmem, stream>>>(d);
       CK(cudaGetLastError());
       profStop(e, 2);
       e = profStart();
@@ -1188,7 +1192,7 @@ int drape_cuda_capture_system(drape_solver* s, double h, float* blocks, float* g
     const int pg = std::max<int>(1, static_cast<int>((n + 255) / 256));
     dcu::k_begin<<<pg, 256, 0, s->stream>>>(d);
     dcu::k_activate<<<pg, 256, 0, s->stream>>>(d);
-    dcu::k_assemble<<<s->assembleGrid, dcu::kAssembleWarps * dcu::kWarp, 0, s->stream>>>(d);
+    dcu::k_assemble<<<s->assembleGrid, dcu::kAssembleWarps * dcu::kWarp, dcu::kAssembleSmem, s->stream>>>(d);
     CK(cudaGetLastError());
     const size_t B = s->m.colIndex.size(), SP = s->dev.P.slotsPadded;
     std::vector<float> planes(9 * SP);
