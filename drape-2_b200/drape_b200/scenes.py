@@ -10,9 +10,10 @@ libs/avatar/include/drape/avatar/collision_bake.hpp:10-14).
 Workloads:
   sheet_on_sphere()  square sheet 0.5 m, 40 x 40 vertices jittered +-1 mm from a seed, dropped from 0.3 m onto a
                      sphere r = 0.15 m (1600 particles, 3042 triangles).
-  seamed_tube()      two 0.55 x 0.7 m panels wrapped around a capsule-union body (torso r = 0.15 m, h = 0.6 m; arms
-                     r = 0.05 m at 45 degrees below horizontal), sewn along both side edges; 63 x 80 vertices per
-                     panel (10,080 particles, 128^3 field at 4 mm) or 154 x 195 (60,060 particles, 256^3 at 2 mm).
+  seamed_tube()      two 0.55 x 0.7 m panels sewn along both side edges into a sleeve around a capsule-union body
+                     lying horizontally (torso r = 0.15 m, h = 0.6 m; arms r = 0.05 m at 45 degrees below
+                     horizontal); 63 x 80 vertices per panel (10,080 particles, 128^3 field at 6 mm) or 154 x 195
+                     (60,060 particles, 256^3 field at 3 mm).
   plus the reference's own test scenes restated on grids (strip, hanging sheet, sewn pair, patch on sphere, slope).
 """
 from __future__ import annotations
