@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -1369,3 +1370,163 @@ int drape_cuda_inject_failure(drape_solver* s, int steps) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------------------------
+// drape_cuda_pcg_noalloc: the PCG on caller-owned device buffers with all scratch in one file-scope device array.
+
+namespace {
+
+constexpr uint32_t kNoAllocMaxBlocks = 256;  // partials capacity (grid = one block per SM)
+
+// Byte layout of the scratch array (every region 256-byte aligned).
+struct NoAllocLayout {
+  static constexpr size_t N = DRAPE_PCG_NOALLOC_MAX_PARTICLES, B = DRAPE_PCG_NOALLOC_MAX_SLOTS;
+  static constexpr size_t vectors = 0;                                   // r, z, p0, p1, ap, apFull
+  static constexpr size_t precond = vectors + 6 * sizeof(float4) * N;    // 3 float4 per particle
+  static constexpr size_t particle = precond + 3 * sizeof(float4) * N;
+  static constexpr size_t contact = particle + sizeof(dcu::Particle) * N;
+  static constexpr size_t diag = contact + sizeof(dcu::Contact) * N;
+  static constexpr size_t cols = diag + sizeof(uint32_t) * N;
+  static constexpr size_t partials = cols + sizeof(uint32_t) * B;
+  static constexpr size_t control = partials + 2 * kNoAllocMaxBlocks * dcu::kPartialStride * sizeof(double);
+  static constexpr size_t total = control + 256;
+};
+static_assert(sizeof(dcu::Control) <= 256, "control block fits its region");
+static_assert(NoAllocLayout::total == DRAPE_PCG_NOALLOC_SCRATCH_BYTES, "scratch size matches the header");
+
+// The scratch. In host code this name is a host-side stand-in, not a device address: the address a kernel may use
+// comes from cudaGetSymbolAddress (noAllocScratch() below).
+__device__ __align__(256) unsigned char g_pcgScratch[NoAllocLayout::total];
+
+struct NoAllocDevice {
+  unsigned char* scratch = nullptr;
+  int sms = 0;
+  bool ready = false;
+};
+constexpr int kNoAllocMaxDevices = 64;
+NoAllocDevice g_noAlloc[kNoAllocMaxDevices];
+std::mutex g_noAllocMutex;
+
+// Once per device, with that device current: the device address of the scratch array and the SM count.
+NoAllocDevice& noAllocScratch(int device) {
+  if (device < 0 || device >= kNoAllocMaxDevices) throw std::runtime_error("cuda: device index out of range");
+  std::lock_guard<std::mutex> lock(g_noAllocMutex);
+  NoAllocDevice& d = g_noAlloc[device];
+  if (!d.ready) {
+    void* p = nullptr;
+    CK(cudaGetSymbolAddress(&p, g_pcgScratch));
+    CK(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, device));
+    if (d.sms < 1 || static_cast<uint32_t>(d.sms) > kNoAllocMaxBlocks)
+      throw std::runtime_error("cuda: unsupported SM count for the no-allocation PCG");
+    d.scratch = static_cast<unsigned char*>(p);
+    d.ready = true;
+  }
+  return d;
+}
+
+}  // namespace
+
+namespace dcu {
+
+// Converts the caller's flags into the solver's layouts inside the scratch (particle pinned flags, contact state,
+// columns with the pinned bit, diagonal slots) and clears the control block and the iteration output.
+__global__ void k_noalloc_prepare(uint32_t n, const uint32_t* __restrict__ rowStart,
+                                  const uint32_t* __restrict__ colIndex, const uint8_t* __restrict__ pinned,
+                                  const uint8_t* __restrict__ active, const float4* __restrict__ normals,
+                                  Particle* particle, Contact* contact, uint32_t* cols, uint32_t* diag, Control* ctl,
+                                  int* iterations) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  if (tid == 0) {
+    *ctl = Control{};
+    *iterations = 0;
+  }
+  for (uint32_t i = tid; i < n; i += stride) {
+    particle[i] = Particle{1.0f, 0u, 0u, pinned[i] ? 1u : 0u};
+    Contact c{};
+    c.active = active && active[i] ? 1u : 0u;
+    c.nearBody = c.active;
+    if (normals) c.normal = make_float4(normals[i].x, normals[i].y, normals[i].z, 0.0f);
+    contact[i] = c;
+    const uint32_t rs = rowStart[i], re = rowStart[i + 1];
+    uint32_t d = re;
+    for (uint32_t s = rs; s < re; ++s) {
+      const uint32_t j = colIndex[s];
+      cols[s] = (j < n && pinned[j]) ? (j | kPinnedBit) : j;
+      if (j == i) d = s;
+    }
+    diag[i] = d;
+  }
+}
+
+__global__ void k_noalloc_finish(const Control* ctl, int* iterations) {
+  *iterations = ctl->error ? -1 : ctl->lastCg;
+}
+
+}  // namespace dcu
+
+extern "C" int drape_cuda_pcg_noalloc(uint32_t n, uint32_t slots, const uint32_t* d_row_start,
+                                      const uint32_t* d_col_index, const float* d_blocks, uint32_t slots_padded,
+                                      const uint8_t* d_pinned, const uint8_t* d_active, const void* d_normals,
+                                      const void* d_grad, int max_iterations, double tolerance, void* d_step,
+                                      void* d_resid, int32_t* d_iterations, void* stream) {
+  return guarded(nullptr, [&] {
+    if (n == 0 || n > DRAPE_PCG_NOALLOC_MAX_PARTICLES)
+      throw std::invalid_argument("pcg_noalloc: n must be in 1.." + std::to_string(DRAPE_PCG_NOALLOC_MAX_PARTICLES) +
+                                  " (got " + std::to_string(n) + ")");
+    if (!d_row_start || !d_col_index || !d_blocks || !d_pinned || !d_grad || !d_step || !d_resid || !d_iterations)
+      throw std::invalid_argument("pcg_noalloc: null device pointer");
+    if (max_iterations < 0) throw std::invalid_argument("pcg_noalloc: negative iteration cap");
+    auto st = static_cast<cudaStream_t>(stream);
+    if (slots > DRAPE_PCG_NOALLOC_MAX_SLOTS)
+      throw std::invalid_argument("pcg_noalloc: " + std::to_string(slots) + " block slots exceed the limit of " +
+                                  std::to_string(DRAPE_PCG_NOALLOC_MAX_SLOTS));
+    if (slots_padded < slots) throw std::invalid_argument("pcg_noalloc: slots_padded < row_start[n]");
+    int device = 0;
+    CK(cudaGetDevice(&device));
+    NoAllocDevice& nd = noAllocScratch(device);
+    unsigned char* base = nd.scratch;
+    using L = NoAllocLayout;
+    auto* vec = reinterpret_cast<float4*>(base + L::vectors);
+    const size_t N = L::N;
+    dcu::Dev d{};
+    d.P.n = n;
+    d.P.nBlocks = slots;
+    d.P.slotsPadded = slots_padded;
+    d.P.maxCg = max_iterations;
+    d.P.cgTolerance = tolerance;
+    d.P.barrierLimitNs = 2000000000ull;
+    d.P.h = 1.0f;
+    d.P.hD = 1.0;
+    d.r = vec;
+    d.z = vec + N;
+    d.p0 = vec + 2 * N;
+    d.p1 = vec + 3 * N;
+    d.ap = vec + 4 * N;
+    d.apFull = vec + 5 * N;
+    d.precond = reinterpret_cast<float4*>(base + L::precond);
+    d.particle = reinterpret_cast<const dcu::Particle*>(base + L::particle);
+    d.contact = reinterpret_cast<dcu::Contact*>(base + L::contact);
+    d.rowStart = d_row_start;
+    d.colIndex = reinterpret_cast<const uint32_t*>(base + L::cols);
+    d.blocks = const_cast<float*>(d_blocks);
+    d.grad = const_cast<float4*>(static_cast<const float4*>(d_grad));
+    d.step = static_cast<float4*>(d_step);
+    d.resid = static_cast<float4*>(d_resid);
+    d.partials = reinterpret_cast<double*>(base + L::partials);
+    d.ctl = reinterpret_cast<dcu::Control*>(base + L::control);
+    auto* diag = reinterpret_cast<uint32_t*>(base + L::diag);
+    const int pg = std::max(1, static_cast<int>((n + 255) / 256));
+    dcu::k_noalloc_prepare<<<pg, 256, 0, st>>>(
+        n, d_row_start, d_col_index, d_pinned, d_active, static_cast<const float4*>(d_normals),
+        reinterpret_cast<dcu::Particle*>(base + L::particle), d.contact, reinterpret_cast<uint32_t*>(base + L::cols),
+        diag, d.ctl, d_iterations);
+    CK(cudaGetLastError());
+    dcu::k_pcg_precondition<<<pg, 256, 0, st>>>(d, diag);
+    CK(cudaGetLastError());
+    void* args[] = {&d};
+    CK(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(dcu::k_pcg_only), dim3(nd.sms), dim3(dcu::kSolveThreads),
+                                   args, 0, st));
+    dcu::k_noalloc_finish<<<1, 1, 0, st>>>(d.ctl, d_iterations);
+    CK(cudaGetLastError());
+  });
+}

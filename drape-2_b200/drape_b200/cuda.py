@@ -85,6 +85,9 @@ def load(build_if_missing: bool = True):
     L.drape_cuda_profile.argtypes = [C.c_void_p, C.c_int]
     L.drape_cuda_profile_read.argtypes = [C.c_void_p, _P(drape_profile)]
     L.drape_cuda_transfer_bytes.argtypes = [C.c_void_p, _P(C.c_uint64), _P(C.c_uint64)]
+    L.drape_cuda_pcg_noalloc.argtypes = [_u32, _u32, C.c_void_p, C.c_void_p, C.c_void_p, _u32, C.c_void_p,
+                                         C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, _d, C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_void_p]
     _lib = L
     return L
 

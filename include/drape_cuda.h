@@ -171,6 +171,33 @@ int drape_cuda_spmv_device(uint32_t n, const uint32_t* d_row_start, const uint32
                            const float* d_blocks, uint32_t slots_padded, const uint8_t* d_pinned, const void* d_x,
                            void* d_y, void* stream);
 
+/* The PCG of drape_cuda_pcg on a system that is already in device memory, allocating nothing. It is for callers that
+   cannot allocate device memory: a host whose device memory is budgeted by another framework's pool allocator (an
+   allocation outside the pool breaks its accounting), and frame-paced simulation loops that may not call
+   cudaMalloc/cudaFree (cudaFree synchronises the whole device and either call can take unbounded time). This entry
+   point has no counterpart in the reference.
+   All of the solver's scratch (work vectors, preconditioner, converted flags, reduction partials, barrier state)
+   lives in one file-scope device array of DRAPE_PCG_NOALLOC_SCRATCH_BYTES, which every GPU that loads the library
+   holds until the process exits. Systems are limited to n <= DRAPE_PCG_NOALLOC_MAX_PARTICLES particles and
+   slots <= DRAPE_PCG_NOALLOC_MAX_SLOTS block slots; larger ones are rejected with DRAPE_INVALID.
+   Inputs and outputs are the caller's device buffers: row_start (n + 1) and col_index (slots = row_start[n], passed
+   by value as `slots`) as u32; blocks as 9 planes of slots_padded floats (component 3 * row + col); pinned and
+   active as one u8 per particle (active may be NULL); normals, grad, step and resid as float4 per particle (normals
+   may be NULL). The iteration count is written to *d_iterations in device memory (-1 if the bounded grid barrier
+   gave up). The work is queued on `stream` (a cudaStream_t, NULL for the legacy default stream) without
+   synchronising; the return value reports argument and launch errors.
+   The first call on a device does a one-time set-up for that device (it looks up the array's device address with
+   the device current); make that first call before any stream capture. Every call shares the one array, which keeps
+   the last call's contents; each call clears what must start at zero. Calls whose work overlaps on the GPU (other
+   streams, other host threads, other devices' calls on the same device) race on the array: serialise them. */
+#define DRAPE_PCG_NOALLOC_MAX_PARTICLES 8192u
+#define DRAPE_PCG_NOALLOC_MAX_SLOTS 131072u
+#define DRAPE_PCG_NOALLOC_SCRATCH_BYTES 2146560u
+int drape_cuda_pcg_noalloc(uint32_t n, uint32_t slots, const uint32_t* d_row_start, const uint32_t* d_col_index,
+                           const float* d_blocks, uint32_t slots_padded, const uint8_t* d_pinned,
+                           const uint8_t* d_active, const void* d_normals, const void* d_grad, int max_iterations,
+                           double tolerance, void* d_step, void* d_resid, int32_t* d_iterations, void* stream);
+
 /* The bounded wait of the device grid barrier, in nanoseconds (0 restores the default of 2 s). A kernel whose barrier
    waits longer sets the handle's error status and returns instead of hanging; the step then fails with
    DRAPE_DEVICE_ERROR and the solver stays usable. */
