@@ -319,6 +319,7 @@ def main():
                   "simulated_seconds": float(results[-1].simulated_seconds),
                   "assembly_seconds": float(results[-1].assembly_seconds), "retries": int(results[-1].retries),
                   "newton_iterations_per_drape": counters.newton_iterations / args.steps,
+                  "ms_per_frame": 1000.0 * statistics.mean(t / max(1, r.frames_run) for t, r in zip(times, results)),
                   "drapes_per_s": world / value if value else None},
         "pcg_iters_per_newton": {"mean": float(np.mean(cg_hist)) if len(cg_hist) else None,
                                  "p50": float(np.percentile(cg_hist, 50)) if len(cg_hist) else None,

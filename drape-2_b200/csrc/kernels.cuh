@@ -24,6 +24,7 @@ constexpr int kAssembleWarps = 8;   // warps per k_assemble block
 constexpr int kRowLanes = 4;        // lanes per block row in the SpMV
 constexpr int kSolveThreads = 1024; // k_solve block size (one block per SM)
 constexpr uint32_t kPinnedBit = 0x80000000u;
+constexpr uint32_t kSmemSlotBytes = 40;      // one block slot in shared memory: 9 floats + a column index
 constexpr int kPartialStride = 4;   // doubles per block in the partials array
 constexpr uint32_t kMaxRowSlots = 64;  // block slots per row the assembly kernel accumulates (checked at build)
 
@@ -90,6 +91,7 @@ struct Params {
   double hD, cgTolerance;
   int maxCg;
   uint32_t n, nStretch, nHinge, nSeam, nBlocks, nGarments, slotsPadded;
+  uint32_t smemSlots;   // k_solve: block slots a block keeps in shared memory
   unsigned long long barrierLimitNs;
 };
 
@@ -158,17 +160,22 @@ struct GridSync {
     parity = 0;
   }
 
-  __device__ bool sync() {
+  // blockSynced: the caller has just passed a __syncthreads after every thread's writes of this phase and only
+  // thread 0 publishes after it (the case of gridReduce), so the leading block barrier can be skipped.
+  __device__ bool sync(bool blockSynced = false) {
     __shared__ int ok;
     target += gridDim.x;
-    __syncthreads();
+    if (!blockSynced) __syncthreads();
     if (threadIdx.x == 0) {
-      cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> a(ctl->barrierArrivals);
-      a.fetch_add(1ull, cuda::memory_order_release);
+      unsigned long long* counter = &ctl->barrierArrivals;
+      asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(counter), "l"(1ull) : "memory");
       int good = 1;
       unsigned int spins = 0;
       const unsigned long long start = globalTimerNs();
-      while (a.load(cuda::memory_order_acquire) < target) {
+      for (;;) {
+        unsigned long long seen;
+        asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(seen) : "l"(counter) : "memory");
+        if (seen >= target) break;
         if ((++spins & 31u) == 0) {
           if (*reinterpret_cast<volatile int*>(&ctl->error) != 0) {
             good = 0;
@@ -246,7 +253,7 @@ __device__ inline bool gridReduce(const Dev& D, GridSync& gs, double (&v)[K], do
 #pragma unroll
       for (int k = 0; k < K; ++k) half[blockIdx.x * kPartialStride + k] = blk[k];
   }
-  if (!gs.sync()) return false;
+  if (!gs.sync(true)) return false;
   if (threadIdx.x < 32) {
     double s[K];
 #pragma unroll
@@ -589,8 +596,14 @@ __device__ inline double energyPartial(const Dev& D, double alpha) {
 
 // ---------------------------------------------------------------------------------------------------------------
 // Persistent solve: PCG with FP64 dot products, then the Newton line search. Every block computes the same scalars
-// from the same partials, so all blocks take the same branches; two grid reductions per CG iteration (the direction
-// update p = z + beta p is folded into the next SpMV, which rebuilds each neighbour's p from z and the previous p).
+// from the same partials, so all blocks take the same branches.
+//
+// Each block owns a contiguous range of rows; at the start of the launch it copies its rows' blocks and column
+// indices into shared memory (up to P.smemSlots slots; any excess is read from global memory), and every CG
+// iteration's SpMV reads them from there.
+//
+// The PCG follows the reference's order (cpu_solver.cpp:169-213): two grid reductions per iteration (p.Ap, then
+// r.r with r.z); the direction update p = z + beta p is folded into the next SpMV.
 
 __device__ __forceinline__ M3 loadPrecond(const Dev& D, uint32_t i) {
   const float4 a = D.precond[3 * i], b = D.precond[3 * i + 1], c = D.precond[3 * i + 2];
@@ -601,13 +614,88 @@ __device__ __forceinline__ double dotd3(float3 a, float3 b) {
   return static_cast<double>(a.x) * b.x + static_cast<double>(a.y) * b.y + static_cast<double>(a.z) * b.z;
 }
 
-// Contact-filtered block-Jacobi PCG (cpu_solver.cpp:169-213): writes step, resid; returns the iteration count, or -1
+struct SmemMatrix {
+  const float* planes;  // 9 planes of `stride` floats in shared memory
+  const uint32_t* cols;
+  uint32_t base, cap, stride, SP;  // slots [base, base + cap) are in shared memory
+  const float* gblocks;
+  const uint32_t* gcols;
+  __device__ __forceinline__ bool local(uint32_t s) const { return s - base < cap; }
+  __device__ __forceinline__ uint32_t col(uint32_t s) const {
+    return local(s) ? cols[s - base] : __ldg(gcols + s);
+  }
+  // Row-major block at slot s.
+  __device__ __forceinline__ void block(uint32_t s, float a[9]) const {
+    if (local(s)) {
+      const float* p = planes + (s - base);
+#pragma unroll
+      for (int k = 0; k < 9; ++k) a[k] = p[k * stride];
+    } else {
+#pragma unroll
+      for (int k = 0; k < 9; ++k) a[k] = __ldg(gblocks + k * SP + s);
+    }
+  }
+};
+
+extern __shared__ float4 solveSmem[];
+
+// Copies this block's slot range into shared memory (all threads; ends with a block barrier).
+__device__ inline SmemMatrix stageMatrix(const Dev& D, uint32_t r0, uint32_t r1) {
+  SmemMatrix A;
+  const uint32_t cap = D.P.smemSlots;
+  float* planes = reinterpret_cast<float*>(solveSmem);
+  uint32_t* cols = reinterpret_cast<uint32_t*>(planes + 9 * cap);
+  A.planes = planes;
+  A.cols = cols;
+  A.SP = D.P.slotsPadded;
+  A.gblocks = D.blocks;
+  A.gcols = D.colIndex;
+  A.base = r0 < r1 ? __ldg(D.rowStart + r0) : 0;
+  const uint32_t end = r0 < r1 ? __ldg(D.rowStart + r1) : 0;
+  const uint32_t count = min(end - A.base, cap);
+  A.stride = cap;
+  A.cap = count;
+  for (uint32_t k = threadIdx.x; k < count; k += blockDim.x) {
+    const uint32_t s = A.base + k;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) planes[c * cap + k] = __ldg(D.blocks + c * A.SP + s);
+    cols[k] = __ldg(D.colIndex + s);
+  }
+  __syncthreads();
+  return A;
+}
+
+// y_i (unfiltered) = sum over unpinned columns j of A_ij x_j for row i, by kRowLanes lanes (lane `sub`), reduced over
+// the group; x_j given by a functor.
+template <class X>
+__device__ __forceinline__ float3 rowProduct(const SmemMatrix& A, uint32_t rs, uint32_t re, int sub, unsigned mask,
+                                             X&& xj) {
+  float3 acc = mk(0, 0, 0);
+  for (uint32_t s = rs + sub; s < re; s += kRowLanes) {
+    const uint32_t col = A.col(s);
+    if (col & kPinnedBit) continue;
+    const float3 v = xj(col);
+    float a[9];
+    A.block(s, a);
+    acc.x += a[0] * v.x + a[1] * v.y + a[2] * v.z;
+    acc.y += a[3] * v.x + a[4] * v.y + a[5] * v.z;
+    acc.z += a[6] * v.x + a[7] * v.y + a[8] * v.z;
+  }
+#pragma unroll
+  for (int o = kRowLanes / 2; o > 0; o >>= 1) {
+    acc.x += __shfl_xor_sync(mask, acc.x, o);
+    acc.y += __shfl_xor_sync(mask, acc.y, o);
+    acc.z += __shfl_xor_sync(mask, acc.z, o);
+  }
+  return acc;
+}
+
+// Contact-filtered block-Jacobi PCG in the reference's order. Writes step, resid; returns the iteration count, or -1
 // when a grid barrier gave up.
-__device__ inline int pcgSolve(const Dev& D, GridSync& gs) {
+__device__ inline int pcgReferenceOrder(const Dev& D, GridSync& gs, const SmemMatrix& A) {
   const uint32_t n = D.P.n;
   uint32_t r0i, r1i;
   blockRange(n, r0i, r1i);
-
   // CG init (kernels.h:252-268): step = 0, resid = -grad, r = filter(resid), z = filter(M r).
   double tot[2];
   {
@@ -634,7 +722,6 @@ __device__ inline int pcgSolve(const Dev& D, GridSync& gs) {
   float4* pCur = D.p1;
   int it = 0;
   const int maxCg = D.P.maxCg;
-  const uint32_t SP = D.P.slotsPadded;
   const uint32_t groups = blockDim.x / kRowLanes;
   const int sub = threadIdx.x & (kRowLanes - 1);
   const unsigned groupMask = ((1u << kRowLanes) - 1u) << ((threadIdx.x & 31) & ~(kRowLanes - 1));
@@ -646,27 +733,13 @@ __device__ inline int pcgSolve(const Dev& D, GridSync& gs) {
     for (uint32_t i = r0i + threadIdx.x / kRowLanes; i < r1i; i += groups) {
       const uint32_t rs = __ldg(D.rowStart + i), re = __ldg(D.rowStart + i + 1);
       float3 acc = mk(0, 0, 0);
-      if (D.particle[i].pinned == 0u) {
-        for (uint32_t s = rs + sub; s < re; s += kRowLanes) {
-          const uint32_t col = __ldg(D.colIndex + s);
-          if (col & kPinnedBit) continue;
-          const float3 zj = ld3(D.z, col);
-          const float3 pj = first ? zj : zj + ld3(pPrev, col) * fb;
-          const float* b = D.blocks + s;
-          const float a0 = __ldg(b), a1 = __ldg(b + SP), a2 = __ldg(b + 2 * SP);
-          const float a3 = __ldg(b + 3 * SP), a4 = __ldg(b + 4 * SP), a5 = __ldg(b + 5 * SP);
-          const float a6 = __ldg(b + 6 * SP), a7 = __ldg(b + 7 * SP), a8 = __ldg(b + 8 * SP);
-          acc.x += a0 * pj.x + a1 * pj.y + a2 * pj.z;
-          acc.y += a3 * pj.x + a4 * pj.y + a5 * pj.z;
-          acc.z += a6 * pj.x + a7 * pj.y + a8 * pj.z;
-        }
-      }
-#pragma unroll
-      for (int o = kRowLanes / 2; o > 0; o >>= 1) {
-        acc.x += __shfl_xor_sync(groupMask, acc.x, o);
-        acc.y += __shfl_xor_sync(groupMask, acc.y, o);
-        acc.z += __shfl_xor_sync(groupMask, acc.z, o);
-      }
+      if (D.particle[i].pinned == 0u)
+        acc = rowProduct(A, rs, re, sub, groupMask, [&](uint32_t j) {
+          const float3 zj = ld3(D.z, j);
+          return first ? zj : zj + ld3(pPrev, j) * fb;
+        });
+      else
+        acc = rowProduct(A, rs, rs, sub, groupMask, [&](uint32_t) { return mk(0, 0, 0); });
       if (sub == 0) {
         const float3 zi = ld3(D.z, i);
         const float3 pi = first ? zi : zi + ld3(pPrev, i) * fb;
@@ -707,6 +780,13 @@ __device__ inline int pcgSolve(const Dev& D, GridSync& gs) {
     pCur = tmp;
   }
   return it;
+}
+
+__device__ inline int pcgSolve(const Dev& D, GridSync& gs) {
+  uint32_t r0i, r1i;
+  blockRange(D.P.n, r0i, r1i);
+  const SmemMatrix A = stageMatrix(D, r0i, r1i);
+  return pcgReferenceOrder(D, gs, A);
 }
 
 __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(Dev D) {

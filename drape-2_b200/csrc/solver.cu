@@ -88,6 +88,17 @@ thread_local std::string g_lastError;
 
 }  // namespace
 
+// Largest slot count of any solve block's contiguous row range (the split the device's blockRange makes).
+static uint32_t maxBlockSlots(const uint32_t* rowStart, uint32_t n, int grid) {
+  const uint32_t per = (n + static_cast<uint32_t>(grid) - 1) / static_cast<uint32_t>(grid);
+  uint32_t most = 0;
+  for (int b = 0; b < grid; ++b) {
+    const uint32_t r0 = std::min<uint32_t>(n, static_cast<uint32_t>(b) * per), r1 = std::min<uint32_t>(n, r0 + per);
+    most = std::max(most, rowStart[r1] - rowStart[r0]);
+  }
+  return most;
+}
+
 struct drape_solver {
   int device = 0;
   int numSMs = 0;
@@ -98,6 +109,8 @@ struct drape_solver {
   int solveGrid = 0, pointGrid = 0, assembleGrid = 0, statsGrid = 0;
   unsigned long long barrierLimitNs = 2000000000ull;  // 2 s
   int failAfter = -1;
+  uint32_t solveSmemCap = 0;       // block slots one solve block can keep in shared memory
+  size_t solveSmemBytes = 0;       // dynamic shared memory of the solve launch for the built scene
 
   DBuf<dcu::Particle> particle;
   DBuf<dcu::Fabric> fabric;
@@ -180,9 +193,23 @@ struct drape_solver {
     CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     CK(cudaFuncSetAttribute(dcu::k_assemble, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             static_cast<int>(dcu::kAssembleSmem)));
-    int perSM = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, dcu::k_solve, dcu::kSolveThreads, 0));
-    if (perSM < 1) throw std::runtime_error("cuda: the solve kernel does not fit on an SM");
+    // The solve kernels keep their rows' matrix blocks in shared memory: as many slots as the opt-in limit leaves.
+    const void* solveKernels[] = {reinterpret_cast<const void*>(dcu::k_solve),
+                                  reinterpret_cast<const void*>(dcu::k_pcg_only)};
+    size_t staticSmem = 0;
+    for (const void* k : solveKernels) {
+      cudaFuncAttributes fa{};
+      CK(cudaFuncGetAttributes(&fa, k));
+      staticSmem = std::max(staticSmem, fa.sharedSizeBytes);
+    }
+    solveSmemCap = static_cast<uint32_t>((prop.sharedMemPerBlockOptin - staticSmem) / dcu::kSmemSlotBytes);
+    const int dynMax = static_cast<int>(solveSmemCap * dcu::kSmemSlotBytes);
+    for (const void* k : solveKernels) {
+      CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, dynMax));
+      int perSM = 0;
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k, dcu::kSolveThreads, dynMax));
+      if (perSM < 1) throw std::runtime_error("cuda: the solve kernel does not fit on an SM");
+    }
     solveGrid = numSMs;  // one 1024-thread block per SM: fewest barrier arrivals
     pointGrid = numSMs * 8;
     statsGrid = numSMs * 2;
@@ -341,6 +368,8 @@ struct drape_solver {
     P.nGarments = static_cast<uint32_t>(m.garments.size());
     P.slotsPadded = SP;
     P.barrierLimitNs = barrierLimitNs;
+    P.smemSlots = std::min(solveSmemCap, maxBlockSlots(m.rowStart.data(), n, solveGrid));
+    solveSmemBytes = static_cast<size_t>(P.smemSlots) * dcu::kSmemSlotBytes;
     d.field.present = !m.fieldValues.empty() ? 1 : 0;
     d.field.ox = static_cast<float>(m.field.origin[0]);
     d.field.oy = static_cast<float>(m.field.origin[1]);
@@ -457,7 +486,7 @@ struct drape_solver {
   void launchSolve(const dcu::Dev& d) {
     void* args[] = {const_cast<dcu::Dev*>(&d)};
     CK(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(dcu::k_solve), dim3(solveGrid), dim3(dcu::kSolveThreads),
-                                   args, 0, stream));
+                                   args, solveSmemBytes, stream));
   }
 
   void enqueueSubstep(double h, int iterations) {
@@ -1261,6 +1290,7 @@ int drape_cuda_pcg(uint32_t n, const uint32_t* row_start, const uint32_t* col_in
     for (DBuf<float4>* b : {&dstep, &dr, &dz, &dp0, &dp1, &dap, &dapf, &dres}) b->alloc(n);
     dpre.alloc(3 * static_cast<size_t>(n));
     dcu::Dev d{};
+    d.P.smemSlots = std::min(s.solveSmemCap, maxBlockSlots(row_start, n, s.solveGrid));
     d.P.n = n;
     d.P.nBlocks = B;
     d.P.slotsPadded = SP;
@@ -1300,7 +1330,8 @@ int drape_cuda_pcg(uint32_t n, const uint32_t* row_start, const uint32_t* col_in
     CK(cudaGetLastError());
     void* args[] = {&d};
     CK(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(dcu::k_pcg_only), dim3(s.solveGrid),
-                                   dim3(dcu::kSolveThreads), args, 0, st));
+                                   dim3(dcu::kSolveThreads), args,
+                                   static_cast<size_t>(d.P.smemSlots) * dcu::kSmemSlotBytes, st));
     std::vector<float4> hs(n), hr(n);
     dcu::Control c{};
     CK(cudaMemcpyAsync(hs.data(), dstep.p, sizeof(float4) * n, cudaMemcpyDeviceToHost, st));
