@@ -1,0 +1,1671 @@
+// Learned preconditioner: network kernels (forward, loss, backward, Adam) and the host Network class.
+//
+// Tile kernels run 128 threads (4 warps). A tile is 128 rows of a GEMM: 128 nodes, 128 slots, or the slots of a
+// "row tile" (consecutive rows of the block-CSR graph whose slots total at most 128, so every row's slots lie in one
+// tile and per-row sums stay inside one CTA, in a fixed order). Operands are staged by the threads into shared memory
+// in the K-major core-matrix layout (umma.cuh), one thread issues the tcgen05 MMAs, the accumulators live in TMEM and
+// come back through tcgen05.ld (thread t of warp w owns row 32 w + t). Weight gradients accumulate in TMEM across a
+// CTA's tiles and leave as per-CTA partials that a second kernel sums in CTA order: no floating-point atomics, so a
+// training step is deterministic.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <stdexcept>
+
+#include "device_math.cuh"
+#include "learned.hpp"
+#include "umma.cuh"
+
+namespace net {
+
+namespace {
+
+void ck(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) throw std::runtime_error(std::string("cuda: ") + what + ": " + cudaGetErrorString(e));
+}
+#define NCK(x) ck((x), #x)
+
+constexpr uint32_t kPinBit = 0x80000000u;
+constexpr int kThreads = 128;
+
+__device__ __forceinline__ bool pinnedRow(const Graph& g, uint32_t i) {
+  return g.pinnedBase != nullptr && g.pinnedBase[static_cast<size_t>(i) * g.pinnedStride] != 0;
+}
+__device__ __forceinline__ bool activeRow(const Graph& g, uint32_t i) {
+  return g.activeBase != nullptr && g.activeBase[static_cast<size_t>(i) * g.activeStride] != 0;
+}
+__device__ __forceinline__ uint32_t colOf(const Graph& g, uint32_t s) { return __ldg(g.colIndex + s) & ~kPinBit; }
+
+__device__ __forceinline__ float blockAt(const Graph& g, uint32_t s, int k) { return __ldg(g.blocks + k * g.SP + s); }
+
+__device__ __forceinline__ void st16(unsigned char* tile, uint32_t r, uint32_t c, uint32_t K, uint4 v) {
+  *reinterpret_cast<uint4*>(tile + umma::kmajorOffset(r, c * 8u, K)) = v;
+}
+__device__ __forceinline__ void st1(unsigned char* tile, uint32_t r, uint32_t k, uint32_t K, __nv_bfloat16 v) {
+  *reinterpret_cast<__nv_bfloat16*>(tile + umma::kmajorOffset(r, k, K)) = v;
+}
+__device__ __forceinline__ uint4 zero4() { return make_uint4(0u, 0u, 0u, 0u); }
+
+__device__ __forceinline__ uint4 packBf16(const float* v) {
+  uint4 out;
+  uint32_t* w = reinterpret_cast<uint32_t*>(&out);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const __nv_bfloat162 p = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
+    w[i] = *reinterpret_cast<const uint32_t*>(&p);
+  }
+  return out;
+}
+__device__ __forceinline__ void unpackBf16(uint4 u, float* v) {
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(&u);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const __nv_bfloat162 p = *reinterpret_cast<const __nv_bfloat162*>(&w[i]);
+    v[2 * i] = __low2float(p);
+    v[2 * i + 1] = __high2float(p);
+  }
+}
+// Scatter a 16-byte chunk (8 BF16 of features 8c..8c+7 of row q) into the transposed tile (row = feature, k = q).
+__device__ __forceinline__ void st16T(unsigned char* tile, uint32_t q, uint32_t c, uint32_t K, uint4 v) {
+  const __nv_bfloat16* e = reinterpret_cast<const __nv_bfloat16*>(&v);
+#pragma unroll
+  for (int i = 0; i < 8; ++i) st1(tile, c * 8u + i, q, K, e[i]);
+}
+
+// Shared state of a tile kernel: one mbarrier for MMA completion and a TMEM allocation held for the whole launch.
+struct TileCtx {
+  uint64_t* bar;
+  uint32_t* slot;
+  uint32_t tmem = 0, parity = 0, cols = 0;
+  int* error;
+  __device__ void init(uint64_t* b, uint32_t* s, uint32_t c, int* err) {
+    bar = b;
+    slot = s;
+    cols = c;
+    error = err;
+    if (threadIdx.x == 0) umma::mbarInit(bar, 1);
+    if (threadIdx.x < 32) umma::tmemAlloc(slot, cols);
+    umma::fenceBeforeSync();
+    __syncthreads();
+    umma::fenceAfterSync();
+    tmem = *slot;
+  }
+  // Publishes the staged operands, lets thread 0 issue the MMAs and one commit, waits for them. All threads get
+  // the same verdict.
+  template <class F>
+  __device__ bool run(F&& issue) {
+    umma::fenceSmemForMma();
+    umma::fenceBeforeSync();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      umma::fenceAfterSync();
+      issue();
+      umma::commit(bar);
+    }
+    const bool good = umma::mbarWait(bar, parity, error);
+    parity ^= 1u;
+    umma::fenceAfterSync();
+    return __syncthreads_and(good) != 0;
+  }
+  __device__ void done() {
+    umma::fenceBeforeSync();
+    __syncthreads();
+    if (threadIdx.x < 32) umma::tmemFree(tmem, cols);
+  }
+  // Row (32 * warp + lane) of the accumulator at column `col`, 16 columns.
+  __device__ void load(uint32_t col, float (&v)[16]) const {
+    umma::load16(umma::tmemAt(tmem, (threadIdx.x / 32u) * 32u, col), v);
+  }
+};
+
+__device__ __forceinline__ unsigned char* alignSmem(unsigned char* p) {
+  return reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(p) + 127u) & ~static_cast<uintptr_t>(127u));
+}
+extern __shared__ unsigned char netSmem[];
+
+// ------------------------------------------------------------------------------------------------------------------
+// Features
+
+// C_i = chol(inv(A_ii)) (lower), identity when A_ii is not SPD, zero for a pinned row. One thread per row.
+__global__ void k_scale(Graph g) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.n) return;
+  float c[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (!pinnedRow(g, i)) {
+    uint32_t d = __ldg(g.rowStart + i);
+    const uint32_t end = __ldg(g.rowStart + i + 1);
+    while (d < end && colOf(g, d) != i) ++d;
+    dcu::M3 A;
+    for (int k = 0; k < 9; ++k) A.m[k] = d < end ? blockAt(g, d, k) : (k % 4 == 0 ? 1.0f : 0.0f);
+    bool ok = false;
+    const dcu::M3 inv = dcu::invertSpd(A, ok);
+    c[0] = c[4] = c[8] = 1.0f;
+    if (ok) {
+      const float l00s = inv.m[0];
+      if (l00s > 0.0f) {
+        const float l00 = sqrtf(l00s), l10 = inv.m[3] / l00, l20 = inv.m[6] / l00;
+        const float l11s = inv.m[4] - l10 * l10;
+        if (l11s > 0.0f) {
+          const float l11 = sqrtf(l11s), l21 = (inv.m[7] - l20 * l10) / l11;
+          const float l22s = inv.m[8] - l20 * l20 - l21 * l21;
+          if (l22s > 0.0f) {
+            c[0] = l00;
+            c[1] = 0.0f;
+            c[2] = 0.0f;
+            c[3] = l10;
+            c[4] = l11;
+            c[5] = 0.0f;
+            c[6] = l20;
+            c[7] = l21;
+            c[8] = sqrtf(l22s);
+          }
+        }
+      }
+    }
+  }
+  for (int k = 0; k < 9; ++k) g.C[9 * static_cast<size_t>(i) + k] = c[k];
+}
+
+// Ahat_s = C_i^T A_s C_j, slot features e_s and node features f_i. One warp per row.
+__global__ void k_features(Graph g) {
+  const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) / 32u;
+  const int lane = threadIdx.x & 31;
+  if (i >= g.n) return;
+  const bool pi = pinnedRow(g, i);
+  float Ci[9];
+  for (int k = 0; k < 9; ++k) Ci[k] = g.C[9 * static_cast<size_t>(i) + k];
+  float deg = 0.0f, sumFro = 0.0f, maxFro = 0.0f, rd0 = 0.0f, rd1 = 0.0f, rd2 = 0.0f;
+  const uint32_t rs = __ldg(g.rowStart + i), re = __ldg(g.rowStart + i + 1);
+  for (uint32_t s = rs + lane; s < re; s += 32) {
+    const uint32_t j = colOf(g, s);
+    const bool live = !pi && !pinnedRow(g, j);
+    float ah[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (live) {
+      float Cj[9], T[9];
+      for (int k = 0; k < 9; ++k) Cj[k] = g.C[9 * static_cast<size_t>(j) + k];
+      // T = A_s C_j; Ahat = C_i^T T.
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c)
+          T[3 * r + c] = blockAt(g, s, 3 * r) * Cj[c] + blockAt(g, s, 3 * r + 1) * Cj[3 + c] +
+                         blockAt(g, s, 3 * r + 2) * Cj[6 + c];
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) ah[3 * r + c] = Ci[r] * T[c] + Ci[3 + r] * T[3 + c] + Ci[6 + r] * T[6 + c];
+    }
+    float fro = 0.0f;
+    for (int k = 0; k < 9; ++k) fro += ah[k] * ah[k];
+    fro = sqrtf(fro);
+    for (int k = 0; k < 9; ++k) g.Ahat[9 * static_cast<size_t>(s) + k] = ah[k];
+    float ev[16] = {0};
+    for (int k = 0; k < 9; ++k) ev[k] = ah[k];
+    ev[9] = fro;
+    ev[10] = j == i ? 1.0f : 0.0f;
+    ev[11] = j < i ? 1.0f : 0.0f;
+    uint4* ep = reinterpret_cast<uint4*>(g.e + 16 * static_cast<size_t>(s));
+    ep[0] = packBf16(ev);
+    ep[1] = packBf16(ev + 8);
+    if (live && j != i) {
+      deg += 1.0f;
+      sumFro += fro;
+      maxFro = fmaxf(maxFro, fro);
+      rd0 += ah[0];
+      rd1 += ah[4];
+      rd2 += ah[8];
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    deg += __shfl_xor_sync(0xffffffffu, deg, o);
+    sumFro += __shfl_xor_sync(0xffffffffu, sumFro, o);
+    maxFro = fmaxf(maxFro, __shfl_xor_sync(0xffffffffu, maxFro, o));
+    rd0 += __shfl_xor_sync(0xffffffffu, rd0, o);
+    rd1 += __shfl_xor_sync(0xffffffffu, rd1, o);
+    rd2 += __shfl_xor_sync(0xffffffffu, rd2, o);
+  }
+  if (lane == 0) {
+    float fv[16] = {0};
+    fv[0] = 1.0f;
+    fv[1] = (activeRow(g, i) && !pi) ? 1.0f : 0.0f;
+    fv[2] = deg / 16.0f;
+    fv[3] = sumFro / fmaxf(deg, 1.0f);
+    fv[4] = maxFro;
+    fv[5] = rd0;
+    fv[6] = rd1;
+    fv[7] = rd2;
+    fv[8] = pi ? 1.0f : 0.0f;
+    uint4* fp = reinterpret_cast<uint4*>(g.f + 16 * static_cast<size_t>(i));
+    fp[0] = packBf16(fv);
+    fp[1] = packBf16(fv + 8);
+  }
+}
+
+// ------------------------------------------------------------------------------------------------------------------
+// Encoder: out = relu(X W^T + b) for `rows` rows of 16 BF16 features; out 64 BF16 per row.
+
+struct EncodeSmem {
+  unsigned char x[128 * 16 * 2];
+  unsigned char w[64 * 16 * 2];
+  float b[64];
+  uint64_t bar;
+  uint32_t tmem;
+};
+
+__global__ void __launch_bounds__(kThreads) k_encode(uint32_t rows, const __nv_bfloat16* __restrict__ X,
+                                                     const __nv_bfloat16* __restrict__ W, const float* __restrict__ b,
+                                                     __nv_bfloat16* __restrict__ out, int* error) {
+  EncodeSmem& S = *reinterpret_cast<EncodeSmem*>(alignSmem(netSmem));
+  TileCtx T;
+  T.init(&S.bar, &S.tmem, 64, error);
+  const int t = threadIdx.x;
+  for (int k = t; k < 64 * 2; k += kThreads)
+    st16(S.w, k / 2, k % 2, 16, reinterpret_cast<const uint4*>(W)[k]);
+  if (t < 64) S.b[t] = b[t];
+  const uint32_t tiles = (rows + 127) / 128;
+  for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const uint32_t r0 = tile * 128;
+    for (int k = t; k < 128 * 2; k += kThreads) {
+      const uint32_t q = k / 2, c = k % 2, r = r0 + q;
+      st16(S.x, q, c, 16, r < rows ? reinterpret_cast<const uint4*>(X + 16 * static_cast<size_t>(r))[c] : zero4());
+    }
+    if (!T.run([&] { umma::gemmIssue(T.tmem, S.x, S.w, 128, 64, 16, false); })) break;
+    const uint32_t r = r0 + t;
+    for (int c = 0; c < 4; ++c) {
+      float v[16];
+      T.load(16 * c, v);
+      if (r < rows) {
+        for (int k = 0; k < 16; ++k) v[k] = fmaxf(v[k] + S.b[16 * c + k], 0.0f);
+        uint4* o = reinterpret_cast<uint4*>(out + 64 * static_cast<size_t>(r));
+        o[2 * c] = packBf16(v);
+        o[2 * c + 1] = packBf16(v + 8);
+      }
+    }
+    umma::fenceBeforeSync();
+    __syncthreads();
+  }
+  T.done();
+}
+
+// ------------------------------------------------------------------------------------------------------------------
+// Message-passing layer over row tiles: m_s = relu(W_m [h_j; eps_s] + b_m) on message slots, a_i = sum m_s / 8 per
+// row, h_i' = h_i + relu(W_u [h_i; a_i] + b_u).
+
+struct TileRows {
+  uint32_t r0, r1, s0, s1;
+};
+
+__device__ __forceinline__ TileRows tileRows(const Graph& g, uint32_t tile) {
+  TileRows t;
+  t.r0 = __ldg(g.tileRow + tile);
+  t.r1 = __ldg(g.tileRow + tile + 1);
+  t.s0 = __ldg(g.rowStart + t.r0);
+  t.s1 = __ldg(g.rowStart + t.r1);
+  return t;
+}
+
+struct LayerSmem {
+  unsigned char x[128 * 128 * 2];
+  unsigned char wm[64 * 128 * 2];
+  unsigned char wu[64 * 128 * 2];
+  float buf[128][65];
+  float bm[64], bu[64];
+  int slotRow[128];   // local row of slot q when it carries a message, else -1
+  int rowFirst[129];  // first local slot of local row r
+  uint64_t bar;
+  uint32_t tmem;
+};
+
+__device__ __forceinline__ void stageWeights(unsigned char* tile, const __nv_bfloat16* W, int rows, int K) {
+  const int chunks = K / 8;
+  for (int k = threadIdx.x; k < rows * chunks; k += blockDim.x)
+    st16(tile, k / chunks, k % chunks, K, reinterpret_cast<const uint4*>(W + static_cast<size_t>(k / chunks) * K)[k % chunks]);
+}
+// Transposed weights W^T (rows = K_in of W, K = rows of W) as a K-major operand.
+__device__ __forceinline__ void stageWeightsT(unsigned char* tile, const __nv_bfloat16* W, int outRows, int inCols) {
+  for (int k = threadIdx.x; k < outRows * inCols; k += blockDim.x) {
+    const int o = k / inCols, i = k % inCols;
+    st1(tile, i, o, outRows, W[static_cast<size_t>(o) * inCols + i]);
+  }
+}
+
+__device__ __forceinline__ void tileSlotInfo(const Graph& g, const TileRows& tr, int* slotRow, int* rowFirst,
+                                             bool messages) {
+  const int t = threadIdx.x;
+  for (uint32_t r = tr.r0 + t; r <= tr.r1 && r - tr.r0 <= 128; r += blockDim.x)
+    rowFirst[r - tr.r0] = static_cast<int>(__ldg(g.rowStart + r) - tr.s0);
+  __syncthreads();
+  for (int q = t; q < 128; q += blockDim.x) {
+    int row = -1;
+    const uint32_t s = tr.s0 + q;
+    if (s < tr.s1) {
+      // Local row: the last r with rowFirst[r] <= q.
+      int lo = 0, hi = static_cast<int>(tr.r1 - tr.r0) - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (rowFirst[mid] <= q) lo = mid; else hi = mid - 1;
+      }
+      const uint32_t i = tr.r0 + lo, j = colOf(g, s);
+      const bool keep = messages ? (j != i && !pinnedRow(g, i) && !pinnedRow(g, j))
+                                 : (j <= i && !pinnedRow(g, i) && !pinnedRow(g, j));
+      row = keep ? lo : -(lo + 2);  // -(lo + 2): in the tile but not kept
+    }
+    slotRow[q] = row;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kThreads) k_layer(Graph g, const __nv_bfloat16* __restrict__ Wm,
+                                                    const __nv_bfloat16* __restrict__ Wu, const float* __restrict__ bm,
+                                                    const float* __restrict__ bu, const __nv_bfloat16* __restrict__ hin,
+                                                    __nv_bfloat16* __restrict__ hout, __nv_bfloat16* __restrict__ aggOut,
+                                                    int* error) {
+  LayerSmem& S = *reinterpret_cast<LayerSmem*>(alignSmem(netSmem));
+  TileCtx T;
+  T.init(&S.bar, &S.tmem, 128, error);
+  const int t = threadIdx.x;
+  stageWeights(S.wm, Wm, 64, 128);
+  stageWeights(S.wu, Wu, 64, 128);
+  if (t < 64) {
+    S.bm[t] = bm[t];
+    S.bu[t] = bu[t];
+  }
+  for (uint32_t tile = blockIdx.x; tile < g.nTiles; tile += gridDim.x) {
+    const TileRows tr = tileRows(g, tile);
+    tileSlotInfo(g, tr, S.slotRow, S.rowFirst, true);
+    // X_msg: [h_j; eps_s] per message slot.
+    for (int k = t; k < 128 * 16; k += kThreads) {
+      const int q = k / 16, c = k % 16;
+      uint4 v = zero4();
+      if (S.slotRow[q] >= 0) {
+        const uint32_t s = tr.s0 + q;
+        v = c < 8 ? reinterpret_cast<const uint4*>(hin + 64 * static_cast<size_t>(colOf(g, s)))[c]
+                  : reinterpret_cast<const uint4*>(g.eps + 64 * static_cast<size_t>(s))[c - 8];
+      }
+      st16(S.x, q, c, 128, v);
+    }
+    if (!T.run([&] { umma::gemmIssue(T.tmem, S.x, S.wm, 128, 64, 128, false); })) break;
+    {
+      const bool keep = S.slotRow[t] >= 0;
+      for (int c = 0; c < 4; ++c) {
+        float v[16];
+        T.load(16 * c, v);
+        for (int k = 0; k < 16; ++k) S.buf[t][16 * c + k] = keep ? fmaxf(v[k] + S.bm[16 * c + k], 0.0f) : 0.0f;
+      }
+    }
+    __syncthreads();
+    // a_i = (1/8) sum over the row's slots, in slot order; X_upd = [h_i; a_i] (reuses the X_msg tile).
+    const int R = static_cast<int>(tr.r1 - tr.r0);
+    for (int k = t; k < 128 * 8; k += kThreads) {
+      const int r = k / 8, c = k % 8;
+      uint4 hv = zero4(), av = zero4();
+      if (r < R) {
+        hv = reinterpret_cast<const uint4*>(hin + 64 * static_cast<size_t>(tr.r0 + r))[c];
+        float a[8];
+        for (int e = 0; e < 8; ++e) {
+          float sum = 0.0f;
+          for (int q = S.rowFirst[r]; q < S.rowFirst[r + 1]; ++q) sum += S.buf[q][8 * c + e];
+          a[e] = sum * kAggScale;
+        }
+        av = packBf16(a);
+        if (aggOut) reinterpret_cast<uint4*>(aggOut + 64 * static_cast<size_t>(tr.r0 + r))[c] = av;
+      }
+      st16(S.x, r, c, 128, hv);
+      st16(S.x, r, 8 + c, 128, av);
+    }
+    if (!T.run([&] { umma::gemmIssue(T.tmem + 64, S.x, S.wu, 128, 64, 128, false); })) break;
+    for (int c = 0; c < 4; ++c) {
+      float v[16];
+      T.load(64 + 16 * c, v);
+      if (t < R) {
+        const size_t row = tr.r0 + t;
+        float h[16];
+        const uint4* hp = reinterpret_cast<const uint4*>(hin + 64 * row);
+        unpackBf16(hp[2 * c], h);
+        unpackBf16(hp[2 * c + 1], h + 8);
+        for (int k = 0; k < 16; ++k) h[k] += fmaxf(v[k] + S.bu[16 * c + k], 0.0f);
+        uint4* op = reinterpret_cast<uint4*>(hout + 64 * row);
+        op[2 * c] = packBf16(h);
+        op[2 * c + 1] = packBf16(h + 8);
+      }
+    }
+    umma::fenceBeforeSync();
+    __syncthreads();
+  }
+  T.done();
+}
+
+// ------------------------------------------------------------------------------------------------------------------
+// Output: o_s = W_o [h_i; h_j; eps_s] + b_o on lower live slots; G_s and L_s = C_i G_s.
+
+struct OutputSmem {
+  unsigned char x[128 * 192 * 2];
+  unsigned char w[16 * 192 * 2];
+  float b[16];
+  int slotRow[128];
+  int rowFirst[129];
+  uint64_t bar;
+  uint32_t tmem;
+};
+
+__device__ __forceinline__ void outputToG(const float* o, bool diag, float* G) {
+  if (diag) {
+    G[0] = expf(fminf(fmaxf(o[0], -kDiagClamp), kDiagClamp));
+    G[1] = 0.0f;
+    G[2] = 0.0f;
+    G[3] = o[3];
+    G[4] = expf(fminf(fmaxf(o[1], -kDiagClamp), kDiagClamp));
+    G[5] = 0.0f;
+    G[6] = o[4];
+    G[7] = o[5];
+    G[8] = expf(fminf(fmaxf(o[2], -kDiagClamp), kDiagClamp));
+  } else {
+    for (int k = 0; k < 9; ++k) G[k] = o[k];
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_output(Graph g, const __nv_bfloat16* __restrict__ Wo,
+                                                     const float* __restrict__ bo, const __nv_bfloat16* __restrict__ h,
+                                                     int training, int* error) {
+  OutputSmem& S = *reinterpret_cast<OutputSmem*>(alignSmem(netSmem));
+  TileCtx T;
+  T.init(&S.bar, &S.tmem, 32, error);
+  const int t = threadIdx.x;
+  stageWeights(S.w, Wo, 16, 192);
+  if (t < 16) S.b[t] = bo[t];
+  for (uint32_t tile = blockIdx.x; tile < g.nTiles; tile += gridDim.x) {
+    const TileRows tr = tileRows(g, tile);
+    tileSlotInfo(g, tr, S.slotRow, S.rowFirst, false);
+    for (int k = t; k < 128 * 24; k += kThreads) {
+      const int q = k / 24, c = k % 24;
+      uint4 v = zero4();
+      const int sr = S.slotRow[q];
+      if (sr >= 0) {
+        const uint32_t s = tr.s0 + q;
+        if (c < 8) v = reinterpret_cast<const uint4*>(h + 64 * static_cast<size_t>(tr.r0 + sr))[c];
+        else if (c < 16) v = reinterpret_cast<const uint4*>(h + 64 * static_cast<size_t>(colOf(g, s)))[c - 8];
+        else v = reinterpret_cast<const uint4*>(g.eps + 64 * static_cast<size_t>(s))[c - 16];
+      }
+      st16(S.x, q, c, 192, v);
+    }
+    if (!T.run([&] { umma::gemmIssue(T.tmem, S.x, S.w, 128, 16, 192, false); })) break;
+    float o[16];
+    T.load(0, o);
+    const int sr = S.slotRow[t];
+    const uint32_t s = tr.s0 + t;
+    if (s < tr.s1) {
+      float G[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, L[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      for (int k = 0; k < 16; ++k) o[k] = sr >= 0 ? o[k] + S.b[k] : 0.0f;
+      if (sr >= 0) {
+        const uint32_t i = tr.r0 + sr;
+        outputToG(o, colOf(g, s) == i, G);
+        const float* C = g.C + 9 * static_cast<size_t>(i);
+        for (int r = 0; r < 3; ++r)
+          for (int c = 0; c < 3; ++c) L[3 * r + c] = C[3 * r] * G[c] + C[3 * r + 1] * G[3 + c] + C[3 * r + 2] * G[6 + c];
+      }
+      for (int k = 0; k < 9; ++k) g.L[k * g.SP + s] = L[k];
+      if (training) {
+        for (int k = 0; k < 9; ++k) g.G[9 * static_cast<size_t>(s) + k] = G[k];
+        for (int k = 0; k < 16; ++k) g.o[16 * static_cast<size_t>(s) + k] = o[k];
+      }
+    }
+    umma::fenceBeforeSync();
+    __syncthreads();
+  }
+  T.done();
+}
+
+// ------------------------------------------------------------------------------------------------------------------
+// Loss: rhat = S^T r, a = G^T rhat, b = G a, e = Ahat b - rhat; backward to d loss / d o. Vectors are float4 (xyz).
+
+__device__ __forceinline__ float3 ld3(const float4* p, uint32_t i) {
+  const float4 v = p[i];
+  return make_float3(v.x, v.y, v.z);
+}
+__device__ __forceinline__ float3 mulM(const float* M, float3 x) {
+  return make_float3(M[0] * x.x + M[1] * x.y + M[2] * x.z, M[3] * x.x + M[4] * x.y + M[5] * x.z,
+                     M[6] * x.x + M[7] * x.y + M[8] * x.z);
+}
+__device__ __forceinline__ float3 mulMT(const float* M, float3 x) {
+  return make_float3(M[0] * x.x + M[3] * x.y + M[6] * x.z, M[1] * x.x + M[4] * x.y + M[7] * x.z,
+                     M[2] * x.x + M[5] * x.y + M[8] * x.z);
+}
+
+__device__ inline void blockSumD(double v, double* out) {
+  __shared__ double red[32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < static_cast<int>((blockDim.x + 31) / 32); ++w) s += red[w];
+    *out = s;
+  }
+}
+
+// rhat_i = C_i^T r_i; partial |rhat|^2 per block.
+__global__ void k_rhat(Graph g, const float* __restrict__ r, float4* rhat, double* partial) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v = 0.0;
+  if (i < g.n) {
+    const float3 x = make_float3(r[3 * i], r[3 * i + 1], r[3 * i + 2]);
+    const float3 y = mulMT(g.C + 9 * static_cast<size_t>(i), x);
+    rhat[i] = make_float4(y.x, y.y, y.z, 0.0f);
+    v = static_cast<double>(y.x) * y.x + static_cast<double>(y.y) * y.y + static_cast<double>(y.z) * y.z;
+  }
+  blockSumD(v, partial + blockIdx.x);
+}
+
+// y_j = sum_{slots (j, i), i >= j} M_{(i, j)}^T x_i, M given per slot (B x 9, zero off the lower live slots).
+__global__ void k_lower_t(Graph g, const float* __restrict__ M, const float4* __restrict__ x, float4* y) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= g.n) return;
+  float3 acc = make_float3(0, 0, 0);
+  for (uint32_t s = __ldg(g.rowStart + j); s < __ldg(g.rowStart + j + 1); ++s) {
+    const uint32_t i = colOf(g, s);
+    if (i < j) continue;
+    const float3 v = mulMT(M + 9 * static_cast<size_t>(__ldg(g.tslot + s)), ld3(x, i));
+    acc.x += v.x;
+    acc.y += v.y;
+    acc.z += v.z;
+  }
+  y[j] = make_float4(acc.x, acc.y, acc.z, 0.0f);
+}
+
+// y_i = sum_{j <= i} M_s x_j.
+__global__ void k_lower(Graph g, const float* __restrict__ M, const float4* __restrict__ x, float4* y) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.n) return;
+  float3 acc = make_float3(0, 0, 0);
+  for (uint32_t s = __ldg(g.rowStart + i); s < __ldg(g.rowStart + i + 1); ++s) {
+    const uint32_t j = colOf(g, s);
+    if (j > i) continue;
+    const float3 v = mulM(M + 9 * static_cast<size_t>(s), ld3(x, j));
+    acc.x += v.x;
+    acc.y += v.y;
+    acc.z += v.z;
+  }
+  y[i] = make_float4(acc.x, acc.y, acc.z, 0.0f);
+}
+
+// y = Ahat x (- sub when given); partial |y|^2 per block.
+__global__ void k_ahat(Graph g, const float4* __restrict__ x, const float4* __restrict__ sub, float4* y,
+                       double* partial) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v = 0.0;
+  if (i < g.n) {
+    float3 acc = make_float3(0, 0, 0);
+    for (uint32_t s = __ldg(g.rowStart + i); s < __ldg(g.rowStart + i + 1); ++s) {
+      const float3 w = mulM(g.Ahat + 9 * static_cast<size_t>(s), ld3(x, colOf(g, s)));
+      acc.x += w.x;
+      acc.y += w.y;
+      acc.z += w.z;
+    }
+    if (sub) {
+      const float3 b = ld3(sub, i);
+      acc.x -= b.x;
+      acc.y -= b.y;
+      acc.z -= b.z;
+    }
+    y[i] = make_float4(acc.x, acc.y, acc.z, 0.0f);
+    v = static_cast<double>(acc.x) * acc.x + static_cast<double>(acc.y) * acc.y + static_cast<double>(acc.z) * acc.z;
+  }
+  blockSumD(v, partial + blockIdx.x);
+}
+
+// out[k] = sum of `count` partials (one block, fixed order).
+__global__ void k_sum(const double* partial, int count, double* out) {
+  __shared__ double s[256];
+  double v = 0.0;
+  for (int k = threadIdx.x; k < count; k += blockDim.x) v += partial[k];
+  s[threadIdx.x] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int k = 0; k < static_cast<int>(blockDim.x); ++k) t += s[k];
+    *out = t;
+  }
+}
+
+// ge = 2 e / |rhat|^2 (scalars[0] = |rhat|^2).
+__global__ void k_ge(uint32_t n, const float4* e, const double* scalars, float4* ge) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float s = static_cast<float>(2.0 / scalars[0]);
+  const float4 v = e[i];
+  ge[i] = make_float4(v.x * s, v.y * s, v.z * s, 0.0f);
+}
+
+// d loss / d o per slot: gG = gb_i a_j^T + rhat_i ga_j^T on lower live slots, mapped through G(o). One warp per row.
+__global__ void k_grad_o(Graph g, const float4* gb, const float4* a, const float4* rhat, const float4* ga,
+                         float* go) {
+  const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) / 32u;
+  const int lane = threadIdx.x & 31;
+  if (i >= g.n) return;
+  const bool pi = pinnedRow(g, i);
+  const float3 gbi = ld3(gb, i), ri = ld3(rhat, i);
+  for (uint32_t s = __ldg(g.rowStart + i) + lane; s < __ldg(g.rowStart + i + 1); s += 32) {
+    const uint32_t j = colOf(g, s);
+    float out[16] = {0};
+    if (!pi && !pinnedRow(g, j) && j <= i) {
+      const float3 aj = ld3(a, j), gaj = ld3(ga, j);
+      const float u[3] = {gbi.x, gbi.y, gbi.z}, v[3] = {aj.x, aj.y, aj.z};
+      const float p[3] = {ri.x, ri.y, ri.z}, w[3] = {gaj.x, gaj.y, gaj.z};
+      float gG[9];
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) gG[3 * r + c] = u[r] * v[c] + p[r] * w[c];
+      if (j == i) {
+        const float* o = g.o + 16 * static_cast<size_t>(s);
+        for (int k = 0; k < 3; ++k) {
+          const float ok = o[k];
+          out[k] = fabsf(ok) < kDiagClamp ? gG[4 * k] * expf(ok) : 0.0f;
+        }
+        out[3] = gG[3];
+        out[4] = gG[6];
+        out[5] = gG[7];
+      } else {
+        for (int k = 0; k < 9; ++k) out[k] = gG[k];
+      }
+    }
+    float4* dst = reinterpret_cast<float4*>(go + 16 * static_cast<size_t>(s));
+    for (int k = 0; k < 4; ++k) dst[k] = make_float4(out[4 * k], out[4 * k + 1], out[4 * k + 2], out[4 * k + 3]);
+  }
+}
+
+// ------------------------------------------------------------------------------------------------------------------
+// Backward, output layer (row tiles): gX = go W_o -> gh_i (row sums into GH), gh_j (GSLOT), geps (GEPS);
+// dW_o^T += X^T go accumulated in TMEM; db_o.
+
+struct BwOutSmem {
+  unsigned char a[128 * 16 * 2];    // go tile (M = 128 slots, K = 16)
+  unsigned char wt[192 * 16 * 2];   // W_o^T (N = 192, K = 16)
+  unsigned char xt[256 * 128 * 2];  // X_out^T (M = 256 features (192 used), K = 128 slots)
+  unsigned char gt[16 * 128 * 2];   // go^T (N = 16, K = 128)
+  float buf[128][65];
+  float gof[128][17];
+  int slotRow[128];
+  int rowFirst[129];
+  uint64_t bar;
+  uint32_t tmem;
+};
+
+__global__ void __launch_bounds__(kThreads) k_bw_output(Graph g, const __nv_bfloat16* __restrict__ Wo,
+                                                        const __nv_bfloat16* __restrict__ h,
+                                                        const float* __restrict__ go, float* GH, float* GSLOT,
+                                                        float* GEPS, float* partials, int* error) {
+  BwOutSmem& S = *reinterpret_cast<BwOutSmem*>(alignSmem(netSmem));
+  TileCtx T;
+  T.init(&S.bar, &S.tmem, 256, error);
+  const int t = threadIdx.x;
+  stageWeightsT(S.wt, Wo, 16, 192);
+  for (int k = t; k < 64 * 128; k += kThreads) st1(S.xt, 192 + k / 128, k % 128, 128, __float2bfloat16_rn(0.0f));
+  float dbAcc = 0.0f;
+  bool first = true, good = true;
+  for (uint32_t tile = blockIdx.x; tile < g.nTiles; tile += gridDim.x) {
+    const TileRows tr = tileRows(g, tile);
+    tileSlotInfo(g, tr, S.slotRow, S.rowFirst, false);
+    const uint32_t nq = tr.s1 - tr.s0;
+    {
+      float v[16] = {0};
+      if (t < static_cast<int>(nq)) {
+        const float4* src = reinterpret_cast<const float4*>(go + 16 * static_cast<size_t>(tr.s0 + t));
+        for (int k = 0; k < 4; ++k) {
+          const float4 w = src[k];
+          v[4 * k] = w.x;
+          v[4 * k + 1] = w.y;
+          v[4 * k + 2] = w.z;
+          v[4 * k + 3] = w.w;
+        }
+      }
+      float rv[16];
+      const uint4 p0 = packBf16(v), p1 = packBf16(v + 8);
+      unpackBf16(p0, rv);
+      unpackBf16(p1, rv + 8);
+      st16(S.a, t, 0, 16, p0);
+      st16(S.a, t, 1, 16, p1);
+      for (int k = 0; k < 16; ++k) {
+        S.gof[t][k] = rv[k];
+        st1(S.gt, k, t, 128, __float2bfloat16_rn(rv[k]));
+      }
+    }
+    for (int k = t; k < 128 * 24; k += kThreads) {
+      const int q = k / 24, c = k % 24;
+      uint4 v = zero4();
+      if (q < static_cast<int>(nq)) {
+        const uint32_t s = tr.s0 + q;
+        const int sr = S.slotRow[q] >= 0 ? S.slotRow[q] : -S.slotRow[q] - 2;
+        if (c < 8) v = reinterpret_cast<const uint4*>(h + 64 * static_cast<size_t>(tr.r0 + sr))[c];
+        else if (c < 16) v = reinterpret_cast<const uint4*>(h + 64 * static_cast<size_t>(colOf(g, s)))[c - 8];
+        else v = reinterpret_cast<const uint4*>(g.eps + 64 * static_cast<size_t>(s))[c - 16];
+      }
+      st16T(S.xt, q, c, 128, v);
+    }
+    const bool acc = !first;
+    good = T.run([&] {
+      umma::gemmIssue(T.tmem, S.a, S.wt, 128, 192, 16, false);
+      umma::gemmIssue(T.tmem + 192, S.xt, S.gt, 128, 16, 128, acc);
+      umma::gemmIssue(T.tmem + 224, S.xt + 16 * (16 * 128), S.gt, 128, 16, 128, acc);
+    });
+    if (!good) break;
+    first = false;
+    for (int c = 0; c < 12; ++c) {
+      float v[16];
+      T.load(16 * c, v);
+      if (t < static_cast<int>(nq)) {
+        const size_t s = tr.s0 + t;
+        if (c < 4) {
+          for (int k = 0; k < 16; ++k) S.buf[t][16 * c + k] = v[k];
+        } else if (c < 8) {
+          float4* d = reinterpret_cast<float4*>(GSLOT + 64 * s + 16 * (c - 4));
+          for (int k = 0; k < 4; ++k) d[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+        } else {
+          float4* d = reinterpret_cast<float4*>(GEPS + 64 * s + 16 * (c - 8));
+          for (int k = 0; k < 4; ++k) d[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+        }
+      }
+    }
+    __syncthreads();
+    const int R = static_cast<int>(tr.r1 - tr.r0);
+    for (int k = t; k < R * 64; k += kThreads) {
+      const int r = k / 64, f = k % 64;
+      float sum = 0.0f;
+      for (int q = S.rowFirst[r]; q < S.rowFirst[r + 1]; ++q) sum += S.buf[q][f];
+      GH[64 * static_cast<size_t>(tr.r0 + r) + f] = sum;
+    }
+    if (t < 16)
+      for (int q = 0; q < static_cast<int>(nq); ++q) dbAcc += S.gof[q][t];
+    umma::fenceBeforeSync();
+    __syncthreads();
+  }
+  float* P = partials + static_cast<size_t>(blockIdx.x) * (Layout::kOB - Layout::kO + kOutputs);
+  if (good && !first) {
+    for (int blk = 0; blk < 2; ++blk) {
+      float v[16];
+      T.load(192 + 32 * blk, v);
+      const int m = 128 * blk + t;
+      if (m < 192)
+        for (int o = 0; o < 16; ++o) P[o * 192 + m] = v[o];
+    }
+  } else {
+    for (int k = t; k < 16 * 192; k += kThreads) P[k] = 0.0f;
+  }
+  if (t < 16) P[16 * 192 + t] = dbAcc;
+  T.done();
+}
+
+// GH[j] (+)= sum over slots (j, i) of GSLOT[(i, j)]: messages (i != j, both live) or lower slots (i >= j).
+__global__ void k_gather(Graph g, const float* __restrict__ GSLOT, float* GH, int messages) {
+  const uint32_t j = (blockIdx.x * blockDim.x + threadIdx.x) / 32u;
+  const int lane = threadIdx.x & 31;
+  if (j >= g.n) return;
+  const bool pj = pinnedRow(g, j);
+  float a0 = GH[64 * static_cast<size_t>(j) + lane], a1 = GH[64 * static_cast<size_t>(j) + 32 + lane];
+  for (uint32_t s = __ldg(g.rowStart + j); s < __ldg(g.rowStart + j + 1); ++s) {
+    const uint32_t i = colOf(g, s);
+    const bool keep = messages ? (i != j && !pj && !pinnedRow(g, i)) : (i >= j);
+    if (!keep) continue;
+    const size_t ts = __ldg(g.tslot + s);
+    a0 += GSLOT[64 * ts + lane];
+    a1 += GSLOT[64 * ts + 32 + lane];
+  }
+  GH[64 * static_cast<size_t>(j) + lane] = a0;
+  GH[64 * static_cast<size_t>(j) + 32 + lane] = a1;
+}
+
+// ------------------------------------------------------------------------------------------------------------------
+// Backward, one message-passing layer (row tiles).
+
+struct BwLayerSmem {
+  unsigned char x[128 * 128 * 2];   // X_upd, then X_msg (M = 128, K = 128)
+  unsigned char xt[128 * 128 * 2];  // transposed X (M = 128 features, K = 128 rows / slots)
+  unsigned char ga[128 * 64 * 2];   // gu / gv (M = 128, K = 64)
+  unsigned char gt[64 * 128 * 2];   // gu^T / gv^T (N = 64, K = 128)
+  unsigned char wu[64 * 128 * 2];   // W_u (N = 64, K = 128)
+  unsigned char wm[64 * 128 * 2];   // W_m
+  unsigned char wut[128 * 64 * 2];  // W_u^T (N = 128, K = 64)
+  unsigned char wmt[128 * 64 * 2];  // W_m^T
+  float buf[128][65];
+  float bu[64], bm[64];
+  int slotRow[128];
+  int rowFirst[129];
+  uint64_t bar;
+  uint32_t tmem;
+};
+
+__global__ void __launch_bounds__(kThreads) k_bw_layer(Graph g, const __nv_bfloat16* __restrict__ Wm,
+                                                       const __nv_bfloat16* __restrict__ Wu,
+                                                       const float* __restrict__ bm, const float* __restrict__ bu,
+                                                       const __nv_bfloat16* __restrict__ hl,
+                                                       const __nv_bfloat16* __restrict__ agg,
+                                                       const float* __restrict__ GH, float* GHprev, float* GSLOT,
+                                                       float* GEPS, float* partials, int* error) {
+  BwLayerSmem& S = *reinterpret_cast<BwLayerSmem*>(alignSmem(netSmem));
+  TileCtx T;
+  T.init(&S.bar, &S.tmem, 512, error);
+  const int t = threadIdx.x;
+  stageWeights(S.wu, Wu, 64, 128);
+  stageWeights(S.wm, Wm, 64, 128);
+  stageWeightsT(S.wut, Wu, 64, 128);
+  stageWeightsT(S.wmt, Wm, 64, 128);
+  if (t < 64) {
+    S.bu[t] = bu[t];
+    S.bm[t] = bm[t];
+  }
+  float dbu = 0.0f, dbm = 0.0f;
+  bool first = true, good = true;
+  constexpr uint32_t kU = 0, kGX = 64, kDWU = 192, kDWM = 256;
+  for (uint32_t tile = blockIdx.x; tile < g.nTiles; tile += gridDim.x) {
+    const TileRows tr = tileRows(g, tile);
+    tileSlotInfo(g, tr, S.slotRow, S.rowFirst, true);
+    const int R = static_cast<int>(tr.r1 - tr.r0);
+    const int nq = static_cast<int>(tr.s1 - tr.s0);
+    const bool acc = !first;
+    // --- node part: u = W_u [h; a] + b_u, gu = GH (u > 0).
+    for (int k = t; k < 128 * 16; k += kThreads) {
+      const int r = k / 16, c = k % 16;
+      uint4 v = zero4();
+      if (r < R)
+        v = c < 8 ? reinterpret_cast<const uint4*>(hl + 64 * static_cast<size_t>(tr.r0 + r))[c]
+                  : reinterpret_cast<const uint4*>(agg + 64 * static_cast<size_t>(tr.r0 + r))[c - 8];
+      st16(S.x, r, c, 128, v);
+      st16T(S.xt, r, c, 128, v);
+    }
+    if (!(good = T.run([&] { umma::gemmIssue(T.tmem + kU, S.x, S.wu, 128, 64, 128, false); }))) break;
+    {
+      float gu[64];
+      for (int c = 0; c < 4; ++c) {
+        float v[16];
+        T.load(kU + 16 * c, v);
+        for (int k = 0; k < 16; ++k) {
+          const int f = 16 * c + k;
+          const float u = v[k] + S.bu[f];
+          gu[f] = (t < R && u > 0.0f) ? GH[64 * static_cast<size_t>(tr.r0 + t) + f] : 0.0f;
+        }
+      }
+      for (int c = 0; c < 8; ++c) {
+        const uint4 p = packBf16(gu + 8 * c);
+        st16(S.ga, t, c, 64, p);
+        float rv[8];
+        unpackBf16(p, rv);
+        for (int k = 0; k < 8; ++k) {
+          S.buf[t][8 * c + k] = rv[k];
+          st1(S.gt, 8 * c + k, t, 128, reinterpret_cast<const __nv_bfloat16*>(&p)[k]);
+        }
+      }
+    }
+    __syncthreads();
+    if (t < 64)
+      for (int q = 0; q < R; ++q) dbu += S.buf[q][t];
+    if (!(good = T.run([&] {
+          umma::gemmIssue(T.tmem + kGX, S.ga, S.wut, 128, 128, 64, false);
+          umma::gemmIssue(T.tmem + kDWU, S.xt, S.gt, 128, 64, 128, acc);
+        })))
+      break;
+    // gh_prev = GH + gX[0:64]; ga = gX[64:128] -> buf.
+    for (int c = 0; c < 8; ++c) {
+      float v[16];
+      T.load(kGX + 16 * c, v);
+      if (t < R) {
+        const size_t row = tr.r0 + t;
+        if (c < 4) {
+          for (int k = 0; k < 16; ++k) GHprev[64 * row + 16 * c + k] = GH[64 * row + 16 * c + k] + v[k];
+        } else {
+          for (int k = 0; k < 16; ++k) S.buf[t][16 * (c - 4) + k] = v[k];
+        }
+      }
+    }
+    __syncthreads();
+    // --- message part: v = W_m [h_j; eps_s] + b_m, gv = (ga_i / 8) (v > 0).
+    for (int k = t; k < 128 * 16; k += kThreads) {
+      const int q = k / 16, c = k % 16;
+      uint4 v = zero4();
+      if (S.slotRow[q] >= 0) {
+        const uint32_t s = tr.s0 + q;
+        v = c < 8 ? reinterpret_cast<const uint4*>(hl + 64 * static_cast<size_t>(colOf(g, s)))[c]
+                  : reinterpret_cast<const uint4*>(g.eps + 64 * static_cast<size_t>(s))[c - 8];
+      }
+      st16(S.x, q, c, 128, v);
+      st16T(S.xt, q, c, 128, v);
+    }
+    if (!(good = T.run([&] { umma::gemmIssue(T.tmem + kU, S.x, S.wm, 128, 64, 128, false); }))) break;
+    float gv[64];
+    {
+      const int sr = S.slotRow[t];
+      for (int c = 0; c < 4; ++c) {
+        float v[16];
+        T.load(kU + 16 * c, v);
+        for (int k = 0; k < 16; ++k) {
+          const int f = 16 * c + k;
+          const float pre = v[k] + S.bm[f];
+          gv[f] = (sr >= 0 && pre > 0.0f) ? S.buf[sr][f] * kAggScale : 0.0f;
+        }
+      }
+    }
+    __syncthreads();  // buf (ga) fully read
+    for (int c = 0; c < 8; ++c) {
+      const uint4 p = packBf16(gv + 8 * c);
+      st16(S.ga, t, c, 64, p);
+      float rv[8];
+      unpackBf16(p, rv);
+      for (int k = 0; k < 8; ++k) {
+        S.buf[t][8 * c + k] = rv[k];
+        st1(S.gt, 8 * c + k, t, 128, reinterpret_cast<const __nv_bfloat16*>(&p)[k]);
+      }
+    }
+    __syncthreads();
+    if (t < 64)
+      for (int q = 0; q < nq; ++q) dbm += S.buf[q][t];
+    if (!(good = T.run([&] {
+          umma::gemmIssue(T.tmem + kGX, S.ga, S.wmt, 128, 128, 64, false);
+          umma::gemmIssue(T.tmem + kDWM, S.xt, S.gt, 128, 64, 128, acc);
+        })))
+      break;
+    first = false;
+    for (int c = 0; c < 8; ++c) {
+      float v[16];
+      T.load(kGX + 16 * c, v);
+      if (t < nq) {
+        const size_t s = tr.s0 + t;
+        if (c < 4) {
+          float4* d = reinterpret_cast<float4*>(GSLOT + 64 * s + 16 * c);
+          for (int k = 0; k < 4; ++k) d[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+        } else if (S.slotRow[t] >= 0) {
+          float* d = GEPS + 64 * s + 16 * (c - 4);
+          for (int k = 0; k < 16; ++k) d[k] += v[k];
+        }
+      }
+    }
+    umma::fenceBeforeSync();
+    __syncthreads();
+  }
+  // Partials in the layer's parameter order: W_m, b_m, W_u, b_u.
+  constexpr size_t W = kHidden * 2 * kHidden;
+  float* P = partials + static_cast<size_t>(blockIdx.x) * Layout::kLayerSize;
+  if (good && !first) {
+    for (int c = 0; c < 4; ++c) {
+      float vm[16], vu[16];
+      T.load(kDWM + 16 * c, vm);
+      T.load(kDWU + 16 * c, vu);
+      for (int k = 0; k < 16; ++k) {
+        P[(16 * c + k) * 128 + t] = vm[k];
+        P[W + kHidden + (16 * c + k) * 128 + t] = vu[k];
+      }
+    }
+  } else {
+    for (size_t k = t; k < Layout::kLayerSize; k += kThreads) P[k] = 0.0f;
+  }
+  __syncthreads();
+  if (t < 64) {
+    P[W + t] = dbm;
+    P[2 * W + kHidden + t] = dbu;
+  }
+  T.done();
+}
+
+// ------------------------------------------------------------------------------------------------------------------
+// Backward of an encoder: q = X W^T + b, gq = G (q > 0); dW^T += X^T gq (X has 16 features, padded to 128 rows).
+
+struct BwEncSmem {
+  unsigned char x[128 * 16 * 2];
+  unsigned char w[64 * 16 * 2];
+  unsigned char xt[128 * 128 * 2];
+  unsigned char gt[64 * 128 * 2];
+  float buf[128][65];
+  float b[64];
+  uint64_t bar;
+  uint32_t tmem;
+};
+
+__global__ void __launch_bounds__(kThreads) k_bw_encode(uint32_t rows, const __nv_bfloat16* __restrict__ X,
+                                                        const __nv_bfloat16* __restrict__ W,
+                                                        const float* __restrict__ b, const float* __restrict__ G,
+                                                        float* partials, int* error) {
+  BwEncSmem& S = *reinterpret_cast<BwEncSmem*>(alignSmem(netSmem));
+  TileCtx T;
+  T.init(&S.bar, &S.tmem, 128, error);
+  const int t = threadIdx.x;
+  for (int k = t; k < 64 * 2; k += kThreads) st16(S.w, k / 2, k % 2, 16, reinterpret_cast<const uint4*>(W)[k]);
+  for (int k = t; k < 112 * 128; k += kThreads) st1(S.xt, 16 + k / 128, k % 128, 128, __float2bfloat16_rn(0.0f));
+  if (t < 64) S.b[t] = b[t];
+  float db = 0.0f;
+  bool first = true, good = true;
+  const uint32_t tiles = (rows + 127) / 128;
+  for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const uint32_t r0 = tile * 128;
+    for (int k = t; k < 128 * 2; k += kThreads) {
+      const uint32_t q = k / 2, c = k % 2, r = r0 + q;
+      const uint4 v = r < rows ? reinterpret_cast<const uint4*>(X + 16 * static_cast<size_t>(r))[c] : zero4();
+      st16(S.x, q, c, 16, v);
+      st16T(S.xt, q, c, 128, v);
+    }
+    if (!(good = T.run([&] { umma::gemmIssue(T.tmem, S.x, S.w, 128, 64, 16, false); }))) break;
+    const uint32_t r = r0 + t;
+    for (int c = 0; c < 4; ++c) {
+      float v[16];
+      T.load(16 * c, v);
+      float gq[16];
+      for (int k = 0; k < 16; ++k) {
+        const float q = v[k] + S.b[16 * c + k];
+        gq[k] = (r < rows && q > 0.0f) ? G[64 * static_cast<size_t>(r) + 16 * c + k] : 0.0f;
+      }
+      const uint4 p0 = packBf16(gq), p1 = packBf16(gq + 8);
+      float rv[16];
+      unpackBf16(p0, rv);
+      unpackBf16(p1, rv + 8);
+      for (int k = 0; k < 16; ++k) {
+        S.buf[t][16 * c + k] = rv[k];
+        st1(S.gt, 16 * c + k, t, 128, __float2bfloat16_rn(rv[k]));
+      }
+    }
+    __syncthreads();
+    if (t < 64)
+      for (int q = 0; q < 128; ++q) db += S.buf[q][t];
+    const bool acc = !first;
+    if (!(good = T.run([&] { umma::gemmIssue(T.tmem + 64, S.xt, S.gt, 128, 64, 128, acc); }))) break;
+    first = false;
+  }
+  float* P = partials + static_cast<size_t>(blockIdx.x) * (64 * 16 + 64);
+  if (good && !first) {
+    for (int c = 0; c < 4; ++c) {
+      float v[16];
+      T.load(64 + 16 * c, v);
+      if (t < 16)
+        for (int k = 0; k < 16; ++k) P[(16 * c + k) * 16 + t] = v[k];
+    }
+  } else {
+    for (int k = t; k < 64 * 16; k += kThreads) P[k] = 0.0f;
+  }
+  if (t < 64) P[64 * 16 + t] = db;
+  T.done();
+}
+
+// ------------------------------------------------------------------------------------------------------------------
+// Gradient reduction and optimiser.
+
+__global__ void k_reduce(const float* __restrict__ partials, int grid, uint32_t count, float* dst, float scale) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= count) return;
+  float s = 0.0f;
+  for (int c = 0; c < grid; ++c) s += partials[static_cast<size_t>(c) * count + p];
+  dst[p] += scale * s;
+}
+
+__global__ void k_adam(float* master, float* grad, float* m, float* v, uint32_t count, float lr, float b1, float b2,
+                       float eps, float c1, float c2, __nv_bfloat16* wb) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= count) return;
+  const float gr = grad[p];
+  const float mm = b1 * m[p] + (1.0f - b1) * gr;
+  const float vv = b2 * v[p] + (1.0f - b2) * gr * gr;
+  m[p] = mm;
+  v[p] = vv;
+  const float w = master[p] - lr * (mm / c1) / (sqrtf(vv / c2) + eps);
+  master[p] = w;
+  wb[p] = __float2bfloat16_rn(w);
+  grad[p] = 0.0f;
+}
+
+__global__ void k_to_bf16(const float* src, __nv_bfloat16* dst, uint32_t count) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < count) dst[p] = __float2bfloat16_rn(src[p]);
+}
+
+template <class T>
+T* dalloc(size_t count) {
+  T* p = nullptr;
+  NCK(cudaMalloc(&p, sizeof(T) * std::max<size_t>(count, 1)));
+  NCK(cudaMemset(p, 0, sizeof(T) * std::max<size_t>(count, 1)));
+  return p;
+}
+
+size_t smemFor(size_t bytes) { return bytes + 128; }
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------------------------------
+// Host side.
+
+std::vector<uint32_t> rowTiles(const std::vector<uint32_t>& rowStart) {
+  std::vector<uint32_t> tiles{0};
+  const uint32_t n = static_cast<uint32_t>(rowStart.size()) - 1;
+  uint32_t first = 0;
+  for (uint32_t r = 0; r < n; ++r) {
+    if (rowStart[r + 1] - rowStart[first] > static_cast<uint32_t>(kTileSlots)) {
+      tiles.push_back(r);
+      first = r;
+    }
+    if (rowStart[r + 1] - rowStart[r] > static_cast<uint32_t>(kTileSlots))
+      throw std::invalid_argument("a row has more than 128 slots");
+  }
+  tiles.push_back(n);
+  return tiles;
+}
+
+std::vector<uint32_t> transposedSlots(const std::vector<uint32_t>& rowStart, const std::vector<uint32_t>& colIndex) {
+  const uint32_t n = static_cast<uint32_t>(rowStart.size()) - 1;
+  std::vector<uint32_t> t(colIndex.size());
+  for (uint32_t i = 0; i < n; ++i)
+    for (uint32_t s = rowStart[i]; s < rowStart[i + 1]; ++s) {
+      const uint32_t j = colIndex[s] & ~kPinBit;
+      const auto b = colIndex.begin() + rowStart[j], e = colIndex.begin() + rowStart[j + 1];
+      auto it = std::lower_bound(b, e, i, [](uint32_t c, uint32_t v) { return (c & ~kPinBit) < v; });
+      if (it == e || (*it & ~kPinBit) != i) throw std::invalid_argument("the block pattern is not symmetric");
+      t[s] = static_cast<uint32_t>(it - colIndex.begin());
+    }
+  return t;
+}
+
+struct GraphStore {
+  Graph g;
+  std::vector<void*> owned;
+  std::vector<float4> residuals;  // residualCount x n (host copies, staged on demand)
+  uint32_t residualCount = 0;
+  float4 *rhat = nullptr, *a = nullptr, *b = nullptr, *e = nullptr, *ge = nullptr, *gb = nullptr, *ga = nullptr;
+  float *r = nullptr, *go = nullptr, *GH = nullptr, *GH2 = nullptr, *GSLOT = nullptr, *GEPS = nullptr;
+  double* partial = nullptr;
+  int partialCount = 0;
+  ~GraphStore() {
+    for (void* p : owned) cudaFree(p);
+  }
+  template <class T>
+  T* own(size_t count) {
+    T* p = dalloc<T>(count);
+    owned.push_back(p);
+    return p;
+  }
+};
+
+namespace {
+
+void allocWorkspace(GraphStore& s, bool training) {
+  Graph& g = s.g;
+  g.C = s.own<float>(9 * static_cast<size_t>(g.n));
+  g.Ahat = s.own<float>(9 * static_cast<size_t>(g.B));
+  g.f = s.own<__nv_bfloat16>(16 * static_cast<size_t>(g.n));
+  g.e = s.own<__nv_bfloat16>(16 * static_cast<size_t>(g.B));
+  g.eps = s.own<__nv_bfloat16>(64 * static_cast<size_t>(g.B));
+  const int hs = training ? kLayers + 1 : 2;
+  for (int l = 0; l < hs; ++l) g.h[l] = s.own<__nv_bfloat16>(64 * static_cast<size_t>(g.n));
+  g.L = s.own<float>(9 * static_cast<size_t>(g.SP));
+  if (training) {
+    for (int l = 0; l < kLayers; ++l) g.agg[l] = s.own<__nv_bfloat16>(64 * static_cast<size_t>(g.n));
+    g.G = s.own<float>(9 * static_cast<size_t>(g.B));
+    g.o = s.own<float>(16 * static_cast<size_t>(g.B));
+    for (float4** v : {&s.rhat, &s.a, &s.b, &s.e, &s.ge, &s.gb, &s.ga}) *v = s.own<float4>(g.n);
+    s.r = s.own<float>(3 * static_cast<size_t>(g.n));
+    s.go = s.own<float>(16 * static_cast<size_t>(g.B));
+    s.GH = s.own<float>(64 * static_cast<size_t>(g.n));
+    s.GH2 = s.own<float>(64 * static_cast<size_t>(g.n));
+    s.GSLOT = s.own<float>(64 * static_cast<size_t>(g.B));
+    s.GEPS = s.own<float>(64 * static_cast<size_t>(g.B));
+    s.partialCount = static_cast<int>((g.n + 255) / 256);
+    s.partial = s.own<double>(s.partialCount + 4);
+  }
+}
+
+int gridFor(uint32_t work, int cap) { return static_cast<int>(std::max<uint32_t>(1, std::min<uint32_t>(work, cap))); }
+
+}  // namespace
+
+Network::Network(int device) : device_(device) {
+  NCK(cudaSetDevice(device));
+  cudaDeviceProp prop{};
+  NCK(cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10) throw std::runtime_error("cuda: the learned preconditioner needs an sm_100 device");
+  numSMs_ = prop.multiProcessorCount;
+  NCK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  master_ = dalloc<float>(Layout::kCount);
+  wBf16_ = dalloc<__nv_bfloat16>(Layout::kCount);
+  grad_ = dalloc<float>(Layout::kCount);
+  adamM_ = dalloc<float>(Layout::kCount);
+  adamV_ = dalloc<float>(Layout::kCount);
+  partialsCount_ = static_cast<size_t>(numSMs_) * Layout::kLayerSize;
+  partials_ = dalloc<float>(partialsCount_);
+  error_ = dalloc<int>(1);
+  scalars_ = dalloc<double>(8);
+  const struct {
+    const void* fn;
+    size_t bytes;
+  } kernels[] = {{reinterpret_cast<const void*>(k_encode), sizeof(EncodeSmem)},
+                 {reinterpret_cast<const void*>(k_layer), sizeof(LayerSmem)},
+                 {reinterpret_cast<const void*>(k_output), sizeof(OutputSmem)},
+                 {reinterpret_cast<const void*>(k_bw_output), sizeof(BwOutSmem)},
+                 {reinterpret_cast<const void*>(k_bw_layer), sizeof(BwLayerSmem)},
+                 {reinterpret_cast<const void*>(k_bw_encode), sizeof(BwEncSmem)}};
+  for (const auto& k : kernels)
+    NCK(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smemFor(k.bytes))));
+}
+
+Network::~Network() {
+  samples_.clear();
+  for (void* p : std::initializer_list<void*>{master_, wBf16_, grad_, adamM_, adamV_, partials_, error_, scalars_})
+    if (p) cudaFree(p);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+void Network::setParams(const float* p, size_t count) {
+  if (count != Layout::kCount) throw std::invalid_argument("expected " + std::to_string(Layout::kCount) + " parameters");
+  NCK(cudaMemcpyAsync(master_, p, sizeof(float) * count, cudaMemcpyHostToDevice, stream_));
+  k_to_bf16<<<(count + 255) / 256, 256, 0, stream_>>>(master_, wBf16_, static_cast<uint32_t>(count));
+  NCK(cudaGetLastError());
+  NCK(cudaMemsetAsync(adamM_, 0, sizeof(float) * count, stream_));
+  NCK(cudaMemsetAsync(adamV_, 0, sizeof(float) * count, stream_));
+  NCK(cudaMemsetAsync(grad_, 0, sizeof(float) * count, stream_));
+  adamStep_ = 0;
+  NCK(cudaStreamSynchronize(stream_));
+}
+
+void Network::getParams(float* p, size_t count) {
+  if (count != Layout::kCount) throw std::invalid_argument("expected " + std::to_string(Layout::kCount) + " parameters");
+  NCK(cudaMemcpyAsync(p, master_, sizeof(float) * count, cudaMemcpyDeviceToHost, stream_));
+  NCK(cudaStreamSynchronize(stream_));
+}
+
+int Network::addSample(uint32_t n, const uint32_t* rowStart, const uint32_t* colIndex, const float* blocks,
+                       const uint8_t* pinned, const uint8_t* active, const float* residuals, uint32_t residualCount) {
+  if (!rowStart || !colIndex || !blocks || !pinned || !active || (residualCount && !residuals))
+    throw std::invalid_argument("null argument");
+  auto s = std::make_unique<GraphStore>();
+  std::vector<uint32_t> rs(rowStart, rowStart + n + 1);
+  const uint32_t B = rs[n];
+  std::vector<uint32_t> ci(colIndex, colIndex + B);
+  for (uint32_t i = 0; i < n; ++i)
+    for (uint32_t k = rs[i]; k < rs[i + 1]; ++k) {
+      if (ci[k] >= n) throw std::invalid_argument("column index out of range");
+      if (k > rs[i] && ci[k] <= ci[k - 1]) throw std::invalid_argument("columns must increase along a row");
+    }
+  const auto tiles = rowTiles(rs);
+  const auto ts = transposedSlots(rs, ci);
+  Graph& g = s->g;
+  g.n = n;
+  g.B = B;
+  g.SP = (B + 31u) & ~31u;
+  g.nTiles = static_cast<uint32_t>(tiles.size() - 1);
+  auto upload = [&](auto* dst, const auto* src, size_t count) {
+    NCK(cudaMemcpyAsync(dst, src, sizeof(*src) * count, cudaMemcpyHostToDevice, stream_));
+  };
+  uint32_t* drs = s->own<uint32_t>(n + 1);
+  uint32_t* dci = s->own<uint32_t>(B);
+  uint32_t* dts = s->own<uint32_t>(B);
+  uint32_t* dtiles = s->own<uint32_t>(tiles.size());
+  float* dbl = s->own<float>(9 * static_cast<size_t>(g.SP));
+  uint8_t* dpin = s->own<uint8_t>(n);
+  uint8_t* dact = s->own<uint8_t>(n);
+  std::vector<float> planes(9 * static_cast<size_t>(g.SP), 0.0f);
+  for (size_t k = 0; k < B; ++k)
+    for (int c = 0; c < 9; ++c) planes[c * g.SP + k] = blocks[9 * k + c];
+  upload(drs, rs.data(), rs.size());
+  upload(dci, ci.data(), ci.size());
+  upload(dts, ts.data(), ts.size());
+  upload(dtiles, tiles.data(), tiles.size());
+  upload(dbl, planes.data(), planes.size());
+  upload(dpin, pinned, n);
+  upload(dact, active, n);
+  g.rowStart = drs;
+  g.colIndex = dci;
+  g.tslot = dts;
+  g.tileRow = dtiles;
+  g.blocks = dbl;
+  g.pinnedBase = dpin;
+  g.activeBase = dact;
+  allocWorkspace(*s, true);
+  s->residualCount = residualCount;
+  s->residuals.resize(static_cast<size_t>(residualCount) * n);
+  for (size_t k = 0; k < static_cast<size_t>(residualCount) * n; ++k)
+    s->residuals[k] = make_float4(residuals[3 * k], residuals[3 * k + 1], residuals[3 * k + 2], 0.0f);
+  NCK(cudaStreamSynchronize(stream_));
+  samples_.push_back(std::move(s));
+  return static_cast<int>(samples_.size()) - 1;
+}
+
+void Network::clearSamples() { samples_.clear(); }
+int Network::sampleCount() const { return static_cast<int>(samples_.size()); }
+
+Graph& Network::graphOf(GraphStore& s) { return s.g; }
+
+std::unique_ptr<GraphStore> Network::bind(uint32_t n, uint32_t B, uint32_t SP, const uint32_t* hostRowStart,
+                                          const uint32_t* hostColIndex, const uint32_t* dRowStart,
+                                          const uint32_t* dColIndex, const float* dBlocks,
+                                          const uint8_t* pinnedBase, uint32_t pinnedStride,
+                                          const uint8_t* activeBase, uint32_t activeStride, cudaStream_t st) {
+  auto s = std::make_unique<GraphStore>();
+  std::vector<uint32_t> rs(hostRowStart, hostRowStart + n + 1), ci(hostColIndex, hostColIndex + B);
+  const auto tiles = rowTiles(rs);
+  const auto ts = transposedSlots(rs, ci);
+  Graph& g = s->g;
+  g.n = n;
+  g.B = B;
+  g.SP = SP;
+  g.nTiles = static_cast<uint32_t>(tiles.size() - 1);
+  uint32_t* dts = s->own<uint32_t>(B);
+  uint32_t* dtiles = s->own<uint32_t>(tiles.size());
+  NCK(cudaMemcpyAsync(dts, ts.data(), sizeof(uint32_t) * B, cudaMemcpyHostToDevice, st));
+  NCK(cudaMemcpyAsync(dtiles, tiles.data(), sizeof(uint32_t) * tiles.size(), cudaMemcpyHostToDevice, st));
+  g.rowStart = dRowStart;
+  g.colIndex = dColIndex;
+  g.tslot = dts;
+  g.tileRow = dtiles;
+  g.blocks = dBlocks;
+  g.pinnedBase = pinnedBase;
+  g.pinnedStride = pinnedStride;
+  g.activeBase = activeBase;
+  g.activeStride = activeStride;
+  allocWorkspace(*s, false);
+  NCK(cudaStreamSynchronize(st));
+  return s;
+}
+
+void Network::forwardOn(Graph& g, cudaStream_t st, bool training) {
+  const int rowBlocks = static_cast<int>((g.n + 127) / 128);
+  k_scale<<<rowBlocks, 128, 0, st>>>(g);
+  k_features<<<static_cast<int>((g.n + 7) / 8), 256, 0, st>>>(g);
+  const int cap = 2 * numSMs_;
+  const __nv_bfloat16* W = wBf16_;
+  const float* M = master_;
+  k_encode<<<gridFor((g.n + 127) / 128, cap), kThreads, smemFor(sizeof(EncodeSmem)), st>>>(
+      g.n, g.f, W + Layout::kNe, M + Layout::kNeB, g.h[0], error_);
+  k_encode<<<gridFor((g.B + 127) / 128, cap), kThreads, smemFor(sizeof(EncodeSmem)), st>>>(
+      g.B, g.e, W + Layout::kEe, M + Layout::kEeB, g.eps, error_);
+  for (int l = 0; l < kLayers; ++l) {
+    const __nv_bfloat16* hin = training ? g.h[l] : g.h[l & 1];
+    __nv_bfloat16* hout = training ? g.h[l + 1] : g.h[(l + 1) & 1];
+    k_layer<<<gridFor(g.nTiles, cap), kThreads, smemFor(sizeof(LayerSmem)), st>>>(
+        g, W + Layout::m(l), W + Layout::u(l), M + Layout::mB(l), M + Layout::uB(l), hin, hout,
+        training ? g.agg[l] : nullptr, error_);
+  }
+  k_output<<<gridFor(g.nTiles, cap), kThreads, smemFor(sizeof(OutputSmem)), st>>>(
+      g, W + Layout::kO, M + Layout::kOB, training ? g.h[kLayers] : g.h[kLayers & 1], training ? 1 : 0, error_);
+  NCK(cudaGetLastError());
+}
+
+void Network::lossForward(GraphStore& s, int residual) {
+  Graph& g = s.g;
+  const int nb = static_cast<int>((g.n + 255) / 256);
+  std::vector<float> r(3 * static_cast<size_t>(g.n));
+  for (uint32_t i = 0; i < g.n; ++i) {
+    const float4 v = s.residuals[static_cast<size_t>(residual) * g.n + i];
+    r[3 * i] = v.x;
+    r[3 * i + 1] = v.y;
+    r[3 * i + 2] = v.z;
+  }
+  NCK(cudaMemcpyAsync(s.r, r.data(), sizeof(float) * r.size(), cudaMemcpyHostToDevice, stream_));
+  k_rhat<<<nb, 256, 0, stream_>>>(g, s.r, s.rhat, s.partial);
+  k_sum<<<1, 256, 0, stream_>>>(s.partial, nb, scalars_ + 0);
+  k_lower_t<<<nb, 256, 0, stream_>>>(g, g.G, s.rhat, s.a);
+  k_lower<<<nb, 256, 0, stream_>>>(g, g.G, s.a, s.b);
+  k_ahat<<<nb, 256, 0, stream_>>>(g, s.b, s.rhat, s.e, s.partial);
+  k_sum<<<1, 256, 0, stream_>>>(s.partial, nb, scalars_ + 1);
+  NCK(cudaStreamSynchronize(stream_));  // the host vector r must outlive the copy
+}
+
+void Network::reduceInto(const float* partials, int grid, size_t count, size_t offset, float scale) {
+  k_reduce<<<static_cast<int>((count + 255) / 256), 256, 0, stream_>>>(partials, grid, static_cast<uint32_t>(count),
+                                                                      grad_ + offset, scale);
+  NCK(cudaGetLastError());
+}
+
+void Network::backward(GraphStore& s) {
+  Graph& g = s.g;
+  const int nb = static_cast<int>((g.n + 255) / 256);
+  const int wb = static_cast<int>((g.n + 7) / 8);
+  k_ge<<<nb, 256, 0, stream_>>>(g.n, s.e, scalars_, s.ge);
+  k_ahat<<<nb, 256, 0, stream_>>>(g, s.ge, nullptr, s.gb, s.partial);
+  k_lower_t<<<nb, 256, 0, stream_>>>(g, g.G, s.gb, s.ga);
+  k_grad_o<<<wb, 256, 0, stream_>>>(g, s.gb, s.a, s.rhat, s.ga, s.go);
+  const __nv_bfloat16* W = wBf16_;
+  const float* M = master_;
+  const int grid = gridFor(g.nTiles, numSMs_);
+  k_bw_output<<<grid, kThreads, smemFor(sizeof(BwOutSmem)), stream_>>>(g, W + Layout::kO, g.h[kLayers], s.go, s.GH,
+                                                                         s.GSLOT, s.GEPS, partials_, error_);
+  reduceInto(partials_, grid, Layout::kOB - Layout::kO + kOutputs, Layout::kO, 1.0f);
+  k_gather<<<wb, 256, 0, stream_>>>(g, s.GSLOT, s.GH, 0);
+  float* gh = s.GH;
+  float* ghPrev = s.GH2;
+  for (int l = kLayers - 1; l >= 0; --l) {
+    k_bw_layer<<<grid, kThreads, smemFor(sizeof(BwLayerSmem)), stream_>>>(
+        g, W + Layout::m(l), W + Layout::u(l), M + Layout::mB(l), M + Layout::uB(l), g.h[l], g.agg[l], gh, ghPrev,
+        s.GSLOT, s.GEPS, partials_, error_);
+    reduceInto(partials_, grid, Layout::kLayerSize, Layout::m(l), 1.0f);
+    k_gather<<<wb, 256, 0, stream_>>>(g, s.GSLOT, ghPrev, 1);
+    std::swap(gh, ghPrev);
+  }
+  const int encGridE = gridFor((g.B + 127) / 128, numSMs_);
+  k_bw_encode<<<encGridE, kThreads, smemFor(sizeof(BwEncSmem)), stream_>>>(g.B, g.e, W + Layout::kEe,
+                                                                            M + Layout::kEeB, s.GEPS, partials_,
+                                                                            error_);
+  reduceInto(partials_, encGridE, 64 * 16 + 64, Layout::kEe, 1.0f);
+  const int encGridN = gridFor((g.n + 127) / 128, numSMs_);
+  k_bw_encode<<<encGridN, kThreads, smemFor(sizeof(BwEncSmem)), stream_>>>(g.n, g.f, W + Layout::kNe,
+                                                                            M + Layout::kNeB, gh, partials_, error_);
+  reduceInto(partials_, encGridN, 64 * 16 + 64, Layout::kNe, 1.0f);
+  NCK(cudaGetLastError());
+}
+
+namespace {
+void checkError(int* err, cudaStream_t st) {
+  int h = 0;
+  NCK(cudaMemcpyAsync(&h, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  NCK(cudaStreamSynchronize(st));
+  if (h) {
+    NCK(cudaMemsetAsync(err, 0, sizeof(int), st));
+    throw std::runtime_error("cuda: a tensor-core wait in the network kernels timed out");
+  }
+}
+}  // namespace
+
+void Network::forward(int sample, float* Gout, float* Lout) {
+  if (sample < 0 || sample >= sampleCount()) throw std::out_of_range("no such sample");
+  GraphStore& s = *samples_[sample];
+  forwardOn(s.g, stream_, true);
+  checkError(error_, stream_);
+  const Graph& g = s.g;
+  if (Gout) NCK(cudaMemcpyAsync(Gout, g.G, sizeof(float) * 9 * g.B, cudaMemcpyDeviceToHost, stream_));
+  if (Lout) {
+    std::vector<float> planes(9 * static_cast<size_t>(g.SP));
+    NCK(cudaMemcpyAsync(planes.data(), g.L, sizeof(float) * planes.size(), cudaMemcpyDeviceToHost, stream_));
+    NCK(cudaStreamSynchronize(stream_));
+    for (uint32_t k = 0; k < g.B; ++k)
+      for (int c = 0; c < 9; ++c) Lout[9 * static_cast<size_t>(k) + c] = planes[c * g.SP + k];
+  }
+  NCK(cudaStreamSynchronize(stream_));
+}
+
+double Network::lossGrad(int sample, int residual, float* grad, bool accumulate) {
+  if (sample < 0 || sample >= sampleCount()) throw std::out_of_range("no such sample");
+  GraphStore& s = *samples_[sample];
+  if (residual < 0 || residual >= static_cast<int>(s.residualCount)) throw std::out_of_range("no such residual");
+  if (!accumulate) NCK(cudaMemsetAsync(grad_, 0, sizeof(float) * Layout::kCount, stream_));
+  forwardOn(s.g, stream_, true);
+  lossForward(s, residual);
+  backward(s);
+  double sc[2] = {0, 0};
+  NCK(cudaMemcpyAsync(sc, scalars_, sizeof(sc), cudaMemcpyDeviceToHost, stream_));
+  if (grad) NCK(cudaMemcpyAsync(grad, grad_, sizeof(float) * Layout::kCount, cudaMemcpyDeviceToHost, stream_));
+  checkError(error_, stream_);
+  return sc[0] > 0.0 ? sc[1] / sc[0] : 0.0;
+}
+
+void Network::apply(int sample, const float* r, float* z) {
+  if (sample < 0 || sample >= sampleCount()) throw std::out_of_range("no such sample");
+  GraphStore& s = *samples_[sample];
+  Graph& g = s.g;
+  forwardOn(g, stream_, true);
+  std::vector<float4> rv(g.n), zv(g.n);
+  for (uint32_t i = 0; i < g.n; ++i) rv[i] = make_float4(r[3 * i], r[3 * i + 1], r[3 * i + 2], 0.0f);
+  NCK(cudaMemcpyAsync(s.rhat, rv.data(), sizeof(float4) * g.n, cudaMemcpyHostToDevice, stream_));
+  // L per slot (B x 9) from the planes, through the AoS lower-slot kernels.
+  const int nb = static_cast<int>((g.n + 255) / 256);
+  std::vector<float> planes(9 * static_cast<size_t>(g.SP)), aos(9 * static_cast<size_t>(g.B));
+  NCK(cudaMemcpyAsync(planes.data(), g.L, sizeof(float) * planes.size(), cudaMemcpyDeviceToHost, stream_));
+  NCK(cudaStreamSynchronize(stream_));
+  for (uint32_t k = 0; k < g.B; ++k)
+    for (int c = 0; c < 9; ++c) aos[9 * static_cast<size_t>(k) + c] = planes[c * g.SP + k];
+  NCK(cudaMemcpyAsync(s.go, aos.data(), sizeof(float) * aos.size(), cudaMemcpyHostToDevice, stream_));
+  k_lower_t<<<nb, 256, 0, stream_>>>(g, s.go, s.rhat, s.a);
+  k_lower<<<nb, 256, 0, stream_>>>(g, s.go, s.a, s.b);
+  NCK(cudaMemcpyAsync(zv.data(), s.b, sizeof(float4) * g.n, cudaMemcpyDeviceToHost, stream_));
+  checkError(error_, stream_);
+  for (uint32_t i = 0; i < g.n; ++i) {
+    z[3 * i] = zv[i].x;
+    z[3 * i + 1] = zv[i].y;
+    z[3 * i + 2] = zv[i].z;
+  }
+}
+
+void Network::train(int steps, float lr, int batch, uint64_t seed, float* losses) {
+  if (samples_.empty()) throw std::invalid_argument("no training samples");
+  if (steps < 0 || batch < 1) throw std::invalid_argument("steps must be >= 0 and batch >= 1");
+  std::mt19937_64 rng(seed);
+  std::vector<std::pair<int, int>> pairs;
+  for (int s = 0; s < sampleCount(); ++s)
+    for (uint32_t r = 0; r < samples_[s]->residualCount; ++r) pairs.emplace_back(s, static_cast<int>(r));
+  if (pairs.empty()) throw std::invalid_argument("the samples carry no residuals");
+  NCK(cudaMemsetAsync(grad_, 0, sizeof(float) * Layout::kCount, stream_));
+  for (int step = 0; step < steps; ++step) {
+    double sum = 0.0;
+    for (int b = 0; b < batch; ++b) {
+      const auto& pr = pairs[rng() % pairs.size()];
+      GraphStore& s = *samples_[pr.first];
+      forwardOn(s.g, stream_, true);
+      lossForward(s, pr.second);
+      backward(s);
+      double sc[2] = {0, 0};
+      NCK(cudaMemcpyAsync(sc, scalars_, sizeof(sc), cudaMemcpyDeviceToHost, stream_));
+      NCK(cudaStreamSynchronize(stream_));
+      sum += sc[0] > 0.0 ? sc[1] / sc[0] : 0.0;
+    }
+    ++adamStep_;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.0f - std::pow(b1, static_cast<float>(adamStep_));
+    const float c2 = 1.0f - std::pow(b2, static_cast<float>(adamStep_));
+    // The gradient accumulates over the batch; Adam is invariant to its scale, so no division is needed.
+    k_adam<<<static_cast<int>((Layout::kCount + 255) / 256), 256, 0, stream_>>>(
+        master_, grad_, adamM_, adamV_, static_cast<uint32_t>(Layout::kCount), lr, b1, b2, 1e-8f * batch, c1, c2,
+        wBf16_);
+    NCK(cudaGetLastError());
+    if (losses) losses[step] = static_cast<float>(sum / batch);
+  }
+  checkError(error_, stream_);
+}
+
+}  // namespace net
+
+// ------------------------------------------------------------------------------------------------------------------
+// C ABI (include/drape_precond.h).
+
+#include "../../include/drape_precond.h"
+
+struct drape_precond {
+  std::unique_ptr<net::Network> net;
+  std::string error;
+};
+
+namespace {
+thread_local std::string g_netError;
+
+template <class F>
+int netGuarded(drape_precond* p, F&& f) {
+  try {
+    f();
+    return DRAPE_OK;
+  } catch (const std::invalid_argument& e) {
+    (p ? p->error : g_netError) = e.what();
+    return DRAPE_INVALID;
+  } catch (const std::out_of_range& e) {
+    (p ? p->error : g_netError) = e.what();
+    return DRAPE_OUT_OF_RANGE;
+  } catch (const std::exception& e) {
+    (p ? p->error : g_netError) = e.what();
+    return DRAPE_DEVICE_ERROR;
+  }
+}
+void needNet(drape_precond* p) {
+  if (!p || !p->net) throw std::invalid_argument("null preconditioner handle");
+}
+}  // namespace
+
+extern "C" {
+
+uint32_t drape_precond_param_count(void) { return static_cast<uint32_t>(net::Layout::kCount); }
+
+int drape_precond_create(int device, drape_precond** out) {
+  return netGuarded(nullptr, [&] {
+    if (!out) throw std::invalid_argument("null argument");
+    auto p = std::make_unique<drape_precond>();
+    p->net = std::make_unique<net::Network>(device);
+    *out = p.release();
+  });
+}
+
+void drape_precond_destroy(drape_precond* p) { delete p; }
+
+const char* drape_precond_last_error(drape_precond* p) { return p ? p->error.c_str() : g_netError.c_str(); }
+
+int drape_precond_set_params(drape_precond* p, const float* params, size_t count) {
+  return netGuarded(p, [&] {
+    needNet(p);
+    if (!params) throw std::invalid_argument("null argument");
+    p->net->setParams(params, count);
+  });
+}
+
+int drape_precond_get_params(drape_precond* p, float* params, size_t count) {
+  return netGuarded(p, [&] {
+    needNet(p);
+    if (!params) throw std::invalid_argument("null argument");
+    p->net->getParams(params, count);
+  });
+}
+
+int drape_precond_add_sample(drape_precond* p, uint32_t n, const uint32_t* row_start, const uint32_t* col_index,
+                             const float* blocks, const uint8_t* pinned, const uint8_t* active,
+                             const float* residuals, uint32_t residual_count, int* sample) {
+  return netGuarded(p, [&] {
+    needNet(p);
+    if (n == 0) throw std::invalid_argument("empty system");
+    for (uint32_t i = 0; row_start && col_index && i < n; ++i) {
+      bool diag = false;
+      for (uint32_t k = row_start[i]; k < row_start[i + 1]; ++k) diag = diag || col_index[k] == i;
+      if (!diag) throw std::invalid_argument("row " + std::to_string(i) + " has no diagonal block");
+    }
+    const int id = p->net->addSample(n, row_start, col_index, blocks, pinned, active, residuals, residual_count);
+    if (sample) *sample = id;
+  });
+}
+
+int drape_precond_clear_samples(drape_precond* p) {
+  return netGuarded(p, [&] {
+    needNet(p);
+    p->net->clearSamples();
+  });
+}
+
+int drape_precond_forward(drape_precond* p, int sample, float* g_blocks, float* l_blocks) {
+  return netGuarded(p, [&] {
+    needNet(p);
+    p->net->forward(sample, g_blocks, l_blocks);
+  });
+}
+
+int drape_precond_loss_grad(drape_precond* p, int sample, int residual, double* loss, float* grad) {
+  return netGuarded(p, [&] {
+    needNet(p);
+    const double v = p->net->lossGrad(sample, residual, grad, false);
+    if (loss) *loss = v;
+  });
+}
+
+int drape_precond_apply(drape_precond* p, int sample, const float* r, float* z) {
+  return netGuarded(p, [&] {
+    needNet(p);
+    if (!r || !z) throw std::invalid_argument("null argument");
+    p->net->apply(sample, r, z);
+  });
+}
+
+int drape_precond_train(drape_precond* p, int steps, float learning_rate, int batch, uint64_t seed, float* losses) {
+  return netGuarded(p, [&] {
+    needNet(p);
+    if (!(learning_rate > 0.0f)) throw std::invalid_argument("learning rate must be positive");
+    p->net->train(steps, learning_rate, batch, seed, losses);
+  });
+}
+
+}  // extern "C"

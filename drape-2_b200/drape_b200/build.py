@@ -11,15 +11,15 @@ CSRC = os.path.join(ROOT, "csrc")
 LIB_DIR = os.path.join(ROOT, "lib")
 LIB = os.path.join(LIB_DIR, "libdrape_cuda.so")
 
-SOURCES = ["solver.cu", "model.cpp"]
-HEADERS = ["kernels.cuh", "device_math.cuh", "model.hpp"]
+SOURCES = ["solver.cu", "learned.cu", "model.cpp"]
+HEADERS = ["kernels.cuh", "device_math.cuh", "model.hpp", "learned.hpp", "umma.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 
 def _inputs():
     files = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
-    files += [os.path.join(REPO, "include", "drape_cuda.h"), os.path.join(REPO, "include", "drape_scene.h")]
+    files += [os.path.join(REPO, "include", h) for h in ("drape_cuda.h", "drape_scene.h", "drape_precond.h")]
     return files
 
 

@@ -1,0 +1,59 @@
+/* Learned preconditioner for the cloth solver's PCG: a message-passing network (4 layers, hidden 64, BF16 weights,
+   FP32 accumulation on tcgen05 tensor cores) over the block-CSR graph of a Newton system, emitting a block
+   lower-triangular factor L with M^-1 = L L^T. L = S G with S = blockdiag(chol(inv(A_ii))), so G = I reproduces
+   block-Jacobi exactly; L's diagonal blocks are lower-triangular with a positive diagonal, so M^-1 is SPD on the
+   unpinned unknowns for any weights.
+
+   No counterpart in the reference, whose PCG is block-Jacobi only (libs/sim/src/cpu_solver.cpp:169-213,
+   libs/sim/kernels/kernels.h:237-249). Status codes are those of drape_cuda.h. */
+#ifndef DRAPE_PRECOND_H
+#define DRAPE_PRECOND_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "drape_cuda.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct drape_precond drape_precond;
+
+/* Number of FP32 parameters; layout: [out][in] row-major weights then the bias, in the order W_ne b_ne (node encoder,
+   64 x 16), W_ee b_ee (slot encoder, 64 x 16), per layer W_m b_m W_u b_u (64 x 128 each), W_o b_o (16 x 192). */
+uint32_t drape_precond_param_count(void);
+
+int drape_precond_create(int device, drape_precond** out);
+void drape_precond_destroy(drape_precond* p);
+/* Message of the last failed call on this handle (NULL: of the last failed create on this thread). */
+const char* drape_precond_last_error(drape_precond* p);
+
+/* FP32 master parameters (count = drape_precond_param_count()); setting them resets the optimiser state. */
+int drape_precond_set_params(drape_precond* p, const float* params, size_t count);
+int drape_precond_get_params(drape_precond* p, float* params, size_t count);
+
+/* A training sample: a Newton system in host memory (CSR with sorted columns and a diagonal block in every row,
+   blocks row-major 9 floats per slot, symmetric pattern), pinned and contact-active flags per particle, and
+   `residual_count` residual vectors (3 n floats each). Returns the sample index in *sample. */
+int drape_precond_add_sample(drape_precond* p, uint32_t n, const uint32_t* row_start, const uint32_t* col_index,
+                             const float* blocks, const uint8_t* pinned, const uint8_t* active,
+                             const float* residuals, uint32_t residual_count, int* sample);
+int drape_precond_clear_samples(drape_precond* p);
+
+/* Network forward on a sample: G and L = S G per slot (9 floats each, row-major; zero off the lower live slots). */
+int drape_precond_forward(drape_precond* p, int sample, float* g_blocks, float* l_blocks);
+/* Loss |Ahat G G^T rhat - rhat|^2 / |rhat|^2 on one residual (rhat = S^T r, Ahat = S^T A S) and its gradient with
+   respect to the parameters (param_count floats; may be NULL). */
+int drape_precond_loss_grad(drape_precond* p, int sample, int residual, double* loss, float* grad);
+/* z = L L^T r on a sample (3 n floats each). */
+int drape_precond_apply(drape_precond* p, int sample, const float* r, float* z);
+/* `steps` Adam steps (beta 0.9 / 0.999), each on the summed gradient of `batch` (sample, residual) pairs drawn with
+   the seed; losses[step] (may be NULL) gets the batch's mean loss before the step. */
+int drape_precond_train(drape_precond* p, int steps, float learning_rate, int batch, uint64_t seed, float* losses);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
