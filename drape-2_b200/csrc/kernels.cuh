@@ -79,6 +79,7 @@ struct Control {
   double lastAlpha, lastSlope, lastE0, lastMaxMove;
   int lastCg;
   int pad;
+  long long learnedSolves, precondFallbacks;  // PCG solves with the learned preconditioner; of those, restarted
 };
 
 constexpr unsigned int kCgLogCapacity = 1u << 16;  // PCG iterations per Newton iteration, ring buffer
@@ -92,6 +93,7 @@ struct Params {
   int maxCg;
   uint32_t n, nStretch, nHinge, nSeam, nBlocks, nGarments, slotsPadded;
   uint32_t smemSlots;   // k_solve: block slots a block keeps in shared memory
+  int learnedSwitch;    // k_solve<true>: block-Jacobi iterations before the learned preconditioner takes over
   unsigned long long barrierLimitNs;
 };
 
@@ -113,6 +115,8 @@ struct Dev {
   const uint32_t* incEntry;
   const uint32_t* incLocal;
   float4 *x, *v, *xStart, *yRel, *u, *grad, *step, *r, *z, *p0, *p1, *ap, *apFull, *resid;
+  const float* Lf;         // learned factor L: 9 planes of slotsPadded floats on lower slots (k_solve<true>)
+  const uint32_t* tslot;   // slot of (j, i) for slot (i, j)
   const float4* fExt;
   const float4* pinPos;
   float* blocks;   // 9 planes of slotsPadded floats, component 3*row+col
@@ -692,7 +696,10 @@ __device__ __forceinline__ float3 rowProduct(const SmemMatrix& A, uint32_t rs, u
 
 // Contact-filtered block-Jacobi PCG in the reference's order. Writes step, resid; returns the iteration count, or -1
 // when a grid barrier gave up.
-__device__ inline int pcgReferenceOrder(const Dev& D, GridSync& gs, const SmemMatrix& A) {
+// At most `budget` iterations (negative: P.maxCg). *r0out gets |r0|; *finished is false only when the budget, not
+// the convergence test or pAp <= 0, ended the loop.
+__device__ inline int pcgReferenceOrder(const Dev& D, GridSync& gs, const SmemMatrix& A, int budget = -1,
+                                        double* r0out = nullptr, bool* finished = nullptr) {
   const uint32_t n = D.P.n;
   uint32_t r0i, r1i;
   blockRange(n, r0i, r1i);
@@ -716,15 +723,17 @@ __device__ inline int pcgReferenceOrder(const Dev& D, GridSync& gs, const SmemMa
   }
   double rz = tot[0];
   const double r0 = sqrt(tot[1]);
+  if (r0out) *r0out = r0;
   bool done = !(r0 > 0.0);
   double beta = 0.0;
   float4* pPrev = D.p0;
   float4* pCur = D.p1;
   int it = 0;
-  const int maxCg = D.P.maxCg;
+  const int maxCg = budget < 0 ? D.P.maxCg : min(budget, D.P.maxCg);
   const uint32_t groups = blockDim.x / kRowLanes;
   const int sub = threadIdx.x & (kRowLanes - 1);
   const unsigned groupMask = ((1u << kRowLanes) - 1u) << ((threadIdx.x & 31) & ~(kRowLanes - 1));
+  if (finished) *finished = true;
   while (!done && it < maxCg) {
     // SpMV with the direction update folded in: p_j = z_j + beta * pPrev_j.
     double vpap[1] = {0.0};
@@ -752,7 +761,7 @@ __device__ inline int pcgReferenceOrder(const Dev& D, GridSync& gs, const SmemMa
     }
     double pAp[1];
     if (!gridReduce<1>(D, gs, vpap, pAp)) return -1;
-    if (!(pAp[0] > 0.0)) break;
+    if (!(pAp[0] > 0.0)) return it;
     const double alpha = rz / pAp[0];
     const float fa = static_cast<float>(alpha);
     ++it;
@@ -772,9 +781,171 @@ __device__ inline int pcgReferenceOrder(const Dev& D, GridSync& gs, const SmemMa
     }
     double t2[2];
     if (!gridReduce<2>(D, gs, v, t2)) return -1;
-    if (sqrt(t2[0]) <= D.P.cgTolerance * r0) break;
+    if (sqrt(t2[0]) <= D.P.cgTolerance * r0) return it;
     beta = t2[1] / rz;
     rz = t2[1];
+    float4* tmp = pPrev;
+    pPrev = pCur;
+    pCur = tmp;
+  }
+  if (finished && !done) *finished = false;
+  return it;
+}
+
+// z = F(L L^T r) over this block's rows, with L the learned factor (planes D.Lf, lower slots) and y = L^T r kept in
+// D.ap between the two products; returns false when a grid barrier gave up. Adds r.z of its rows to *rz.
+__device__ inline bool applyLearned(const Dev& D, GridSync& gs, uint32_t r0i, uint32_t r1i, double* rz) {
+  const uint32_t groups = blockDim.x / kRowLanes;
+  const int sub = threadIdx.x & (kRowLanes - 1);
+  const unsigned groupMask = ((1u << kRowLanes) - 1u) << ((threadIdx.x & 31) & ~(kRowLanes - 1));
+  const uint32_t SP = D.P.slotsPadded;
+  // y_j = sum over slots (j, i), i >= j, of L_(i, j)^T r_i.
+  for (uint32_t j = r0i + threadIdx.x / kRowLanes; j < r1i; j += groups) {
+    float3 acc = mk(0, 0, 0);
+    for (uint32_t s = __ldg(D.rowStart + j) + sub; s < __ldg(D.rowStart + j + 1); s += kRowLanes) {
+      const uint32_t col = __ldg(D.colIndex + s);
+      if ((col & kPinnedBit) || col < j) continue;
+      const uint32_t t = __ldg(D.tslot + s);
+      const float3 v = ld3(D.r, col);
+      const float* L = D.Lf + t;
+      acc.x += L[0] * v.x + L[3 * SP] * v.y + L[6 * SP] * v.z;
+      acc.y += L[SP] * v.x + L[4 * SP] * v.y + L[7 * SP] * v.z;
+      acc.z += L[2 * SP] * v.x + L[5 * SP] * v.y + L[8 * SP] * v.z;
+    }
+#pragma unroll
+    for (int o = kRowLanes / 2; o > 0; o >>= 1) {
+      acc.x += __shfl_xor_sync(groupMask, acc.x, o);
+      acc.y += __shfl_xor_sync(groupMask, acc.y, o);
+      acc.z += __shfl_xor_sync(groupMask, acc.z, o);
+    }
+    if (sub == 0) D.ap[j] = f4(acc);
+  }
+  if (!gs.sync()) return false;
+  // z_i = F(sum over slots (i, j), j <= i, of L_(i, j) y_j).
+  for (uint32_t i = r0i + threadIdx.x / kRowLanes; i < r1i; i += groups) {
+    float3 acc = mk(0, 0, 0);
+    for (uint32_t s = __ldg(D.rowStart + i) + sub; s < __ldg(D.rowStart + i + 1); s += kRowLanes) {
+      const uint32_t col = __ldg(D.colIndex + s);
+      if ((col & kPinnedBit) || col > i) continue;
+      const float3 v = ld3(D.ap, col);
+      const float* L = D.Lf + s;
+      acc.x += L[0] * v.x + L[SP] * v.y + L[2 * SP] * v.z;
+      acc.y += L[3 * SP] * v.x + L[4 * SP] * v.y + L[5 * SP] * v.z;
+      acc.z += L[6 * SP] * v.x + L[7 * SP] * v.y + L[8 * SP] * v.z;
+    }
+#pragma unroll
+    for (int o = kRowLanes / 2; o > 0; o >>= 1) {
+      acc.x += __shfl_xor_sync(groupMask, acc.x, o);
+      acc.y += __shfl_xor_sync(groupMask, acc.y, o);
+      acc.z += __shfl_xor_sync(groupMask, acc.z, o);
+    }
+    if (sub == 0) {
+      const float3 zi = filterContact(D.contact[i], acc);
+      D.z[i] = f4(zi);
+      *rz += dotd3(ld3(D.r, i), zi);
+    }
+  }
+  return true;
+}
+
+// PCG with the learned preconditioner M^-1 = L L^T (contact-filtered), in the reference's order otherwise: four grid
+// synchronisations per iteration (p.Ap, r.r, y = L^T r, r.z). The convergence test is the reference's, on the
+// unpreconditioned residual. Returns the iteration count, -1 when a barrier gave up, or -2 - iterations when the
+// solve broke down (a non-finite scalar, or |r|^2 above 1e6 |r0|^2): the caller then solves again with block-Jacobi.
+// M^-1 = L L^T is SPD for any finite L with a positive block diagonal, so a finite solve converges like any PCG; its
+// unpreconditioned |r| is not monotone and is no stall signal. With `warm`, step, resid and r hold a partial solve (a block-Jacobi phase) and
+// the iteration continues from them, with `r0In` (that solve's initial |r|) in the convergence test; `budget` bounds
+// the iterations.
+__device__ inline int pcgLearned(const Dev& D, GridSync& gs, const SmemMatrix& A, bool warm = false,
+                                 double r0In = 0.0, int budget = -1) {
+  const uint32_t n = D.P.n;
+  uint32_t r0i, r1i;
+  blockRange(n, r0i, r1i);
+  double rr0;
+  {
+    double v[1] = {0.0};
+    for (uint32_t i = r0i + threadIdx.x; i < r1i; i += blockDim.x) {
+      if (warm) {
+        v[0] += dotd3(ld3(D.r, i), ld3(D.r, i));
+        continue;
+      }
+      const float3 res = -ld3(D.grad, i);
+      const float3 ri = filterContact(D.contact[i], res);
+      D.step[i] = make_float4(0, 0, 0, 0);
+      D.resid[i] = f4(res);
+      D.r[i] = f4(ri);
+      v[0] += dotd3(ri, ri);
+    }
+    double t[1];
+    if (!gridReduce<1>(D, gs, v, t)) return -1;
+    rr0 = t[0];
+  }
+  const double r0 = warm ? r0In : sqrt(rr0);
+  if (!(r0 > 0.0) || !(rr0 > 0.0)) return 0;
+  double rz;
+  {
+    double v[1] = {0.0};
+    if (!applyLearned(D, gs, r0i, r1i, &v[0])) return -1;
+    double t[1];
+    if (!gridReduce<1>(D, gs, v, t)) return -1;
+    rz = t[0];
+  }
+  if (!isfinite(rz)) return -2;
+  double beta = 0.0;
+  float4* pPrev = D.p0;
+  float4* pCur = D.p1;
+  int it = 0;
+  const int maxCg = budget < 0 ? D.P.maxCg : min(budget, D.P.maxCg);
+  const uint32_t groups = blockDim.x / kRowLanes;
+  const int sub = threadIdx.x & (kRowLanes - 1);
+  const unsigned groupMask = ((1u << kRowLanes) - 1u) << ((threadIdx.x & 31) & ~(kRowLanes - 1));
+  while (it < maxCg) {
+    double vpap[1] = {0.0};
+    const float fb = static_cast<float>(beta);
+    const bool first = it == 0;
+    for (uint32_t i = r0i + threadIdx.x / kRowLanes; i < r1i; i += groups) {
+      const uint32_t rs = __ldg(D.rowStart + i), re = D.particle[i].pinned == 0u ? __ldg(D.rowStart + i + 1) : rs;
+      const float3 acc = rowProduct(A, rs, re, sub, groupMask, [&](uint32_t j) {
+        const float3 zj = ld3(D.z, j);
+        return first ? zj : zj + ld3(pPrev, j) * fb;
+      });
+      if (sub == 0) {
+        const float3 zi = ld3(D.z, i);
+        const float3 pi = first ? zi : zi + ld3(pPrev, i) * fb;
+        pCur[i] = f4(pi);
+        const float3 filtered = filterContact(D.contact[i], acc);
+        D.apFull[i] = f4(acc);
+        D.ap[i] = f4(filtered);
+        vpap[0] += dotd3(pi, filtered);
+      }
+    }
+    double pAp[1];
+    if (!gridReduce<1>(D, gs, vpap, pAp)) return -1;
+    if (!isfinite(pAp[0])) return -2 - it;
+    if (!(pAp[0] > 0.0)) break;
+    const float fa = static_cast<float>(rz / pAp[0]);
+    ++it;
+    double v[1] = {0.0};
+    for (uint32_t i = r0i + threadIdx.x; i < r1i; i += blockDim.x) {
+      const float3 pi = ld3(pCur, i);
+      D.step[i] = f4(ld3(D.step, i) + pi * fa);
+      const float3 ri = ld3(D.r, i) - ld3(D.ap, i) * fa;
+      D.r[i] = f4(ri);
+      D.resid[i] = f4(ld3(D.resid, i) - ld3(D.apFull, i) * fa);
+      v[0] += dotd3(ri, ri);
+    }
+    double rr[1];
+    if (!gridReduce<1>(D, gs, v, rr)) return -1;
+    if (!isfinite(rr[0])) return -2 - it;
+    if (sqrt(rr[0]) <= D.P.cgTolerance * r0) break;
+    if (rr[0] > 1e6 * rr0) return -2 - it;
+    double vz[1] = {0.0};
+    if (!applyLearned(D, gs, r0i, r1i, &vz[0])) return -1;
+    double rzNew[1];
+    if (!gridReduce<1>(D, gs, vz, rzNew)) return -1;
+    if (!isfinite(rzNew[0])) return -2 - it;
+    beta = rzNew[0] / rz;
+    rz = rzNew[0];
     float4* tmp = pPrev;
     pPrev = pCur;
     pCur = tmp;
@@ -782,13 +953,33 @@ __device__ inline int pcgReferenceOrder(const Dev& D, GridSync& gs, const SmemMa
   return it;
 }
 
+// The solve's PCG: block-Jacobi (reference order), or the learned schedule: P.learnedSwitch block-Jacobi iterations
+// first (0: none), then, when the solve has not converged, the learned preconditioner from the current iterate within
+// the remaining iteration budget; a learned phase that stalls is followed by a full block-Jacobi solve. Returns the
+// total iteration count of all phases, or -1 when a barrier gave up.
+template <bool Learned>
 __device__ inline int pcgSolve(const Dev& D, GridSync& gs) {
   uint32_t r0i, r1i;
   blockRange(D.P.n, r0i, r1i);
   const SmemMatrix A = stageMatrix(D, r0i, r1i);
-  return pcgReferenceOrder(D, gs, A);
+  if (!Learned) return pcgReferenceOrder(D, gs, A);
+  int first = 0;
+  double r0 = 0.0;
+  const int sw = D.P.learnedSwitch;
+  if (sw > 0) {
+    bool finished = false;
+    first = pcgReferenceOrder(D, gs, A, sw, &r0, &finished);
+    if (first < 0 || finished || first >= D.P.maxCg) return first;
+  }
+  const int it = pcgLearned(D, gs, A, sw > 0, r0, D.P.maxCg - first);
+  if (blockIdx.x == 0 && threadIdx.x == 0) D.ctl->learnedSolves += 1;
+  if (it >= -1) return it < 0 ? it : first + it;
+  if (blockIdx.x == 0 && threadIdx.x == 0) D.ctl->precondFallbacks += 1;
+  const int jac = pcgReferenceOrder(D, gs, A);
+  return jac < 0 ? jac : jac + first + (-2 - it);
 }
 
+template <bool Learned>
 __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(Dev D) {
   Control* ctl = D.ctl;
   if (ctl->newtonDone) return;
@@ -797,7 +988,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(Dev D) {
   const uint32_t n = D.P.n;
   uint32_t r0i, r1i;
   blockRange(n, r0i, r1i);
-  const int it = pcgSolve(D, gs);
+  const int it = pcgSolve<Learned>(D, gs);
   if (it < 0) return;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     if (D.cgLog) D.cgLog[static_cast<unsigned long long>(ctl->newtonIterations) % kCgLogCapacity] = it;
@@ -1014,7 +1205,7 @@ __global__ void k_pcg_precondition(Dev D, const uint32_t* __restrict__ diag) {
 __global__ void __launch_bounds__(kSolveThreads, 1) k_pcg_only(Dev D) {
   GridSync gs;
   gs.init(D.ctl, D.P.barrierLimitNs);
-  const int it = pcgSolve(D, gs);
+  const int it = pcgSolve<false>(D, gs);
   if (it >= 0 && blockIdx.x == 0 && threadIdx.x == 0) D.ctl->lastCg = it;
 }
 

@@ -669,6 +669,74 @@ __global__ void k_grad_o(Graph g, const float4* gb, const float4* a, const float
   }
 }
 
+// Kaporin objective on a probe w: b = G w, c = Ahat b, t = b.c (k_ahat_dot), logdet = sum of clamped o0..o2 over live
+// diagonal slots (k_logdet); d/dG_(i,j) = (2 / t) c_i w_j^T, d/do_k (diagonal) -= 2 / N.
+__global__ void k_ahat_dot(Graph g, const float4* __restrict__ x, float4* y, double* partial) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v = 0.0;
+  if (i < g.n) {
+    float3 acc = make_float3(0, 0, 0);
+    for (uint32_t s = __ldg(g.rowStart + i); s < __ldg(g.rowStart + i + 1); ++s) {
+      const float3 w = mulM(g.Ahat + 9 * static_cast<size_t>(s), ld3(x, colOf(g, s)));
+      acc.x += w.x;
+      acc.y += w.y;
+      acc.z += w.z;
+    }
+    y[i] = make_float4(acc.x, acc.y, acc.z, 0.0f);
+    const float3 xi = ld3(x, i);
+    v = static_cast<double>(xi.x) * acc.x + static_cast<double>(xi.y) * acc.y + static_cast<double>(xi.z) * acc.z;
+  }
+  blockSumD(v, partial + blockIdx.x);
+}
+
+__global__ void k_logdet(Graph g, double* partial) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v = 0.0;
+  if (i < g.n && !pinnedRow(g, i)) {
+    uint32_t d = __ldg(g.rowStart + i);
+    while (d < __ldg(g.rowStart + i + 1) && colOf(g, d) != i) ++d;
+    const float* o = g.o + 16 * static_cast<size_t>(d);
+    for (int k = 0; k < 3; ++k) v += fminf(fmaxf(o[k], -kDiagClamp), kDiagClamp);
+  }
+  blockSumD(v, partial + blockIdx.x);
+}
+
+// One warp per row. scalars[0] = t; invN = 1 / N.
+__global__ void k_grad_o_kaporin(Graph g, const float4* c, const float4* w, const double* scalars, float invN,
+                                 float* go) {
+  const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) / 32u;
+  const int lane = threadIdx.x & 31;
+  if (i >= g.n) return;
+  const bool pi = pinnedRow(g, i);
+  const float scale = static_cast<float>(2.0 / scalars[0]);
+  const float3 ci = ld3(c, i);
+  for (uint32_t s = __ldg(g.rowStart + i) + lane; s < __ldg(g.rowStart + i + 1); s += 32) {
+    const uint32_t j = colOf(g, s);
+    float out[16] = {0};
+    if (!pi && !pinnedRow(g, j) && j <= i) {
+      const float3 wj = ld3(w, j);
+      const float u[3] = {ci.x * scale, ci.y * scale, ci.z * scale}, v[3] = {wj.x, wj.y, wj.z};
+      float gG[9];
+      for (int r = 0; r < 3; ++r)
+        for (int k = 0; k < 3; ++k) gG[3 * r + k] = u[r] * v[k];
+      if (j == i) {
+        const float* o = g.o + 16 * static_cast<size_t>(s);
+        for (int k = 0; k < 3; ++k) {
+          const bool inside = fabsf(o[k]) < kDiagClamp;
+          out[k] = inside ? gG[4 * k] * expf(o[k]) - 2.0f * invN : 0.0f;
+        }
+        out[3] = gG[3];
+        out[4] = gG[6];
+        out[5] = gG[7];
+      } else {
+        for (int k = 0; k < 9; ++k) out[k] = gG[k];
+      }
+    }
+    float4* dst = reinterpret_cast<float4*>(go + 16 * static_cast<size_t>(s));
+    for (int k = 0; k < 4; ++k) dst[k] = make_float4(out[4 * k], out[4 * k + 1], out[4 * k + 2], out[4 * k + 3]);
+  }
+}
+
 // ------------------------------------------------------------------------------------------------------------------
 // Backward, output layer (row tiles): gX = go W_o -> gh_i (row sums into GH), gh_j (GSLOT), geps (GEPS);
 // dW_o^T += X^T go accumulated in TMEM; db_o.
@@ -1076,6 +1144,34 @@ __global__ void __launch_bounds__(kThreads) k_bw_encode(uint32_t rows, const __n
   T.done();
 }
 
+// Vector steps of the evaluation PCG (scaled system): y += a x, and partial dot products.
+__global__ void k_axpy(uint32_t n, const double* coef, int index, float sign, const float4* x, float4* y) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float a = sign * static_cast<float>(coef[index]);
+  const float4 u = x[i], v = y[i];
+  y[i] = make_float4(v.x + a * u.x, v.y + a * u.y, v.z + a * u.z, 0.0f);
+}
+// p = z + beta p with beta = coef[0] / coef[1].
+__global__ void k_xpby(uint32_t n, const double* coef, const float4* z, float4* p) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float b = static_cast<float>(coef[0] / coef[1]);
+  const float4 u = z[i], v = p[i];
+  p[i] = make_float4(u.x + b * v.x, u.y + b * v.y, u.z + b * v.z, 0.0f);
+}
+__global__ void k_dot(uint32_t n, const float4* x, const float4* y, double* partial) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v = 0.0;
+  if (i < n) {
+    const float4 a = x[i], b = y[i];
+    v = static_cast<double>(a.x) * b.x + static_cast<double>(a.y) * b.y + static_cast<double>(a.z) * b.z;
+  }
+  blockSumD(v, partial + blockIdx.x);
+}
+// coef[dst] = coef[num] / coef[den].
+__global__ void k_ratio(double* coef, int num, int den, int dst) { coef[dst] = coef[num] / coef[den]; }
+
 // ------------------------------------------------------------------------------------------------------------------
 // Gradient reduction and optimiser.
 
@@ -1161,6 +1257,7 @@ struct GraphStore {
   float *r = nullptr, *go = nullptr, *GH = nullptr, *GH2 = nullptr, *GSLOT = nullptr, *GEPS = nullptr;
   double* partial = nullptr;
   int partialCount = 0;
+  uint32_t liveUnknowns = 0;  // 3 x unpinned rows
   ~GraphStore() {
     for (void* p : owned) cudaFree(p);
   }
@@ -1307,6 +1404,7 @@ int Network::addSample(uint32_t n, const uint32_t* rowStart, const uint32_t* col
   g.activeBase = dact;
   allocWorkspace(*s, true);
   s->residualCount = residualCount;
+  for (uint32_t i = 0; i < n; ++i) s->liveUnknowns += pinned[i] ? 0u : 3u;
   s->residuals.resize(static_cast<size_t>(residualCount) * n);
   for (size_t k = 0; k < static_cast<size_t>(residualCount) * n; ++k)
     s->residuals[k] = make_float4(residuals[3 * k], residuals[3 * k + 1], residuals[3 * k + 2], 0.0f);
@@ -1320,7 +1418,9 @@ int Network::sampleCount() const { return static_cast<int>(samples_.size()); }
 
 Graph& Network::graphOf(GraphStore& s) { return s.g; }
 
-std::unique_ptr<GraphStore> Network::bind(uint32_t n, uint32_t B, uint32_t SP, const uint32_t* hostRowStart,
+void GraphStoreDeleter::operator()(GraphStore* s) const { delete s; }
+
+GraphHandle Network::bind(uint32_t n, uint32_t B, uint32_t SP, const uint32_t* hostRowStart,
                                           const uint32_t* hostColIndex, const uint32_t* dRowStart,
                                           const uint32_t* dColIndex, const float* dBlocks,
                                           const uint8_t* pinnedBase, uint32_t pinnedStride,
@@ -1349,10 +1449,11 @@ std::unique_ptr<GraphStore> Network::bind(uint32_t n, uint32_t B, uint32_t SP, c
   g.activeStride = activeStride;
   allocWorkspace(*s, false);
   NCK(cudaStreamSynchronize(st));
-  return s;
+  return GraphHandle(s.release());
 }
 
-void Network::forwardOn(Graph& g, cudaStream_t st, bool training) {
+void Network::forwardOn(Graph& g, cudaStream_t st, bool training, int* error) {
+  int* error_ = error ? error : this->error_;
   const int rowBlocks = static_cast<int>((g.n + 127) / 128);
   k_scale<<<rowBlocks, 128, 0, st>>>(g);
   k_features<<<static_cast<int>((g.n + 7) / 8), 256, 0, st>>>(g);
@@ -1378,6 +1479,18 @@ void Network::forwardOn(Graph& g, cudaStream_t st, bool training) {
 void Network::lossForward(GraphStore& s, int residual) {
   Graph& g = s.g;
   const int nb = static_cast<int>((g.n + 255) / 256);
+  if (objective_ == 1) {
+    std::vector<float4> w(s.residuals.begin() + static_cast<size_t>(residual) * g.n,
+                          s.residuals.begin() + static_cast<size_t>(residual + 1) * g.n);
+    NCK(cudaMemcpyAsync(s.rhat, w.data(), sizeof(float4) * g.n, cudaMemcpyHostToDevice, stream_));
+    k_lower<<<nb, 256, 0, stream_>>>(g, g.G, s.rhat, s.b);
+    k_ahat_dot<<<nb, 256, 0, stream_>>>(g, s.b, s.e, s.partial);
+    k_sum<<<1, 256, 0, stream_>>>(s.partial, nb, scalars_ + 0);
+    k_logdet<<<nb, 256, 0, stream_>>>(g, s.partial);
+    k_sum<<<1, 256, 0, stream_>>>(s.partial, nb, scalars_ + 1);
+    NCK(cudaStreamSynchronize(stream_));  // w must outlive the copy
+    return;
+  }
   std::vector<float> r(3 * static_cast<size_t>(g.n));
   for (uint32_t i = 0; i < g.n; ++i) {
     const float4 v = s.residuals[static_cast<size_t>(residual) * g.n + i];
@@ -1405,10 +1518,14 @@ void Network::backward(GraphStore& s) {
   Graph& g = s.g;
   const int nb = static_cast<int>((g.n + 255) / 256);
   const int wb = static_cast<int>((g.n + 7) / 8);
-  k_ge<<<nb, 256, 0, stream_>>>(g.n, s.e, scalars_, s.ge);
-  k_ahat<<<nb, 256, 0, stream_>>>(g, s.ge, nullptr, s.gb, s.partial);
-  k_lower_t<<<nb, 256, 0, stream_>>>(g, g.G, s.gb, s.ga);
-  k_grad_o<<<wb, 256, 0, stream_>>>(g, s.gb, s.a, s.rhat, s.ga, s.go);
+  if (objective_ == 1) {
+    k_grad_o_kaporin<<<wb, 256, 0, stream_>>>(g, s.e, s.rhat, scalars_, 1.0f / std::max(1u, s.liveUnknowns), s.go);
+  } else {
+    k_ge<<<nb, 256, 0, stream_>>>(g.n, s.e, scalars_, s.ge);
+    k_ahat<<<nb, 256, 0, stream_>>>(g, s.ge, nullptr, s.gb, s.partial);
+    k_lower_t<<<nb, 256, 0, stream_>>>(g, g.G, s.gb, s.ga);
+    k_grad_o<<<wb, 256, 0, stream_>>>(g, s.gb, s.a, s.rhat, s.ga, s.go);
+  }
   const __nv_bfloat16* W = wBf16_;
   const float* M = master_;
   const int grid = gridFor(g.nTiles, numSMs_);
@@ -1467,6 +1584,14 @@ void Network::forward(int sample, float* Gout, float* Lout) {
   NCK(cudaStreamSynchronize(stream_));
 }
 
+double Network::lossValue(const GraphStore& s, const double* sc) const {
+  if (objective_ == 1) {
+    const double N = std::max(1u, s.liveUnknowns);
+    return std::log(sc[0] / N) - 2.0 * sc[1] / N;
+  }
+  return sc[0] > 0.0 ? sc[1] / sc[0] : 0.0;
+}
+
 double Network::lossGrad(int sample, int residual, float* grad, bool accumulate) {
   if (sample < 0 || sample >= sampleCount()) throw std::out_of_range("no such sample");
   GraphStore& s = *samples_[sample];
@@ -1479,7 +1604,7 @@ double Network::lossGrad(int sample, int residual, float* grad, bool accumulate)
   NCK(cudaMemcpyAsync(sc, scalars_, sizeof(sc), cudaMemcpyDeviceToHost, stream_));
   if (grad) NCK(cudaMemcpyAsync(grad, grad_, sizeof(float) * Layout::kCount, cudaMemcpyDeviceToHost, stream_));
   checkError(error_, stream_);
-  return sc[0] > 0.0 ? sc[1] / sc[0] : 0.0;
+  return lossValue(s, sc);
 }
 
 void Network::apply(int sample, const float* r, float* z) {
@@ -1509,6 +1634,66 @@ void Network::apply(int sample, const float* r, float* z) {
   }
 }
 
+int Network::pcg(int sample, int rhs, bool useLearned, int maxIterations, double tolerance, double* relres) {
+  if (sample < 0 || sample >= sampleCount()) throw std::out_of_range("no such sample");
+  GraphStore& s = *samples_[sample];
+  if (rhs < 0 || rhs >= static_cast<int>(s.residualCount)) throw std::out_of_range("no such residual");
+  Graph& g = s.g;
+  forwardOn(g, stream_, true);
+  const uint32_t n = g.n;
+  const int nb = static_cast<int>((n + 255) / 256);
+  // Scaled system Ahat x = rhat (rhat = S^T r); the preconditioner is G G^T, or the identity (block-Jacobi).
+  std::vector<float> r(3 * static_cast<size_t>(n));
+  for (uint32_t i = 0; i < n; ++i) {
+    const float4 v = s.residuals[static_cast<size_t>(rhs) * n + i];
+    r[3 * i] = v.x;
+    r[3 * i + 1] = v.y;
+    r[3 * i + 2] = v.z;
+  }
+  NCK(cudaMemcpyAsync(s.r, r.data(), sizeof(float) * r.size(), cudaMemcpyHostToDevice, stream_));
+  float4 *R = s.rhat, *Z = s.a, *P = s.b, *Q = s.e, *X = s.ge, *T = s.gb;
+  double* coef = scalars_;  // 0 rz, 1 rz_old, 2 pq, 3 alpha, 4 rr, 5 rr0
+  k_rhat<<<nb, 256, 0, stream_>>>(g, s.r, R, s.partial);
+  k_sum<<<1, 256, 0, stream_>>>(s.partial, nb, coef + 5);
+  NCK(cudaMemsetAsync(X, 0, sizeof(float4) * n, stream_));
+  auto precondition = [&] {
+    if (useLearned) {
+      k_lower_t<<<nb, 256, 0, stream_>>>(g, g.G, R, T);
+      k_lower<<<nb, 256, 0, stream_>>>(g, g.G, T, Z);
+    } else {
+      NCK(cudaMemcpyAsync(Z, R, sizeof(float4) * n, cudaMemcpyDeviceToDevice, stream_));
+    }
+    k_dot<<<nb, 256, 0, stream_>>>(n, R, Z, s.partial);
+    k_sum<<<1, 256, 0, stream_>>>(s.partial, nb, coef + 0);
+  };
+  precondition();
+  NCK(cudaMemcpyAsync(P, Z, sizeof(float4) * n, cudaMemcpyDeviceToDevice, stream_));
+  double host[6] = {0, 0, 0, 0, 0, 0};
+  int it = 0;
+  for (; it < maxIterations;) {
+    k_ahat_dot<<<nb, 256, 0, stream_>>>(g, P, Q, s.partial);
+    k_sum<<<1, 256, 0, stream_>>>(s.partial, nb, coef + 2);
+    k_ratio<<<1, 1, 0, stream_>>>(coef, 0, 2, 3);
+    k_axpy<<<nb, 256, 0, stream_>>>(n, coef, 3, 1.0f, P, X);
+    k_axpy<<<nb, 256, 0, stream_>>>(n, coef, 3, -1.0f, Q, R);
+    ++it;
+    k_dot<<<nb, 256, 0, stream_>>>(n, R, R, s.partial);
+    k_sum<<<1, 256, 0, stream_>>>(s.partial, nb, coef + 4);
+    NCK(cudaMemcpyAsync(host, coef, sizeof(host), cudaMemcpyDeviceToHost, stream_));
+    NCK(cudaStreamSynchronize(stream_));
+    if (!(host[2] > 0.0) || std::sqrt(host[4]) <= tolerance * std::sqrt(host[5])) break;
+    NCK(cudaMemcpyAsync(coef + 1, coef + 0, sizeof(double), cudaMemcpyDeviceToDevice, stream_));
+    precondition();
+    k_xpby<<<nb, 256, 0, stream_>>>(n, coef, Z, P);
+  }
+  NCK(cudaGetLastError());
+  NCK(cudaMemcpyAsync(host, coef, sizeof(host), cudaMemcpyDeviceToHost, stream_));
+  NCK(cudaStreamSynchronize(stream_));
+  if (relres) *relres = host[5] > 0.0 ? std::sqrt(host[4] / host[5]) : 0.0;
+  checkError(error_, stream_);
+  return it;
+}
+
 void Network::train(int steps, float lr, int batch, uint64_t seed, float* losses) {
   if (samples_.empty()) throw std::invalid_argument("no training samples");
   if (steps < 0 || batch < 1) throw std::invalid_argument("steps must be >= 0 and batch >= 1");
@@ -1529,7 +1714,7 @@ void Network::train(int steps, float lr, int batch, uint64_t seed, float* losses
       double sc[2] = {0, 0};
       NCK(cudaMemcpyAsync(sc, scalars_, sizeof(sc), cudaMemcpyDeviceToHost, stream_));
       NCK(cudaStreamSynchronize(stream_));
-      sum += sc[0] > 0.0 ? sc[1] / sc[0] : 0.0;
+      sum += lossValue(s, sc);
     }
     ++adamStep_;
     const float b1 = 0.9f, b2 = 0.999f;
@@ -1551,11 +1736,6 @@ void Network::train(int steps, float lr, int batch, uint64_t seed, float* losses
 // C ABI (include/drape_precond.h).
 
 #include "../../include/drape_precond.h"
-
-struct drape_precond {
-  std::unique_ptr<net::Network> net;
-  std::string error;
-};
 
 namespace {
 thread_local std::string g_netError;
@@ -1657,6 +1837,24 @@ int drape_precond_apply(drape_precond* p, int sample, const float* r, float* z) 
     needNet(p);
     if (!r || !z) throw std::invalid_argument("null argument");
     p->net->apply(sample, r, z);
+  });
+}
+
+int drape_precond_pcg(drape_precond* p, int sample, int rhs, int use_learned, int max_iterations, double tolerance,
+                      int* iterations, double* relative_residual) {
+  return netGuarded(p, [&] {
+    needNet(p);
+    if (!iterations || max_iterations < 1) throw std::invalid_argument("bad argument");
+    *iterations = p->net->pcg(sample, rhs, use_learned != 0, max_iterations, tolerance, relative_residual);
+  });
+}
+
+int drape_precond_set_objective(drape_precond* p, int objective) {
+  return netGuarded(p, [&] {
+    needNet(p);
+    if (objective != DRAPE_PRECOND_DEFECT && objective != DRAPE_PRECOND_KAPORIN)
+      throw std::invalid_argument("unknown objective");
+    p->net->setObjective(objective);
   });
 }
 

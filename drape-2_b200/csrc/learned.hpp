@@ -65,6 +65,10 @@ struct Graph {
 
 // Host-owned device buffers of a graph built from host arrays (a training sample) or bound to a solver's arrays.
 struct GraphStore;
+struct GraphStoreDeleter {
+  void operator()(GraphStore* s) const;
+};
+using GraphHandle = std::unique_ptr<GraphStore, GraphStoreDeleter>;
 
 class Network {
  public:
@@ -87,11 +91,16 @@ class Network {
   double lossGrad(int sample, int residual, float* grad, bool accumulate);  // grad (host, count) may be null
   void apply(int sample, const float* r, float* z);                        // z = L L^T r (host, 3n each)
   void train(int steps, float lr, int batch, uint64_t seed, float* losses);
+  // PCG on a sample's scaled system with residual `rhs` as the right-hand side; returns the iterations.
+  int pcg(int sample, int rhs, bool useLearned, int maxIterations, double tolerance, double* relres);
+  // 0: residual defect |Ahat G G^T rhat - rhat|^2 / |rhat|^2; 1: stochastic Kaporin objective on the probe vectors.
+  void setObjective(int objective) { objective_ = objective; }
 
-  // Forward on a solver's system: writes g.L (and the workspace) on `st`. Params must be set.
-  void forwardOn(Graph& g, cudaStream_t st, bool training);
+  // Forward on a solver's system: writes g.L (and the workspace) on `st`. Params must be set. A tensor-core wait that
+  // gives up raises *error (the network's own flag when null).
+  void forwardOn(Graph& g, cudaStream_t st, bool training, int* error = nullptr);
   // Builds a graph workspace for a solver's CSR (device arrays owned by the solver); returns the store to keep.
-  std::unique_ptr<GraphStore> bind(uint32_t n, uint32_t B, uint32_t SP, const uint32_t* hostRowStart,
+  GraphHandle bind(uint32_t n, uint32_t B, uint32_t SP, const uint32_t* hostRowStart,
                                    const uint32_t* hostColIndex, const uint32_t* dRowStart, const uint32_t* dColIndex,
                                    const float* dBlocks, const uint8_t* pinnedBase, uint32_t pinnedStride,
                                    const uint8_t* activeBase, uint32_t activeStride, cudaStream_t st);
@@ -103,6 +112,7 @@ class Network {
   void lossForward(GraphStore& s, int residual);
   void backward(GraphStore& s);
   void reduceInto(const float* partials, int grid, size_t count, size_t offset, float scale);
+  double lossValue(const GraphStore& s, const double* scalars) const;
 
   int device_;
   int numSMs_ = 0;
@@ -117,6 +127,7 @@ class Network {
   int* error_ = nullptr;           // device error flag (bounded waits)
   double* scalars_ = nullptr;      // device FP64 scratch (norms, loss)
   int adamStep_ = 0;
+  int objective_ = 1;
   std::vector<std::unique_ptr<GraphStore>> samples_;
 };
 
@@ -125,3 +136,9 @@ std::vector<uint32_t> rowTiles(const std::vector<uint32_t>& rowStart);
 std::vector<uint32_t> transposedSlots(const std::vector<uint32_t>& rowStart, const std::vector<uint32_t>& colIndex);
 
 }  // namespace net
+
+// The C ABI's handle (include/drape_precond.h).
+struct drape_precond {
+  std::unique_ptr<net::Network> net;
+  std::string error;
+};

@@ -17,7 +17,9 @@
 #include <vector>
 
 #include "../../include/drape_cuda.h"
+#include "../../include/drape_precond.h"
 #include "kernels.cuh"
+#include "learned.hpp"
 #include "model.hpp"
 
 using drape_b200::Model;
@@ -110,6 +112,13 @@ struct drape_solver {
   unsigned long long barrierLimitNs = 2000000000ull;  // 2 s
   int failAfter = -1;
   uint32_t solveSmemCap = 0;       // block slots one solve block can keep in shared memory
+  // Learned preconditioner: the solver's own copy of the network and its workspace on this solver's CSR.
+  std::unique_ptr<net::Network> net;
+  net::GraphHandle netGraph;
+  bool learnedOn = false;
+  int precondRefresh = 1;           // run the network on every precondRefresh-th Newton iteration
+  int precondSwitch = 0;            // block-Jacobi iterations before the learned preconditioner takes over
+  uint64_t netNewtonCounter = 0;
   size_t solveSmemBytes = 0;       // dynamic shared memory of the solve launch for the built scene
 
   DBuf<dcu::Particle> particle;
@@ -194,7 +203,8 @@ struct drape_solver {
     CK(cudaFuncSetAttribute(dcu::k_assemble, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             static_cast<int>(dcu::kAssembleSmem)));
     // The solve kernels keep their rows' matrix blocks in shared memory: as many slots as the opt-in limit leaves.
-    const void* solveKernels[] = {reinterpret_cast<const void*>(dcu::k_solve),
+    const void* solveKernels[] = {reinterpret_cast<const void*>(dcu::k_solve<false>),
+                                  reinterpret_cast<const void*>(dcu::k_solve<true>),
                                   reinterpret_cast<const void*>(dcu::k_pcg_only)};
     size_t staticSmem = 0;
     for (const void* k : solveKernels) {
@@ -415,10 +425,45 @@ struct drape_solver {
     d.ctl = ctl.p;
     d.cgLog = cgLog.p;
     dev = d;
+    netGraph.reset();
+    if (learnedOn) bindNet();
     assembleGrid = static_cast<int>(std::max<uint32_t>(1, std::min<uint32_t>((n + dcu::kAssembleWarps - 1) / dcu::kAssembleWarps,
                                                                            static_cast<uint32_t>(numSMs) * 16)));
     CK(cudaStreamSynchronize(s));
     built = true;
+  }
+
+  // The network's workspace on this solver's CSR; the learned factor and transposed-slot map go into the device view.
+  void bindNet() {
+    const uint32_t n = static_cast<uint32_t>(m.pinned.size()), B = static_cast<uint32_t>(m.colIndex.size());
+    std::vector<uint32_t> cols(m.colIndex);
+    for (auto& c : cols)
+      if (m.pinned[c]) c |= dcu::kPinnedBit;
+    netGraph = net->bind(n, B, dev.P.slotsPadded, m.rowStart.data(), cols.data(), rowStart.p, colIndex.p, blocks.p,
+                         reinterpret_cast<const uint8_t*>(particle.p) + offsetof(dcu::Particle, pinned),
+                         sizeof(dcu::Particle),
+                         reinterpret_cast<const uint8_t*>(contact.p) + offsetof(dcu::Contact, active),
+                         sizeof(dcu::Contact), stream);
+    dev.Lf = net->graphOf(*netGraph).L;
+    dev.tslot = net->graphOf(*netGraph).tslot;
+    netNewtonCounter = 0;
+  }
+
+  void setPrecond(drape_precond* p) {
+    if (!p) {
+      learnedOn = false;
+      netGraph.reset();
+      dev.Lf = nullptr;
+      dev.tslot = nullptr;
+      return;
+    }
+    if (!p->net) throw std::invalid_argument("null preconditioner handle");
+    std::vector<float> w(net::Layout::kCount);
+    p->net->getParams(w.data(), w.size());
+    if (!net) net = std::make_unique<net::Network>(device);
+    net->setParams(w.data(), w.size());
+    learnedOn = true;
+    if (built) bindNet();
   }
 
   void requireBuilt() const {
@@ -485,8 +530,9 @@ struct drape_solver {
 
   void launchSolve(const dcu::Dev& d) {
     void* args[] = {const_cast<dcu::Dev*>(&d)};
-    CK(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(dcu::k_solve), dim3(solveGrid), dim3(dcu::kSolveThreads),
-                                   args, solveSmemBytes, stream));
+    void* kernel = learnedOn && netGraph ? reinterpret_cast<void*>(dcu::k_solve<true>)
+                                         : reinterpret_cast<void*>(dcu::k_solve<false>);
+    CK(cudaLaunchCooperativeKernel(kernel, dim3(solveGrid), dim3(dcu::kSolveThreads), args, solveSmemBytes, stream));
   }
 
   void enqueueSubstep(double h, int iterations) {
@@ -495,6 +541,7 @@ struct drape_solver {
     d.P.invH2 = static_cast<float>(1.0 / (h * h));
     d.P.hD = h;
     d.P.barrierLimitNs = barrierLimitNs;
+    d.P.learnedSwitch = precondSwitch;
     const uint32_t n = d.P.n;
     const int pg = std::max(1, static_cast<int>(std::min<uint32_t>((n + 255) / 256, static_cast<uint32_t>(pointGrid))));
     cudaEvent_t e = profStart();
@@ -509,6 +556,11 @@ struct drape_solver {
       dcu::k_assemble<<<assembleGrid, dcu::kAssembleWarps * dcu::kWarp, dcu::kAssembleSmem, stream>>>(d);
       CK(cudaGetLastError());
       profStop(e, 2);
+      if (learnedOn && netGraph && netNewtonCounter++ % static_cast<uint64_t>(precondRefresh) == 0) {
+        e = profStart();
+        net->forwardOn(net->graphOf(*netGraph), stream, false, &ctl.p->error);
+        profStop(e, 6);
+      }
       e = profStart();
       launchSolve(d);
       profStop(e, 3);
@@ -579,6 +631,8 @@ struct drape_solver {
     c.newton_iterations = hCtl.p->newtonIterations;
     c.cg_iterations = hCtl.p->cgIterations;
     c.line_search_halvings = hCtl.p->lineSearchHalvings;
+    c.precond_fallbacks = hCtl.p->precondFallbacks;
+    c.learned_solves = hCtl.p->learnedSolves;
     return c;
   }
 
@@ -588,6 +642,7 @@ struct drape_solver {
     CK(cudaStreamSynchronize(stream));
     dcu::Control c = *hCtl.p;
     c.substeps = c.newtonIterations = c.cgIterations = c.lineSearchHalvings = c.energyEvaluations = 0;
+    c.learnedSolves = c.precondFallbacks = 0;
     *hCtl.p = c;
     CK(cudaMemcpyAsync(ctl.p, hCtl.p, sizeof(dcu::Control), cudaMemcpyHostToDevice, stream));
     CK(cudaStreamSynchronize(stream));
@@ -855,7 +910,7 @@ int drape_cuda_is_available(void) {
     cudaDeviceProp prop{};
     if (cudaGetDeviceProperties(&prop, d) == cudaSuccess && prop.major == 10) {
       cudaFuncAttributes attr{};
-      if (cudaFuncGetAttributes(&attr, dcu::k_solve) == cudaSuccess) return 1;
+      if (cudaFuncGetAttributes(&attr, dcu::k_solve<false>) == cudaSuccess) return 1;
       cudaGetLastError();
     }
   }
@@ -1367,6 +1422,40 @@ int drape_cuda_spmv_device(uint32_t n, const uint32_t* d_row_start, const uint32
         n, d_row_start, d_col_index, d_blocks, slots_padded, d_pinned, static_cast<const float4*>(d_x),
         static_cast<float4*>(d_y));
     CK(cudaGetLastError());
+  });
+}
+
+int drape_cuda_set_precond(drape_solver* s, drape_precond* p) {
+  return guarded(s, [&] {
+    need(s);
+    s->use();
+    s->setPrecond(p);
+  });
+}
+
+int drape_cuda_precond_factor(drape_solver* s, float* l_blocks) {
+  return guarded(s, [&] {
+    need(s);
+    s->requireBuilt();
+    if (!l_blocks) throw std::invalid_argument("null argument");
+    if (!s->netGraph) throw std::logic_error("the learned preconditioner is not in use");
+    s->use();
+    const net::Graph& g = s->net->graphOf(*s->netGraph);
+    std::vector<float> planes(9 * static_cast<size_t>(g.SP));
+    CK(cudaMemcpyAsync(planes.data(), g.L, sizeof(float) * planes.size(), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    for (uint32_t k = 0; k < g.B; ++k)
+      for (int c = 0; c < 9; ++c) l_blocks[9 * static_cast<size_t>(k) + c] = planes[c * g.SP + k];
+  });
+}
+
+int drape_cuda_set_precond_schedule(drape_solver* s, int refresh_every, int jacobi_first) {
+  return guarded(s, [&] {
+    need(s);
+    if (refresh_every < 1) throw std::invalid_argument("refresh interval must be >= 1");
+    if (jacobi_first < 0) throw std::invalid_argument("jacobi_first must be >= 0");
+    s->precondRefresh = refresh_every;
+    s->precondSwitch = jacobi_first;
   });
 }
 

@@ -78,6 +78,9 @@ def load(build_if_missing: bool = True):
     L.drape_cuda_spmv_device.argtypes = [_u32, C.c_void_p, C.c_void_p, C.c_void_p, _u32, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_void_p]
     L.drape_cuda_set_barrier_limit.argtypes = [C.c_void_p, C.c_uint64]
+    L.drape_cuda_set_precond.argtypes = [C.c_void_p, C.c_void_p]
+    L.drape_cuda_set_precond_schedule.argtypes = [C.c_void_p, C.c_int, C.c_int]
+    L.drape_cuda_precond_factor.argtypes = [C.c_void_p, _P(_f)]
     L.drape_cuda_test_barrier_timeout.argtypes = [C.c_int, C.c_int, C.c_uint64, _P(C.c_int)]
     L.drape_cuda_inject_failure.argtypes = [C.c_void_p, C.c_int]
     L.drape_cuda_cg_history.argtypes = [C.c_void_p, _P(_i32), C.c_size_t, _P(C.c_size_t)]
@@ -92,11 +95,11 @@ def load(build_if_missing: bool = True):
     return L
 
 
-KERNEL_NAMES = ("k_begin", "k_activate", "k_assemble", "k_solve", "k_finish", "k_stats")
+KERNEL_NAMES = ("k_begin", "k_activate", "k_assemble", "k_solve", "k_finish", "k_stats", "net_forward")
 
 
 class drape_profile(C.Structure):
-    _fields_ = [("launches", C.c_int64 * 6), ("milliseconds", C.c_double * 6), ("cg_iterations", C.c_int64),
+    _fields_ = [("launches", C.c_int64 * 7), ("milliseconds", C.c_double * 7), ("cg_iterations", C.c_int64),
                 ("energy_evaluations", C.c_int64)]
 
 
@@ -292,6 +295,20 @@ class CudaSolver:
 
     def set_barrier_limit(self, nanoseconds: int) -> None:
         self._check(self.L.drape_cuda_set_barrier_limit(self.h, int(nanoseconds)))
+
+    def set_precond(self, precond) -> None:
+        """Use a LearnedPreconditioner's current parameters for the Newton solves (None: block-Jacobi)."""
+        self._check(self.L.drape_cuda_set_precond(self.h, None if precond is None else precond.h))
+
+    def precond_factor(self) -> np.ndarray:
+        """L per slot (B, 3, 3) from the solver's last network run."""
+        B = len(self.structure()["col_index"])
+        out = np.zeros((B, 3, 3), np.float32)
+        self._check(self.L.drape_cuda_precond_factor(self.h, _p(out, _f)))
+        return out
+
+    def set_precond_schedule(self, refresh_every: int = 1, jacobi_first: int = 0) -> None:
+        self._check(self.L.drape_cuda_set_precond_schedule(self.h, int(refresh_every), int(jacobi_first)))
 
     def inject_failure(self, steps: int) -> None:
         self._check(self.L.drape_cuda_inject_failure(self.h, int(steps)))

@@ -19,6 +19,7 @@ _P = C.POINTER
 _u8, _u32, _f, _d = C.c_uint8, C.c_uint32, C.c_float, C.c_double
 
 HIDDEN, LAYERS = 64, 4
+DEFECT, KAPORIN = 0, 1
 WEIGHTS_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights")
 
 
@@ -42,6 +43,8 @@ def _lib():
     L.drape_precond_loss_grad.argtypes = [C.c_void_p, C.c_int, C.c_int, _P(_d), _P(_f)]
     L.drape_precond_apply.argtypes = [C.c_void_p, C.c_int, _P(_f), _P(_f)]
     L.drape_precond_train.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_int, C.c_uint64, _P(_f)]
+    L.drape_precond_set_objective.argtypes = [C.c_void_p, C.c_int]
+    L.drape_precond_pcg.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, _P(C.c_int), _P(_d)]
     L._precond_bound = True
     return L
 
@@ -123,6 +126,10 @@ class LearnedPreconditioner:
         self.samples.append((len(rs) - 1, len(ci)))
         return sid.value
 
+    def set_objective(self, objective: int) -> None:
+        """KAPORIN (default; the samples' residual vectors are the random probes) or DEFECT."""
+        self._check(self.L.drape_precond_set_objective(self.h, int(objective)))
+
     def clear_samples(self) -> None:
         self._check(self.L.drape_precond_clear_samples(self.h))
         self.samples = []
@@ -146,6 +153,14 @@ class LearnedPreconditioner:
         z = np.zeros((n, 3), np.float32)
         self._check(self.L.drape_precond_apply(self.h, sample, rr.ctypes.data_as(_P(_f)), z.ctypes.data_as(_P(_f))))
         return z
+
+    def pcg(self, sample: int, rhs: int = 0, use_learned: bool = True, max_iterations: int = 500,
+            tolerance: float = 1e-2):
+        """(iterations, relative residual) of PCG on the sample's scaled system (drape_precond_pcg)."""
+        it, rel = C.c_int(), C.c_double()
+        self._check(self.L.drape_precond_pcg(self.h, sample, rhs, int(use_learned), max_iterations, tolerance,
+                                             C.byref(it), C.byref(rel)))
+        return it.value, rel.value
 
     def train(self, steps: int, lr: float = 1e-3, batch: int = 4, seed: int = 0) -> np.ndarray:
         losses = np.zeros(max(steps, 1), np.float32)

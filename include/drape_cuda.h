@@ -114,7 +114,7 @@ int drape_cuda_stream(const drape_solver* s, void** stream);
 /* Kernel timing: with profiling on, every launch is bracketed by CUDA events on the solver's stream and its device
    time accumulated per kernel: [0] begin (predict + contact setup), [1] activate, [2] assemble, [3] solve
    (persistent PCG + line search), [4] finish, [5] stats. */
-enum { DRAPE_KERNEL_COUNT = 6 };
+enum { DRAPE_KERNEL_COUNT = 7 };
 typedef struct drape_profile {
   int64_t launches[DRAPE_KERNEL_COUNT];
   double milliseconds[DRAPE_KERNEL_COUNT];

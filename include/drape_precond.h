@@ -43,14 +43,47 @@ int drape_precond_clear_samples(drape_precond* p);
 
 /* Network forward on a sample: G and L = S G per slot (9 floats each, row-major; zero off the lower live slots). */
 int drape_precond_forward(drape_precond* p, int sample, float* g_blocks, float* l_blocks);
-/* Loss |Ahat G G^T rhat - rhat|^2 / |rhat|^2 on one residual (rhat = S^T r, Ahat = S^T A S) and its gradient with
-   respect to the parameters (param_count floats; may be NULL). */
+/* Evaluation PCG on a sample (no contact filter): solves S^T A S x = S^T r, r the sample's residual `rhs`, with the
+   preconditioner G G^T (use_learned != 0) or the identity, which on the scaled system is block-Jacobi; stops at
+   |r_k| <= tolerance |r_0| or max_iterations. Gives both preconditioners the same system for an ablation. */
+int drape_precond_pcg(drape_precond* p, int sample, int rhs, int use_learned, int max_iterations, double tolerance,
+                      int* iterations, double* relative_residual);
+
+/* Training objectives. DRAPE_PRECOND_KAPORIN (the default): log(w^T G^T Ahat G w / N) - (2 / N) log det G on a
+   probe w (the sample's residual vectors, which should then be random with identity covariance), N the live
+   unknowns: a stochastic estimate of Kaporin's condition number of the preconditioned operator, minimised on a fixed
+   pattern by the factorised sparse approximate inverse. DRAPE_PRECOND_DEFECT: |Ahat G G^T rhat - rhat|^2 / |rhat|^2
+   with rhat = S^T r. Ahat = S^T A S. */
+#define DRAPE_PRECOND_DEFECT 0
+#define DRAPE_PRECOND_KAPORIN 1
+int drape_precond_set_objective(drape_precond* p, int objective);
+
+/* The objective on one residual (probe) and its gradient with respect to the parameters (param_count floats; may be
+   NULL). */
 int drape_precond_loss_grad(drape_precond* p, int sample, int residual, double* loss, float* grad);
 /* z = L L^T r on a sample (3 n floats each). */
 int drape_precond_apply(drape_precond* p, int sample, const float* r, float* z);
 /* `steps` Adam steps (beta 0.9 / 0.999), each on the summed gradient of `batch` (sample, residual) pairs drawn with
    the seed; losses[step] (may be NULL) gets the batch's mean loss before the step. */
 int drape_precond_train(drape_precond* p, int steps, float learning_rate, int batch, uint64_t seed, float* losses);
+
+/* Makes the solver's Newton solves use the learned preconditioner with the parameters `p` holds now (copied; `p` may
+   be destroyed afterwards), or block-Jacobi again when `p` is NULL. Each Newton iteration then runs the network on
+   the assembled system and the PCG applies z = F L L^T F r; a solve that breaks down (a non-finite scalar, or |r|^2
+   above 1e6 |r0|^2) is restarted with block-Jacobi and counted in
+   drape_counters.precond_fallbacks. The convergence test stays the reference's (cpu_solver.cpp:205-207). */
+int drape_cuda_set_precond(drape_solver* s, drape_precond* p);
+/* Inspection: the factor L (9 floats per slot, row-major; zero off the lower slots) of the solver's last network
+   run. */
+int drape_cuda_precond_factor(drape_solver* s, float* l_blocks);
+
+/* Schedule of the learned preconditioner. The network runs on every `refresh_every`-th Newton iteration only (default
+   1; the factor in between is the last one: any factor keeps M^-1 SPD, so a stale one only changes the iteration
+   count; the count restarts at each build). Each PCG solve first runs `jacobi_first` block-Jacobi iterations (default
+   0) and, when those have not met the convergence test, continues from the current iterate with the learned
+   preconditioner within the same iteration cap: a Newton system whose right-hand side is local converges under
+   block-Jacobi in a few iterations, where the learned factor's coupling to neighbours costs iterations. */
+int drape_cuda_set_precond_schedule(drape_solver* s, int refresh_every, int jacobi_first);
 
 #ifdef __cplusplus
 }

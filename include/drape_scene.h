@@ -129,6 +129,7 @@ typedef struct drape_counters {
   int64_t cg_iterations;
   int64_t line_search_halvings;
   int64_t precond_fallbacks; /* learned preconditioner abandoned for block-Jacobi */
+  int64_t learned_solves;    /* PCG solves that started with the learned preconditioner */
 } drape_counters;
 
 #ifdef __cplusplus

@@ -302,6 +302,40 @@ def backward(g: Graph, cache, go, emulate=True):
     return pack(grads)
 
 
+def live_unknowns(g: Graph) -> int:
+    return 3 * int((~g.pinned).sum())
+
+
+def kaporin(g: Graph, G, o, w):
+    """Stochastic Kaporin objective of B = G^T Ahat G on a probe w (E[w w^T] = I):
+    log(w^T G^T Ahat G w / N) - (2 / N) sum over live diagonal slots of the clamped o0..o2 (= log det G),
+    N the number of live unknowns. Its minimiser over G on a fixed lower pattern is the factorised sparse approximate
+    inverse (Kolotilina and Yeremin 1993), whose condition number bounds PCG's iteration count."""
+    w = np.asarray(w, np.float64)
+    b = apply_lower(g, G, w)
+    c = apply_full(g, g.Ahat, b)
+    t = float((b * c).sum())
+    N = live_unknowns(g)
+    d = g.lower & g.diag
+    logdet = float(np.clip(o[d, :3], -DIAG_CLAMP, DIAG_CLAMP).sum())
+    return np.log(t / N) - 2.0 * logdet / N, dict(w=w, b=b, c=c, t=t, N=N)
+
+
+def kaporin_grad_o(g: Graph, o, parts):
+    gG = (2.0 / parts["t"]) * np.einsum("sa,sb->sab", parts["c"][g.row], parts["w"][g.ci])
+    gG[~g.lower] = 0.0
+    go = grad_o(g, o, gG)
+    d = g.lower & g.diag
+    go[d, :3] -= (2.0 / parts["N"]) * (np.abs(o[d, :3]) < DIAG_CLAMP)
+    return go
+
+
+def kaporin_and_grad(g: Graph, flat, w, emulate=True):
+    G, o, cache = forward(g, flat, emulate)
+    value, parts = kaporin(g, G, o, w)
+    return value, backward(g, cache, kaporin_grad_o(g, o, parts), emulate)
+
+
 def loss_and_grad(g: Graph, flat, r, emulate=True):
     G, o, cache = forward(g, flat, emulate)
     value, parts = loss(g, G, r)

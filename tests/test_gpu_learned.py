@@ -74,14 +74,7 @@ def test_forward_matches_oracle(gpu, sysm, pinned_rows):
     assert np.all(G[~g.lower] == 0) and np.all(L[~g.lower] == 0)
 
 
-def test_loss_and_gradient_match_oracle(gpu, sysm):
-    flat = _random_params(2)
-    net = learned.LearnedPreconditioner(0, flat)
-    sid = _sample(net, sysm)
-    loss, grad = net.loss_grad(sid, 0)
-    g = graph_of(sysm)
-    loss_ref, grad_ref = mpnn.loss_and_grad(g, flat.astype(np.float64), -sysm["grad"], emulate=True)
-    assert abs(loss - loss_ref) <= 1e-2 * loss_ref
+def _groups_close(grad, grad_ref):
     assert np.linalg.norm(grad - grad_ref) <= 3e-2 * np.linalg.norm(grad_ref)
     k = 0
     for name, shape in mpnn.param_shapes():
@@ -93,6 +86,30 @@ def test_loss_and_gradient_match_oracle(gpu, sysm):
             assert cos > 0.99, (name, cos)
 
 
+def test_kaporin_objective_and_gradient_match_oracle(gpu, sysm):
+    flat = _random_params(4)
+    net = learned.LearnedPreconditioner(0, flat)
+    w = np.random.default_rng(5).standard_normal((len(sysm["diag_slot"]), 3))
+    sid = _sample(net, sysm, residuals=[w])
+    value, grad = net.loss_grad(sid, 0)
+    g = graph_of(sysm)
+    ref, grad_ref = mpnn.kaporin_and_grad(g, flat.astype(np.float64), w.astype(np.float32), emulate=True)
+    assert abs(value - ref) <= 1e-3 * max(1.0, abs(ref))
+    _groups_close(grad, grad_ref)
+
+
+def test_loss_and_gradient_match_oracle(gpu, sysm):
+    flat = _random_params(2)
+    net = learned.LearnedPreconditioner(0, flat)
+    net.set_objective(learned.DEFECT)
+    sid = _sample(net, sysm)
+    loss, grad = net.loss_grad(sid, 0)
+    g = graph_of(sysm)
+    loss_ref, grad_ref = mpnn.loss_and_grad(g, flat.astype(np.float64), -sysm["grad"], emulate=True)
+    assert abs(loss - loss_ref) <= 1e-2 * loss_ref
+    _groups_close(grad, grad_ref)
+
+
 def test_gradient_is_deterministic(gpu, sysm):
     net = learned.LearnedPreconditioner(0, _random_params(3))
     sid = _sample(net, sysm)
@@ -101,14 +118,28 @@ def test_gradient_is_deterministic(gpu, sysm):
     assert l1 == l2 and np.array_equal(g1, g2)
 
 
-def test_training_on_device_reduces_the_loss(gpu, sysm):
+def test_training_on_device_reduces_the_defect(gpu, sysm):
     rng = np.random.default_rng(0)
     n = len(sysm["diag_slot"])
     res = [-sysm["grad"]] + [rng.standard_normal((n, 3)) for _ in range(3)]
     net = learned.LearnedPreconditioner(0)
+    net.set_objective(learned.DEFECT)
     sid = _sample(net, sysm, residuals=res)
     before = np.mean([net.loss_grad(sid, k)[0] for k in range(4)])
     losses = net.train(150, lr=1e-3, batch=4, seed=1)
     after = np.mean([net.loss_grad(sid, k)[0] for k in range(4)])
     assert np.isfinite(losses).all()
     assert after < 0.6 * before, (before, after)
+
+
+def test_kaporin_training_lowers_the_condition_estimate(gpu, sysm):
+    """Kaporin training moves toward the factorised sparse approximate inverse: the objective (the log of a condition
+    estimate of the preconditioned operator) falls."""
+    rng = np.random.default_rng(1)
+    n = len(sysm["diag_slot"])
+    net = learned.LearnedPreconditioner(0)
+    sid = _sample(net, sysm, residuals=[rng.standard_normal((n, 3)) for _ in range(8)])
+    before = np.mean([net.loss_grad(sid, k)[0] for k in range(8)])
+    net.train(300, lr=1e-3, batch=4, seed=2)
+    after = np.mean([net.loss_grad(sid, k)[0] for k in range(8)])
+    assert after < before - 0.05, (before, after)

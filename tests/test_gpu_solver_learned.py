@@ -1,0 +1,113 @@
+"""The solver with the learned preconditioner (drape_cuda_set_precond), through the C ABI.
+
+An identity-initialised network is block-Jacobi up to FP32 rounding (M^-1 = C C^T instead of inv(A_ii)), so its
+trajectories match the Jacobi solver's closely and it passes the reference's known-answer tests. A network whose
+output is not finite stalls on the first residual and is restarted with block-Jacobi, which makes the trajectory
+bit-identical to the Jacobi solver's.
+"""
+import numpy as np
+import pytest
+
+from drape_b200 import learned
+from drape_b200 import scenes as S
+from physics_cases import CASES
+
+pytestmark = pytest.mark.gpu
+
+
+def _small_tube():
+    return S.seamed_tube(24, 30, field_n=64, field_cell=0.008)
+
+
+def _run(gpu, scene, precond=None, frames=10, iterations=2):
+    s = gpu.CudaSolver(0)
+    if precond is not None:
+        s.set_precond(precond)
+    s.build(scene)
+    gid = scene.garments[0].id
+    for f in range(frames):
+        if f == 5:
+            s.set_phase(gid, 1)
+        s.step(1 / 60, 1, iterations)
+    return s
+
+
+def test_identity_network_tracks_jacobi(gpu):
+    """Two frames of the assembling tube: the same PCG iteration counts and positions within 1e-4 m. (Later frames
+    of this scene branch on contact activation and line-search decisions, where FP32 rounding differences between
+    C C^T and inv(A_ii) grow to centimetres, as they do between any two FP32 orderings.)"""
+    p = learned.LearnedPreconditioner(0)
+    a = _run(gpu, _small_tube(), frames=2)
+    b = _run(gpu, _small_tube(), p, frames=2)
+    ca, cb = a.counters(), b.counters()
+    assert ca.learned_solves == 0 and cb.learned_solves == cb.newton_iterations > 0
+    assert cb.precond_fallbacks == 0
+    dev = np.abs(a.positions().astype(np.float64) - b.positions()).max()
+    assert dev < 1e-4, dev
+    assert np.array_equal(a.cg_history(), b.cg_history())
+
+
+def test_non_finite_network_falls_back_to_jacobi_bit_identically(gpu):
+    params = learned.init_params(0)
+    k = learned.param_count() - 16 - 16 * 192  # W_o
+    params[k:k + 16 * 192] = np.nan
+    p = learned.LearnedPreconditioner(0, params)
+    a = _run(gpu, _small_tube())
+    b = _run(gpu, _small_tube(), p)
+    cb = b.counters()
+    assert cb.precond_fallbacks == cb.learned_solves == cb.newton_iterations > 0
+    assert np.array_equal(a.positions(), b.positions())
+    assert a.counters().cg_iterations == cb.cg_iterations
+
+
+def test_switching_back_to_jacobi(gpu):
+    p = learned.LearnedPreconditioner(0)
+    s = gpu.CudaSolver(0)
+    s.set_precond(p)
+    s.build(_small_tube())
+    s.step(1 / 60, 1, 2)
+    assert s.counters().learned_solves > 0
+    s.set_precond(None)
+    s.reset_counters()
+    s.step(1 / 60, 1, 2)
+    assert s.counters().learned_solves == 0
+
+
+def _identity_learned(gpu):
+    s = gpu.CudaSolver(0)
+    s.set_precond(learned.LearnedPreconditioner(0))
+    return s
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_learned_known_answers(gpu, case):
+    CASES[case](lambda: _identity_learned(gpu))
+
+
+def test_solver_factor_matches_network_on_the_same_system(gpu):
+    """The factor the solver's network run produces (inference path, on the solver's own device arrays) equals the
+    sample path's (training forward) on the captured system that the next Newton iteration assembles."""
+    p = learned.LearnedPreconditioner(0, learned.load_weights("tube"))
+    s = gpu.CudaSolver(0)
+    s.set_precond(p)
+    scene = _small_tube()
+    s.build(scene)
+    for _ in range(3):
+        s.step(1 / 60, 1, 2)
+    sysm = s.capture_system(1 / 60)
+    s.step(1 / 60, 1, 1)
+    Ls = s.precond_factor()
+    n = len(sysm["diag_slot"])
+    sid = p.add_sample(sysm["row_start"], sysm["col_index"], sysm["blocks"], np.zeros(n, np.uint8), sysm["active"],
+                       np.zeros((1, n, 3), np.float32))
+    _, Lp = p.forward(sid)
+    assert np.linalg.norm(Ls - Lp) <= 1e-5 * np.linalg.norm(Lp)
+
+
+def test_trained_network_needs_fewer_pcg_iterations_on_held_out_systems(gpu):
+    """Ablation on the same systems: Newton systems of a held-out tube variant (10k particles, never trained on),
+    solved to the reference's tolerance 1e-2 with block-Jacobi and with the shipped trained network."""
+    from drape_b200 import train
+    systems = train.capture_along_drape(S.tube_variant(8, 10000, field_n=96), frames=120, every=20)
+    res = train.ablation(learned.load_weights("tube"), systems, 1e-2)
+    assert res["ratio"] > 1.3, res

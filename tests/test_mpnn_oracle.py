@@ -139,3 +139,30 @@ def test_adam_reduces_the_loss(sysm):
         flat = mpnn.adam(flat, grad, state, lr=1e-3)
     last = np.mean([mpnn.loss(g, mpnn.forward(g, flat)[0], r)[0] for r in rs])
     assert last < 0.6 * first, (first, last)
+
+
+def test_kaporin_gradient_matches_finite_differences(sysm):
+    g = graph_of(sysm)
+    flat = _random_params(4)
+    w = np.random.default_rng(5).standard_normal((g.n, 3))
+    value, grad = mpnn.kaporin_and_grad(g, flat, w, emulate=False)
+    rng = np.random.default_rng(9)
+    for _ in range(4):
+        d = rng.standard_normal(flat.shape)
+        d /= np.linalg.norm(d)
+        h = 1e-6
+        fp = mpnn.kaporin(g, *mpnn.forward(g, flat + h * d, emulate=False)[:2], w)[0]
+        fm = mpnn.kaporin(g, *mpnn.forward(g, flat - h * d, emulate=False)[:2], w)[0]
+        fd = (fp - fm) / (2 * h)
+        an = float(grad @ d)
+        assert abs(fd - an) <= 1e-5 * max(abs(fd), 1e-3 * np.linalg.norm(grad)), (fd, an)
+
+
+def test_kaporin_at_identity_is_log_of_normalised_trace(sysm):
+    """G = I: the objective is log(w^T Ahat w / N), about log(1) = 0 since Ahat has identity diagonal blocks."""
+    g = graph_of(sysm)
+    G, o, _ = mpnn.forward(g, mpnn.init_params(0), emulate=False)
+    w = np.random.default_rng(1).standard_normal((g.n, 3))
+    value, parts = mpnn.kaporin(g, G, o, w)
+    ref = float((w.reshape(-1) @ (mpnn.apply_full(g, g.Ahat, w).reshape(-1)))) / mpnn.live_unknowns(g)
+    assert abs(value - np.log(ref)) < 1e-12
