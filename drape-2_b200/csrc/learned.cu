@@ -1208,6 +1208,8 @@ T* dalloc(size_t count) {
   T* p = nullptr;
   NCK(cudaMalloc(&p, sizeof(T) * std::max<size_t>(count, 1)));
   NCK(cudaMemset(p, 0, sizeof(T) * std::max<size_t>(count, 1)));
+  // The zeroing is on the legacy default stream, unordered with the network's and the solver's non-blocking streams.
+  NCK(cudaStreamSynchronize(nullptr));
   return p;
 }
 

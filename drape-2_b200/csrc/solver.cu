@@ -53,11 +53,14 @@ struct DBuf {
     p = nullptr;
     n = 0;
   }
+  // The zeroing runs on the legacy default stream, which is not ordered with the solver's non-blocking stream: wait
+  // for it here, or it could land after the uploads and kernels that follow.
   void alloc(size_t count) {
     release();
     n = count;
     CK(cudaMalloc(&p, sizeof(T) * std::max<size_t>(count, 1)));
     CK(cudaMemset(p, 0, sizeof(T) * std::max<size_t>(count, 1)));
+    CK(cudaStreamSynchronize(nullptr));
   }
   void upload(const T* src, size_t count, cudaStream_t s) {
     if (count > n || !p) alloc(count);
