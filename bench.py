@@ -167,6 +167,185 @@ def run_reference(args):
     return 0
 
 
+def learned_leg(CU, device, scene, gid, init, flush, args, jacobi_value, jacobi_final, max_over_ranks):
+    """The same drape with the learned preconditioner (shipped trained weights, the network run on every Newton
+    iteration, PCG cap and tolerance unchanged), on the same GPU, from the same initial state, L2 flushed the same
+    way. Reports its settle time beside block-Jacobi's, its PCG iterations per Newton iteration, and how far its
+    settled shape lies from the block-Jacobi drape's."""
+    import torch
+    from drape_b200 import learned as LR
+    p = LR.LearnedPreconditioner(device, LR.load_weights("tube"))
+    s = CU.CudaSolver(device)
+    s.set_precond(p)
+    s.build(scene)
+    s.restore(init)
+    stream = torch.cuda.ExternalStream(s.stream_handle())
+
+    def drape():
+        s.restore(init)
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        res = s.drape_to_rest([gid])
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b) / 1000.0, res
+
+    drape()  # warm-up
+    s.reset_counters()
+    s.profile(True)
+    times, results = [], []
+    for _ in range(max(1, min(args.steps, 2))):
+        t, r = drape()
+        times.append(t)
+        results.append(r)
+    prof = s.profile_read()
+    s.profile(False)
+    c = s.counters()
+    hist = s.cg_history()
+    value = max_over_ranks(statistics.mean(times))
+    d = np.linalg.norm(s.positions().astype(np.float64) - jacobi_final, axis=1)
+    total_ms = sum(prof["milliseconds"].values())
+    out = {
+        "precond": "learned (trained weights drape_b200/weights/tube.npy), network run every Newton iteration",
+        "settle_s": value, "jacobi_settle_s": jacobi_value,
+        "speedup_vs_jacobi": jacobi_value / value if value else None,
+        "frames": int(results[-1].frames_run), "settled": bool(results[-1].settled),
+        "ms_per_frame": 1000.0 * statistics.mean(t / max(1, r.frames_run) for t, r in zip(times, results)),
+        "pcg_iters_per_newton": {"mean": float(np.mean(hist)) if len(hist) else None,
+                                 "p50": float(np.percentile(hist, 50)) if len(hist) else None,
+                                 "p95": float(np.percentile(hist, 95)) if len(hist) else None},
+        "learned_solves": int(c.learned_solves), "jacobi_fallbacks": int(c.precond_fallbacks),
+        "kernel_share": {k: (v / total_ms if total_ms else 0.0) for k, v in prof["milliseconds"].items()},
+        "settled_shape_vs_jacobi_m": {"max": float(d.max()), "rms": float(np.sqrt(np.mean(d * d)))},
+    }
+    s.close()
+    p.close()
+    return out
+
+
+def spmv_leg(CU, solver, peak, tiles=12, reps=20):
+    """The standalone block-CSR SpMV (drape_cuda_spmv_device) on an HBM-resident matrix: the 60k tube's first Newton
+    system tiled block-diagonally `tiles` times (each tile's columns shifted), larger than the 126 MB L2, timed with
+    CUDA events over `reps` launches on one stream. Algorithmic bytes: 40 per block slot + 44 per row."""
+    import torch
+    sysm = solver.capture_system(1.0 / 60.0)
+    rs, ci = sysm["row_start"].astype(np.int64), sysm["col_index"].astype(np.int64)
+    n1, b1 = len(rs) - 1, len(ci)
+    n, B = n1 * tiles, b1 * tiles
+    SP = (B + 31) // 32 * 32
+    rs_all = np.concatenate([rs[:-1] + t * b1 for t in range(tiles)] + [np.array([B])]).astype(np.uint32)
+    ci_all = np.concatenate([ci + t * n1 for t in range(tiles)]).astype(np.uint32)
+    planes = np.zeros((9, SP), np.float32)
+    planes[:, :B] = np.tile(sysm["blocks"].reshape(b1, 9).T, (1, tiles))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    d_rs = torch.from_numpy(rs_all.view(np.int32)).to(dev)
+    d_ci = torch.from_numpy(ci_all.view(np.int32)).to(dev)
+    d_bl = torch.from_numpy(planes).to(dev)
+    d_pin = torch.zeros(n, dtype=torch.uint8, device=dev)
+    gen = torch.Generator(device="cpu").manual_seed(3)
+    d_x = torch.randn((n, 4), generator=gen).to(dev)
+    d_y = torch.zeros((n, 4), device=dev)
+    L = CU.load()
+    st = torch.cuda.current_stream()
+
+    def launch():
+        code = L.drape_cuda_spmv_device(n, d_rs.data_ptr(), d_ci.data_ptr(), d_bl.data_ptr(), SP, d_pin.data_ptr(),
+                                        d_x.data_ptr(), d_y.data_ptr(), st.cuda_stream)
+        if code != 0:
+            raise RuntimeError(L.drape_cuda_last_error(None))
+
+    for _ in range(3):
+        launch()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    for _ in range(reps):
+        launch()
+    b.record(st)
+    b.synchronize()
+    ms = a.elapsed_time(b) / reps
+    # Check against a host product on a few rows of the first tile.
+    y = d_y[:n1].cpu().numpy()
+    bl = sysm["blocks"].reshape(b1, 3, 3).astype(np.float64)
+    x = d_x[:n1, :3].cpu().numpy().astype(np.float64)
+    err = 0.0
+    for i in range(0, n1, max(1, n1 // 200)):
+        ref = sum(bl[s] @ x[ci[s]] for s in range(rs[i], rs[i + 1]))
+        err = max(err, float(np.abs(ref - y[i, :3]).max() / (np.abs(ref).max() + 1e-30)))
+    algo = 40.0 * B + 44.0 * n
+    achieved = algo / (ms / 1e3) / 1e9
+    return {"kernel": "k_spmv", "rows": n, "block_slots": B, "matrix_mb": 36.0 * B / 1e6,
+            "ms_per_launch": ms, "algorithmic_bytes_per_launch": algo, "achieved": achieved, "peak": peak,
+            "unit": "GB/s", "frac": achieved / peak, "max_rel_error_vs_host": err,
+            "workload": f"60k tube Newton system tiled {tiles}x block-diagonally (inputs larger than L2)"}
+
+
+def batch_leg(args, device, world, rank, max_over_ranks, peak):
+    """Batched drapes: the 64 uneven seeded tubes (2k-40k particles, each on its own seeded body), this rank's share
+    (drape_b200.batch.shard), autotuned, draped to rest through the batch's graphed frames."""
+    import torch
+    from drape_b200 import batch as BT
+    from drape_b200 import scenes as S
+    scenes = S.batch_tubes(args.batch_garments)
+    sizes = [sc.garments[0].vertex_count for sc in scenes]
+    mine = BT.shard(sizes, world)[rank]
+    b = BT.BatchSolver(device)
+    for g in mine:
+        b.add(scenes[g])
+    b.build()
+    G, N, B = b.size()
+    b.save()
+    tuning = b.autotune(2)
+    stream = torch.cuda.ExternalStream(b.stream_handle())
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    b.restore()
+    b.reset_counters()
+    b.profile(False)
+    e0.record(stream)
+    t0 = time.perf_counter()
+    res, secs = b.drape_to_rest()
+    e1.record(stream)
+    e1.synchronize()
+    wall = time.perf_counter() - t0
+    dev_s = e0.elapsed_time(e1) / 1000.0
+    prof_graph = b.profile_read()
+    total = max_over_ranks(max(wall, dev_s))
+    # Roofline of the batch solve: 10 profiled frames from the initial state (direct launches, events per solve).
+    b.restore()
+    b.reset_counters()
+    b.profile(True)
+    for _ in range(10):
+        b.step(1.0 / 60.0, 1, 2)
+    p = b.profile_read()
+    b.profile(False)
+    achieved = p["pcg_bytes"] / (p["solve_ms"] / 1e3) / 1e9 if p["solve_ms"] > 0 else 0.0
+    settled = [bool(r.settled) for r in res]
+    frames = [int(r.frames_run) for r in res]
+    out = {
+        "workload": f"{args.batch_garments} seamed tubes, particles log-uniform 2k-40k, each on its own seeded "
+                    "capsule-union body (32^3-128^3 field), one persistent solve launch per Newton iteration, frames "
+                    "replayed from a CUDA graph, autotuned solve variant, block-Jacobi PCG cap 50 / tol 1e-2",
+        "garments": G, "particles": N, "block_slots": B, "rank_garments": len(mine),
+        "drape_s": total, "drapes_per_s": args.batch_garments / total if total else None,
+        "per_drape_settle_s": {"median": float(np.median(secs)), "p90": float(np.percentile(secs, 90)),
+                               "max": float(np.max(secs))},
+        "settled": int(sum(settled)), "frames": {"median": float(np.median(frames)), "max": int(max(frames))},
+        "tuning": tuning, "graph_launches": int(prof_graph["graph_launches"]),
+        "kernel_launches": int(prof_graph["kernel_launches"]),
+        "roofline": {"kernel": "k_solve_batch", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak if peak else None,
+                     "avg_launch_ms": p["solve_ms"] / max(1, p["solve_launches"]),
+                     "algorithmic_bytes_per_launch": p["pcg_bytes"] / max(1, p["solve_launches"]),
+                     "sample": "10 frames from the initial state, profiled (direct launches)"},
+    }
+    b.close()
+    return out
+
+
 def cpu_baseline(workload: str):
     try:
         value, desc, _ = reference_settle_seconds(workload, 1)
@@ -184,6 +363,8 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="tube60k")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=0, help="end-to-end steps (0: same as --steps)")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner leg")
+    ap.add_argument("--batch-garments", type=int, default=64, help="garments of the batched leg (0: skip it)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -301,6 +482,8 @@ def main():
         h2d.append(b1[0] - b0[0])
         d2h.append(b1[1] - b0[1])
     e2e_value = max_over_ranks(statistics.mean(e2e_times))
+    solver.restore(init)
+    solver.drape_to_rest([gid])  # the Jacobi drape's final shape, for the learned leg's comparison
 
     line = {
         "metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -327,6 +510,14 @@ def main():
                                  "cap": 50},
         "sizes": sizes,
     }
+    if not args.no_learned:
+        jac_final = solver.positions().astype(np.float64)
+        line["precond"] = learned_leg(CU, local, scene, gid, init, flush, args, value, jac_final, max_over_ranks)
+    peak, _ = measured_peaks()
+    solver.restore(init)
+    line["spmv"] = spmv_leg(CU, solver, peak)
+    if args.batch_garments > 0:
+        line["batch"] = batch_leg(args, local, world, rank, max_over_ranks, peak)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.workload)
     if rank == 0:

@@ -128,16 +128,18 @@ struct Dev {
 };
 
 // ---------------------------------------------------------------------------------------------------------------
-// Grid-wide synchronisation for the cooperative persistent kernels (cooperative launch guarantees co-residency).
+// Synchronisation of a group of co-resident blocks for the cooperative persistent kernels (cooperative launch
+// guarantees co-residency). A group is the whole grid for one solver, or the blocks a batched launch gives one
+// garment: `rank` is the block's index in its group and `size` the group's block count.
 //
-// Arrivals only ever increase: a launch's k-th barrier completes when the counter reaches base + k * gridDim.x, base
-// being the counter at the launch's start rounded down to a multiple of gridDim.x (no barrier can complete before
+// Arrivals only ever increase: a launch's k-th barrier completes when the counter reaches base + k * size, base
+// being the counter at the launch's start rounded down to a multiple of size (no barrier can complete before
 // every block has arrived, so a block that reads the counter late still rounds to the same base). Thread 0 adds its
 // block's arrival with release semantics after publishing the block's partial sums and polls with acquire loads; a
 // time limit turns a lost block into an error status and a return instead of a hang.
 //
-// Reductions alternate between two halves of the partials array, so a block that has already passed a barrier and
-// publishes its next partial cannot overwrite values a slower block is still summing.
+// Reductions alternate between two halves of the group's partials array, so a block that has already passed a
+// barrier and publishes its next partial cannot overwrite values a slower block is still summing.
 
 __device__ __forceinline__ unsigned long long globalTimerNs() {
   unsigned long long t;
@@ -149,26 +151,31 @@ struct GridSync {
   Control* ctl;
   unsigned long long target, limitNs;
   unsigned int parity;
+  uint32_t rank, size;
 
-  __device__ void init(Control* c, unsigned long long lim) {
+  __device__ void init(Control* c, unsigned long long lim, uint32_t rank_, uint32_t size_) {
     __shared__ unsigned long long base;
     if (threadIdx.x == 0) {
       cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> a(c->barrierArrivals);
       const unsigned long long now = a.load(cuda::memory_order_relaxed);
-      base = now - now % gridDim.x;
+      base = now - now % size_;
     }
     __syncthreads();
     ctl = c;
     target = base;
     limitNs = lim;
     parity = 0;
+    rank = rank_;
+    size = size_;
   }
+  // The whole grid as one group.
+  __device__ void init(Control* c, unsigned long long lim) { init(c, lim, blockIdx.x, gridDim.x); }
 
   // blockSynced: the caller has just passed a __syncthreads after every thread's writes of this phase and only
   // thread 0 publishes after it (the case of gridReduce), so the leading block barrier can be skipped.
   __device__ bool sync(bool blockSynced = false) {
     __shared__ int ok;
-    target += gridDim.x;
+    target += size;
     if (!blockSynced) __syncthreads();
     if (threadIdx.x == 0) {
       unsigned long long* counter = &ctl->barrierArrivals;
@@ -230,7 +237,7 @@ __device__ inline void blockSum(double (&v)[K], double* out) {
 template <int K, bool Max = false>
 __device__ inline bool gridReduce(const Dev& D, GridSync& gs, double (&v)[K], double (&out)[K]) {
   __shared__ double res[K];
-  double* half = D.partials + static_cast<size_t>(gs.parity) * gridDim.x * kPartialStride;
+  double* half = D.partials + static_cast<size_t>(gs.parity) * gs.size * kPartialStride;
   gs.parity ^= 1u;
   if (Max) {
     __shared__ double mred[K][32];
@@ -248,21 +255,21 @@ __device__ inline bool gridReduce(const Dev& D, GridSync& gs, double (&v)[K], do
       for (int k = 0; k < K; ++k) {
         double m = mred[k][0];
         for (int w = 1; w < static_cast<int>((blockDim.x + 31) >> 5); ++w) m = fmax(m, mred[k][w]);
-        half[blockIdx.x * kPartialStride + k] = m;
+        half[gs.rank * kPartialStride + k] = m;
       }
   } else {
     double blk[K];
     blockSum<K>(v, blk);
     if (threadIdx.x == 0)
 #pragma unroll
-      for (int k = 0; k < K; ++k) half[blockIdx.x * kPartialStride + k] = blk[k];
+      for (int k = 0; k < K; ++k) half[gs.rank * kPartialStride + k] = blk[k];
   }
   if (!gs.sync(true)) return false;
   if (threadIdx.x < 32) {
     double s[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) s[k] = Max ? -INFINITY : 0.0;
-    for (unsigned int b = threadIdx.x; b < gridDim.x; b += 32)
+    for (unsigned int b = threadIdx.x; b < gs.size; b += 32)
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         const double x = __ldcg(half + b * kPartialStride + k);
@@ -285,11 +292,12 @@ __device__ inline bool gridReduce(const Dev& D, GridSync& gs, double (&v)[K], do
   return true;
 }
 
-// This block's contiguous share of [0, n): the persistent kernels give each block one range of rows, so the
-// neighbour gathers of the SpMV mostly hit rows the same block (hence the same SM's L1) just touched.
-__device__ __forceinline__ void blockRange(uint32_t n, uint32_t& r0, uint32_t& r1) {
-  const uint32_t per = (n + gridDim.x - 1) / gridDim.x;
-  r0 = min(n, blockIdx.x * per);
+// Block `rank`'s contiguous share of [0, n) in a group of `size` blocks: the persistent kernels give each block one
+// range of rows, so the neighbour gathers of the SpMV mostly hit rows the same block (hence the same SM's L1) just
+// touched.
+__device__ __forceinline__ void blockRange(uint32_t n, uint32_t rank, uint32_t size, uint32_t& r0, uint32_t& r1) {
+  const uint32_t per = (n + size - 1) / size;
+  r0 = min(n, rank * per);
   r1 = min(n, r0 + per);
 }
 
@@ -335,13 +343,15 @@ __device__ inline void contactSetupOne(const Dev& D, uint32_t i, float3 xs, Cont
   }
 }
 
-__global__ void k_begin(Dev D) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+// The point kernels' bodies take the block's rank in the blocks that cover the solver (the grid, or a garment's
+// share of a batched launch) and that share's size.
+__device__ inline void beginRows(const Dev& D, uint32_t rank, uint32_t size) {
+  if (rank == 0 && threadIdx.x == 0) {
     D.ctl->newtonDone = 0;
     D.ctl->substeps += 1;
   }
   const float h = D.P.h;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < D.P.n; i += gridDim.x * blockDim.x) {
+  for (uint32_t i = rank * blockDim.x + threadIdx.x; i < D.P.n; i += size * blockDim.x) {
     const float4 x4 = D.x[i];
     D.xStart[i] = x4;
     const Particle pa = D.particle[i];
@@ -361,19 +371,10 @@ __global__ void k_begin(Dev D) {
   }
 }
 
-// Contact candidates for given positions (test entry point; same code as k_begin).
-__global__ void k_contact_candidates(Dev D, const float4* xs, Contact* out) {
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < D.P.n; i += gridDim.x * blockDim.x) {
-    Contact c{};
-    contactSetupOne(D, i, xyz(xs[i]), c);
-    out[i] = c;
-  }
-}
-
 // Holds near particles on their plane for this Newton iteration, projecting any below it (kernels.h:85-99).
-__global__ void k_activate(Dev D) {
+__device__ inline void activateRows(const Dev& D, uint32_t rank, uint32_t size) {
   if (D.ctl->newtonDone) return;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < D.P.n; i += gridDim.x * blockDim.x) {
+  for (uint32_t i = rank * blockDim.x + threadIdx.x; i < D.P.n; i += size * blockDim.x) {
     Contact c = D.contact[i];
     if (c.nearBody == 0u) continue;
     const float3 n = xyz(c.normal);
@@ -447,14 +448,14 @@ __device__ inline int evalEntry(const Dev& D, uint32_t code, float3& g, M3 H[4])
   return 2;
 }
 
-__global__ void __launch_bounds__(kAssembleWarps * kWarp) k_assemble(Dev D) {
+__device__ inline void assembleRows(const Dev& D, uint32_t rank, uint32_t size) {
   if (D.ctl->newtonDone) return;
   extern __shared__ __align__(16) unsigned char assembleSmem[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   AssembleWarp& sh = reinterpret_cast<AssembleWarp*>(assembleSmem)[w];
-  const uint32_t warpsTotal = gridDim.x * kAssembleWarps;
+  const uint32_t warpsTotal = size * kAssembleWarps;
   const uint32_t SP = D.P.slotsPadded;
-  for (uint32_t i = blockIdx.x * kAssembleWarps + w; i < D.P.n; i += warpsTotal) {
+  for (uint32_t i = rank * kAssembleWarps + w; i < D.P.n; i += warpsTotal) {
     const uint32_t rs = D.rowStart[i], L = D.rowStart[i + 1] - rs;
     const uint32_t diagLocal = D.diagSlot[i] - rs;
     const Particle pa = D.particle[i];
@@ -556,17 +557,17 @@ __global__ void __launch_bounds__(kAssembleWarps * kWarp) k_assemble(Dev D) {
 // ---------------------------------------------------------------------------------------------------------------
 // Energy at u + alpha * step, in FP64, summed per thread over particles (inertia + friction) and terms.
 
-__device__ inline double energyPartial(const Dev& D, double alpha) {
+__device__ inline double energyPartial(const Dev& D, const GridSync& gs, double alpha) {
   double e = 0.0;
   const uint32_t n = D.P.n, S = D.P.nStretch, H = D.P.nHinge, K = D.P.nSeam;
   const uint32_t total = n + S + H + K;
-  const uint32_t stride = gridDim.x * blockDim.x;
+  const uint32_t stride = gs.size * blockDim.x;
   auto pos = [&](uint32_t v0, uint32_t vk) -> d3 {
     const d3 rel = toD(ld3(D.xStart, vk)) - toD(ld3(D.xStart, v0));
     return rel + (toD(ld3(D.u, vk)) + alpha * toD(ld3(D.step, vk)));
   };
   const double invH2 = 1.0 / (D.P.hD * D.P.hD);
-  for (uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += stride) {
+  for (uint32_t idx = gs.rank * blockDim.x + threadIdx.x; idx < total; idx += stride) {
     if (idx < n) {
       const uint32_t i = idx;
       const Particle pa = D.particle[i];
@@ -669,13 +670,13 @@ __device__ inline SmemMatrix stageMatrix(const Dev& D, uint32_t r0, uint32_t r1)
   return A;
 }
 
-// y_i (unfiltered) = sum over unpinned columns j of A_ij x_j for row i, by kRowLanes lanes (lane `sub`), reduced over
-// the group; x_j given by a functor.
-template <class X>
+// y_i (unfiltered) = sum over unpinned columns j of A_ij x_j for row i, by RL lanes (lane `sub`), reduced over the
+// lanes; x_j given by a functor.
+template <int RL, class X>
 __device__ __forceinline__ float3 rowProduct(const SmemMatrix& A, uint32_t rs, uint32_t re, int sub, unsigned mask,
                                              X&& xj) {
   float3 acc = mk(0, 0, 0);
-  for (uint32_t s = rs + sub; s < re; s += kRowLanes) {
+  for (uint32_t s = rs + sub; s < re; s += RL) {
     const uint32_t col = A.col(s);
     if (col & kPinnedBit) continue;
     const float3 v = xj(col);
@@ -686,7 +687,7 @@ __device__ __forceinline__ float3 rowProduct(const SmemMatrix& A, uint32_t rs, u
     acc.z += a[6] * v.x + a[7] * v.y + a[8] * v.z;
   }
 #pragma unroll
-  for (int o = kRowLanes / 2; o > 0; o >>= 1) {
+  for (int o = RL / 2; o > 0; o >>= 1) {
     acc.x += __shfl_xor_sync(mask, acc.x, o);
     acc.y += __shfl_xor_sync(mask, acc.y, o);
     acc.z += __shfl_xor_sync(mask, acc.z, o);
@@ -698,11 +699,12 @@ __device__ __forceinline__ float3 rowProduct(const SmemMatrix& A, uint32_t rs, u
 // when a grid barrier gave up.
 // At most `budget` iterations (negative: P.maxCg). *r0out gets |r0|; *finished is false only when the budget, not
 // the convergence test or pAp <= 0, ended the loop.
+template <int RL>
 __device__ inline int pcgReferenceOrder(const Dev& D, GridSync& gs, const SmemMatrix& A, int budget = -1,
                                         double* r0out = nullptr, bool* finished = nullptr) {
   const uint32_t n = D.P.n;
   uint32_t r0i, r1i;
-  blockRange(n, r0i, r1i);
+  blockRange(n, gs.rank, gs.size, r0i, r1i);
   // CG init (kernels.h:252-268): step = 0, resid = -grad, r = filter(resid), z = filter(M r).
   double tot[2];
   {
@@ -730,25 +732,25 @@ __device__ inline int pcgReferenceOrder(const Dev& D, GridSync& gs, const SmemMa
   float4* pCur = D.p1;
   int it = 0;
   const int maxCg = budget < 0 ? D.P.maxCg : min(budget, D.P.maxCg);
-  const uint32_t groups = blockDim.x / kRowLanes;
-  const int sub = threadIdx.x & (kRowLanes - 1);
-  const unsigned groupMask = ((1u << kRowLanes) - 1u) << ((threadIdx.x & 31) & ~(kRowLanes - 1));
+  const uint32_t groups = blockDim.x / RL;
+  const int sub = threadIdx.x & (RL - 1);
+  const unsigned groupMask = ((1u << RL) - 1u) << ((threadIdx.x & 31) & ~(RL - 1));
   if (finished) *finished = true;
   while (!done && it < maxCg) {
     // SpMV with the direction update folded in: p_j = z_j + beta * pPrev_j.
     double vpap[1] = {0.0};
     const float fb = static_cast<float>(beta);
     const bool first = it == 0;
-    for (uint32_t i = r0i + threadIdx.x / kRowLanes; i < r1i; i += groups) {
+    for (uint32_t i = r0i + threadIdx.x / RL; i < r1i; i += groups) {
       const uint32_t rs = __ldg(D.rowStart + i), re = __ldg(D.rowStart + i + 1);
       float3 acc = mk(0, 0, 0);
       if (D.particle[i].pinned == 0u)
-        acc = rowProduct(A, rs, re, sub, groupMask, [&](uint32_t j) {
+        acc = rowProduct<RL>(A, rs, re, sub, groupMask, [&](uint32_t j) {
           const float3 zj = ld3(D.z, j);
           return first ? zj : zj + ld3(pPrev, j) * fb;
         });
       else
-        acc = rowProduct(A, rs, rs, sub, groupMask, [&](uint32_t) { return mk(0, 0, 0); });
+        acc = rowProduct<RL>(A, rs, rs, sub, groupMask, [&](uint32_t) { return mk(0, 0, 0); });
       if (sub == 0) {
         const float3 zi = ld3(D.z, i);
         const float3 pi = first ? zi : zi + ld3(pPrev, i) * fb;
@@ -794,15 +796,16 @@ __device__ inline int pcgReferenceOrder(const Dev& D, GridSync& gs, const SmemMa
 
 // z = F(L L^T r) over this block's rows, with L the learned factor (planes D.Lf, lower slots) and y = L^T r kept in
 // D.ap between the two products; returns false when a grid barrier gave up. Adds r.z of its rows to *rz.
+template <int RL>
 __device__ inline bool applyLearned(const Dev& D, GridSync& gs, uint32_t r0i, uint32_t r1i, double* rz) {
-  const uint32_t groups = blockDim.x / kRowLanes;
-  const int sub = threadIdx.x & (kRowLanes - 1);
-  const unsigned groupMask = ((1u << kRowLanes) - 1u) << ((threadIdx.x & 31) & ~(kRowLanes - 1));
+  const uint32_t groups = blockDim.x / RL;
+  const int sub = threadIdx.x & (RL - 1);
+  const unsigned groupMask = ((1u << RL) - 1u) << ((threadIdx.x & 31) & ~(RL - 1));
   const uint32_t SP = D.P.slotsPadded;
   // y_j = sum over slots (j, i), i >= j, of L_(i, j)^T r_i.
-  for (uint32_t j = r0i + threadIdx.x / kRowLanes; j < r1i; j += groups) {
+  for (uint32_t j = r0i + threadIdx.x / RL; j < r1i; j += groups) {
     float3 acc = mk(0, 0, 0);
-    for (uint32_t s = __ldg(D.rowStart + j) + sub; s < __ldg(D.rowStart + j + 1); s += kRowLanes) {
+    for (uint32_t s = __ldg(D.rowStart + j) + sub; s < __ldg(D.rowStart + j + 1); s += RL) {
       const uint32_t col = __ldg(D.colIndex + s);
       if ((col & kPinnedBit) || col < j) continue;
       const uint32_t t = __ldg(D.tslot + s);
@@ -813,7 +816,7 @@ __device__ inline bool applyLearned(const Dev& D, GridSync& gs, uint32_t r0i, ui
       acc.z += L[2 * SP] * v.x + L[5 * SP] * v.y + L[8 * SP] * v.z;
     }
 #pragma unroll
-    for (int o = kRowLanes / 2; o > 0; o >>= 1) {
+    for (int o = RL / 2; o > 0; o >>= 1) {
       acc.x += __shfl_xor_sync(groupMask, acc.x, o);
       acc.y += __shfl_xor_sync(groupMask, acc.y, o);
       acc.z += __shfl_xor_sync(groupMask, acc.z, o);
@@ -822,9 +825,9 @@ __device__ inline bool applyLearned(const Dev& D, GridSync& gs, uint32_t r0i, ui
   }
   if (!gs.sync()) return false;
   // z_i = F(sum over slots (i, j), j <= i, of L_(i, j) y_j).
-  for (uint32_t i = r0i + threadIdx.x / kRowLanes; i < r1i; i += groups) {
+  for (uint32_t i = r0i + threadIdx.x / RL; i < r1i; i += groups) {
     float3 acc = mk(0, 0, 0);
-    for (uint32_t s = __ldg(D.rowStart + i) + sub; s < __ldg(D.rowStart + i + 1); s += kRowLanes) {
+    for (uint32_t s = __ldg(D.rowStart + i) + sub; s < __ldg(D.rowStart + i + 1); s += RL) {
       const uint32_t col = __ldg(D.colIndex + s);
       if ((col & kPinnedBit) || col > i) continue;
       const float3 v = ld3(D.ap, col);
@@ -834,7 +837,7 @@ __device__ inline bool applyLearned(const Dev& D, GridSync& gs, uint32_t r0i, ui
       acc.z += L[6 * SP] * v.x + L[7 * SP] * v.y + L[8 * SP] * v.z;
     }
 #pragma unroll
-    for (int o = kRowLanes / 2; o > 0; o >>= 1) {
+    for (int o = RL / 2; o > 0; o >>= 1) {
       acc.x += __shfl_xor_sync(groupMask, acc.x, o);
       acc.y += __shfl_xor_sync(groupMask, acc.y, o);
       acc.z += __shfl_xor_sync(groupMask, acc.z, o);
@@ -856,11 +859,12 @@ __device__ inline bool applyLearned(const Dev& D, GridSync& gs, uint32_t r0i, ui
 // unpreconditioned |r| is not monotone and is no stall signal. With `warm`, step, resid and r hold a partial solve (a block-Jacobi phase) and
 // the iteration continues from them, with `r0In` (that solve's initial |r|) in the convergence test; `budget` bounds
 // the iterations.
+template <int RL>
 __device__ inline int pcgLearned(const Dev& D, GridSync& gs, const SmemMatrix& A, bool warm = false,
                                  double r0In = 0.0, int budget = -1) {
   const uint32_t n = D.P.n;
   uint32_t r0i, r1i;
-  blockRange(n, r0i, r1i);
+  blockRange(n, gs.rank, gs.size, r0i, r1i);
   double rr0;
   {
     double v[1] = {0.0};
@@ -885,7 +889,7 @@ __device__ inline int pcgLearned(const Dev& D, GridSync& gs, const SmemMatrix& A
   double rz;
   {
     double v[1] = {0.0};
-    if (!applyLearned(D, gs, r0i, r1i, &v[0])) return -1;
+    if (!applyLearned<RL>(D, gs, r0i, r1i, &v[0])) return -1;
     double t[1];
     if (!gridReduce<1>(D, gs, v, t)) return -1;
     rz = t[0];
@@ -896,16 +900,16 @@ __device__ inline int pcgLearned(const Dev& D, GridSync& gs, const SmemMatrix& A
   float4* pCur = D.p1;
   int it = 0;
   const int maxCg = budget < 0 ? D.P.maxCg : min(budget, D.P.maxCg);
-  const uint32_t groups = blockDim.x / kRowLanes;
-  const int sub = threadIdx.x & (kRowLanes - 1);
-  const unsigned groupMask = ((1u << kRowLanes) - 1u) << ((threadIdx.x & 31) & ~(kRowLanes - 1));
+  const uint32_t groups = blockDim.x / RL;
+  const int sub = threadIdx.x & (RL - 1);
+  const unsigned groupMask = ((1u << RL) - 1u) << ((threadIdx.x & 31) & ~(RL - 1));
   while (it < maxCg) {
     double vpap[1] = {0.0};
     const float fb = static_cast<float>(beta);
     const bool first = it == 0;
-    for (uint32_t i = r0i + threadIdx.x / kRowLanes; i < r1i; i += groups) {
+    for (uint32_t i = r0i + threadIdx.x / RL; i < r1i; i += groups) {
       const uint32_t rs = __ldg(D.rowStart + i), re = D.particle[i].pinned == 0u ? __ldg(D.rowStart + i + 1) : rs;
-      const float3 acc = rowProduct(A, rs, re, sub, groupMask, [&](uint32_t j) {
+      const float3 acc = rowProduct<RL>(A, rs, re, sub, groupMask, [&](uint32_t j) {
         const float3 zj = ld3(D.z, j);
         return first ? zj : zj + ld3(pPrev, j) * fb;
       });
@@ -940,7 +944,7 @@ __device__ inline int pcgLearned(const Dev& D, GridSync& gs, const SmemMatrix& A
     if (sqrt(rr[0]) <= D.P.cgTolerance * r0) break;
     if (rr[0] > 1e6 * rr0) return -2 - it;
     double vz[1] = {0.0};
-    if (!applyLearned(D, gs, r0i, r1i, &vz[0])) return -1;
+    if (!applyLearned<RL>(D, gs, r0i, r1i, &vz[0])) return -1;
     double rzNew[1];
     if (!gridReduce<1>(D, gs, vz, rzNew)) return -1;
     if (!isfinite(rzNew[0])) return -2 - it;
@@ -957,40 +961,39 @@ __device__ inline int pcgLearned(const Dev& D, GridSync& gs, const SmemMatrix& A
 // first (0: none), then, when the solve has not converged, the learned preconditioner from the current iterate within
 // the remaining iteration budget; a learned phase that stalls is followed by a full block-Jacobi solve. Returns the
 // total iteration count of all phases, or -1 when a barrier gave up.
-template <bool Learned>
+template <bool Learned, int RL>
 __device__ inline int pcgSolve(const Dev& D, GridSync& gs) {
   uint32_t r0i, r1i;
-  blockRange(D.P.n, r0i, r1i);
+  blockRange(D.P.n, gs.rank, gs.size, r0i, r1i);
   const SmemMatrix A = stageMatrix(D, r0i, r1i);
-  if (!Learned) return pcgReferenceOrder(D, gs, A);
+  if (!Learned) return pcgReferenceOrder<RL>(D, gs, A);
   int first = 0;
   double r0 = 0.0;
   const int sw = D.P.learnedSwitch;
   if (sw > 0) {
     bool finished = false;
-    first = pcgReferenceOrder(D, gs, A, sw, &r0, &finished);
+    first = pcgReferenceOrder<RL>(D, gs, A, sw, &r0, &finished);
     if (first < 0 || finished || first >= D.P.maxCg) return first;
   }
-  const int it = pcgLearned(D, gs, A, sw > 0, r0, D.P.maxCg - first);
-  if (blockIdx.x == 0 && threadIdx.x == 0) D.ctl->learnedSolves += 1;
+  const int it = pcgLearned<RL>(D, gs, A, sw > 0, r0, D.P.maxCg - first);
+  if (gs.rank == 0 && threadIdx.x == 0) D.ctl->learnedSolves += 1;
   if (it >= -1) return it < 0 ? it : first + it;
-  if (blockIdx.x == 0 && threadIdx.x == 0) D.ctl->precondFallbacks += 1;
-  const int jac = pcgReferenceOrder(D, gs, A);
+  if (gs.rank == 0 && threadIdx.x == 0) D.ctl->precondFallbacks += 1;
+  const int jac = pcgReferenceOrder<RL>(D, gs, A);
   return jac < 0 ? jac : jac + first + (-2 - it);
 }
 
-template <bool Learned>
-__global__ void __launch_bounds__(kSolveThreads, 1) k_solve(Dev D) {
+// One Newton iteration's solve for the blocks of one group (the whole grid for one solver, or a garment's blocks in
+// a batched launch); gs is initialised.
+template <bool Learned, int RL>
+__device__ inline void solveGroup(const Dev& D, GridSync& gs) {
   Control* ctl = D.ctl;
-  if (ctl->newtonDone) return;
-  GridSync gs;
-  gs.init(ctl, D.P.barrierLimitNs);
   const uint32_t n = D.P.n;
   uint32_t r0i, r1i;
-  blockRange(n, r0i, r1i);
-  const int it = pcgSolve<Learned>(D, gs);
+  blockRange(n, gs.rank, gs.size, r0i, r1i);
+  const int it = pcgSolve<Learned, RL>(D, gs);
   if (it < 0) return;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (gs.rank == 0 && threadIdx.x == 0) {
     if (D.cgLog) D.cgLog[static_cast<unsigned long long>(ctl->newtonIterations) % kCgLogCapacity] = it;
     ctl->cgIterations += it;
     ctl->newtonIterations += 1;
@@ -1008,12 +1011,12 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(Dev D) {
       D.contact[i].force = c.active != 0u ? fmaxf(0.0f, -dot(res, xyz(c.normal))) : 0.0f;
       v[0] += dotd3(ld3(D.grad, i), ld3(D.step, i));
     }
-    v[1] = energyPartial(D, 0.0);
+    v[1] = energyPartial(D, gs, 0.0);
     if (!gridReduce<2>(D, gs, v, se)) return;
   }
   const double slope = se[0], e0 = se[1];
   if (!(slope < 0.0)) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (gs.rank == 0 && threadIdx.x == 0) {
       ctl->newtonDone = 1;
       ctl->lastSlope = slope;
     }
@@ -1022,13 +1025,13 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(Dev D) {
   // Backtracking line search, Armijo c = 1e-4, at most 20 halvings (cpu_solver.cpp:269-274).
   double alpha = 1.0;
   for (int ls = 0; ls < 20; ++ls) {
-    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->energyEvaluations += 1;
-    double v[1] = {energyPartial(D, alpha)};
+    if (gs.rank == 0 && threadIdx.x == 0) ctl->energyEvaluations += 1;
+    double v[1] = {energyPartial(D, gs, alpha)};
     double e[1];
     if (!gridReduce<1>(D, gs, v, e)) return;
     if (e[0] <= e0 + 1e-4 * alpha * slope) break;
     alpha *= 0.5;
-    if (blockIdx.x == 0 && threadIdx.x == 0) ctl->lineSearchHalvings += 1;
+    if (gs.rank == 0 && threadIdx.x == 0) ctl->lineSearchHalvings += 1;
   }
   // Apply the step; max move; the next Newton iteration's friction uses this solve's forces (kernels.h:407-414).
   double mv[1] = {0.0};
@@ -1042,7 +1045,7 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(Dev D) {
   }
   double maxMove[1];
   if (!gridReduce<1, true>(D, gs, mv, maxMove)) return;
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (gs.rank == 0 && threadIdx.x == 0) {
     ctl->lastAlpha = alpha;
     ctl->lastSlope = slope;
     ctl->lastE0 = e0;
@@ -1055,9 +1058,9 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(Dev D) {
 // Finish: x = xStart + u, post-solve push-out below the snap tolerance, pins, damped velocity (kernels.h:419-448,
 // cpu_solver.cpp:285-313); the assembly clock of Assembling garments advances by h.
 
-__global__ void k_finish(Dev D) {
+__device__ inline void finishRows(const Dev& D, uint32_t rank, uint32_t size) {
   const float h = D.P.h;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < D.P.n; i += gridDim.x * blockDim.x) {
+  for (uint32_t i = rank * blockDim.x + threadIdx.x; i < D.P.n; i += size * blockDim.x) {
     const Particle pa = D.particle[i];
     const Fabric fab = D.fabric[pa.fabric];
     const float3 xs = ld3(D.xStart, i);
@@ -1082,13 +1085,8 @@ __global__ void k_finish(Dev D) {
   }
 }
 
-__global__ void k_advance_clock(Dev D) {
-  for (uint32_t g = threadIdx.x; g < D.P.nGarments; g += blockDim.x)
-    if (D.garment[g].phase == 0) D.garment[g].assemblyTime += D.P.hD;
-}
-
 // ---------------------------------------------------------------------------------------------------------------
-// Statistics (sim_model.cpp:222-241) in FP64: per-block partials, the last block to finish combines them.
+// Statistics of one solver or one garment (sim_model.cpp:222-241), reduced on the device in FP64.
 
 struct StatsOut {
   double kineticEnergy, sumV2, maxSeamGap, maxPenetration;
@@ -1096,162 +1094,5 @@ struct StatsOut {
   int nonFinite;
   int pad;
 };
-
-__global__ void k_stats(Dev D, double* part, unsigned int* done, StatsOut* out) {
-  double ke = 0, v2s = 0, gap = 0, pen = 0;
-  unsigned long long moving = 0;
-  int bad = 0;
-  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
-  for (uint32_t i = tid; i < D.P.n; i += stride) {
-    const float3 x = ld3(D.x, i), v = ld3(D.v, i);
-    if (!isfinite(x.x) || !isfinite(x.y) || !isfinite(x.z) || !isfinite(v.x) || !isfinite(v.y) || !isfinite(v.z)) bad = 1;
-    if (D.field.present) {
-      const double phi = fieldSampleD(D.fieldValues, D.field, x.x, x.y, x.z, D.fieldOrigin[0], D.fieldOrigin[1],
-                                      D.fieldOrigin[2], D.fieldCell);
-      pen = fmax(pen, -phi);
-    }
-    const Particle pa = D.particle[i];
-    if (pa.pinned != 0u) continue;
-    const double vv = static_cast<double>(v.x) * v.x + static_cast<double>(v.y) * v.y + static_cast<double>(v.z) * v.z;
-    ke += 0.5 * static_cast<double>(pa.mass) * vv;
-    v2s += vv;
-    ++moving;
-  }
-  for (uint32_t k = tid; k < D.P.nSeam; k += stride) {
-    const Seam s = D.seam[k];
-    const float3 d = ld3(D.x, s.a) - ld3(D.x, s.b);
-    gap = fmax(gap, static_cast<double>(sqrtf(d.x * d.x + d.y * d.y + d.z * d.z)));
-  }
-  double sums[2] = {ke, v2s};
-  __shared__ double r2[2];
-  blockSum<2>(sums, r2);
-  __shared__ double mx[2][32];
-  __shared__ unsigned long long mv[32];
-  __shared__ int bd[32];
-  for (int o = 16; o > 0; o >>= 1) {
-    gap = fmax(gap, __shfl_down_sync(0xffffffffu, gap, o));
-    pen = fmax(pen, __shfl_down_sync(0xffffffffu, pen, o));
-    moving += __shfl_down_sync(0xffffffffu, moving, o);
-    bad |= __shfl_down_sync(0xffffffffu, bad, o);
-  }
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-  if (lane == 0) {
-    mx[0][w] = gap;
-    mx[1][w] = pen;
-    mv[w] = moving;
-    bd[w] = bad;
-  }
-  __syncthreads();
-  __shared__ bool last;
-  if (threadIdx.x == 0) {
-    double g = 0, p = 0;
-    unsigned long long m = 0;
-    int b = 0;
-    for (int k = 0; k < nw; ++k) {
-      g = fmax(g, mx[0][k]);
-      p = fmax(p, mx[1][k]);
-      m += mv[k];
-      b |= bd[k];
-    }
-    double* row = part + blockIdx.x * 8;
-    row[0] = r2[0];
-    row[1] = r2[1];
-    row[2] = g;
-    row[3] = p;
-    row[4] = static_cast<double>(m);
-    row[5] = b;
-    __threadfence();
-    last = atomicAdd(done, 1u) == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (last && threadIdx.x == 0) {
-    __threadfence();
-    StatsOut s{};
-    for (unsigned int b = 0; b < gridDim.x; ++b) {
-      const double* row = part + b * 8;
-      s.kineticEnergy += __ldcg(row + 0);
-      s.sumV2 += __ldcg(row + 1);
-      s.maxSeamGap = fmax(s.maxSeamGap, __ldcg(row + 2));
-      s.maxPenetration = fmax(s.maxPenetration, __ldcg(row + 3));
-      s.moving += static_cast<unsigned long long>(__ldcg(row + 4));
-      s.nonFinite |= __ldcg(row + 5) != 0.0;
-    }
-    *out = s;
-    *done = 0;
-  }
-}
-
-// PCG on a given system (test and measurement entry point): block-Jacobi inverse of each diagonal block, then the
-// same persistent PCG as k_solve.
-__global__ void k_pcg_precondition(Dev D, const uint32_t* __restrict__ diag) {
-  const uint32_t SP = D.P.slotsPadded;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < D.P.n; i += gridDim.x * blockDim.x) {
-    M3 A;
-#pragma unroll
-    for (int k = 0; k < 9; ++k) A.m[k] = D.blocks[k * SP + diag[i]];
-    M3 inv;
-    if (D.particle[i].pinned != 0u) {
-      zero(inv);
-    } else {
-      bool ok = false;
-      inv = invertSpd(A, ok);
-    }
-    D.precond[3 * i + 0] = make_float4(inv.m[0], inv.m[1], inv.m[2], 0.0f);
-    D.precond[3 * i + 1] = make_float4(inv.m[3], inv.m[4], inv.m[5], 0.0f);
-    D.precond[3 * i + 2] = make_float4(inv.m[6], inv.m[7], inv.m[8], 0.0f);
-  }
-}
-
-__global__ void __launch_bounds__(kSolveThreads, 1) k_pcg_only(Dev D) {
-  GridSync gs;
-  gs.init(D.ctl, D.P.barrierLimitNs);
-  const int it = pcgSolve<false>(D, gs);
-  if (it >= 0 && blockIdx.x == 0 && threadIdx.x == 0) D.ctl->lastCg = it;
-}
-
-// ---------------------------------------------------------------------------------------------------------------
-// Standalone block-CSR SpMV (kRowLanes lanes per row), y = A x over unpinned rows and columns.
-
-__global__ void k_spmv(uint32_t n, const uint32_t* __restrict__ rowStart, const uint32_t* __restrict__ colIndex,
-                       const float* __restrict__ blocks, uint32_t SP, const uint8_t* __restrict__ pinned,
-                       const float4* __restrict__ x, float4* __restrict__ y) {
-  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
-  const uint32_t gid = tid / kRowLanes, groups = stride / kRowLanes;
-  const int sub = threadIdx.x & (kRowLanes - 1);
-  const unsigned groupMask = ((1u << kRowLanes) - 1u) << ((threadIdx.x & 31) & ~(kRowLanes - 1));
-  const uint32_t rounds = (n + groups - 1) / groups;
-  for (uint32_t r = 0; r < rounds; ++r) {
-    const uint32_t i = gid + r * groups;
-    float3 acc = mk(0, 0, 0);
-    if (i < n && !pinned[i]) {
-      const uint32_t rs = rowStart[i], re = rowStart[i + 1];
-      for (uint32_t s = rs + sub; s < re; s += kRowLanes) {
-        const uint32_t j = colIndex[s];
-        if (pinned[j]) continue;
-        const float3 pj = xyz(x[j]);
-        acc.x += blocks[0 * SP + s] * pj.x + blocks[1 * SP + s] * pj.y + blocks[2 * SP + s] * pj.z;
-        acc.y += blocks[3 * SP + s] * pj.x + blocks[4 * SP + s] * pj.y + blocks[5 * SP + s] * pj.z;
-        acc.z += blocks[6 * SP + s] * pj.x + blocks[7 * SP + s] * pj.y + blocks[8 * SP + s] * pj.z;
-      }
-    }
-#pragma unroll
-    for (int o = kRowLanes / 2; o > 0; o >>= 1) {
-      acc.x += __shfl_xor_sync(groupMask, acc.x, o);
-      acc.y += __shfl_xor_sync(groupMask, acc.y, o);
-      acc.z += __shfl_xor_sync(groupMask, acc.z, o);
-    }
-    if (sub == 0 && i < n) y[i] = f4(acc);
-  }
-}
-
-// A barrier that waits for one more block than the grid has: it can only end by its time limit. Used by the test of
-// the bounded wait; returns the status the blocks read back in *out (1: gave up).
-__global__ void k_barrier_probe(Control* ctl, unsigned long long limitNs, int* out) {
-  GridSync gs;
-  gs.init(ctl, limitNs);
-  gs.target += 1;  // one arrival that never comes
-  const bool released = gs.sync();
-  if (threadIdx.x == 0 && blockIdx.x == 0) *out = released ? 0 : ctl->error;
-}
 
 }  // namespace dcu

@@ -18,7 +18,10 @@
 
 #include "../../include/drape_cuda.h"
 #include "../../include/drape_precond.h"
+#include "device_buffer.hpp"
+#include "device_model.hpp"
 #include "kernels.cuh"
+#include "solver_kernels.cuh"
 #include "learned.hpp"
 #include "model.hpp"
 
@@ -26,68 +29,11 @@ using drape_b200::Model;
 
 namespace {
 
-void check(cudaError_t e, const char* what) {
-  if (e != cudaSuccess) throw std::runtime_error(std::string("cuda: ") + what + ": " + cudaGetErrorString(e));
-}
+using dbuf::check;
 #define CK(x) check((x), #x)
-
-// Host -> device byte counter of the solver whose public call is running on this thread (see CountTransfers).
-thread_local uint64_t* g_h2d = nullptr;
-
-struct CountTransfers {
-  uint64_t* prev;
-  explicit CountTransfers(uint64_t* c) : prev(g_h2d) { g_h2d = c; }
-  ~CountTransfers() { g_h2d = prev; }
-};
-
-template <class T>
-struct DBuf {
-  T* p = nullptr;
-  size_t n = 0;
-  DBuf() = default;
-  DBuf(const DBuf&) = delete;
-  DBuf& operator=(const DBuf&) = delete;
-  ~DBuf() { release(); }
-  void release() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
-  }
-  // The zeroing runs on the legacy default stream, which is not ordered with the solver's non-blocking stream: wait
-  // for it here, or it could land after the uploads and kernels that follow.
-  void alloc(size_t count) {
-    release();
-    n = count;
-    CK(cudaMalloc(&p, sizeof(T) * std::max<size_t>(count, 1)));
-    CK(cudaMemset(p, 0, sizeof(T) * std::max<size_t>(count, 1)));
-    CK(cudaStreamSynchronize(nullptr));
-  }
-  void upload(const T* src, size_t count, cudaStream_t s) {
-    if (count > n || !p) alloc(count);
-    if (count) CK(cudaMemcpyAsync(p, src, sizeof(T) * count, cudaMemcpyHostToDevice, s));
-    if (g_h2d) *g_h2d += sizeof(T) * count;
-  }
-  void upload(const std::vector<T>& v, cudaStream_t s) { upload(v.data(), v.size(), s); }
-};
-
-template <class T>
-struct HostPinned {
-  T* p = nullptr;
-  HostPinned() = default;
-  HostPinned(const HostPinned&) = delete;
-  HostPinned& operator=(const HostPinned&) = delete;
-  ~HostPinned() {
-    if (p) cudaFreeHost(p);
-  }
-  void alloc() {
-    if (!p) {
-      CK(cudaMallocHost(&p, sizeof(T)));
-      std::memset(static_cast<void*>(p), 0, sizeof(T));
-    }
-  }
-};
-
-float4 f4(drape_b200::Vec3f v) { return make_float4(v.x, v.y, v.z, 0.0f); }
+using dbuf::CountTransfers;
+using dbuf::DBuf;
+using dbuf::HostPinned;
 
 thread_local std::string g_lastError;
 
@@ -251,46 +197,11 @@ struct drape_solver {
 
   void use() const { CK(cudaSetDevice(device)); }
 
-  std::vector<dcu::Particle> particleData() const {
-    std::vector<dcu::Particle> out(m.x.size());
-    for (size_t i = 0; i < out.size(); ++i)
-      out[i] = {static_cast<float>(m.mass[i]), m.pFabric[i], m.pGarment[i], m.pinned[i] ? 1u : 0u};
-    return out;
-  }
-  std::vector<dcu::Fabric> fabricData() const {
-    std::vector<dcu::Fabric> out;
-    for (const auto& f : m.fabrics) {
-      dcu::Fabric d{};
-      d.k[0] = static_cast<float>(f.stretch_warp);
-      d.k[1] = static_cast<float>(f.stretch_weft);
-      d.k[2] = static_cast<float>(f.stretch_bias);
-      d.limit[0] = static_cast<float>(f.strain_limit_warp);
-      d.limit[1] = static_cast<float>(f.strain_limit_weft);
-      d.thickness = static_cast<float>(f.thickness);
-      d.friction = static_cast<float>(f.friction);
-      d.damping = static_cast<float>(f.damping);
-      out.push_back(d);
-    }
-    if (out.empty()) out.push_back(dcu::Fabric{});
-    return out;
-  }
-  std::vector<dcu::Garment> garmentData() const {
-    std::vector<dcu::Garment> out;
-    for (const auto& g : m.garments) out.push_back({g.phase, 0, g.assemblyTime});
-    if (out.empty()) out.push_back(dcu::Garment{});
-    return out;
-  }
-  std::vector<dcu::Hinge> hingeData() const {
-    std::vector<dcu::Hinge> out;
-    for (const auto& h : m.hinges)
-      out.push_back({{h.v[0], h.v[1], h.v[2], h.v[3]}, static_cast<float>(h.K), static_cast<float>(h.restAngle), {0, 0}});
-    return out;
-  }
-  std::vector<dcu::Seam> seamData() const {
-    std::vector<dcu::Seam> out;
-    for (const auto& s : m.seams) out.push_back({s.a, s.b, s.garment, s.startGap});
-    return out;
-  }
+  std::vector<dcu::Particle> particleData() const { return dmodel::particles(m); }
+  std::vector<dcu::Fabric> fabricData() const { return dmodel::fabrics(m); }
+  std::vector<dcu::Garment> garmentData() const { return dmodel::garments(m); }
+  std::vector<dcu::Hinge> hingeData() const { return dmodel::hinges(m); }
+  std::vector<dcu::Seam> seamData() const { return dmodel::seams(m); }
 
   void build(const drape_scene_desc& scene) {
     use();
@@ -304,28 +215,11 @@ struct drape_solver {
     particle.upload(particleData(), s);
     fabric.upload(fabricData(), s);
     garment.upload(garmentData(), s);
-    {
-      std::vector<dcu::Stretch> st;
-      for (const auto& t : m.stretch) {
-        dcu::Stretch d{};
-        for (int k = 0; k < 3; ++k) d.v[k] = t.v[k];
-        d.fabric = t.fabric;
-        d.d = make_float4(static_cast<float>(t.dmInv[0][0]), static_cast<float>(t.dmInv[1][0]),
-                          static_cast<float>(t.dmInv[0][1]), static_cast<float>(t.dmInv[1][1]));
-        d.area = static_cast<float>(t.area);
-        st.push_back(d);
-      }
-      stretch.upload(st, s);
-    }
+    stretch.upload(dmodel::stretches(m), s);
     hinge.upload(hingeData(), s);
     seam.upload(seamData(), s);
     rowStart.upload(m.rowStart, s);
-    {
-      std::vector<uint32_t> cols(m.colIndex);
-      for (auto& c : cols)
-        if (m.pinned[c]) c |= dcu::kPinnedBit;
-      colIndex.upload(cols, s);
-    }
+    colIndex.upload(dmodel::columns(m), s);
     diagSlot.upload(m.diagSlot, s);
     incStart.upload(m.incStart, s);
     incEntry.upload(m.incEntry, s);
@@ -341,14 +235,8 @@ struct drape_solver {
     precond.alloc(static_cast<size_t>(n) * 3);
     contact.alloc(n);
     {
-      std::vector<float4> xs(n), vs(n), fe(n), pp(n);
-      for (uint32_t i = 0; i < n; ++i) {
-        xs[i] = f4(m.x[i]);
-        vs[i] = f4(m.v[i]);
-        fe[i] = make_float4(static_cast<float>(m.fExt[i].x), static_cast<float>(m.fExt[i].y),
-                            static_cast<float>(m.fExt[i].z), 0.0f);
-      }
-      for (const auto& [i, pos] : m.pins) pp[i] = f4(pos);
+      std::vector<float4> xs, vs, fe, pp;
+      dmodel::state(m, xs, vs, fe, pp);
       x.upload(xs, s);
       v.upload(vs, s);
       fExt.upload(fe, s);
@@ -358,40 +246,9 @@ struct drape_solver {
     CK(cudaMemcpyAsync(ctl.p, &c0, sizeof(c0), cudaMemcpyHostToDevice, s));
     // Launch view.
     dcu::Dev d{};
-    auto& P = d.P;
-    P.gravity[0] = static_cast<float>(m.settings.gravity[0]);
-    P.gravity[1] = static_cast<float>(m.settings.gravity[1]);
-    P.gravity[2] = static_cast<float>(m.settings.gravity[2]);
-    P.limitScale = static_cast<float>(m.settings.strain_limit_stiffness_scale);
-    P.seamStiffness = static_cast<float>(m.settings.seam_stiffness);
-    P.closingSpeed = static_cast<float>(m.settings.assembly_closing_speed);
-    P.frictionSlip = static_cast<float>(m.settings.friction_slip_speed);
-    P.collisionOffset = static_cast<float>(m.settings.collision_offset);
-    P.dampingScale = static_cast<float>(m.settings.damping_scale);
-    P.assemblyExtraDamping = static_cast<float>(m.settings.assembly_extra_damping);
-    P.contactReach = static_cast<float>(drape_b200::kContactReach);
-    P.contactSnap = static_cast<float>(drape_b200::kContactSnap);
-    P.cgTolerance = m.settings.cg_tolerance;
-    P.maxCg = m.settings.max_cg_iterations;
-    P.n = n;
-    P.nStretch = static_cast<uint32_t>(m.stretch.size());
-    P.nHinge = static_cast<uint32_t>(m.hinges.size());
-    P.nSeam = static_cast<uint32_t>(m.seams.size());
-    P.nBlocks = B;
-    P.nGarments = static_cast<uint32_t>(m.garments.size());
-    P.slotsPadded = SP;
-    P.barrierLimitNs = barrierLimitNs;
-    P.smemSlots = std::min(solveSmemCap, maxBlockSlots(m.rowStart.data(), n, solveGrid));
-    solveSmemBytes = static_cast<size_t>(P.smemSlots) * dcu::kSmemSlotBytes;
-    d.field.present = !m.fieldValues.empty() ? 1 : 0;
-    d.field.ox = static_cast<float>(m.field.origin[0]);
-    d.field.oy = static_cast<float>(m.field.origin[1]);
-    d.field.oz = static_cast<float>(m.field.origin[2]);
-    d.field.cell = static_cast<float>(m.field.cell_size);
-    d.field.band = static_cast<float>(m.hasBody ? m.field.band : 0.02);
-    for (int a = 0; a < 3; ++a) d.field.dims[a] = m.field.dims[a];
-    for (int a = 0; a < 3; ++a) d.fieldOrigin[a] = m.field.origin[a];
-    d.fieldCell = m.field.cell_size;
+    dmodel::params(m, SP, barrierLimitNs, d);
+    d.P.smemSlots = std::min(solveSmemCap, maxBlockSlots(m.rowStart.data(), n, solveGrid));
+    solveSmemBytes = static_cast<size_t>(d.P.smemSlots) * dcu::kSmemSlotBytes;
     d.fieldValues = fieldValues.p;
     d.particle = particle.p;
     d.fabric = fabric.p;
@@ -439,9 +296,7 @@ struct drape_solver {
   // The network's workspace on this solver's CSR; the learned factor and transposed-slot map go into the device view.
   void bindNet() {
     const uint32_t n = static_cast<uint32_t>(m.pinned.size()), B = static_cast<uint32_t>(m.colIndex.size());
-    std::vector<uint32_t> cols(m.colIndex);
-    for (auto& c : cols)
-      if (m.pinned[c]) c |= dcu::kPinnedBit;
+    const std::vector<uint32_t> cols = dmodel::columns(m);
     netGraph = net->bind(n, B, dev.P.slotsPadded, m.rowStart.data(), cols.data(), rowStart.p, colIndex.p, blocks.p,
                          reinterpret_cast<const uint8_t*>(particle.p) + offsetof(dcu::Particle, pinned),
                          sizeof(dcu::Particle),
@@ -506,8 +361,8 @@ struct drape_solver {
       CK(cudaStreamSynchronize(stream));
     }
     for (size_t i = 0; i < n; ++i) {
-      xs[i] = f4(m.x[i]);
-      vs[i] = f4(m.v[i]);
+      xs[i] = dmodel::f4(m.x[i]);
+      vs[i] = dmodel::f4(m.v[i]);
       cs[i].force = static_cast<float>(m.contactForce[i]);
     }
     x.upload(xs, stream);

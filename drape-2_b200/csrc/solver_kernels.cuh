@@ -1,0 +1,198 @@
+// The single solver's kernels (one solver per launch grid) over the device functions of kernels.cuh; the batch
+// (batch.cu) launches its own wrappers of the same functions.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace dcu {
+
+__global__ void k_begin(Dev D) { beginRows(D, blockIdx.x, gridDim.x); }
+
+// Contact candidates for given positions (test entry point; same code as k_begin).
+__global__ void k_contact_candidates(Dev D, const float4* xs, Contact* out) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < D.P.n; i += gridDim.x * blockDim.x) {
+    Contact c{};
+    contactSetupOne(D, i, xyz(xs[i]), c);
+    out[i] = c;
+  }
+}
+
+__global__ void k_activate(Dev D) { activateRows(D, blockIdx.x, gridDim.x); }
+
+__global__ void __launch_bounds__(kAssembleWarps * kWarp) k_assemble(Dev D) {
+  assembleRows(D, blockIdx.x, gridDim.x);
+}
+
+// One Newton iteration's persistent solve; the whole grid is one group.
+template <bool Learned>
+__global__ void __launch_bounds__(kSolveThreads, 1) k_solve(Dev D) {
+  if (D.ctl->newtonDone) return;
+  GridSync gs;
+  gs.init(D.ctl, D.P.barrierLimitNs);
+  solveGroup<Learned, kRowLanes>(D, gs);
+}
+
+__global__ void k_finish(Dev D) { finishRows(D, blockIdx.x, gridDim.x); }
+
+__global__ void k_advance_clock(Dev D) {
+  for (uint32_t g = threadIdx.x; g < D.P.nGarments; g += blockDim.x)
+    if (D.garment[g].phase == 0) D.garment[g].assemblyTime += D.P.hD;
+}
+
+// Statistics: per-block partials, the last block to finish combines them.
+__global__ void k_stats(Dev D, double* part, unsigned int* done, StatsOut* out) {
+  double ke = 0, v2s = 0, gap = 0, pen = 0;
+  unsigned long long moving = 0;
+  int bad = 0;
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  for (uint32_t i = tid; i < D.P.n; i += stride) {
+    const float3 x = ld3(D.x, i), v = ld3(D.v, i);
+    if (!isfinite(x.x) || !isfinite(x.y) || !isfinite(x.z) || !isfinite(v.x) || !isfinite(v.y) || !isfinite(v.z)) bad = 1;
+    if (D.field.present) {
+      const double phi = fieldSampleD(D.fieldValues, D.field, x.x, x.y, x.z, D.fieldOrigin[0], D.fieldOrigin[1],
+                                      D.fieldOrigin[2], D.fieldCell);
+      pen = fmax(pen, -phi);
+    }
+    const Particle pa = D.particle[i];
+    if (pa.pinned != 0u) continue;
+    const double vv = static_cast<double>(v.x) * v.x + static_cast<double>(v.y) * v.y + static_cast<double>(v.z) * v.z;
+    ke += 0.5 * static_cast<double>(pa.mass) * vv;
+    v2s += vv;
+    ++moving;
+  }
+  for (uint32_t k = tid; k < D.P.nSeam; k += stride) {
+    const Seam s = D.seam[k];
+    const float3 d = ld3(D.x, s.a) - ld3(D.x, s.b);
+    gap = fmax(gap, static_cast<double>(sqrtf(d.x * d.x + d.y * d.y + d.z * d.z)));
+  }
+  double sums[2] = {ke, v2s};
+  __shared__ double r2[2];
+  blockSum<2>(sums, r2);
+  __shared__ double mx[2][32];
+  __shared__ unsigned long long mv[32];
+  __shared__ int bd[32];
+  for (int o = 16; o > 0; o >>= 1) {
+    gap = fmax(gap, __shfl_down_sync(0xffffffffu, gap, o));
+    pen = fmax(pen, __shfl_down_sync(0xffffffffu, pen, o));
+    moving += __shfl_down_sync(0xffffffffu, moving, o);
+    bad |= __shfl_down_sync(0xffffffffu, bad, o);
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  if (lane == 0) {
+    mx[0][w] = gap;
+    mx[1][w] = pen;
+    mv[w] = moving;
+    bd[w] = bad;
+  }
+  __syncthreads();
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    double g = 0, p = 0;
+    unsigned long long m = 0;
+    int b = 0;
+    for (int k = 0; k < nw; ++k) {
+      g = fmax(g, mx[0][k]);
+      p = fmax(p, mx[1][k]);
+      m += mv[k];
+      b |= bd[k];
+    }
+    double* row = part + blockIdx.x * 8;
+    row[0] = r2[0];
+    row[1] = r2[1];
+    row[2] = g;
+    row[3] = p;
+    row[4] = static_cast<double>(m);
+    row[5] = b;
+    __threadfence();
+    last = atomicAdd(done, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    StatsOut s{};
+    for (unsigned int b = 0; b < gridDim.x; ++b) {
+      const double* row = part + b * 8;
+      s.kineticEnergy += __ldcg(row + 0);
+      s.sumV2 += __ldcg(row + 1);
+      s.maxSeamGap = fmax(s.maxSeamGap, __ldcg(row + 2));
+      s.maxPenetration = fmax(s.maxPenetration, __ldcg(row + 3));
+      s.moving += static_cast<unsigned long long>(__ldcg(row + 4));
+      s.nonFinite |= __ldcg(row + 5) != 0.0;
+    }
+    *out = s;
+    *done = 0;
+  }
+}
+
+// PCG on a given system (test and measurement entry point): block-Jacobi inverse of each diagonal block, then the
+// same persistent PCG as k_solve.
+__global__ void k_pcg_precondition(Dev D, const uint32_t* __restrict__ diag) {
+  const uint32_t SP = D.P.slotsPadded;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < D.P.n; i += gridDim.x * blockDim.x) {
+    M3 A;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) A.m[k] = D.blocks[k * SP + diag[i]];
+    M3 inv;
+    if (D.particle[i].pinned != 0u) {
+      zero(inv);
+    } else {
+      bool ok = false;
+      inv = invertSpd(A, ok);
+    }
+    D.precond[3 * i + 0] = make_float4(inv.m[0], inv.m[1], inv.m[2], 0.0f);
+    D.precond[3 * i + 1] = make_float4(inv.m[3], inv.m[4], inv.m[5], 0.0f);
+    D.precond[3 * i + 2] = make_float4(inv.m[6], inv.m[7], inv.m[8], 0.0f);
+  }
+}
+
+__global__ void __launch_bounds__(kSolveThreads, 1) k_pcg_only(Dev D) {
+  GridSync gs;
+  gs.init(D.ctl, D.P.barrierLimitNs);
+  const int it = pcgSolve<false, kRowLanes>(D, gs);
+  if (it >= 0 && blockIdx.x == 0 && threadIdx.x == 0) D.ctl->lastCg = it;
+}
+
+// Standalone block-CSR SpMV (kRowLanes lanes per row), y = A x over unpinned rows and columns.
+__global__ void k_spmv(uint32_t n, const uint32_t* __restrict__ rowStart, const uint32_t* __restrict__ colIndex,
+                       const float* __restrict__ blocks, uint32_t SP, const uint8_t* __restrict__ pinned,
+                       const float4* __restrict__ x, float4* __restrict__ y) {
+  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  const uint32_t gid = tid / kRowLanes, groups = stride / kRowLanes;
+  const int sub = threadIdx.x & (kRowLanes - 1);
+  const unsigned groupMask = ((1u << kRowLanes) - 1u) << ((threadIdx.x & 31) & ~(kRowLanes - 1));
+  const uint32_t rounds = (n + groups - 1) / groups;
+  for (uint32_t r = 0; r < rounds; ++r) {
+    const uint32_t i = gid + r * groups;
+    float3 acc = mk(0, 0, 0);
+    if (i < n && !pinned[i]) {
+      const uint32_t rs = rowStart[i], re = rowStart[i + 1];
+      for (uint32_t s = rs + sub; s < re; s += kRowLanes) {
+        const uint32_t j = colIndex[s];
+        if (pinned[j]) continue;
+        const float3 pj = xyz(x[j]);
+        acc.x += blocks[0 * SP + s] * pj.x + blocks[1 * SP + s] * pj.y + blocks[2 * SP + s] * pj.z;
+        acc.y += blocks[3 * SP + s] * pj.x + blocks[4 * SP + s] * pj.y + blocks[5 * SP + s] * pj.z;
+        acc.z += blocks[6 * SP + s] * pj.x + blocks[7 * SP + s] * pj.y + blocks[8 * SP + s] * pj.z;
+      }
+    }
+#pragma unroll
+    for (int o = kRowLanes / 2; o > 0; o >>= 1) {
+      acc.x += __shfl_xor_sync(groupMask, acc.x, o);
+      acc.y += __shfl_xor_sync(groupMask, acc.y, o);
+      acc.z += __shfl_xor_sync(groupMask, acc.z, o);
+    }
+    if (sub == 0 && i < n) y[i] = f4(acc);
+  }
+}
+
+// A barrier that waits for one more block than the grid has: it can only end by its time limit. Used by the test of
+// the bounded wait; returns the status the blocks read back in *out (1: gave up).
+__global__ void k_barrier_probe(Control* ctl, unsigned long long limitNs, int* out) {
+  GridSync gs;
+  gs.init(ctl, limitNs);
+  gs.target += 1;  // one arrival that never comes
+  const bool released = gs.sync();
+  if (threadIdx.x == 0 && blockIdx.x == 0) *out = released ? 0 : ctl->error;
+}
+
+}  // namespace dcu

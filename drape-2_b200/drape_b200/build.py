@@ -11,15 +11,16 @@ CSRC = os.path.join(ROOT, "csrc")
 LIB_DIR = os.path.join(ROOT, "lib")
 LIB = os.path.join(LIB_DIR, "libdrape_cuda.so")
 
-SOURCES = ["solver.cu", "learned.cu", "model.cpp"]
-HEADERS = ["kernels.cuh", "device_math.cuh", "model.hpp", "learned.hpp", "umma.cuh"]
+SOURCES = ["solver.cu", "batch.cu", "learned.cu", "model.cpp"]
+HEADERS = ["kernels.cuh", "device_math.cuh", "model.hpp", "learned.hpp", "umma.cuh", "device_model.hpp",
+           "device_buffer.hpp", "solver_kernels.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 
 def _inputs():
     files = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
-    files += [os.path.join(REPO, "include", h) for h in ("drape_cuda.h", "drape_scene.h", "drape_precond.h")]
+    files += [os.path.join(REPO, "include", h) for h in ("drape_cuda.h", "drape_scene.h", "drape_precond.h", "drape_batch.h")]
     return files
 
 

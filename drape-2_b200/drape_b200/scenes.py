@@ -263,7 +263,7 @@ def tube_60k(**kw) -> Scene:
     return seamed_tube(154, 195, field_n=256, field_cell=0.003, **kw)
 
 
-def tube_variant(seed: int, n_particles: int, field_n: int = 128) -> Scene:
+def tube_variant(seed: int, n_particles: int, field_n: int = 128, settings: Optional[Settings] = None) -> Scene:
     """A seeded tube variant: panel sizes +-20 %, torso and arm radii +-15 %, about n_particles particles."""
     rng = np.random.default_rng(seed)
     w = 0.55 * rng.uniform(0.8, 1.2)
@@ -276,7 +276,21 @@ def tube_variant(seed: int, n_particles: int, field_n: int = 128) -> Scene:
     radius = tr + 0.05
     cell = 0.762 / (field_n - 1)
     return seamed_tube(nx, ny, width=w, height=h, radius=radius, field_n=field_n, field_cell=cell, torso_radius=tr,
-                       arm_radius=ar, gid=f"tube{seed}")
+                       arm_radius=ar, settings=settings, gid=f"tube{seed}")
+
+
+def batch_tubes(count: int = 64, seed: int = 5, n_min: int = 2000, n_max: int = 40000):
+    """Uneven batch of seeded tube variants: particle counts log-uniform in [n_min, n_max], each tube on its own
+    seeded capsule-union body whose field resolution grows with the garment, from 32^3 samples at n_min to 128^3 at
+    n_max (log-linear). Returns the scenes in order."""
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(math.log(n_min), math.log(n_max), count))
+    scenes = []
+    for k, n in enumerate(ns):
+        t = math.log(n / n_min) / math.log(n_max / n_min) if n_max > n_min else 0.0
+        field_n = int(round(32 * 4 ** t))
+        scenes.append(tube_variant(seed * 1000 + k, int(round(n)), field_n=field_n))
+    return scenes
 
 
 # ---------------------------------------------------------------------------------------------------------------

@@ -12,10 +12,10 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_functions():
     names = set()
-    for h in ("drape_cuda.h", "drape_scene.h"):
+    for h in sorted(os.listdir(os.path.join(ROOT, "include"))):
         src = open(os.path.join(ROOT, "include", h)).read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-        names.update(re.findall(r"\b((?:drape_cuda|drape_model)_[a-z0-9_]+)\s*\(", src))
+        names.update(re.findall(r"\b((?:drape_cuda|drape_model|drape_precond|drape_batch)_[a-z0-9_]+)\s*\(", src))
     return sorted(names)
 
 
@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol(cuda_mod):
     for name in declared_functions():
         assert hasattr(lib, name), name
     out = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True, text=True, check=True).stdout
-    exported = set(re.findall(r" T ((?:drape_cuda|drape_model)_\w+)", out))
+    exported = set(re.findall(r" T ((?:drape_cuda|drape_model|drape_precond|drape_batch)_\w+)", out))
     assert set(declared_functions()) <= exported
 
 
@@ -53,6 +53,10 @@ def test_no_device_is_a_loud_error(cuda_mod):
 
 
 def test_null_handle_errors(cuda_mod):
+    from drape_b200 import batch
+    B = batch._lib()
+    assert B.drape_batch_step(None, 1 / 60, 1, 2) == cuda_mod.INVALID
+    assert B.drape_batch_build(None) == cuda_mod.INVALID
     L = cuda_mod.load()
     assert L.drape_cuda_step(None, 1 / 60, 1, 2) == cuda_mod.INVALID
     assert L.drape_cuda_build(None, None) == cuda_mod.INVALID
