@@ -320,13 +320,17 @@ struct Variant {
   SolveKernel jacobi, learned;
 };
 
+// Product scheme (0: slot-parallel, else lanes per row) x block size.
 const Variant kVariants[] = {
+    {0, 256, bcu::k_solve_batch<false, 0, 256>, bcu::k_solve_batch<true, 0, 256>},
     {2, 256, bcu::k_solve_batch<false, 2, 256>, bcu::k_solve_batch<true, 2, 256>},
     {4, 256, bcu::k_solve_batch<false, 4, 256>, bcu::k_solve_batch<true, 4, 256>},
     {8, 256, bcu::k_solve_batch<false, 8, 256>, bcu::k_solve_batch<true, 8, 256>},
+    {0, 512, bcu::k_solve_batch<false, 0, 512>, bcu::k_solve_batch<true, 0, 512>},
     {2, 512, bcu::k_solve_batch<false, 2, 512>, bcu::k_solve_batch<true, 2, 512>},
     {4, 512, bcu::k_solve_batch<false, 4, 512>, bcu::k_solve_batch<true, 4, 512>},
     {8, 512, bcu::k_solve_batch<false, 8, 512>, bcu::k_solve_batch<true, 8, 512>},
+    {0, 1024, bcu::k_solve_batch<false, 0, 1024>, bcu::k_solve_batch<true, 0, 1024>},
     {2, 1024, bcu::k_solve_batch<false, 2, 1024>, bcu::k_solve_batch<true, 2, 1024>},
     {4, 1024, bcu::k_solve_batch<false, 4, 1024>, bcu::k_solve_batch<true, 4, 1024>},
     {8, 1024, bcu::k_solve_batch<false, 8, 1024>, bcu::k_solve_batch<true, 8, 1024>},
@@ -372,7 +376,9 @@ std::vector<uint32_t> apportion(const std::vector<double>& weight, uint32_t tota
     used += out[g];
     rem.push_back({share - std::floor(share), g});
   }
-  std::sort(rem.begin(), rem.end(), [](const auto& a, const auto& b) { return a.first > b.first || (a.first == b.first && a.second < b.second); });
+  std::sort(rem.begin(), rem.end(), [](const auto& a, const auto& b) {
+    return a.first > b.first || (a.first == b.first && a.second < b.second);
+  });
   for (size_t k = 0; used < total && k < rem.size(); ++k, ++used) ++out[rem[k].second];
   return out;
 }
@@ -433,7 +439,7 @@ struct drape_batch {
   DBuf<uint32_t> gRowStart, gColIndex;
   bool learnedOn = false;
 
-  int variant = 7;          // kVariants index: 4 lanes, 1024 threads
+  int variant = 0;          // kVariants index: slot-parallel products, 256 threads
   int solveBlocks = 0;      // blocks of the solve launch for the variant
   uint32_t capSlots = 0;    // shared-memory slot capacity of one solve block for the variant
   size_t solveSmem = 0;
@@ -716,10 +722,10 @@ struct drape_batch {
     uint32_t* hs = solveStartHost();
     for (uint32_t g = 0; g <= G; ++g) hs[g] = start[g];
     bcu::SegRun* rr = runs();
-    for (uint32_t g = 0; g < G; ++g)
-      rr[g].smemSlots = count[g] ? std::min(capSlots, maxRangeSlots(models[g].rowStart,
-                                                                    static_cast<uint32_t>(models[g].x.size()), count[g]))
-                                 : 0;
+    for (uint32_t g = 0; g < G; ++g) {
+      const uint32_t ng = static_cast<uint32_t>(models[g].x.size());
+      rr[g].smemSlots = count[g] ? std::min(capSlots, maxRangeSlots(models[g].rowStart, ng, count[g])) : 0;
+    }
   }
 
   // ---- learned preconditioner ----
@@ -1175,9 +1181,10 @@ struct drape_batch {
     save();
     const bool wasProfiling = profiling;
     const drape_batch_profile keep = prof;
-    int best = variant;
+    int best = variant, timed = 0;
     double bestMs = INFINITY;
     for (int vi = 0; vi < kVariantCount; ++vi) {
+      ++timed;
       setVariant(vi);
       restore();
       profiling = true;
@@ -1205,7 +1212,7 @@ struct drape_batch {
     saved = wasSaved;
     resetCounters();
     drape_batch_tuning t = tuning();
-    t.variants_timed = kVariantCount;
+    t.variants_timed = timed;
     t.ms_per_newton = bestMs;
     return t;
   }
@@ -1214,7 +1221,7 @@ struct drape_batch {
     int found = -1;
     for (int vi = 0; vi < kVariantCount; ++vi)
       if (kVariants[vi].rowLanes == t.row_lanes && kVariants[vi].threads == t.block_threads) found = vi;
-    if (found < 0) throw std::invalid_argument("row_lanes must be 2, 4 or 8 and block_threads 256, 512 or 1024");
+    if (found < 0) throw std::invalid_argument("row_lanes must be 0, 2, 4 or 8 and block_threads 256, 512 or 1024");
     use();
     if (built) setVariant(found); else variant = found;
     dropGraph();

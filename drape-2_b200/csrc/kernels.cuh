@@ -695,11 +695,110 @@ __device__ __forceinline__ float3 rowProduct(const SmemMatrix& A, uint32_t rs, u
   return acc;
 }
 
+// The PCG's product Ap for the direction p = z + beta * pPrev (p = z on the first iteration) over this block's rows
+// [r0, r1). The row's product is handed to `out(i, p_i, Ap_i)` (pinned rows: Ap_i = 0; pinned columns add nothing).
+// Two schemes, chosen at compile time:
+//   RL > 0  RL lanes per row, the lanes' partial sums reduced by shuffles (the matrix mostly in shared memory or L2:
+//           no block barriers);
+//   RL = 0  slot-parallel (an HBM-resident matrix): the rows are taken kSpmvRows at a time and their slots in passes
+//           of kSpmvChunk, each thread computing the products A_s p_j of consecutive slots (coalesced loads of the
+//           block planes and column indices); the products are staged in shared memory and the row's thread adds
+//           them in slot order.
+constexpr uint32_t kSpmvRows = 128;    // slot-parallel: rows per pass (the block needs more threads than this)
+constexpr uint32_t kSpmvChunk = 1024;  // slot-parallel: slot products staged per pass
+
+struct SpmvStage {
+  uint32_t rowOff[kSpmvRows + 1];
+  float prod[3][kSpmvChunk];
+};
+
+template <int RL, class Dir, class Out>
+__device__ inline void directionProducts(const Dev& D, const SmemMatrix& A, uint32_t r0, uint32_t r1, Dir&& dir,
+                                         Out&& out) {
+  if constexpr (RL > 0) {
+    const uint32_t groups = blockDim.x / RL;
+    const int sub = threadIdx.x & (RL - 1);
+    const unsigned groupMask = ((1u << RL) - 1u) << ((threadIdx.x & 31) & ~(RL - 1));
+    for (uint32_t i = r0 + threadIdx.x / RL; i < r1; i += groups) {
+      const uint32_t rs = __ldg(D.rowStart + i), re = D.particle[i].pinned == 0u ? __ldg(D.rowStart + i + 1) : rs;
+      const float3 acc = rowProduct<RL>(A, rs, re, sub, groupMask, dir);
+      if (sub == 0) out(i, dir(i), acc);
+    }
+  } else {
+    __shared__ SpmvStage st;
+    const uint32_t t = threadIdx.x;
+    for (uint32_t rr = r0; rr < r1; rr += kSpmvRows) {
+      const uint32_t R = min(kSpmvRows, r1 - rr);
+      const uint32_t s0 = __ldg(D.rowStart + rr);
+      if (t <= R) st.rowOff[t] = __ldg(D.rowStart + rr + t) - s0;
+      __syncthreads();
+      const uint32_t S = st.rowOff[R];
+      float3 acc = mk(0, 0, 0);
+      for (uint32_t c = 0; c < S; c += kSpmvChunk) {
+        const uint32_t cn = min(kSpmvChunk, S - c);
+        for (uint32_t k = t; k < cn; k += blockDim.x) {
+          const uint32_t s = s0 + c + k;
+          const uint32_t col = A.col(s);
+          float3 v = mk(0, 0, 0);
+          if (!(col & kPinnedBit)) {
+            float a[9];
+            A.block(s, a);
+            const float3 x = dir(col);
+            v.x = a[0] * x.x + a[1] * x.y + a[2] * x.z;
+            v.y = a[3] * x.x + a[4] * x.y + a[5] * x.z;
+            v.z = a[6] * x.x + a[7] * x.y + a[8] * x.z;
+          }
+          st.prod[0][k] = v.x;
+          st.prod[1][k] = v.y;
+          st.prod[2][k] = v.z;
+        }
+        __syncthreads();
+        if (t < R) {
+          const uint32_t lo = max(st.rowOff[t], c), hi = min(st.rowOff[t + 1], c + cn);
+          for (uint32_t q = lo; q < hi; ++q) {
+            acc.x += st.prod[0][q - c];
+            acc.y += st.prod[1][q - c];
+            acc.z += st.prod[2][q - c];
+          }
+        }
+        __syncthreads();
+      }
+      if (t < R) {
+        const uint32_t i = rr + t;
+        out(i, dir(i), D.particle[i].pinned != 0u ? mk(0, 0, 0) : acc);
+      }
+      __syncthreads();  // rowOff is rewritten for the next rows
+    }
+  }
+}
+
+// One PCG iteration's product with the direction update folded in (p_j = z_j + beta * pPrev_j): writes p_i (pCur),
+// Ap_i (apFull) and the contact-filtered Ap_i (ap); returns this thread's share of p . filtered Ap.
+template <int RL>
+__device__ inline double directionStep(const Dev& D, const SmemMatrix& A, uint32_t r0, uint32_t r1,
+                                       const float4* pPrev, float4* pCur, float fb, bool first) {
+  double vpap = 0.0;
+  directionProducts<RL>(
+      D, A, r0, r1,
+      [&](uint32_t j) {
+        const float3 zj = ld3(D.z, j);
+        return first ? zj : zj + ld3(pPrev, j) * fb;
+      },
+      [&](uint32_t i, float3 pi, float3 acc) {
+        pCur[i] = f4(pi);
+        const float3 filtered = filterContact(D.contact[i], acc);
+        D.apFull[i] = f4(acc);
+        D.ap[i] = f4(filtered);
+        vpap += dotd3(pi, filtered);
+      });
+  return vpap;
+}
+
 // Contact-filtered block-Jacobi PCG in the reference's order. Writes step, resid; returns the iteration count, or -1
 // when a grid barrier gave up.
 // At most `budget` iterations (negative: P.maxCg). *r0out gets |r0|; *finished is false only when the budget, not
 // the convergence test or pAp <= 0, ended the loop.
-template <int RL>
+template <int PL>
 __device__ inline int pcgReferenceOrder(const Dev& D, GridSync& gs, const SmemMatrix& A, int budget = -1,
                                         double* r0out = nullptr, bool* finished = nullptr) {
   const uint32_t n = D.P.n;
@@ -732,35 +831,10 @@ __device__ inline int pcgReferenceOrder(const Dev& D, GridSync& gs, const SmemMa
   float4* pCur = D.p1;
   int it = 0;
   const int maxCg = budget < 0 ? D.P.maxCg : min(budget, D.P.maxCg);
-  const uint32_t groups = blockDim.x / RL;
-  const int sub = threadIdx.x & (RL - 1);
-  const unsigned groupMask = ((1u << RL) - 1u) << ((threadIdx.x & 31) & ~(RL - 1));
   if (finished) *finished = true;
   while (!done && it < maxCg) {
     // SpMV with the direction update folded in: p_j = z_j + beta * pPrev_j.
-    double vpap[1] = {0.0};
-    const float fb = static_cast<float>(beta);
-    const bool first = it == 0;
-    for (uint32_t i = r0i + threadIdx.x / RL; i < r1i; i += groups) {
-      const uint32_t rs = __ldg(D.rowStart + i), re = __ldg(D.rowStart + i + 1);
-      float3 acc = mk(0, 0, 0);
-      if (D.particle[i].pinned == 0u)
-        acc = rowProduct<RL>(A, rs, re, sub, groupMask, [&](uint32_t j) {
-          const float3 zj = ld3(D.z, j);
-          return first ? zj : zj + ld3(pPrev, j) * fb;
-        });
-      else
-        acc = rowProduct<RL>(A, rs, rs, sub, groupMask, [&](uint32_t) { return mk(0, 0, 0); });
-      if (sub == 0) {
-        const float3 zi = ld3(D.z, i);
-        const float3 pi = first ? zi : zi + ld3(pPrev, i) * fb;
-        pCur[i] = f4(pi);
-        const float3 filtered = filterContact(D.contact[i], acc);
-        D.apFull[i] = f4(acc);
-        D.ap[i] = f4(filtered);
-        vpap[0] += dotd3(pi, filtered);
-      }
-    }
+    double vpap[1] = {directionStep<PL>(D, A, r0i, r1i, pPrev, pCur, static_cast<float>(beta), it == 0)};
     double pAp[1];
     if (!gridReduce<1>(D, gs, vpap, pAp)) return -1;
     if (!(pAp[0] > 0.0)) return it;
@@ -856,10 +930,10 @@ __device__ inline bool applyLearned(const Dev& D, GridSync& gs, uint32_t r0i, ui
 // unpreconditioned residual. Returns the iteration count, -1 when a barrier gave up, or -2 - iterations when the
 // solve broke down (a non-finite scalar, or |r|^2 above 1e6 |r0|^2): the caller then solves again with block-Jacobi.
 // M^-1 = L L^T is SPD for any finite L with a positive block diagonal, so a finite solve converges like any PCG; its
-// unpreconditioned |r| is not monotone and is no stall signal. With `warm`, step, resid and r hold a partial solve (a block-Jacobi phase) and
-// the iteration continues from them, with `r0In` (that solve's initial |r|) in the convergence test; `budget` bounds
-// the iterations.
-template <int RL>
+// unpreconditioned |r| is not monotone and is no stall signal. With `warm`, step, resid and r hold a partial solve
+// (a block-Jacobi phase) and the iteration continues from them, with `r0In` (that solve's initial |r|) in the
+// convergence test; `budget` bounds the iterations.
+template <int PL>
 __device__ inline int pcgLearned(const Dev& D, GridSync& gs, const SmemMatrix& A, bool warm = false,
                                  double r0In = 0.0, int budget = -1) {
   const uint32_t n = D.P.n;
@@ -889,7 +963,7 @@ __device__ inline int pcgLearned(const Dev& D, GridSync& gs, const SmemMatrix& A
   double rz;
   {
     double v[1] = {0.0};
-    if (!applyLearned<RL>(D, gs, r0i, r1i, &v[0])) return -1;
+    if (!applyLearned<(PL > 0 ? PL : kRowLanes)>(D, gs, r0i, r1i, &v[0])) return -1;
     double t[1];
     if (!gridReduce<1>(D, gs, v, t)) return -1;
     rz = t[0];
@@ -900,29 +974,9 @@ __device__ inline int pcgLearned(const Dev& D, GridSync& gs, const SmemMatrix& A
   float4* pCur = D.p1;
   int it = 0;
   const int maxCg = budget < 0 ? D.P.maxCg : min(budget, D.P.maxCg);
-  const uint32_t groups = blockDim.x / RL;
-  const int sub = threadIdx.x & (RL - 1);
-  const unsigned groupMask = ((1u << RL) - 1u) << ((threadIdx.x & 31) & ~(RL - 1));
   while (it < maxCg) {
-    double vpap[1] = {0.0};
-    const float fb = static_cast<float>(beta);
-    const bool first = it == 0;
-    for (uint32_t i = r0i + threadIdx.x / RL; i < r1i; i += groups) {
-      const uint32_t rs = __ldg(D.rowStart + i), re = D.particle[i].pinned == 0u ? __ldg(D.rowStart + i + 1) : rs;
-      const float3 acc = rowProduct<RL>(A, rs, re, sub, groupMask, [&](uint32_t j) {
-        const float3 zj = ld3(D.z, j);
-        return first ? zj : zj + ld3(pPrev, j) * fb;
-      });
-      if (sub == 0) {
-        const float3 zi = ld3(D.z, i);
-        const float3 pi = first ? zi : zi + ld3(pPrev, i) * fb;
-        pCur[i] = f4(pi);
-        const float3 filtered = filterContact(D.contact[i], acc);
-        D.apFull[i] = f4(acc);
-        D.ap[i] = f4(filtered);
-        vpap[0] += dotd3(pi, filtered);
-      }
-    }
+    // SpMV with the direction update folded in: p_j = z_j + beta * pPrev_j.
+    double vpap[1] = {directionStep<PL>(D, A, r0i, r1i, pPrev, pCur, static_cast<float>(beta), it == 0)};
     double pAp[1];
     if (!gridReduce<1>(D, gs, vpap, pAp)) return -1;
     if (!isfinite(pAp[0])) return -2 - it;
@@ -944,7 +998,7 @@ __device__ inline int pcgLearned(const Dev& D, GridSync& gs, const SmemMatrix& A
     if (sqrt(rr[0]) <= D.P.cgTolerance * r0) break;
     if (rr[0] > 1e6 * rr0) return -2 - it;
     double vz[1] = {0.0};
-    if (!applyLearned<RL>(D, gs, r0i, r1i, &vz[0])) return -1;
+    if (!applyLearned<(PL > 0 ? PL : kRowLanes)>(D, gs, r0i, r1i, &vz[0])) return -1;
     double rzNew[1];
     if (!gridReduce<1>(D, gs, vz, rzNew)) return -1;
     if (!isfinite(rzNew[0])) return -2 - it;
@@ -961,37 +1015,38 @@ __device__ inline int pcgLearned(const Dev& D, GridSync& gs, const SmemMatrix& A
 // first (0: none), then, when the solve has not converged, the learned preconditioner from the current iterate within
 // the remaining iteration budget; a learned phase that stalls is followed by a full block-Jacobi solve. Returns the
 // total iteration count of all phases, or -1 when a barrier gave up.
-template <bool Learned, int RL>
+template <bool Learned, int PL>
 __device__ inline int pcgSolve(const Dev& D, GridSync& gs) {
   uint32_t r0i, r1i;
   blockRange(D.P.n, gs.rank, gs.size, r0i, r1i);
   const SmemMatrix A = stageMatrix(D, r0i, r1i);
-  if (!Learned) return pcgReferenceOrder<RL>(D, gs, A);
+  if (!Learned) return pcgReferenceOrder<PL>(D, gs, A);
   int first = 0;
   double r0 = 0.0;
   const int sw = D.P.learnedSwitch;
   if (sw > 0) {
     bool finished = false;
-    first = pcgReferenceOrder<RL>(D, gs, A, sw, &r0, &finished);
+    first = pcgReferenceOrder<PL>(D, gs, A, sw, &r0, &finished);
     if (first < 0 || finished || first >= D.P.maxCg) return first;
   }
-  const int it = pcgLearned<RL>(D, gs, A, sw > 0, r0, D.P.maxCg - first);
+  const int it = pcgLearned<PL>(D, gs, A, sw > 0, r0, D.P.maxCg - first);
   if (gs.rank == 0 && threadIdx.x == 0) D.ctl->learnedSolves += 1;
   if (it >= -1) return it < 0 ? it : first + it;
   if (gs.rank == 0 && threadIdx.x == 0) D.ctl->precondFallbacks += 1;
-  const int jac = pcgReferenceOrder<RL>(D, gs, A);
+  const int jac = pcgReferenceOrder<PL>(D, gs, A);
   return jac < 0 ? jac : jac + first + (-2 - it);
 }
 
 // One Newton iteration's solve for the blocks of one group (the whole grid for one solver, or a garment's blocks in
-// a batched launch); gs is initialised.
-template <bool Learned, int RL>
+// a batched launch); gs is initialised. PL: the scheme of the PCG's product A p (lanes per row, or 0 for
+// slot-parallel; see directionProducts), also the lanes of the learned factor's products when positive.
+template <bool Learned, int PL>
 __device__ inline void solveGroup(const Dev& D, GridSync& gs) {
   Control* ctl = D.ctl;
   const uint32_t n = D.P.n;
   uint32_t r0i, r1i;
   blockRange(n, gs.rank, gs.size, r0i, r1i);
-  const int it = pcgSolve<Learned, RL>(D, gs);
+  const int it = pcgSolve<Learned, PL>(D, gs);
   if (it < 0) return;
   if (gs.rank == 0 && threadIdx.x == 0) {
     if (D.cgLog) D.cgLog[static_cast<unsigned long long>(ctl->newtonIterations) % kCgLogCapacity] = it;

@@ -152,36 +152,61 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_pcg_only(Dev D) {
   if (it >= 0 && blockIdx.x == 0 && threadIdx.x == 0) D.ctl->lastCg = it;
 }
 
-// Standalone block-CSR SpMV (kRowLanes lanes per row), y = A x over unpinned rows and columns.
-__global__ void k_spmv(uint32_t n, const uint32_t* __restrict__ rowStart, const uint32_t* __restrict__ colIndex,
-                       const float* __restrict__ blocks, uint32_t SP, const uint8_t* __restrict__ pinned,
-                       const float4* __restrict__ x, float4* __restrict__ y) {
-  const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
-  const uint32_t gid = tid / kRowLanes, groups = stride / kRowLanes;
-  const int sub = threadIdx.x & (kRowLanes - 1);
-  const unsigned groupMask = ((1u << kRowLanes) - 1u) << ((threadIdx.x & 31) & ~(kRowLanes - 1));
-  const uint32_t rounds = (n + groups - 1) / groups;
-  for (uint32_t r = 0; r < rounds; ++r) {
-    const uint32_t i = gid + r * groups;
+// Standalone block-CSR SpMV, y = A x over unpinned rows and columns, slot-parallel: block b owns rows
+// [b * kSpmvRows, (b + 1) * kSpmvRows) and walks their slots in chunks of kSpmvChunk, each thread computing the products
+// A_s x_j of consecutive slots (coalesced loads of every block plane and column index, kSpmvChunk / blockDim slots in
+// flight per thread), staged in shared memory; one thread per row then adds its slots' products in slot order.
+constexpr uint32_t kSpmvThreads = 256;  // kSpmvRows and kSpmvChunk: kernels.cuh
+
+__global__ void __launch_bounds__(kSpmvThreads) k_spmv(uint32_t n, const uint32_t* __restrict__ rowStart,
+                                                       const uint32_t* __restrict__ colIndex,
+                                                       const float* __restrict__ blocks, uint32_t SP,
+                                                       const uint8_t* __restrict__ pinned,
+                                                       const float4* __restrict__ x, float4* __restrict__ y) {
+  __shared__ uint32_t rowOff[kSpmvRows + 1];
+  __shared__ float prod[3][kSpmvChunk];
+  const uint32_t t = threadIdx.x;
+  for (uint32_t r0 = blockIdx.x * kSpmvRows; r0 < n; r0 += gridDim.x * kSpmvRows) {
+    const uint32_t R = min(kSpmvRows, n - r0);
+    const uint32_t s0 = __ldg(rowStart + r0);
+    if (t <= R) rowOff[t] = __ldg(rowStart + r0 + t) - s0;
+    __syncthreads();
+    const uint32_t S = rowOff[R];
     float3 acc = mk(0, 0, 0);
-    if (i < n && !pinned[i]) {
-      const uint32_t rs = rowStart[i], re = rowStart[i + 1];
-      for (uint32_t s = rs + sub; s < re; s += kRowLanes) {
-        const uint32_t j = colIndex[s];
-        if (pinned[j]) continue;
-        const float3 pj = xyz(x[j]);
-        acc.x += blocks[0 * SP + s] * pj.x + blocks[1 * SP + s] * pj.y + blocks[2 * SP + s] * pj.z;
-        acc.y += blocks[3 * SP + s] * pj.x + blocks[4 * SP + s] * pj.y + blocks[5 * SP + s] * pj.z;
-        acc.z += blocks[6 * SP + s] * pj.x + blocks[7 * SP + s] * pj.y + blocks[8 * SP + s] * pj.z;
-      }
-    }
+    const bool rowLive = t < R && pinned[r0 + t] == 0;
+    for (uint32_t c = 0; c < S; c += kSpmvChunk) {
+      const uint32_t cn = min(kSpmvChunk, S - c);
+#pragma unroll 4
+      for (uint32_t k = t; k < cn; k += kSpmvThreads) {
+        const uint32_t s = s0 + c + k;
+        const uint32_t j = __ldg(colIndex + s);
+        float a[9];
 #pragma unroll
-    for (int o = kRowLanes / 2; o > 0; o >>= 1) {
-      acc.x += __shfl_xor_sync(groupMask, acc.x, o);
-      acc.y += __shfl_xor_sync(groupMask, acc.y, o);
-      acc.z += __shfl_xor_sync(groupMask, acc.z, o);
+        for (int q = 0; q < 9; ++q) a[q] = __ldg(blocks + q * SP + s);
+        float3 v = mk(0, 0, 0);
+        if (pinned[j] == 0) {
+          const float3 xj = xyz(__ldg(x + j));
+          v.x = a[0] * xj.x + a[1] * xj.y + a[2] * xj.z;
+          v.y = a[3] * xj.x + a[4] * xj.y + a[5] * xj.z;
+          v.z = a[6] * xj.x + a[7] * xj.y + a[8] * xj.z;
+        }
+        prod[0][k] = v.x;
+        prod[1][k] = v.y;
+        prod[2][k] = v.z;
+      }
+      __syncthreads();
+      if (t < R) {
+        const uint32_t lo = max(rowOff[t], c), hi = min(rowOff[t + 1], c + cn);
+        for (uint32_t q = lo; q < hi; ++q) {
+          acc.x += prod[0][q - c];
+          acc.y += prod[1][q - c];
+          acc.z += prod[2][q - c];
+        }
+      }
+      __syncthreads();
     }
-    if (sub == 0 && i < n) y[i] = f4(acc);
+    if (t < R) y[r0 + t] = f4(rowLive ? acc : mk(0, 0, 0));
+    __syncthreads();  // rowOff is rewritten for the next row range
   }
 }
 

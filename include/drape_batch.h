@@ -44,15 +44,17 @@ int drape_batch_build(drape_batch* b);
 int drape_batch_set_precond(drape_batch* b, drape_precond* p);
 
 typedef struct drape_batch_tuning {
-  int32_t row_lanes;      /* lanes per block row in the solve's sparse products: 2, 4 or 8 */
+  int32_t row_lanes;      /* the PCG's product A p: 0 = slot-parallel (each thread a run of consecutive block
+                             slots, row sums through shared memory), or 2, 4, 8 lanes per block row (also the lanes of
+                             the learned factor's products; 4 with slot-parallel) */
   int32_t block_threads;  /* threads per block of the solve launch: 256, 512 or 1024 (1024 / this blocks per SM) */
   int32_t blocks;         /* blocks of the solve launch */
   int32_t variants_timed; /* 0 when set by hand */
   double ms_per_newton;   /* the chosen variant's mean solve time per Newton iteration during tuning */
 } drape_batch_tuning;
 
-/* Times each solve variant on the batch's current state for `frames` frames (restoring the state after each) and
-   keeps the fastest. */
+/* Times the 12 solve variants (product scheme x block size) on the batch's current state for `frames` frames each
+   (restoring the state after each) and keeps the fastest. */
 int drape_batch_autotune(drape_batch* b, int frames, drape_batch_tuning* out);
 /* Sets the variant by hand (row_lanes and block_threads of *tuning; the other fields are written back). */
 int drape_batch_set_tuning(drape_batch* b, drape_batch_tuning* tuning);

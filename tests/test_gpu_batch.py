@@ -1,16 +1,18 @@
 """Batched drapes (include/drape_batch.h) through the C ABI, against one drape_solver per garment.
 
 A batch garment runs the same kernels as a single solver built from its scene. What changes is the grouping of the
-FP64 reductions (a garment's solve group has fewer blocks than a solver's grid) and, for the autotuner's 2- and 8-lane
-variants, the order of each row's FP32 sums in the SpMV. FP64 regrouping leaves the FP32-rounded PCG scalars as they
-are, so those runs track each other closely; an FP32 difference, like any rounding difference, grows over frames on
-these drops (contact activation, Armijo halvings and PCG iteration counts are discrete decisions): on the tubes here a
-5e-7 m difference after one frame reaches centimetres after three. Bars:
-  - eight frames of three uneven garments on their own bodies (PCG converged to 1e-6): 1e-4 m from the single
-    solvers, the same Newton iteration and substep counts;
+FP64 reductions (a garment's solve group has fewer blocks than a solver's grid) and, with the autotuner's product
+schemes (slot-parallel, or 2, 4, 8 lanes per row), the order of each row's FP32 sums in the SpMV. FP64 regrouping
+leaves the FP32-rounded PCG scalars as they are, so those runs track each other closely; an FP32 difference, like
+any rounding difference, grows over frames on these drops (contact activation, Armijo halvings and PCG iteration
+counts are discrete decisions): on the tubes here a 5e-7 m difference after one frame reaches centimetres after
+three. Bars:
+  - eight frames of three uneven garments on their own bodies (PCG converged to 1e-6, the single solver's product
+    scheme): 1e-4 m from the single solvers, the same Newton iteration and substep counts;
   - graph replay and direct launches: bit-identical;
   - autotuning leaves the state as it was (bit-identical) and picks one of its variants;
-  - every solve variant: one frame within 1e-5 m of the default (the one-frame trajectory bar of the parity tests);
+  - every solve variant: one frame within 1e-5 m of the default (the one-frame trajectory bar of the parity tests),
+    the same PCG iteration counts; block sizes alone regroup only FP64 sums;
   - the learned preconditioner with an identity network tracks block-Jacobi (1e-4 m after two frames);
   - drape to rest: the batch runner settles the garments the single solver settles, with the same assembly length
     (two frames) and a settle frame count within 25 %.
@@ -30,17 +32,22 @@ ASSEMBLING, SETTLING = 0, 1
 
 def _scenes(tolerance=1e-6, cap=1000):
     st = Settings(cg_tolerance=tolerance, max_cg_iterations=cap)
-    return [S.tube_variant(11, 1500, field_n=48, settings=st), S.sheet_on_sphere(20, cg_tolerance=tolerance, max_cg=cap),
+    return [S.tube_variant(11, 1500, field_n=48, settings=st),
+            S.sheet_on_sphere(20, cg_tolerance=tolerance, max_cg=cap),
             S.tube_variant(12, 3200, field_n=64, settings=Settings(cg_tolerance=tolerance, max_cg_iterations=cap))]
 
 
-def _batch(gpu, scenes, precond=None):
+def _batch(gpu, scenes, precond=None, like_single=False):
+    """A built batch; like_single: the single solver's product scheme (4 lanes per row), so that both do the same FP32
+    arithmetic and differ only in the grouping of FP64 sums."""
     b = BT.BatchSolver(0)
     for sc in scenes:
         b.add(sc)
     if precond is not None:
         b.set_precond(precond)
     b.build()
+    if like_single:
+        b.set_tuning(4, 1024)
     return b
 
 
@@ -55,7 +62,7 @@ def _frames(stepper, phase_fn, frames=8, settle_at=4):
 
 def test_batch_tracks_single_solvers(gpu):
     scenes = _scenes()
-    b = _batch(gpu, scenes)
+    b = _batch(gpu, scenes, like_single=True)
     _frames(lambda: b.step(1 / 60, 1, 2), lambda ph: [b.set_phase(i, ph) for i in range(len(scenes))])
     for i, sc in enumerate(scenes):
         s = gpu.CudaSolver(0)
@@ -70,7 +77,7 @@ def test_batch_tracks_single_solvers(gpu):
 
 def test_batch_stats_match_single_solver(gpu):
     scenes = _scenes()
-    b = _batch(gpu, scenes)
+    b = _batch(gpu, scenes, like_single=True)
     b.step(1 / 60, 1, 2)
     for i, sc in enumerate(scenes):
         s = gpu.CudaSolver(0)
@@ -104,14 +111,14 @@ def test_autotune_keeps_the_state_and_picks_a_variant(gpu):
     b.step(1 / 60, 1, 2)
     before = [b.positions(i) for i in range(3)]
     t = b.autotune(1)
-    assert t["row_lanes"] in (2, 4, 8) and t["block_threads"] in (256, 512, 1024) and t["variants_timed"] == 9
+    assert t["row_lanes"] in (0, 2, 4, 8) and t["block_threads"] in (256, 512, 1024) and t["variants_timed"] == 12
     assert t["ms_per_newton"] > 0
     for i in range(3):
         assert np.array_equal(before[i], b.positions(i))
     assert b.counters(0).newton_iterations == 0
 
 
-@pytest.mark.parametrize("lanes,threads", [(2, 256), (4, 256), (8, 512), (2, 1024), (8, 1024)])
+@pytest.mark.parametrize("lanes,threads", [(0, 256), (2, 256), (4, 256), (8, 512), (0, 1024), (4, 1024)])
 def test_every_variant_gives_the_same_frame(gpu, lanes, threads):
     ref = _batch(gpu, _scenes(1e-2, 50))
     b = _batch(gpu, _scenes(1e-2, 50))
@@ -154,7 +161,7 @@ def test_errors_map_to_reference_exceptions(gpu):
 
 def test_drape_to_rest_matches_single_solver_runs(gpu):
     scenes = [S.tube_10k(), S.seamed_tube(24, 30, field_n=64, field_cell=0.008, gid="small")]
-    b = _batch(gpu, scenes)
+    b = _batch(gpu, scenes, like_single=True)
     res, secs = b.drape_to_rest()
     assert len(res) == 2 and np.all(secs > 0)
     single = []

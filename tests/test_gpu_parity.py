@@ -255,13 +255,27 @@ def test_errors_map_to_reference_exceptions(gpu):
         s.restore(snap)
 
 
-def test_drape_to_rest_settles_small_tube(gpu):
+def test_drape_to_rest_settles_the_10k_tube(gpu):
+    """The 10k seamed tube settles (the FP64 oracle settles it in 221 frames)."""
+    scene = S.tube_10k()
+    s = gpu.CudaSolver(0)
+    s.build(scene)
+    res = s.drape_to_rest(["tube"])
+    assert res.settled == 1 and res.retries == 0 and 0 < res.frames_run < 1200
+    st = s.stats()
+    assert not st.has_non_finite
+    assert st.max_body_penetration <= 0.002
+
+
+def test_drape_to_rest_ends_a_marginal_drape_in_a_terminal_state(gpu):
+    """A 24 x 30 tube that the FP64 oracle does not settle within the 20 s limit either: the runner stops in one of
+    its terminal states (timed out, or failed after max_retries doubled-substep retries) with a sane state."""
     scene = S.seamed_tube(24, 30, field_n=64, field_cell=0.008)
     s = gpu.CudaSolver(0)
     s.build(scene)
     res = s.drape_to_rest(["tube"])
     assert res.frames_run > 0
-    assert res.settled == 1 or res.simulated_seconds >= 19.9
+    assert res.settled == 1 or res.simulated_seconds >= 19.9 or (res.failed == 1 and res.retries == 3)
     st = s.stats()
     assert not st.has_non_finite
     assert st.max_body_penetration <= 0.002

@@ -106,8 +106,10 @@ def test_solver_factor_matches_network_on_the_same_system(gpu):
 
 def test_trained_network_needs_fewer_pcg_iterations_on_held_out_systems(gpu):
     """Ablation on the same systems: Newton systems of a held-out tube variant (10k particles, never trained on),
-    solved to the reference's tolerance 1e-2 with block-Jacobi and with the shipped trained network."""
+    solved to a relative residual of 1e-4 with block-Jacobi and with the shipped trained network. (At the reference's
+    1e-2 many of these systems need only 4-20 block-Jacobi iterations, too few for a stable ratio; the systems come
+    from a drape whose trajectory depends on FP32 rounding.)"""
     from drape_b200 import train
     systems = train.capture_along_drape(S.tube_variant(8, 10000, field_n=96), frames=120, every=20)
-    res = train.ablation(learned.load_weights("tube"), systems, 1e-2)
-    assert res["ratio"] > 1.3, res
+    res = train.ablation(learned.load_weights("tube"), systems, 1e-4)
+    assert res["ratio"] > 1.5, res
