@@ -227,14 +227,23 @@ __global__ void k_clock_batch(View V, int substep) {
   if (gr->phase == 0) gr->assemblyTime += V.run[g].hD;
 }
 
-// Statistics of every garment (sim_model.cpp:222-241) in FP64, one block per garment.
-__global__ void k_stats_batch(View V) {
-  const uint32_t g = blockIdx.x;
+// Statistics of every garment (sim_model.cpp:222-241) in FP64 over the point-kernel partition: each block reduces
+// its share of its garment's particles and seams into a row of `part`; the garment's last block to finish combines
+// the garment's rows in block order (deterministic, no floating-point atomics) and resets the garment's counter.
+__global__ void k_stats_batch(View V, double* part, unsigned int* done) {
+  __shared__ uint32_t g, rank, size;
+  if (threadIdx.x == 0) {
+    g = segmentOf(V.pointStart, V.G, blockIdx.x);
+    rank = blockIdx.x - V.pointStart[g];
+    size = V.pointStart[g + 1] - V.pointStart[g];
+  }
+  __syncthreads();
   const dcu::Dev& D = V.segs[g];
   double ke = 0, v2s = 0, gap = 0, pen = 0;
   unsigned long long moving = 0;
   int bad = 0;
-  for (uint32_t i = threadIdx.x; i < D.P.n; i += blockDim.x) {
+  const uint32_t stride = size * blockDim.x;
+  for (uint32_t i = rank * blockDim.x + threadIdx.x; i < D.P.n; i += stride) {
     const float4 x4 = D.x[i], v4 = D.v[i];
     if (!isfinite(x4.x) || !isfinite(x4.y) || !isfinite(x4.z) || !isfinite(v4.x) || !isfinite(v4.y) ||
         !isfinite(v4.z))
@@ -251,7 +260,7 @@ __global__ void k_stats_batch(View V) {
     v2s += vv;
     ++moving;
   }
-  for (uint32_t k = threadIdx.x; k < D.P.nSeam; k += blockDim.x) {
+  for (uint32_t k = rank * blockDim.x + threadIdx.x; k < D.P.nSeam; k += stride) {
     const float4 a = D.x[D.seam[k].a], b = D.x[D.seam[k].b];
     const float dx = a.x - b.x, dy = a.y - b.y, dz = a.z - b.z;
     gap = fmax(gap, static_cast<double>(sqrtf(dx * dx + dy * dy + dz * dz)));
@@ -276,17 +285,42 @@ __global__ void k_stats_batch(View V) {
     bd[w] = bad;
   }
   __syncthreads();
+  __shared__ bool last;
   if (threadIdx.x == 0) {
-    StatsOut s{};
-    s.kineticEnergy = tot[0];
-    s.sumV2 = tot[1];
+    double gp = 0, pn = 0;
+    unsigned long long m = 0;
+    int bb = 0;
     for (int k = 0; k < nw; ++k) {
-      s.maxSeamGap = fmax(s.maxSeamGap, mx[0][k]);
-      s.maxPenetration = fmax(s.maxPenetration, mx[1][k]);
-      s.moving += mv[k];
-      s.nonFinite |= bd[k];
+      gp = fmax(gp, mx[0][k]);
+      pn = fmax(pn, mx[1][k]);
+      m += mv[k];
+      bb |= bd[k];
+    }
+    double* row = part + blockIdx.x * 8ull;
+    row[0] = tot[0];
+    row[1] = tot[1];
+    row[2] = gp;
+    row[3] = pn;
+    row[4] = static_cast<double>(m);
+    row[5] = bb;
+    __threadfence();
+    last = atomicAdd(done + g, 1u) == size - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    StatsOut s{};
+    for (uint32_t b = V.pointStart[g]; b < V.pointStart[g + 1]; ++b) {
+      const double* row = part + b * 8ull;
+      s.kineticEnergy += __ldcg(row + 0);
+      s.sumV2 += __ldcg(row + 1);
+      s.maxSeamGap = fmax(s.maxSeamGap, __ldcg(row + 2));
+      s.maxPenetration = fmax(s.maxPenetration, __ldcg(row + 3));
+      s.moving += static_cast<unsigned long long>(__ldcg(row + 4));
+      s.nonFinite |= __ldcg(row + 5) != 0.0;
     }
     V.stats[g] = s;
+    done[g] = 0;
   }
 }
 
@@ -427,6 +461,8 @@ struct drape_batch {
   DBuf<dcu::Control> ctl;
   DBuf<dcu::Dev> segs;
   DBuf<bcu::StatsOut> stats;
+  DBuf<double> statsPart;         // 8 doubles per point-kernel block
+  DBuf<unsigned int> statsDone;   // per garment: blocks of k_stats_batch finished
   DBuf<unsigned char> control;  // frame control: G SegRun, then G + 1 solve-block starts
   HostPinned<unsigned char> hControl;
   HostPinned<bcu::StatsOut> hStats;
@@ -617,6 +653,8 @@ struct drape_batch {
                                               (dcu::kAssembleWarps * kAssembleRowsPerWarp));
     }
     const auto pStart = prefix(pointCount), aStart = prefix(asmCount);
+    statsPart.alloc(8ull * pStart[G]);
+    statsDone.alloc(G);
     std::vector<uint32_t> st(pStart);
     st.insert(st.end(), aStart.begin(), aStart.end());
     starts.upload(st, s);
@@ -848,7 +886,7 @@ struct drape_batch {
       bcu::k_clock_batch<<<(G + 127) / 128, 128, 0, stream>>>(view, s);
       launches += 2;
     }
-    bcu::k_stats_batch<<<G, 256, 0, stream>>>(view);
+    bcu::k_stats_batch<<<pointGrid, kPointThreads, 0, stream>>>(view, statsPart.p, statsDone.p);
     ++launches;
     BCK(cudaGetLastError());
     BCK(cudaMemcpyAsync(hStats.p, stats.p, sizeof(bcu::StatsOut) * G, cudaMemcpyDeviceToHost, stream));

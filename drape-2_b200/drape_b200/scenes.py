@@ -263,6 +263,17 @@ def tube_60k(**kw) -> Scene:
     return seamed_tube(154, 195, field_n=256, field_cell=0.003, **kw)
 
 
+def _tube_of_size(n_particles: int, w: float, h: float, tr: float, ar: float, field_n: int,
+                  settings: Optional[Settings], gid: str, radius: Optional[float] = None) -> Scene:
+    per_panel = n_particles / 2
+    nx = max(4, int(round(math.sqrt(per_panel * w / h))))
+    ny = max(4, int(round(per_panel / nx)))
+    radius = tr + 0.05 if radius is None else radius
+    cell = 0.762 / (field_n - 1)
+    return seamed_tube(nx, ny, width=w, height=h, radius=radius, field_n=field_n, field_cell=cell, torso_radius=tr,
+                       arm_radius=ar, settings=settings, gid=gid)
+
+
 def tube_variant(seed: int, n_particles: int, field_n: int = 128, settings: Optional[Settings] = None) -> Scene:
     """A seeded tube variant: panel sizes +-20 %, torso and arm radii +-15 %, about n_particles particles."""
     rng = np.random.default_rng(seed)
@@ -270,17 +281,21 @@ def tube_variant(seed: int, n_particles: int, field_n: int = 128, settings: Opti
     h = 0.7 * rng.uniform(0.8, 1.2)
     tr = TORSO_RADIUS * rng.uniform(0.85, 1.15)
     ar = ARM_RADIUS * rng.uniform(0.85, 1.15)
-    per_panel = n_particles / 2
-    nx = max(4, int(round(math.sqrt(per_panel * w / h))))
-    ny = max(4, int(round(per_panel / nx)))
-    radius = tr + 0.05
-    cell = 0.762 / (field_n - 1)
-    return seamed_tube(nx, ny, width=w, height=h, radius=radius, field_n=field_n, field_cell=cell, torso_radius=tr,
-                       arm_radius=ar, settings=settings, gid=f"tube{seed}")
+    return _tube_of_size(n_particles, w, h, tr, ar, field_n, settings, f"tube{seed}")
+
+
+def body_tube(seed: int, n_particles: int, field_n: int = 128) -> Scene:
+    """The seamed tube of the tube workloads (two 0.55 x 0.7 m panels on a 0.2 m cylinder) at about n_particles
+    particles, on its own seeded capsule-union body: torso radius 0.15 m +-5 %, arm radius 0.05 m +-10 %, so every
+    sleeve is as loose on its torso as the workloads' tube (its circumference 1.17 x the torso's, +-5 %)."""
+    rng = np.random.default_rng(seed)
+    tr = TORSO_RADIUS * rng.uniform(0.95, 1.05)
+    ar = ARM_RADIUS * rng.uniform(0.9, 1.1)
+    return _tube_of_size(n_particles, 0.55, 0.7, tr, ar, field_n, None, f"body{seed}", radius=0.2)
 
 
 def batch_tubes(count: int = 64, seed: int = 5, n_min: int = 2000, n_max: int = 40000):
-    """Uneven batch of seeded tube variants: particle counts log-uniform in [n_min, n_max], each tube on its own
+    """Uneven batch of seeded tubes (body_tube): particle counts log-uniform in [n_min, n_max], each tube on its own
     seeded capsule-union body whose field resolution grows with the garment, from 32^3 samples at n_min to 128^3 at
     n_max (log-linear). Returns the scenes in order."""
     rng = np.random.default_rng(seed)
@@ -289,7 +304,7 @@ def batch_tubes(count: int = 64, seed: int = 5, n_min: int = 2000, n_max: int = 
     for k, n in enumerate(ns):
         t = math.log(n / n_min) / math.log(n_max / n_min) if n_max > n_min else 0.0
         field_n = int(round(32 * 4 ** t))
-        scenes.append(tube_variant(seed * 1000 + k, int(round(n)), field_n=field_n))
+        scenes.append(body_tube(seed * 1000 + k, int(round(n)), field_n=field_n))
     return scenes
 
 
