@@ -96,8 +96,31 @@ def lib():
         L.oracle_land_on_body.argtypes = [_P(drape_field_desc), _f, _P(_f), _P(_f), _P(_f)]
         L.oracle_pcg.argtypes = [_u32, _P(_u32), _P(_u32), _P(_d), _P(_u8), _P(_u8), _P(_d), _P(_d), C.c_int, _d,
                                  _P(_d), _P(_d), _P(C.c_int)]
+        from drape_b200.bake import drape_bake_options, drape_mesh_desc
+        L.oracle_bake.argtypes = [_P(drape_mesh_desc), _u32, _P(drape_bake_options), _P(_d), _P(_i32)]
+        L.oracle_bake_values.argtypes = [_P(_f), C.c_size_t]
+        L.oracle_bake_last_error.restype = C.c_char_p
         _lib = L
     return _lib
+
+
+def bake(components, cell_size: float = 0.004, padding: float = 0.05, band: float = 0.02):
+    """bakeCollisionField restated serially on the CPU (bake_impl.hpp): returns a scene.Field. Raises ValueError for
+    an open component, as the reference throws std::invalid_argument."""
+    from drape_b200.bake import MeshArray, drape_bake_options
+    from drape_b200.scene import Field
+    L = lib()
+    arr = MeshArray(components)
+    opts = drape_bake_options(cell_size, padding, band)
+    origin, dims = (_d * 3)(), (_i32 * 3)()
+    code = L.oracle_bake(arr.descs, arr.count, C.byref(opts), origin, dims)
+    if code != 0:
+        raise (ValueError if code == -1 else RuntimeError)(L.oracle_bake_last_error().decode())
+    d = tuple(int(x) for x in dims)
+    values = np.zeros(d[0] * d[1] * d[2], np.float32)
+    if L.oracle_bake_values(_p(values, _f), values.size) != 0:
+        raise RuntimeError("oracle bake values")
+    return Field(np.array(origin[:]), float(cell_size), d, float(band), values.reshape(d[2], d[1], d[0]))
 
 
 def ref_available() -> bool:

@@ -20,6 +20,7 @@
 #ifndef DRAPE_ORACLE_API_H
 #define DRAPE_ORACLE_API_H
 
+#include "../include/drape_bake.h"
 #include "../include/drape_scene.h"
 
 #ifdef __cplusplus
@@ -103,6 +104,13 @@ void oracle_land_on_body(const drape_field_desc* f, float radius, const float fr
 int oracle_pcg(uint32_t n, const uint32_t* row_start, const uint32_t* col_index, const double* blocks,
                const uint8_t* pinned, const uint8_t* active, const double* normals, const double* grad,
                int max_iterations, double tolerance, double* step, double* resid, int* iterations);
+
+/* bakeCollisionField restated serially (bake_impl.hpp): bakes, keeps the field for oracle_bake_values, returns the
+   grid. -1 (invalid_argument) for an open component. */
+int oracle_bake(const drape_mesh_desc* components, uint32_t count, const drape_bake_options* options, double origin[3],
+                int32_t dims[3]);
+int oracle_bake_values(float* values, size_t count);
+const char* oracle_bake_last_error(void);
 
 #ifdef __cplusplus
 }

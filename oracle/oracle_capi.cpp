@@ -1,5 +1,6 @@
 // ORACLE — test infrastructure only (see oracle_api.h). C entry points over oracle_impl.hpp.
 #include "oracle_impl.hpp"
+#include "bake_impl.hpp"
 
 // ---------------------------------------------------------------------------------------------------------------
 // C API.
@@ -474,5 +475,49 @@ int oracle_pcg(uint32_t n, const uint32_t* row_start, const uint32_t* col_index,
     *iterations = static_cast<int>(s.counters.cg_iterations);
   });
 }
+
+namespace {
+thread_local obake::Field g_bake;
+thread_local std::string g_bakeError;
+}  // namespace
+
+int oracle_bake(const drape_mesh_desc* components, uint32_t count, const drape_bake_options* options, double origin[3],
+                int32_t dims[3]) {
+  try {
+    if (!components || !options || !origin || !dims) throw std::invalid_argument("null argument");
+    std::vector<obake::Mesh> meshes(count);
+    for (uint32_t c = 0; c < count; ++c) {
+      const drape_mesh_desc& d = components[c];
+      for (uint32_t i = 0; i < d.vertex_count; ++i)
+        meshes[c].v.push_back({d.vertices[3 * i], d.vertices[3 * i + 1], d.vertices[3 * i + 2]});
+      for (uint32_t t = 0; t < d.triangle_count; ++t) {
+        const uint32_t* tr = d.triangles + 3ull * t;
+        if (tr[0] >= d.vertex_count || tr[1] >= d.vertex_count || tr[2] >= d.vertex_count)
+          throw std::invalid_argument("triangle vertex index out of range");
+        meshes[c].t.push_back({tr[0], tr[1], tr[2]});
+      }
+    }
+    g_bake = obake::bake(meshes, options->cell_size, options->padding, options->band);
+    for (int a = 0; a < 3; ++a) {
+      origin[a] = g_bake.origin[a];
+      dims[a] = g_bake.dims[a];
+    }
+    return 0;
+  } catch (const std::invalid_argument& e) {
+    g_bakeError = e.what();
+    return -1;
+  } catch (const std::exception& e) {
+    g_bakeError = e.what();
+    return -3;
+  }
+}
+
+int oracle_bake_values(float* values, size_t count) {
+  if (!values || count != g_bake.values.size()) return -1;
+  std::copy(g_bake.values.begin(), g_bake.values.end(), values);
+  return 0;
+}
+
+const char* oracle_bake_last_error(void) { return g_bakeError.c_str(); }
 
 }  // extern "C"
