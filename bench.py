@@ -353,6 +353,31 @@ def batch_leg(args, device, world, rank, max_over_ranks, peak):
     return out
 
 
+def bake_leg(peak):
+    """The collision-field bake (drape_bake_field) of the reference's five-component test body at its default 4 mm
+    cells (the reference's bar: under 2 s, test_collision_perf.cpp:11-19) and of the tube workloads' capsule-union
+    body at 3 mm, device time per bake (mean of 3 after one warm-up), beside the oracle's serial restatement of the
+    same bake on one host core."""
+    import oracle as O
+    from drape_b200 import bake as BK
+    from drape_b200 import meshes as M
+    out = {}
+    for name, comps, opts in (("test_body_4mm", M.test_body(), BK.options()),
+                              ("capsule_union_3mm", M.capsule_union_body(), BK.options(cell_size=0.003))):
+        f = BK.bake_field(comps, opts)
+        ms = []
+        for _ in range(3):
+            BK.bake_field(comps, opts)
+            ms.append(BK.last_ms())
+        t0 = time.perf_counter()
+        ref = O.bake(comps, opts.cell_size, opts.padding, opts.band)
+        cpu = time.perf_counter() - t0
+        out[name] = {"triangles": M.triangle_count(comps), "samples": int(np.prod(f.dims)),
+                     "device_ms": statistics.mean(ms), "cpu_oracle_ms_1_core": 1000.0 * cpu,
+                     "bit_exact_vs_oracle": bool(np.array_equal(f.values, ref.values))}
+    return out
+
+
 def run_profile_case(args):
     """One small case for an ncu capture (not a benchmark line): "spmv" times the standalone SpMV on the tiled tube
     system; "batch" builds the first --batch-garments tubes of the batched workload and runs --batch-frames frames
@@ -560,6 +585,8 @@ def main():
     line["spmv"] = spmv_leg(CU, solver, peak)
     if args.batch_garments > 0:
         line["batch"] = batch_leg(args, local, world, rank, max_over_ranks, peak)
+    if rank == 0:
+        line["bake"] = bake_leg(peak)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.workload)
     if rank == 0:

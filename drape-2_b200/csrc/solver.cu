@@ -1272,7 +1272,7 @@ int drape_cuda_spmv_device(uint32_t n, const uint32_t* d_row_start, const uint32
     CK(cudaGetDevice(&dev));
     int sms = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const uint32_t blocksNeeded = (n + dcu::kSpmvRows - 1) / dcu::kSpmvRows;
+    const uint32_t blocksNeeded = (n + dcu::kSpmvBlockRows - 1) / dcu::kSpmvBlockRows;
     const uint32_t grid = std::min<uint32_t>(blocksNeeded, static_cast<uint32_t>(sms) * 64);
     dcu::k_spmv<<<grid, dcu::kSpmvThreads, 0, static_cast<cudaStream_t>(stream)>>>(
         n, d_row_start, d_col_index, d_blocks, slots_padded, d_pinned, static_cast<const float4*>(d_x),

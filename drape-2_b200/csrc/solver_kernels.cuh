@@ -153,29 +153,30 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_pcg_only(Dev D) {
 }
 
 // Standalone block-CSR SpMV, y = A x over unpinned rows and columns, slot-parallel: block b owns rows
-// [b * kSpmvRows, (b + 1) * kSpmvRows) and walks their slots in chunks of kSpmvChunk, each thread computing the products
-// A_s x_j of consecutive slots (coalesced loads of every block plane and column index, kSpmvChunk / blockDim slots in
-// flight per thread), staged in shared memory; one thread per row then adds its slots' products in slot order.
-constexpr uint32_t kSpmvThreads = 256;  // kSpmvRows and kSpmvChunk: kernels.cuh
+// [b * Rows, (b + 1) * Rows) and walks their slots in chunks of Chunk, each thread computing the products A_s x_j of
+// consecutive slots (coalesced loads of every block plane and column index), staged in shared memory; one thread per
+// row then adds its slots' products in slot order. Configuration: 256 threads, 128 rows, 1024-slot chunks (4.36 TB/s
+// on the tiled 60k-tube system; a 128-thread, 64-row variant held to 32 registers reached 4.19 there).
+constexpr uint32_t kSpmvThreads = 256, kSpmvBlockRows = 128, kSpmvBlockChunk = 1024;
 
 __global__ void __launch_bounds__(kSpmvThreads) k_spmv(uint32_t n, const uint32_t* __restrict__ rowStart,
-                                                       const uint32_t* __restrict__ colIndex,
-                                                       const float* __restrict__ blocks, uint32_t SP,
-                                                       const uint8_t* __restrict__ pinned,
-                                                       const float4* __restrict__ x, float4* __restrict__ y) {
-  __shared__ uint32_t rowOff[kSpmvRows + 1];
-  __shared__ float prod[3][kSpmvChunk];
+                                                           const uint32_t* __restrict__ colIndex,
+                                                           const float* __restrict__ blocks, uint32_t SP,
+                                                           const uint8_t* __restrict__ pinned,
+                                                           const float4* __restrict__ x, float4* __restrict__ y) {
+  __shared__ uint32_t rowOff[kSpmvBlockRows + 1];
+  __shared__ float prod[3][kSpmvBlockChunk];
   const uint32_t t = threadIdx.x;
-  for (uint32_t r0 = blockIdx.x * kSpmvRows; r0 < n; r0 += gridDim.x * kSpmvRows) {
-    const uint32_t R = min(kSpmvRows, n - r0);
+  for (uint32_t r0 = blockIdx.x * kSpmvBlockRows; r0 < n; r0 += gridDim.x * kSpmvBlockRows) {
+    const uint32_t R = min(kSpmvBlockRows, n - r0);
     const uint32_t s0 = __ldg(rowStart + r0);
     if (t <= R) rowOff[t] = __ldg(rowStart + r0 + t) - s0;
     __syncthreads();
     const uint32_t S = rowOff[R];
     float3 acc = mk(0, 0, 0);
     const bool rowLive = t < R && pinned[r0 + t] == 0;
-    for (uint32_t c = 0; c < S; c += kSpmvChunk) {
-      const uint32_t cn = min(kSpmvChunk, S - c);
+    for (uint32_t c = 0; c < S; c += kSpmvBlockChunk) {
+      const uint32_t cn = min(kSpmvBlockChunk, S - c);
 #pragma unroll 4
       for (uint32_t k = t; k < cn; k += kSpmvThreads) {
         const uint32_t s = s0 + c + k;
