@@ -381,7 +381,7 @@ def bake_leg(peak):
 def run_profile_case(args):
     """One small case for an ncu capture (not a benchmark line): "spmv" times the standalone SpMV on the tiled tube
     system; "batch" builds the first --batch-garments tubes of the batched workload and runs --batch-frames frames
-    (the first frame launches directly, the rest replay its CUDA graph)."""
+    (the first frame launches directly, the rest replay its CUDA graph); "bake" bakes the reference's test body."""
     import torch
     from drape_b200 import cuda as CU
     torch.cuda.set_device(0)
@@ -390,6 +390,12 @@ def run_profile_case(args):
         s = CU.CudaSolver(0)
         s.build(make_scene("tube60k"))
         print(json.dumps(spmv_leg(CU, s, peak, tiles=args.spmv_tiles)))
+        return 0
+    if args.profile_case == "bake":
+        from drape_b200 import bake as BK
+        from drape_b200 import meshes as M
+        f = BK.bake_field(M.test_body())
+        print(json.dumps({"case": "bake", "samples": int(np.prod(f.dims)), "device_ms": BK.last_ms()}))
         return 0
     from drape_b200 import batch as BT
     from drape_b200 import scenes as S
@@ -426,7 +432,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=0, help="end-to-end steps (0: same as --steps)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner leg")
     ap.add_argument("--batch-garments", type=int, default=64, help="garments of the batched leg (0: skip it)")
-    ap.add_argument("--profile-case", choices=["spmv", "batch"], default=None,
+    ap.add_argument("--profile-case", choices=["spmv", "batch", "bake"], default=None,
                     help="run one small case for a profiler capture instead of the benchmark")
     ap.add_argument("--spmv-tiles", type=int, default=12)
     ap.add_argument("--batch-frames", type=int, default=6)

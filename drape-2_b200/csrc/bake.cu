@@ -178,47 +178,60 @@ __global__ void k_bake_sign(Grid g, Mesh m, const uint32_t* owner, int8_t* sign,
   }
 }
 
-__device__ __forceinline__ bool far(const Grid& g, const unsigned long long* dist2, size_t i) {
-  return __longlong_as_double(static_cast<long long>(dist2[i])) > g.band2;
-}
+// Flood-fill state per sample: bit 0 far (farther than the band), bit 1 outside. Seeds: far samples on the grid
+// boundary.
+constexpr uint8_t kFar = 1, kOutside = 2;
 
-// Flood fill seeds: far samples on the grid boundary.
-__global__ void k_bake_seed(Grid g, const unsigned long long* dist2, uint8_t* outside, size_t count) {
+__global__ void k_bake_seed(Grid g, const unsigned long long* dist2, uint8_t* state, size_t count) {
   for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < count;
        i += static_cast<size_t>(gridDim.x) * blockDim.x) {
     const int x = static_cast<int>(i % g.nx), y = static_cast<int>((i / g.nx) % g.ny),
               z = static_cast<int>(i / (static_cast<size_t>(g.nx) * g.ny));
     const bool boundary = x == 0 || y == 0 || z == 0 || x == g.nx - 1 || y == g.ny - 1 || z == g.nz - 1;
-    outside[i] = boundary && far(g, dist2, i) ? 1 : 0;
+    const bool far = __longlong_as_double(static_cast<long long>(dist2[i])) > g.band2;
+    state[i] = far ? (boundary ? kFar | kOutside : kFar) : 0;
   }
 }
 
 // One sweep along `axis` in direction `dir` (+1 / -1): every line carries "outside" through consecutive far samples.
-// Sets *changed when it marks a sample.
-__global__ void k_bake_sweep(Grid g, const unsigned long long* dist2, uint8_t* outside, int axis, int dir,
-                             int* changed) {
+// A thread takes its line 32 samples at a time (independent loads) as bit masks in walking order, F (far) and O
+// (outside, a subset of F); with the carry c_in from the previous word, the sum F + O + c_in carries through exactly
+// the far runs that hold a seed or continue the previous run, so the reached set is O | ((F + O + c_in) ^ F ^ O) & F
+// and the carry out of bit 31 goes to the next word. Sets *changed when it marks a sample.
+__global__ void k_bake_sweep(Grid g, uint8_t* state, int axis, int dir, int* changed) {
   const int n[3] = {g.nx, g.ny, g.nz};
   const int u = axis == 0 ? 1 : 0, w = axis == 2 ? 1 : 2;  // the two other axes
   const size_t lines = static_cast<size_t>(n[u]) * n[w];
   const size_t strides[3] = {1, static_cast<size_t>(g.nx), static_cast<size_t>(g.nx) * g.ny};
+  const int len = n[axis];
   int marked = 0;
   for (size_t l = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; l < lines;
        l += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    const size_t cu = l % n[u], cw = l / n[u];
-    const size_t base = cu * strides[u] + cw * strides[w];
-    bool carry = false;
-    for (int s = 0; s < n[axis]; ++s) {
-      const int c = dir > 0 ? s : n[axis] - 1 - s;
-      const size_t i = base + static_cast<size_t>(c) * strides[axis];
-      if (!far(g, dist2, i)) {
-        carry = false;
-        continue;
+    const size_t base = (l % n[u]) * strides[u] + (l / n[u]) * strides[w];
+    const long long step = dir > 0 ? static_cast<long long>(strides[axis]) : -static_cast<long long>(strides[axis]);
+    const size_t first = dir > 0 ? base : base + static_cast<size_t>(len - 1) * strides[axis];
+    uint32_t cin = 0;
+    for (int s0 = 0; s0 < len; s0 += 32) {
+      const int cnt = min(32, len - s0);
+      uint8_t st[32];
+#pragma unroll
+      for (int e = 0; e < 32; ++e)
+        st[e] = e < cnt ? state[static_cast<size_t>(static_cast<long long>(first) + (s0 + e) * step)] : 0;
+      uint32_t F = 0, O = 0;
+#pragma unroll
+      for (int e = 0; e < 32; ++e) {
+        F |= static_cast<uint32_t>(st[e] & kFar) << e;
+        O |= static_cast<uint32_t>((st[e] & kOutside) >> 1) << e;
       }
-      if (outside[i]) {
-        carry = true;
-      } else if (carry) {
-        outside[i] = 1;
+      const unsigned long long sum = static_cast<unsigned long long>(F) + O + cin;
+      const uint32_t reached = O | ((static_cast<uint32_t>(sum) ^ F ^ O) & F);
+      cin = static_cast<uint32_t>(sum >> 32);
+      const uint32_t fresh = reached & ~O;
+      if (fresh) {
         marked = 1;
+#pragma unroll
+        for (int e = 0; e < 32; ++e)
+          if (fresh >> e & 1u) state[static_cast<size_t>(static_cast<long long>(first) + (s0 + e) * step)] = kFar | kOutside;
       }
     }
   }
@@ -226,7 +239,7 @@ __global__ void k_bake_sweep(Grid g, const unsigned long long* dist2, uint8_t* o
 }
 
 // Combine this component into the field (collision_bake.cpp:196-204).
-__global__ void k_bake_combine(Grid g, const unsigned long long* dist2, const int8_t* sign, const uint8_t* outside,
+__global__ void k_bake_combine(Grid g, const unsigned long long* dist2, const int8_t* sign, const uint8_t* state,
                                float* values, size_t count) {
   for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < count;
        i += static_cast<size_t>(gridDim.x) * blockDim.x) {
@@ -235,7 +248,7 @@ __global__ void k_bake_combine(Grid g, const unsigned long long* dist2, const in
     if (d2 <= g.band2) {
       v = static_cast<double>(sign[i]) * __dsqrt_rn(d2);
     } else {
-      v = outside[i] ? g.band : -g.band;
+      v = (state[i] & kOutside) ? g.band : -g.band;
     }
     v = fmin(fmax(v, -g.band), g.band);
     values[i] = fminf(values[i], __double2float_rn(v));
@@ -384,13 +397,13 @@ int drape_bake_field(int device, const drape_mesh_desc* components, uint32_t cou
     DBuf<unsigned long long> dist2;
     DBuf<uint32_t> owner;
     DBuf<int8_t> sign;
-    DBuf<uint8_t> outside;
+    DBuf<uint8_t> state;  // flood-fill state per sample (far, outside)
     DBuf<float> field;
     DBuf<int> changed;
     dist2.alloc(total);
     owner.alloc(total);
     sign.alloc(total);
-    outside.alloc(total);
+    state.alloc(total);
     field.alloc(total);
     changed.alloc(1);
     const int pointGrid = sms * 8;
@@ -490,7 +503,7 @@ int drape_bake_field(int device, const drape_mesh_desc* components, uint32_t cou
       bake::k_bake_distance<false><<<triGrid, 256, 0, st>>>(g, dm, dist2.p, owner.p);
       bake::k_bake_distance<true><<<triGrid, 256, 0, st>>>(g, dm, dist2.p, owner.p);
       bake::k_bake_sign<<<pointGrid, 256, 0, st>>>(g, dm, owner.p, sign.p, total);
-      bake::k_bake_seed<<<pointGrid, 256, 0, st>>>(g, dist2.p, outside.p, total);
+      bake::k_bake_seed<<<pointGrid, 256, 0, st>>>(g, dist2.p, state.p, total);
       KCK(cudaGetLastError());
       // Sweeps until a full round of six marks nothing (bounded by the number of samples, which is never reached).
       for (size_t round = 0; round < total; ++round) {
@@ -500,7 +513,7 @@ int drape_bake_field(int device, const drape_mesh_desc* components, uint32_t cou
             const size_t lines = static_cast<size_t>(axis == 0 ? dims[1] * dims[2]
                                                                : (axis == 1 ? dims[0] * dims[2] : dims[0] * dims[1]));
             const int grid = static_cast<int>(std::min<size_t>((lines + 255) / 256, static_cast<size_t>(sms) * 8));
-            bake::k_bake_sweep<<<grid, 256, 0, st>>>(g, dist2.p, outside.p, axis, dir, changed.p);
+            bake::k_bake_sweep<<<grid, 256, 0, st>>>(g, state.p, axis, dir, changed.p);
           }
         KCK(cudaGetLastError());
         int h = 0;
@@ -508,7 +521,7 @@ int drape_bake_field(int device, const drape_mesh_desc* components, uint32_t cou
         KCK(cudaStreamSynchronize(st));
         if (!h) break;
       }
-      bake::k_bake_combine<<<pointGrid, 256, 0, st>>>(g, dist2.p, sign.p, outside.p, field.p, total);
+      bake::k_bake_combine<<<pointGrid, 256, 0, st>>>(g, dist2.p, sign.p, state.p, field.p, total);
       KCK(cudaGetLastError());
       KCK(cudaStreamSynchronize(st));
     }
