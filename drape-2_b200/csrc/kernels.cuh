@@ -21,7 +21,7 @@ namespace dcu {
 
 constexpr int kWarp = 32;
 constexpr int kAssembleWarps = 8;   // warps per k_assemble block
-constexpr int kRowLanes = 4;        // lanes per block row in the SpMV
+constexpr int kRowLanes = 2;        // lanes per block row in the single solver's SpMV
 constexpr int kSolveThreads = 1024; // k_solve block size (one block per SM)
 constexpr uint32_t kPinnedBit = 0x80000000u;
 constexpr uint32_t kSmemSlotBytes = 40;      // one block slot in shared memory: 9 floats + a column index
@@ -206,15 +206,18 @@ struct GridSync {
   }
 };
 
-// Block-wide FP64 sums; thread 0 gets the result. Fixed tree shape, so deterministic.
-template <int K>
-__device__ inline void blockSum(double (&v)[K], double* out) {
+// Block-wide FP64 sums (or maxima); thread 0 gets the result in out. Fixed tree shape, so deterministic.
+template <int K, bool Max = false>
+__device__ inline void blockReduce(double (&v)[K], double* out) {
   __shared__ double red[K][32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
 #pragma unroll
   for (int k = 0; k < K; ++k)
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+    for (int o = 16; o > 0; o >>= 1) {
+      const double y = __shfl_down_sync(0xffffffffu, v[k], o);
+      v[k] = Max ? fmax(v[k], y) : v[k] + y;
+    }
   __syncthreads();
   if (lane == 0)
 #pragma unroll
@@ -223,69 +226,48 @@ __device__ inline void blockSum(double (&v)[K], double* out) {
   if (w == 0) {
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      double s = lane < nw ? red[k][lane] : 0.0;
+      double s = lane < nw ? red[k][lane] : (Max ? -INFINITY : 0.0);
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+      for (int o = 16; o > 0; o >>= 1) {
+        const double y = __shfl_down_sync(0xffffffffu, s, o);
+        s = Max ? fmax(s, y) : s + y;
+      }
       if (lane == 0) out[k] = s;
     }
   }
 }
 
-// Grid-wide FP64 sums (or maxima): every block publishes its block total, passes the barrier, then warp 0 of every
-// block combines all blocks' totals in the same fixed order, so every block obtains bit-identical results and takes
-// the same branches. Returns false when the barrier gave up.
+template <int K>
+__device__ inline void blockSum(double (&v)[K], double* out) {
+  blockReduce<K, false>(v, out);
+}
+
+// Grid-wide FP64 sums (or maxima): every block publishes its block total and passes the barrier; then thread t of
+// every block reads the totals of blocks t, t + blockDim, ... and the block combines them in its fixed tree, so every
+// block obtains bit-identical results and takes the same branches. Returns false when the barrier gave up.
 template <int K, bool Max = false>
 __device__ inline bool gridReduce(const Dev& D, GridSync& gs, double (&v)[K], double (&out)[K]) {
   __shared__ double res[K];
   double* half = D.partials + static_cast<size_t>(gs.parity) * gs.size * kPartialStride;
   gs.parity ^= 1u;
-  if (Max) {
-    __shared__ double mred[K][32];
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) v[k] = fmax(v[k], __shfl_down_sync(0xffffffffu, v[k], o));
-    __syncthreads();
-    if ((threadIdx.x & 31) == 0)
-#pragma unroll
-      for (int k = 0; k < K; ++k) mred[k][threadIdx.x >> 5] = v[k];
-    __syncthreads();
-    if (threadIdx.x == 0)
-#pragma unroll
-      for (int k = 0; k < K; ++k) {
-        double m = mred[k][0];
-        for (int w = 1; w < static_cast<int>((blockDim.x + 31) >> 5); ++w) m = fmax(m, mred[k][w]);
-        half[gs.rank * kPartialStride + k] = m;
-      }
-  } else {
+  {
     double blk[K];
-    blockSum<K>(v, blk);
+    blockReduce<K, Max>(v, blk);
     if (threadIdx.x == 0)
 #pragma unroll
       for (int k = 0; k < K; ++k) half[gs.rank * kPartialStride + k] = blk[k];
   }
   if (!gs.sync(true)) return false;
-  if (threadIdx.x < 32) {
-    double s[K];
+  double s[K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) s[k] = Max ? -INFINITY : 0.0;
-    for (unsigned int b = threadIdx.x; b < gs.size; b += 32)
+  for (int k = 0; k < K; ++k) s[k] = Max ? -INFINITY : 0.0;
+  for (unsigned int b = threadIdx.x; b < gs.size; b += blockDim.x)
 #pragma unroll
-      for (int k = 0; k < K; ++k) {
-        const double x = __ldcg(half + b * kPartialStride + k);
-        s[k] = Max ? fmax(s[k], x) : s[k] + x;
-      }
-#pragma unroll
-    for (int k = 0; k < K; ++k)
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const double y = __shfl_xor_sync(0xffffffffu, s[k], o);
-        s[k] = Max ? fmax(s[k], y) : s[k] + y;
-      }
-    if (threadIdx.x == 0)
-#pragma unroll
-      for (int k = 0; k < K; ++k) res[k] = s[k];
-  }
+    for (int k = 0; k < K; ++k) {
+      const double x = __ldcg(half + b * kPartialStride + k);
+      s[k] = Max ? fmax(s[k], x) : s[k] + x;
+    }
+  blockReduce<K, Max>(s, res);
   __syncthreads();
 #pragma unroll
   for (int k = 0; k < K; ++k) out[k] = res[k];
@@ -671,20 +653,34 @@ __device__ inline SmemMatrix stageMatrix(const Dev& D, uint32_t r0, uint32_t r1)
 }
 
 // y_i (unfiltered) = sum over unpinned columns j of A_ij x_j for row i, by RL lanes (lane `sub`), reduced over the
-// lanes; x_j given by a functor.
+// lanes; x_j given by a functor. Each lane takes its slots kGatherDepth at a time: their column indices first, then
+// all their x_j loads (predicated, so they are in flight together), then the products in slot order; the sums are the
+// same as one slot at a time.
+constexpr int kGatherDepth = 4;
+
 template <int RL, class X>
 __device__ __forceinline__ float3 rowProduct(const SmemMatrix& A, uint32_t rs, uint32_t re, int sub, unsigned mask,
                                              X&& xj) {
   float3 acc = mk(0, 0, 0);
-  for (uint32_t s = rs + sub; s < re; s += RL) {
-    const uint32_t col = A.col(s);
-    if (col & kPinnedBit) continue;
-    const float3 v = xj(col);
-    float a[9];
-    A.block(s, a);
-    acc.x += a[0] * v.x + a[1] * v.y + a[2] * v.z;
-    acc.y += a[3] * v.x + a[4] * v.y + a[5] * v.z;
-    acc.z += a[6] * v.x + a[7] * v.y + a[8] * v.z;
+  for (uint32_t s0 = rs + sub; s0 < re; s0 += kGatherDepth * RL) {
+    uint32_t col[kGatherDepth];
+#pragma unroll
+    for (int k = 0; k < kGatherDepth; ++k) {
+      const uint32_t s = s0 + k * RL;
+      col[k] = s < re ? A.col(s) : kPinnedBit;
+    }
+    float3 v[kGatherDepth];
+#pragma unroll
+    for (int k = 0; k < kGatherDepth; ++k) v[k] = (col[k] & kPinnedBit) ? mk(0, 0, 0) : xj(col[k]);
+#pragma unroll
+    for (int k = 0; k < kGatherDepth; ++k) {
+      if (col[k] & kPinnedBit) continue;
+      float a[9];
+      A.block(s0 + k * RL, a);
+      acc.x += a[0] * v[k].x + a[1] * v[k].y + a[2] * v[k].z;
+      acc.y += a[3] * v[k].x + a[4] * v[k].y + a[5] * v[k].z;
+      acc.z += a[6] * v[k].x + a[7] * v[k].y + a[8] * v[k].z;
+    }
   }
 #pragma unroll
   for (int o = RL / 2; o > 0; o >>= 1) {
@@ -712,6 +708,12 @@ struct SpmvStage {
   float prod[3][kSpmvChunk];
 };
 
+// The one staging area of a block (every instantiation of directionProducts shares it; its uses never overlap).
+__device__ __forceinline__ SpmvStage& spmvStage() {
+  __shared__ SpmvStage st;
+  return st;
+}
+
 template <int RL, class Dir, class Out>
 __device__ inline void directionProducts(const Dev& D, const SmemMatrix& A, uint32_t r0, uint32_t r1, Dir&& dir,
                                          Out&& out) {
@@ -725,7 +727,7 @@ __device__ inline void directionProducts(const Dev& D, const SmemMatrix& A, uint
       if (sub == 0) out(i, dir(i), acc);
     }
   } else {
-    __shared__ SpmvStage st;
+    SpmvStage& st = spmvStage();
     const uint32_t t = threadIdx.x;
     for (uint32_t rr = r0; rr < r1; rr += kSpmvRows) {
       const uint32_t R = min(kSpmvRows, r1 - rr);

@@ -38,7 +38,7 @@ def _scenes(tolerance=1e-6, cap=1000):
 
 
 def _batch(gpu, scenes, precond=None, like_single=False):
-    """A built batch; like_single: the single solver's product scheme (4 lanes per row), so that both do the same FP32
+    """A built batch; like_single: the single solver's product scheme (2 lanes per row), so that both do the same FP32
     arithmetic and differ only in the grouping of FP64 sums."""
     b = BT.BatchSolver(0)
     for sc in scenes:
@@ -47,7 +47,7 @@ def _batch(gpu, scenes, precond=None, like_single=False):
         b.set_precond(precond)
     b.build()
     if like_single:
-        b.set_tuning(4, 1024)
+        b.set_tuning(2, 1024)
     return b
 
 
