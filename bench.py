@@ -1,8 +1,8 @@
 #!/usr/bin/env python
 """Benchmark of the cloth solver's Newton-step hot path on B200: drape settle time.
 
-One step = eight drapes of the seamed-tube workload to rest (its own start state and seven with every coordinate moved
-by a seeded uniform +-1 um), each run by the solver's drape runner (DrapeSession semantics,
+One step = sixteen drapes of the seamed-tube workload to rest (its own start state and fifteen with every coordinate
+moved by a seeded uniform +-1 um), each run by the solver's drape runner (DrapeSession semantics,
 libs/sim/src/drape_session.cpp:32-95: Assembling until the seams close, then Settling until the RMS speed stays below
 2 mm/s for 60 frames). The metric is the mean device time to settle one drape; PCG iterations per Newton step are
 reported beside it.
@@ -44,13 +44,13 @@ WORKLOADS = {
                     particles=10080),
 }
 SETTLE_FIXTURE = os.path.join(ROOT, "tests", "golden", "settle_frames.json")
-# Drapes per timed step: the workload's own start state and seven copies with every coordinate moved by a seeded
+# Drapes per timed step: the workload's own start state and fifteen copies with every coordinate moved by a seeded
 # uniform +-1 um. The settle frame count of one start state is a first-passage time of an RMS speed that hovers at the
-# 2 mm/s threshold for hundreds of frames (332-890 frames over these start states on the 60k tube), so one drape
+# 2 mm/s threshold for hundreds of frames (332-1110 frames over such start states on the 60k tube), so one drape
 # alone does not measure the solver.
-SEEDS = 8
-SEED_DESC = ("each step drapes 8 start states: the workload's own and 7 with every coordinate moved by uniform "
-             "+-1 um (numpy default_rng(seed), seeds 1-7); value and e2e are means over all of them")
+SEEDS = 16
+SEED_DESC = ("each step drapes 16 start states: the workload's own and 15 with every coordinate moved by uniform "
+             "+-1 um (numpy default_rng(seed), seeds 1-15); value and e2e are means over all of them")
 
 
 def seeded_positions(base32: np.ndarray, seed: int) -> np.ndarray:
@@ -398,7 +398,8 @@ def bake_leg(peak):
 def run_profile_case(args):
     """One small case for an ncu capture (not a benchmark line): "spmv" times the standalone SpMV on the tiled tube
     system; "batch" builds the first --batch-garments tubes of the batched workload and runs --batch-frames frames
-    (the first frame launches directly, the rest replay its CUDA graph); "bake" bakes the reference's test body."""
+    (the first frame launches directly, the rest replay its CUDA graph); "bake" bakes the reference's test body;
+    "drape" runs --batch-frames frames of the --workload drape (direct launches, from its own start state)."""
     import torch
     from drape_b200 import cuda as CU
     torch.cuda.set_device(0)
@@ -407,6 +408,15 @@ def run_profile_case(args):
         s = CU.CudaSolver(0)
         s.build(make_scene("tube60k"))
         print(json.dumps(spmv_leg(CU, s, peak, tiles=args.spmv_tiles)))
+        return 0
+    if args.profile_case == "drape":
+        s = CU.CudaSolver(0)
+        s.build(make_scene(args.workload))
+        for _ in range(args.batch_frames):
+            s.step(1.0 / 60.0, 1, 2)
+        c = s.counters()
+        print(json.dumps({"case": "drape", "workload": args.workload, "frames": args.batch_frames,
+                          "newton_iterations": int(c.newton_iterations), "cg_iterations": int(c.cg_iterations)}))
         return 0
     if args.profile_case == "bake":
         from drape_b200 import bake as BK
@@ -441,7 +451,7 @@ def cpu_baseline(workload: str):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="tube60k")
@@ -449,7 +459,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=1, help="end-to-end steps (0: same as --steps)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner leg")
     ap.add_argument("--batch-garments", type=int, default=64, help="garments of the batched leg (0: skip it)")
-    ap.add_argument("--profile-case", choices=["spmv", "batch", "bake"], default=None,
+    ap.add_argument("--profile-case", choices=["spmv", "batch", "bake", "drape"], default=None,
                     help="run one small case for a profiler capture instead of the benchmark")
     ap.add_argument("--spmv-tiles", type=int, default=12)
     ap.add_argument("--batch-frames", type=int, default=6)
@@ -599,7 +609,7 @@ def main():
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e_value, "unit": "s", "h2d_bytes_per_step": int(sum(h2d) / e2e_steps),
                 "d2h_bytes_per_step": int(sum(d2h) / e2e_steps), "drapes": len(e2e_times),
-                "note": "mean seconds per drape; bytes per step of 8 drapes"},
+                "note": "mean seconds per drape; bytes per step of 16 drapes"},
         "roofline": roofline,
         "clocks": clocks,
         "gpu_launches": int(sum(prof["launches"].values())),

@@ -185,6 +185,21 @@ __global__ void k_points(View V, int substep) {
   if (Kind == 2) dcu::finishRows(sD, rank, size);
 }
 
+// Per-term derivative records of every advancing garment (dcu::termsRows), on the assembly partition.
+__global__ void __launch_bounds__(dcu::kAssembleWarps * dcu::kWarp) k_terms_batch(View V) {
+  __shared__ dcu::Dev sD;
+  __shared__ uint32_t g, rank, size;
+  if (threadIdx.x == 0) {
+    g = segmentOf(V.asmStart, V.G, blockIdx.x);
+    rank = blockIdx.x - V.asmStart[g];
+    size = V.asmStart[g + 1] - V.asmStart[g];
+  }
+  __syncthreads();
+  if (V.segs[g].ctl->newtonDone) return;
+  loadSegment(V, g, sD);
+  dcu::termsRows(sD, rank, size);
+}
+
 __global__ void __launch_bounds__(dcu::kAssembleWarps * dcu::kWarp) k_assemble_batch(View V) {
   __shared__ dcu::Dev sD;
   __shared__ uint32_t g, rank, size;
@@ -456,6 +471,7 @@ struct drape_batch {
   DBuf<float> fieldValues, blocks, snapGap;
   DBuf<float4> x, v, xStart, yRel, u, grad, step, r, z, p0, p1, ap, apFull, resid, fExt, pinPos, precond;
   DBuf<float4> snapX, snapV, saveX, saveV;
+  DBuf<float4> stretchDer, hingeDer;  // per-term derivative records (6 and 4 float4 per term)
   DBuf<dcu::Contact> contact, snapC, saveC;
   DBuf<double> partials;
   DBuf<dcu::Control> ctl;
@@ -630,6 +646,8 @@ struct drape_batch {
                               &fExt, &pinPos, &snapX, &snapV, &saveX, &saveV})
       buf->alloc(N);
     precond.alloc(static_cast<size_t>(N) * 3);
+    stretchDer.alloc(std::max<size_t>(1, 6ull * t));
+    hingeDer.alloc(std::max<size_t>(1, 4ull * h));
     for (DBuf<dcu::Contact>* buf : {&contact, &snapC, &saveC}) buf->alloc(N);
     x.upload(hx, s);
     v.upload(hv, s);
@@ -675,6 +693,8 @@ struct drape_batch {
       d.garment = garment.p + g;
       d.stretch = stretch.p + tBase[g];
       d.hinge = hinge.p + hBase[g];
+      d.stretchDer = stretchDer.p + 6ull * tBase[g];
+      d.hingeDer = hingeDer.p + 4ull * hBase[g];
       d.seam = seam.p + kBase[g];
       d.rowStart = rowStart.p + rBase[g];
       d.colIndex = colIndex.p + sBase[g];
@@ -873,8 +893,9 @@ struct drape_batch {
       ++launches;
       for (int it = 0; it < iterations; ++it) {
         bcu::k_points<1><<<pointGrid, kPointThreads, 0, stream>>>(view, s);
+        bcu::k_terms_batch<<<asmGrid, dcu::kAssembleWarps * dcu::kWarp, 0, stream>>>(view);
         bcu::k_assemble_batch<<<asmGrid, dcu::kAssembleWarps * dcu::kWarp, dcu::kAssembleSmem, stream>>>(view);
-        launches += 2;
+        launches += 3;
         if (learnedOn && netGraph) {
           net->forwardOn(net->graphOf(*netGraph), stream, false, &ctl.p->error);
           launches += 8;

@@ -124,32 +124,34 @@ __device__ __forceinline__ float coef(float4 d, int column, int k) {
 
 // Stretch term (warp |f_u| - 1, weft |f_v| - 1, bias n_u . n_v, each 1/2 K C^2 with K = k area; tension stiffness
 // for C > 0 and the one-sided strain limit at limitScale K; energies.cpp:27-62, stretch.hpp:15-49) at x[0..2]
-// (relative to vertex 0): gradient of vertex a and Hessian row a.
-__device__ inline void stretchRow(const StretchIn& t, const float3 x[3], int a, float3& g, M3 H[3]) {
-  g = mk(0, 0, 0);
-#pragma unroll
-  for (int b = 0; b < 3; ++b) zero(H[b]);
+// (relative to vertex 0), in two parts: stretchDerivs evaluates the term once and keeps what every vertex's row needs
+// (per direction the unit vector n = f / |f| and the gradient, Gauss-Newton and tension scales; for the bias the
+// derivatives of n_u . n_v with respect to f_u and f_v and its scales), and stretchRowFrom forms the gradient of
+// vertex a and its Hessian row from that record and the term's dmInv coefficients.
+struct StretchDer {
+  float4 w[6];  // warp: (n, gs), (hs, ts, flags, -); weft: (n, gs), (hs, ts, -, -); bias: (dfu, K c), (dfv, K)
+};
+constexpr uint32_t kStretchWarp = 1u, kStretchWeft = 2u, kStretchBias = 4u;  // flags: parts that contribute
+
+__device__ inline void stretchDerivs(const StretchIn& t, const float3 x[3], StretchDer& o) {
   const float3 e1 = x[1] - x[0], e2 = x[2] - x[0];
   const float3 fu = e1 * t.d.x + e2 * t.d.y;
   const float3 fv = e1 * t.d.z + e2 * t.d.w;
   const float lu = len(fu), lv = len(fv);
   const float tiny = 1e-12f;
+  uint32_t flags = 0;
 #pragma unroll
   for (int which = 0; which < 2; ++which) {
+    o.w[2 * which] = make_float4(0, 0, 0, 0);
+    o.w[2 * which + 1] = make_float4(0, 0, 0, 0);
     if (!(t.k[which] > 0.0f)) continue;
     const float3 f = which == 0 ? fu : fv;
     const float l = which == 0 ? lu : lv;
-    if (!(l > tiny)) {
-      // C = 0 and a zero gradient: only the (zero) Gauss-Newton term, nothing to add.
-      continue;
-    }
+    if (!(l > tiny)) continue;  // C = 0 and a zero gradient: nothing to add
     const float3 n = div(f, l);
     const float C = l - 1.0f;
     const float K = t.k[which] * t.area;
-    float3 gr[3];
-#pragma unroll
-    for (int b = 0; b < 3; ++b) gr[b] = n * coef(t.d, which, b);
-    float gs = K * C, hs = K;  // gradient and Gauss-Newton scales
+    float gs = K * C, hs = K;                // gradient and Gauss-Newton scales
     float ts = C > 0.0f ? K * C / l : 0.0f;  // tension scale (addTension with |f| >= 1e-12)
     if (t.limit[which] > 0.0f && C > t.limit[which]) {
       const float KL = t.limitScale * K, ex = C - t.limit[which];
@@ -157,24 +159,53 @@ __device__ inline void stretchRow(const StretchIn& t, const float3 x[3], int a, 
       hs += KL;
       if (ex > 0.0f) ts += KL * ex / l;
     }
-    g += gr[a] * gs;
-    const float ca = coef(t.d, which, a);
-#pragma unroll
-    for (int b = 0; b < 3; ++b) {
-      addOuter(H[b], hs, gr[a], gr[b]);
-      if (ts != 0.0f) addProjector(H[b], ts * ca * coef(t.d, which, b), n);
-    }
+    o.w[2 * which] = f4(n, gs);
+    o.w[2 * which + 1] = make_float4(hs, ts, 0.0f, 0.0f);
+    flags |= which == 0 ? kStretchWarp : kStretchWeft;
   }
+  o.w[4] = make_float4(0, 0, 0, 0);
+  o.w[5] = make_float4(0, 0, 0, 0);
   if (t.k[2] > 0.0f && lu > tiny && lv > tiny) {
     const float3 nu = div(fu, lu), nv = div(fv, lv);
     const float c = dot(nu, nv);
     const float3 dfu = div(nv - nu * c, lu);
     const float3 dfv = div(nu - nv * c, lv);
     const float K = t.k[2] * t.area;
+    o.w[4] = f4(dfu, K * c);
+    o.w[5] = f4(dfv, K);
+    flags |= kStretchBias;
+  }
+  o.w[1].z = __uint_as_float(flags);
+}
+
+__device__ inline void stretchRowFrom(float4 d, const StretchDer& o, int a, float3& g, M3 H[3]) {
+  g = mk(0, 0, 0);
+#pragma unroll
+  for (int b = 0; b < 3; ++b) zero(H[b]);
+  const uint32_t flags = __float_as_uint(o.w[1].z);
+#pragma unroll
+  for (int which = 0; which < 2; ++which) {
+    if (!(flags & (which == 0 ? kStretchWarp : kStretchWeft))) continue;
+    const float3 n = xyz(o.w[2 * which]);
+    const float gs = o.w[2 * which].w, hs = o.w[2 * which + 1].x, ts = o.w[2 * which + 1].y;
     float3 gr[3];
 #pragma unroll
-    for (int b = 0; b < 3; ++b) gr[b] = dfu * coef(t.d, 0, b) + dfv * coef(t.d, 1, b);
-    g += gr[a] * (K * c);
+    for (int b = 0; b < 3; ++b) gr[b] = n * coef(d, which, b);
+    g += gr[a] * gs;
+    const float ca = coef(d, which, a);
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      addOuter(H[b], hs, gr[a], gr[b]);
+      if (ts != 0.0f) addProjector(H[b], ts * ca * coef(d, which, b), n);
+    }
+  }
+  if (flags & kStretchBias) {
+    const float3 dfu = xyz(o.w[4]), dfv = xyz(o.w[5]);
+    const float Kc = o.w[4].w, K = o.w[5].w;
+    float3 gr[3];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) gr[b] = dfu * coef(d, 0, b) + dfv * coef(d, 1, b);
+    g += gr[a] * Kc;
 #pragma unroll
     for (int b = 0; b < 3; ++b) addOuter(H[b], K, gr[a], gr[b]);
   }
@@ -203,12 +234,28 @@ __device__ inline float dihedral(const float3 x[4], float3 g[4]) {
   return theta;
 }
 
-// Hinge term 1/2 K (theta - theta0)^2 with a Gauss-Newton Hessian (energies.cpp:64-69): row a.
-__device__ inline void hingeRow(float K, float rest, const float3 x[4], int a, float3& g, M3 H[4]) {
+// Hinge term 1/2 K (theta - theta0)^2 with a Gauss-Newton Hessian (energies.cpp:64-69), in two parts: hingeDerivs
+// evaluates theta and its gradient once per term, hingeRowFrom forms vertex a's gradient and Hessian row.
+struct HingeDer {
+  float4 w[4];  // gradient of theta at vertex k (xyz); w[0].w = K (theta - rest), w[1].w = K
+};
+
+__device__ inline void hingeDerivs(float K, float rest, const float3 x[4], HingeDer& o) {
   float3 gr[4];
   const float theta = dihedral(x, gr);
   const float C = theta - rest;
-  g = gr[a] * (K * C);
+  o.w[0] = f4(gr[0], K * C);
+  o.w[1] = f4(gr[1], K);
+  o.w[2] = f4(gr[2]);
+  o.w[3] = f4(gr[3]);
+}
+
+__device__ inline void hingeRowFrom(const HingeDer& o, int a, float3& g, M3 H[4]) {
+  float3 gr[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) gr[k] = xyz(o.w[k]);
+  const float KC = o.w[0].w, K = o.w[1].w;
+  g = gr[a] * KC;
 #pragma unroll
   for (int b = 0; b < 4; ++b) {
     zero(H[b]);

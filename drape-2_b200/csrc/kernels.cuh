@@ -115,6 +115,8 @@ struct Dev {
   const uint32_t* incEntry;
   const uint32_t* incLocal;
   float4 *x, *v, *xStart, *yRel, *u, *grad, *step, *r, *z, *p0, *p1, *ap, *apFull, *resid;
+  float4* stretchDer;      // per stretch term: its StretchDer record (6 float4), written by termsRows
+  float4* hingeDer;        // per hinge term: its HingeDer record (4 float4)
   const float* Lf;         // learned factor L: 9 planes of slotsPadded floats on lower slots (k_solve<true>)
   const uint32_t* tslot;   // slot of (j, i) for slot (i, j)
   const float4* fExt;
@@ -404,23 +406,51 @@ __device__ inline StretchIn stretchIn(const Dev& D, const Stretch& t) {
   return s;
 }
 
-// Evaluates incidence entry `code` for its vertex a: gradient g, Hessian row H[0..N-1]; returns N.
+// Per-term derivative records of one Newton iteration (every stretch and hinge term evaluated once, one thread per
+// term); the assembly then forms each incident row from them.
+__device__ inline void termsRows(const Dev& D, uint32_t rank, uint32_t size) {
+  if (D.ctl->newtonDone) return;
+  const uint32_t S = D.P.nStretch, total = S + D.P.nHinge;
+  for (uint32_t idx = rank * blockDim.x + threadIdx.x; idx < total; idx += size * blockDim.x) {
+    if (idx < S) {
+      const Stretch t = D.stretch[idx];
+      float3 x[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) x[k] = relPos(D, t.v[0], t.v[k]);
+      StretchDer o;
+      stretchDerivs(stretchIn(D, t), x, o);
+#pragma unroll
+      for (int k = 0; k < 6; ++k) D.stretchDer[6ull * idx + k] = o.w[k];
+    } else {
+      const uint32_t h = idx - S;
+      const Hinge t = D.hinge[h];
+      float3 x[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) x[k] = relPos(D, t.v[0], t.v[k]);
+      HingeDer o;
+      hingeDerivs(t.K, t.rest, x, o);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) D.hingeDer[4ull * h + k] = o.w[k];
+    }
+  }
+}
+
+// Incidence entry `code` for its vertex a: gradient g, Hessian row H[0..N-1] from the term's record (seam springs,
+// a few hundred per garment, are evaluated here); returns N.
 __device__ inline int evalEntry(const Dev& D, uint32_t code, float3& g, M3 H[4]) {
   const uint32_t kind = code >> 30, term = (code >> 2) & 0x0FFFFFFFu, a = code & 3u;
   if (kind == 0) {
-    const Stretch t = D.stretch[term];
-    float3 x[3];
+    StretchDer o;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) x[k] = relPos(D, t.v[0], t.v[k]);
-    stretchRow(stretchIn(D, t), x, static_cast<int>(a), g, H);
+    for (int k = 0; k < 6; ++k) o.w[k] = D.stretchDer[6ull * term + k];
+    stretchRowFrom(D.stretch[term].d, o, static_cast<int>(a), g, H);
     return 3;
   }
   if (kind == 1) {
-    const Hinge t = D.hinge[term];
-    float3 x[4];
+    HingeDer o;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) x[k] = relPos(D, t.v[0], t.v[k]);
-    hingeRow(t.K, t.rest, x, static_cast<int>(a), g, H);
+    for (int k = 0; k < 4; ++k) o.w[k] = D.hingeDer[4ull * term + k];
+    hingeRowFrom(o, static_cast<int>(a), g, H);
     return 4;
   }
   const Seam s = D.seam[term];

@@ -57,7 +57,7 @@ struct drape_solver {
   std::string error;
   Model m;
   bool built = false;
-  int solveGrid = 0, pointGrid = 0, assembleGrid = 0, statsGrid = 0;
+  int solveGrid = 0, pointGrid = 0, assembleGrid = 0, termsGrid = 0, statsGrid = 0;
   unsigned long long barrierLimitNs = 2000000000ull;  // 2 s
   int failAfter = -1;
   uint32_t solveSmemCap = 0;       // block slots one solve block can keep in shared memory
@@ -79,6 +79,7 @@ struct drape_solver {
   DBuf<uint32_t> rowStart, colIndex, diagSlot, incStart, incEntry, incLocal;
   DBuf<float> fieldValues, blocks;
   DBuf<float4> x, v, xStart, yRel, u, grad, step, r, z, p0, p1, ap, apFull, resid, fExt, pinPos, precond;
+  DBuf<float4> stretchDer, hingeDer;
   DBuf<dcu::Contact> contact;
   DBuf<double> partials, statsPartials;
   DBuf<dcu::Control> ctl;
@@ -233,6 +234,8 @@ struct drape_solver {
     for (DBuf<float4>* b : {&x, &v, &xStart, &yRel, &u, &grad, &step, &r, &z, &p0, &p1, &ap, &apFull, &resid, &fExt, &pinPos})
       b->alloc(n);
     precond.alloc(static_cast<size_t>(n) * 3);
+    stretchDer.alloc(std::max<size_t>(1, 6 * m.stretch.size()));
+    hingeDer.alloc(std::max<size_t>(1, 4 * m.hinges.size()));
     contact.alloc(n);
     {
       std::vector<float4> xs, vs, fe, pp;
@@ -276,6 +279,8 @@ struct drape_solver {
     d.ap = ap.p;
     d.apFull = apFull.p;
     d.resid = resid.p;
+    d.stretchDer = stretchDer.p;
+    d.hingeDer = hingeDer.p;
     d.fExt = fExt.p;
     d.pinPos = pinPos.p;
     d.blocks = blocks.p;
@@ -289,6 +294,9 @@ struct drape_solver {
     if (learnedOn) bindNet();
     assembleGrid = static_cast<int>(std::max<uint32_t>(1, std::min<uint32_t>((n + dcu::kAssembleWarps - 1) / dcu::kAssembleWarps,
                                                                            static_cast<uint32_t>(numSMs) * 16)));
+    const size_t terms = m.stretch.size() + m.hinges.size();
+    termsGrid = static_cast<int>(std::max<size_t>(1, std::min<size_t>((terms + dcu::kTermThreads - 1) / dcu::kTermThreads,
+                                                                      static_cast<size_t>(numSMs) * 16)));
     CK(cudaStreamSynchronize(s));
     built = true;
   }
@@ -410,6 +418,9 @@ struct drape_solver {
       e = profStart();
       dcu::k_activate<<<pg, 256, 0, stream>>>(d);
       profStop(e, 1);
+      e = profStart();
+      dcu::k_terms<<<termsGrid, dcu::kTermThreads, 0, stream>>>(d);
+      profStop(e, 2);
       e = profStart();
       dcu::k_assemble<<<assembleGrid, dcu::kAssembleWarps * dcu::kWarp, dcu::kAssembleSmem, stream>>>(d);
       CK(cudaGetLastError());
@@ -1135,6 +1146,7 @@ int drape_cuda_capture_system(drape_solver* s, double h, float* blocks, float* g
     const int pg = std::max<int>(1, static_cast<int>((n + 255) / 256));
     dcu::k_begin<<<pg, 256, 0, s->stream>>>(d);
     dcu::k_activate<<<pg, 256, 0, s->stream>>>(d);
+    dcu::k_terms<<<s->termsGrid, dcu::kTermThreads, 0, s->stream>>>(d);
     dcu::k_assemble<<<s->assembleGrid, dcu::kAssembleWarps * dcu::kWarp, dcu::kAssembleSmem, s->stream>>>(d);
     CK(cudaGetLastError());
     const size_t B = s->m.colIndex.size(), SP = s->dev.P.slotsPadded;

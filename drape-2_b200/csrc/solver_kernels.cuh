@@ -19,6 +19,10 @@ __global__ void k_contact_candidates(Dev D, const float4* xs, Contact* out) {
 
 __global__ void k_activate(Dev D) { activateRows(D, blockIdx.x, gridDim.x); }
 
+constexpr int kTermThreads = 256;  // k_terms block size
+
+__global__ void __launch_bounds__(kTermThreads) k_terms(Dev D) { termsRows(D, blockIdx.x, gridDim.x); }
+
 __global__ void __launch_bounds__(kAssembleWarps * kWarp) k_assemble(Dev D) {
   assembleRows(D, blockIdx.x, gridDim.x);
 }
