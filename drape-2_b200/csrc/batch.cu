@@ -186,7 +186,7 @@ __global__ void k_points(View V, int substep) {
 }
 
 // Per-term derivative records of every advancing garment (dcu::termsRows), on the assembly partition.
-__global__ void __launch_bounds__(dcu::kAssembleWarps * dcu::kWarp) k_terms_batch(View V) {
+__global__ void __launch_bounds__(dcu::kAssembleThreads) k_terms_batch(View V) {
   __shared__ dcu::Dev sD;
   __shared__ uint32_t g, rank, size;
   if (threadIdx.x == 0) {
@@ -200,7 +200,7 @@ __global__ void __launch_bounds__(dcu::kAssembleWarps * dcu::kWarp) k_terms_batc
   dcu::termsRows(sD, rank, size);
 }
 
-__global__ void __launch_bounds__(dcu::kAssembleWarps * dcu::kWarp) k_assemble_batch(View V) {
+__global__ void __launch_bounds__(dcu::kAssembleThreads) k_assemble_batch(View V) {
   __shared__ dcu::Dev sD;
   __shared__ uint32_t g, rank, size;
   if (threadIdx.x == 0) {
@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(dcu::kAssembleWarps * dcu::kWarp) k_assemble_b
   __syncthreads();
   if (V.segs[g].ctl->newtonDone) return;
   loadSegment(V, g, sD);
-  dcu::assembleRows(sD, rank, size);
+  dcu::assembleSlots(sD, rank, size);
 }
 
 // One Newton iteration's solve for every advancing garment: the blocks of garment g form its group.
@@ -360,7 +360,6 @@ thread_local std::string g_batchError;
 
 constexpr int kPointThreads = 256;
 constexpr int kPointRowsPerBlock = 1024;  // rows per point-kernel block (grid-stride within the garment's share)
-constexpr int kAssembleRowsPerWarp = 4;
 
 using SolveKernel = void (*)(bcu::View);
 
@@ -466,7 +465,7 @@ struct drape_batch {
   DBuf<dcu::Stretch> stretch;
   DBuf<dcu::Hinge> hinge;
   DBuf<dcu::Seam> seam, saveSeam;
-  DBuf<uint32_t> rowStart, colIndex, diagSlot, incStart, incEntry, incLocal, tslot;
+  DBuf<uint32_t> rowStart, colIndex, diagSlot, incStart, incEntry, incLocal, slotRow, tslot;
   DBuf<uint32_t> starts, bases;  // point and assembly prefixes; pBase and kBase
   DBuf<float> fieldValues, blocks, snapGap;
   DBuf<float4> x, v, xStart, yRel, u, grad, step, r, z, p0, p1, ap, apFull, resid, fExt, pinPos, precond;
@@ -518,8 +517,6 @@ struct drape_batch {
     if (!prop.cooperativeLaunch) throw std::runtime_error("cuda: device does not support cooperative launch");
     numSMs = prop.multiProcessorCount;
     BCK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-    BCK(cudaFuncSetAttribute(bcu::k_assemble_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(dcu::kAssembleSmem)));
     hStats.alloc(1);
     hCtl.alloc(1);
   }
@@ -598,7 +595,7 @@ struct drape_batch {
     std::vector<dcu::Stretch> hs;
     std::vector<dcu::Hinge> hh;
     std::vector<dcu::Seam> hk;
-    std::vector<uint32_t> hrs, hci, hds, his, hie, hil, hts;
+    std::vector<uint32_t> hrs, hci, hds, his, hie, hil, hsr, hts;
     std::vector<float> hfv;
     std::vector<float4> hx, hv, hfe, hpp;
     for (uint32_t g = 0; g < G; ++g) {
@@ -617,6 +614,7 @@ struct drape_batch {
       append(his, m.incStart);
       append(hie, m.incEntry);
       append(hil, m.incLocal);
+      append(hsr, m.slotRow);
       append(hts, net::transposedSlots(m.rowStart, cols));
       if (m.fieldValues.empty()) hfv.push_back(0.0f); else append(hfv, m.fieldValues);
       std::vector<float4> xs, vs, fe, pp;
@@ -639,6 +637,7 @@ struct drape_batch {
     incStart.upload(his, s);
     incEntry.upload(hie, s);
     incLocal.upload(hil, s);
+    slotRow.upload(hsr, s);
     tslot.upload(hts, s);
     fieldValues.upload(hfv, s);
     blocks.alloc(static_cast<size_t>(SP) * 9);
@@ -667,8 +666,8 @@ struct drape_batch {
     for (uint32_t g = 0; g < G; ++g) {
       const uint32_t ng = static_cast<uint32_t>(models[g].x.size());
       pointCount[g] = std::max<uint32_t>(1, (ng + kPointRowsPerBlock - 1) / kPointRowsPerBlock);
-      asmCount[g] = std::max<uint32_t>(1, (ng + dcu::kAssembleWarps * kAssembleRowsPerWarp - 1) /
-                                              (dcu::kAssembleWarps * kAssembleRowsPerWarp));
+      const uint32_t bg = static_cast<uint32_t>(models[g].colIndex.size());
+      asmCount[g] = std::max<uint32_t>(1, (bg + dcu::kAssembleThreads - 1) / dcu::kAssembleThreads);
     }
     const auto pStart = prefix(pointCount), aStart = prefix(asmCount);
     statsPart.alloc(8ull * pStart[G]);
@@ -702,6 +701,7 @@ struct drape_batch {
       d.incStart = incStart.p + rBase[g];
       d.incEntry = incEntry.p + eBase[g];
       d.incLocal = incLocal.p + eBase[g];
+      d.slotRow = slotRow.p + sBase[g];
       for (auto [dst, src] : {std::pair<float4**, float4*>{&d.x, x.p}, {&d.v, v.p}, {&d.xStart, xStart.p},
                               {&d.yRel, yRel.p}, {&d.u, u.p}, {&d.grad, grad.p}, {&d.step, step.p}, {&d.r, r.p},
                               {&d.z, z.p}, {&d.p0, p0.p}, {&d.p1, p1.p}, {&d.ap, ap.p}, {&d.apFull, apFull.p},
@@ -893,8 +893,8 @@ struct drape_batch {
       ++launches;
       for (int it = 0; it < iterations; ++it) {
         bcu::k_points<1><<<pointGrid, kPointThreads, 0, stream>>>(view, s);
-        bcu::k_terms_batch<<<asmGrid, dcu::kAssembleWarps * dcu::kWarp, 0, stream>>>(view);
-        bcu::k_assemble_batch<<<asmGrid, dcu::kAssembleWarps * dcu::kWarp, dcu::kAssembleSmem, stream>>>(view);
+        bcu::k_terms_batch<<<asmGrid, dcu::kAssembleThreads, 0, stream>>>(view);
+        bcu::k_assemble_batch<<<asmGrid, dcu::kAssembleThreads, 0, stream>>>(view);
         launches += 3;
         if (learnedOn && netGraph) {
           net->forwardOn(net->graphOf(*netGraph), stream, false, &ctl.p->error);

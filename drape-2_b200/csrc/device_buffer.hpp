@@ -42,10 +42,13 @@ struct DBuf {
   }
   // The zeroing runs on the legacy default stream, which is not ordered with the handles' non-blocking streams: wait
   // for it here, or it could land after the uploads and kernels that follow.
+  // An allocation of the same size is reused (a rebuild of the same scene allocates nothing).
   void alloc(size_t count) {
-    release();
-    n = count;
-    check(cudaMalloc(&p, sizeof(T) * std::max<size_t>(count, 1)), "cudaMalloc");
+    if (!p || count != n) {
+      release();
+      check(cudaMalloc(&p, sizeof(T) * std::max<size_t>(count, 1)), "cudaMalloc");
+      n = count;
+    }
     check(cudaMemset(p, 0, sizeof(T) * std::max<size_t>(count, 1)), "cudaMemset");
     check(cudaStreamSynchronize(nullptr), "cudaStreamSynchronize(legacy stream)");
   }

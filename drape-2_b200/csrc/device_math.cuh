@@ -211,6 +211,36 @@ __device__ inline void stretchRowFrom(float4 d, const StretchDer& o, int a, floa
   }
 }
 
+// Block (a, b) of a stretch term's Hessian and the gradient of vertex a, read from the term's record in global memory:
+// the operations stretchRowFrom performs for H[b] of row a and for its g, in the same order.
+__device__ inline void stretchBlockFrom(float4 d, const float4* __restrict__ rec, int a, int b, float3& g, M3& H) {
+  zero(H);
+  g = mk(0, 0, 0);
+  const float4 w1 = rec[1];
+  const uint32_t flags = __float_as_uint(w1.z);
+#pragma unroll
+  for (int which = 0; which < 2; ++which) {
+    if (!(flags & (which == 0 ? kStretchWarp : kStretchWeft))) continue;
+    const float4 wn = rec[2 * which];
+    const float4 ws = which == 0 ? w1 : rec[3];
+    const float3 n = xyz(wn);
+    const float gs = wn.w, hs = ws.x, ts = ws.y;
+    const float ca = coef(d, which, a), cb = coef(d, which, b);
+    const float3 gra = n * ca, grb = n * cb;
+    g += gra * gs;
+    addOuter(H, hs, gra, grb);
+    if (ts != 0.0f) addProjector(H, ts * ca * cb, n);
+  }
+  if (flags & kStretchBias) {
+    const float4 w4 = rec[4], w5 = rec[5];
+    const float3 dfu = xyz(w4), dfv = xyz(w5);
+    const float3 gra = dfu * coef(d, 0, a) + dfv * coef(d, 1, a);
+    const float3 grb = dfu * coef(d, 0, b) + dfv * coef(d, 1, b);
+    g += gra * w4.w;
+    addOuter(H, w5.w, gra, grb);
+  }
+}
+
 // Dihedral angle theta = atan2((n1 x n2) . e, n1 . n2) and its gradient (Bridson, Marino & Fedkiw 2003, sign as in
 // bending.hpp:29-51).
 __device__ inline float dihedral(const float3 x[4], float3 g[4]) {
@@ -261,6 +291,15 @@ __device__ inline void hingeRowFrom(const HingeDer& o, int a, float3& g, M3 H[4]
     zero(H[b]);
     addOuter(H[b], K, gr[a], gr[b]);
   }
+}
+
+// Block (a, b) of a hinge term's Hessian and the gradient of vertex a from its record (hingeRowFrom's operations).
+__device__ inline void hingeBlockFrom(const float4* __restrict__ rec, int a, int b, float3& g, M3& H) {
+  const float4 wa = rec[a], wb = rec[b];
+  const float KC = rec[0].w, K = rec[1].w;
+  g = xyz(wa) * KC;
+  zero(H);
+  addOuter(H, K, xyz(wa), xyz(wb));
 }
 
 // One-sided seam spring 1/2 K (d - target)^2 for d > target (energies.cpp:71-91): row a of the 2 x 2 block system.

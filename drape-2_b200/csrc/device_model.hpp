@@ -123,7 +123,7 @@ inline void params(const Model& m, uint32_t slotsPadded, unsigned long long barr
   P.nGarments = static_cast<uint32_t>(m.garments.size());
   P.slotsPadded = slotsPadded;
   P.barrierLimitNs = barrierLimitNs;
-  d.field.present = !m.fieldValues.empty() ? 1 : 0;
+  d.field.present = m.fieldCount > 0 ? 1 : 0;
   d.field.ox = static_cast<float>(m.field.origin[0]);
   d.field.oy = static_cast<float>(m.field.origin[1]);
   d.field.oz = static_cast<float>(m.field.origin[2]);

@@ -6,8 +6,10 @@
 // libs/sim/kernels/kernels.h:30-448). Per Newton iteration this file runs three launches instead of the reference's
 // ~40 + 13 per CG iteration dispatches with host round trips (gpu_solver_core.cpp:325-407):
 //   k_activate   contact activation (kernels.h:85-99)
-//   k_assemble   gradient, 3x3 block Hessian, block-Jacobi inverse and contact release, computed by the owner of each
-//                block row from its incident terms (replaces term kernels + gather, kernels.h:104-231)
+//   k_terms      every stretch and hinge term evaluated once into a derivative record (kernels.h:137-176)
+//   k_assemble   each 3x3 Hessian block summed by the thread that owns its slot from the records of the row's incident
+//                terms; the diagonal slot's thread adds the gradient, block-Jacobi inverse and contact release
+//                (replaces the contribution buffers + gather, kernels.h:104-231)
 //   k_solve      one cooperative persistent launch: PCG (kernels.h:237-347), contact force, FP64 Newton slope, FP64
 //                line search and step application (cpu_solver.cpp:264-283) with device-side decisions.
 #pragma once
@@ -20,13 +22,12 @@
 namespace dcu {
 
 constexpr int kWarp = 32;
-constexpr int kAssembleWarps = 8;   // warps per k_assemble block
+constexpr int kAssembleThreads = 256;  // k_assemble block size (one thread per block slot)
 constexpr int kRowLanes = 2;        // lanes per block row in the single solver's SpMV
 constexpr int kSolveThreads = 1024; // k_solve block size (one block per SM)
 constexpr uint32_t kPinnedBit = 0x80000000u;
 constexpr uint32_t kSmemSlotBytes = 40;      // one block slot in shared memory: 9 floats + a column index
 constexpr int kPartialStride = 4;   // doubles per block in the partials array
-constexpr uint32_t kMaxRowSlots = 64;  // block slots per row the assembly kernel accumulates (checked at build)
 
 struct Particle {
   float mass;
@@ -114,6 +115,7 @@ struct Dev {
   const uint32_t* incStart;
   const uint32_t* incEntry;
   const uint32_t* incLocal;
+  const uint32_t* slotRow;   // row of each block slot
   float4 *x, *v, *xStart, *yRel, *u, *grad, *step, *r, *z, *p0, *p1, *ap, *apFull, *resid;
   float4* stretchDer;      // per stretch term: its StretchDer record (6 float4), written by termsRows
   float4* hingeDer;        // per hinge term: its HingeDer record (4 float4)
@@ -374,19 +376,12 @@ __device__ inline void activateRows(const Dev& D, uint32_t rank, uint32_t size) 
 }
 
 // ---------------------------------------------------------------------------------------------------------------
-// Owner-computes assembly: one warp per block row i. Each lane evaluates one incident term (kind, id, local vertex a)
-// for vertex a only (its gradient and Hessian row) and stages the N blocks in shared memory with their row-local
-// slots. The warp then adds the staged blocks into the row's slot accumulators one entry at a time, in incidence-list
-// order, after the particle's own inertia and friction term: the reference's fixed gather order
-// (gpu_solver_core.cpp:184-224), deterministic and without atomics.
-
-struct AssembleWarp {
-  float blk[kWarp][4][9];        // staged Hessian-row blocks of up to 32 entries
-  float g[kWarp][3];             // staged gradient of vertex a
-  uint8_t tgt[kWarp][4];         // row-local slot of each staged block (0xFF: none)
-  float acc[kMaxRowSlots][9];    // the row's block accumulators
-};
-constexpr size_t kAssembleSmem = sizeof(AssembleWarp) * kAssembleWarps;
+// Assembly in two passes. termsRows evaluates every stretch and hinge term once into a derivative record;
+// assembleSlots then gives every block slot (i, j) one thread, which walks row i's incidence list (the reference's
+// fixed gather order, gpu_solver_core.cpp:184-224) and adds block (a, b) of each incident term that couples i (its
+// vertex a) with j (its vertex b), formed from the term's record. The diagonal slot's thread starts from the
+// particle's own inertia and friction term and also sums the row's gradient. Every slot's sum runs in the same order
+// as the reference's gather; deterministic, no atomics, no shared memory.
 
 __device__ inline float3 relPos(const Dev& D, uint32_t v0, uint32_t vk) {
   return (ld3(D.xStart, vk) - ld3(D.xStart, v0)) + ld3(D.u, vk);
@@ -435,134 +430,84 @@ __device__ inline void termsRows(const Dev& D, uint32_t rank, uint32_t size) {
   }
 }
 
-// Incidence entry `code` for its vertex a: gradient g, Hessian row H[0..N-1] from the term's record (seam springs,
-// a few hundred per garment, are evaluated here); returns N.
-__device__ inline int evalEntry(const Dev& D, uint32_t code, float3& g, M3 H[4]) {
-  const uint32_t kind = code >> 30, term = (code >> 2) & 0x0FFFFFFFu, a = code & 3u;
+// Block (a, b) of the term an incidence entry names, and the gradient of its vertex a (seam springs, a few hundred
+// per garment, are evaluated here; stretch and hinge terms come from their records).
+__device__ inline void entryBlock(const Dev& D, uint32_t code, int b, float3& g, M3& H) {
+  const uint32_t kind = code >> 30, term = (code >> 2) & 0x0FFFFFFFu;
+  const int a = static_cast<int>(code & 3u);
   if (kind == 0) {
-    StretchDer o;
-#pragma unroll
-    for (int k = 0; k < 6; ++k) o.w[k] = D.stretchDer[6ull * term + k];
-    stretchRowFrom(D.stretch[term].d, o, static_cast<int>(a), g, H);
-    return 3;
+    stretchBlockFrom(D.stretch[term].d, D.stretchDer + 6ull * term, a, b, g, H);
+  } else if (kind == 1) {
+    hingeBlockFrom(D.hingeDer + 4ull * term, a, b, g, H);
+  } else {
+    const Seam sp = D.seam[term];
+    M3 H2[2];
+    seamRow(D.P.seamStiffness, seamTarget(D, sp), ld3(D.u, sp.a), relPos(D, sp.a, sp.b), a, g, H2);
+    H = H2[b & 1];
   }
-  if (kind == 1) {
-    HingeDer o;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) o.w[k] = D.hingeDer[4ull * term + k];
-    hingeRowFrom(o, static_cast<int>(a), g, H);
-    return 4;
-  }
-  const Seam s = D.seam[term];
-  const float3 x0 = ld3(D.u, s.a);
-  const float3 x1 = relPos(D, s.a, s.b);
-  seamRow(D.P.seamStiffness, seamTarget(D, s), x0, x1, static_cast<int>(a), g, H);
-  return 2;
 }
 
-__device__ inline void assembleRows(const Dev& D, uint32_t rank, uint32_t size) {
+__device__ inline void assembleSlots(const Dev& D, uint32_t rank, uint32_t size) {
   if (D.ctl->newtonDone) return;
-  extern __shared__ __align__(16) unsigned char assembleSmem[];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  AssembleWarp& sh = reinterpret_cast<AssembleWarp*>(assembleSmem)[w];
-  const uint32_t warpsTotal = size * kAssembleWarps;
   const uint32_t SP = D.P.slotsPadded;
-  for (uint32_t i = rank * kAssembleWarps + w; i < D.P.n; i += warpsTotal) {
-    const uint32_t rs = D.rowStart[i], L = D.rowStart[i + 1] - rs;
-    const uint32_t diagLocal = D.diagSlot[i] - rs;
-    const Particle pa = D.particle[i];
-    const Contact c = D.contact[i];
-    // The particle's own term: inertia 1/2 (m/h^2)|u - yRel|^2 and friction (kernels.h:104-129).
-    float3 gOwn = mk(0, 0, 0);
-    M3 hOwn;
-    zero(hOwn);
-    if (pa.pinned == 0u) {
-      const float k = pa.mass * D.P.invH2;
-      gOwn = (ld3(D.u, i) - ld3(D.yRel, i)) * k;
-      hOwn.m[0] = hOwn.m[4] = hOwn.m[8] = k;
-    }
-    if (c.frictionLambda > 0.0f)
-      frictionRow(ld3(D.u, i), xyz(c.normal), D.fabric[pa.fabric].friction * c.frictionLambda,
-                  D.P.frictionSlip * D.P.h, gOwn, hOwn);
-    for (uint32_t k = lane; k < 9u * L; k += kWarp) (&sh.acc[0][0])[k] = 0.0f;
-    __syncwarp();
-    if (lane < 9) {
-      float own = 0.0f;
-#pragma unroll
-      for (int k = 0; k < 9; ++k)
-        if (k == lane) own = hOwn.m[k];
-      sh.acc[diagLocal][lane] = own;
-    }
-    // Lanes 27..29 accumulate the gradient components, starting with the own term.
-    float gAcc = lane == 27 ? gOwn.x : (lane == 28 ? gOwn.y : (lane == 29 ? gOwn.z : 0.0f));
-    const uint32_t es = D.incStart[i], ee = D.incStart[i + 1];
-    for (uint32_t base = es; base < ee; base += kWarp) {
-      const uint32_t cnt = min(static_cast<uint32_t>(kWarp), ee - base);
-      __syncwarp();
-      if (static_cast<uint32_t>(lane) < cnt) {
-        const uint32_t code = D.incEntry[base + lane];
-        const uint32_t local = D.incLocal[base + lane];
-        float3 g;
-        M3 H[4];
-        const int N = evalEntry(D, code, g, H);
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-          sh.tgt[lane][b] = b < N ? static_cast<uint8_t>((local >> (8 * b)) & 0xFFu) : 0xFFu;
-          if (b < N)
-#pragma unroll
-            for (int k = 0; k < 9; ++k) sh.blk[lane][b][k] = H[b].m[k];
-        }
-        sh.g[lane][0] = g.x;
-        sh.g[lane][1] = g.y;
-        sh.g[lane][2] = g.z;
+  for (uint32_t s = rank * blockDim.x + threadIdx.x; s < D.P.nBlocks; s += size * blockDim.x) {
+    const uint32_t i = D.slotRow[s];
+    const uint32_t rs = D.rowStart[i];
+    const bool diag = D.diagSlot[i] == s;
+    M3 acc;
+    zero(acc);
+    float3 gAcc = mk(0, 0, 0);
+    Particle pa{};
+    Contact c{};
+    if (diag) {
+      // The particle's own term: inertia 1/2 (m/h^2)|u - yRel|^2 and friction (kernels.h:104-129).
+      pa = D.particle[i];
+      c = D.contact[i];
+      if (pa.pinned == 0u) {
+        const float k = pa.mass * D.P.invH2;
+        gAcc = (ld3(D.u, i) - ld3(D.yRel, i)) * k;
+        acc.m[0] = acc.m[4] = acc.m[8] = k;
       }
-      __syncwarp();
-      // Entry by entry: lanes 0..26 add blocks 0..2 (block lane / 9, component lane % 9), lanes 0..8 then block 3;
-      // the N slots of one entry are distinct, so no two lanes of one step touch the same accumulator.
-      const int b0 = lane / 9, comp = lane - 9 * (lane / 9);
-      for (uint32_t e = 0; e < cnt; ++e) {
-        if (lane < 27) {
-          const uint32_t t = sh.tgt[e][b0];
-          if (t != 0xFFu) sh.acc[t][comp] += sh.blk[e][b0][comp];
-        } else if (lane < 30) {
-          gAcc += sh.g[e][lane - 27];
-        }
-        if (lane < 9) {
-          const uint32_t t = sh.tgt[e][3];
-          if (t != 0xFFu) sh.acc[t][lane] += sh.blk[e][3][lane];
-        }
-        __syncwarp();
-      }
+      if (c.frictionLambda > 0.0f)
+        frictionRow(ld3(D.u, i), xyz(c.normal), D.fabric[pa.fabric].friction * c.frictionLambda,
+                    D.P.frictionSlip * D.P.h, gAcc, acc);
     }
-    __syncwarp();
-    // Blocks out (coalesced planes).
-    for (uint32_t k = lane; k < L; k += kWarp)
+    // The entry touches this slot where one of its N packed row-local positions equals ours (the N positions of an
+    // entry are distinct; the unused high bytes are masked off).
+    const uint32_t mine = (s - rs) * 0x01010101u;
+    const uint32_t ee = D.incStart[i + 1];
+    for (uint32_t e = D.incStart[i]; e < ee; ++e) {
+      const uint32_t code = D.incEntry[e];
+      const uint32_t kind = code >> 30;
+      const uint32_t valid = kind == 1 ? 0xFFFFFFFFu : (kind == 0 ? 0x00FFFFFFu : 0x0000FFFFu);
+      const uint32_t hit = __vcmpeq4(D.incLocal[e], mine) & valid;
+      if (hit == 0u) continue;
+      float3 g;
+      M3 H;
+      entryBlock(D, code, (__ffs(hit) - 1) >> 3, g, H);
 #pragma unroll
-      for (int cc = 0; cc < 9; ++cc) D.blocks[cc * SP + rs + k] = sh.acc[k][cc];
-    const float gx = __shfl_sync(0xffffffffu, gAcc, 27);
-    const float gy = __shfl_sync(0xffffffffu, gAcc, 28);
-    const float gz = __shfl_sync(0xffffffffu, gAcc, 29);
-    if (lane == 0) {
+      for (int k = 0; k < 9; ++k) acc.m[k] += H.m[k];
+      gAcc += g;
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) D.blocks[k * SP + s] = acc.m[k];
+    if (diag) {
       // Block-Jacobi inverse of the diagonal block (kernels.h:237-249); zero for pinned particles.
       M3 inv;
       if (pa.pinned != 0u) {
         zero(inv);
       } else {
-        M3 A;
-#pragma unroll
-        for (int k = 0; k < 9; ++k) A.m[k] = sh.acc[diagLocal][k];
         bool ok = false;
-        inv = invertSpd(A, ok);
+        inv = invertSpd(acc, ok);
       }
       D.precond[3 * i + 0] = make_float4(inv.m[0], inv.m[1], inv.m[2], 0.0f);
       D.precond[3 * i + 1] = make_float4(inv.m[3], inv.m[4], inv.m[5], 0.0f);
       D.precond[3 * i + 2] = make_float4(inv.m[6], inv.m[7], inv.m[8], 0.0f);
       // Gradient (pinned rows zero) and contact release (kernels.h:204-231).
-      const float3 gi = pa.pinned != 0u ? mk(0, 0, 0) : mk(gx, gy, gz);
+      const float3 gi = pa.pinned != 0u ? mk(0, 0, 0) : gAcc;
       D.grad[i] = f4(gi);
       if (c.active != 0u && dot(gi, xyz(c.normal)) < 0.0f) D.contact[i].active = 0u;
     }
-    __syncwarp();
   }
 }
 

@@ -60,7 +60,7 @@ uint32_t Model::slot(uint32_t row, uint32_t col) const {
   return static_cast<uint32_t>(std::lower_bound(begin, end, col) - colIndex.begin());
 }
 
-Model Model::build(const drape_scene_desc& scene) {
+Model Model::build(const drape_scene_desc& scene, bool copyField) {
   Model next;
   next.settings = scene.settings;
   if (scene.body) {
@@ -71,7 +71,12 @@ Model Model::build(const drape_scene_desc& scene) {
     if (scene.body->values && count > 0) {
       if (scene.body->dims[0] < 2 || scene.body->dims[1] < 2 || scene.body->dims[2] < 2)
         throw std::invalid_argument("collision field needs at least 2 samples per axis");
-      next.fieldValues.assign(scene.body->values, scene.body->values + count);
+      next.fieldCount = static_cast<std::size_t>(count);
+      if (copyField) {
+        next.fieldValues.assign(scene.body->values, scene.body->values + count);
+      } else {
+        next.fieldSource = scene.body->values;
+      }
     }
     next.field.values = nullptr;
   }
@@ -111,6 +116,7 @@ Model Model::build(const drape_scene_desc& scene) {
       const double f0 = rest(c, 0) - rest(a, 0), f1 = rest(c, 1) - rest(a, 1);
       return 0.5 * std::abs(e0 * f1 - e1 * f0);
     };
+    next.stretch.reserve(next.stretch.size() + sg.triangle_count);
     // Stretch terms: rest shape in the piece's grain frame, dmInv = Dm^-1, area = |det Dm| / 2 (sim_model.cpp:107-123).
     for (uint32_t t = 0; t < sg.triangle_count; ++t) {
       const uint32_t piece = sg.triangle_piece[t];
@@ -135,15 +141,34 @@ Model Model::build(const drape_scene_desc& scene) {
       next.stretch.push_back(st);
     }
     // Edge occurrences in insertion order (triangle t, then k = 0, 1, 2), stably sorted by (min, max): the same
-    // sequence a std::map<pair<min,max>, vector<tri>> iterates.
-    std::vector<std::pair<uint64_t, uint32_t>> occ;
-    occ.reserve(3 * sg.triangle_count);
-    for (uint32_t t = 0; t < sg.triangle_count; ++t)
-      for (int k = 0; k < 3; ++k) occ.push_back({edgeKey(T[3 * t + k], T[3 * t + (k + 1) % 3]), t});
-    std::stable_sort(occ.begin(), occ.end(),
-                     [](const std::pair<uint64_t, uint32_t>& p, const std::pair<uint64_t, uint32_t>& q) {
-                       return p.first < q.first;
-                     });
+    // sequence a std::map<pair<min,max>, vector<tri>> iterates. Counting sort by the smaller vertex (stable), then a
+    // stable insertion sort of each vertex's few edges by the larger one.
+    std::vector<std::pair<uint64_t, uint32_t>> occ(3 * static_cast<std::size_t>(sg.triangle_count));
+    {
+      std::vector<uint32_t> start(sg.vertex_count + 1, 0);
+      for (uint32_t t = 0; t < sg.triangle_count; ++t)
+        for (int k = 0; k < 3; ++k) ++start[std::min(T[3 * t + k], T[3 * t + (k + 1) % 3]) + 1];
+      for (uint32_t v = 0; v < sg.vertex_count; ++v) start[v + 1] += start[v];
+      std::vector<uint32_t> fill(start.begin(), start.end() - 1);
+      for (uint32_t t = 0; t < sg.triangle_count; ++t)
+        for (int k = 0; k < 3; ++k) {
+          const uint64_t key = edgeKey(T[3 * t + k], T[3 * t + (k + 1) % 3]);
+          occ[fill[key >> 32]++] = {key, t};
+        }
+      for (uint32_t v = 0; v < sg.vertex_count; ++v)
+        for (uint32_t i = start[v] + 1; i < start[v + 1]; ++i) {
+          const auto item = occ[i];
+          uint32_t j = i;
+          for (; j > start[v] && occ[j - 1].first > item.first; --j) occ[j] = occ[j - 1];
+          occ[j] = item;
+        }
+    }
+    {
+      const std::size_t more = occ.size() / 2 + sg.seam_pair_count;
+      next.hinges.reserve(next.hinges.size() + more);
+      next.hingeSides.reserve(next.hingeSides.size() + more);
+      next.hingeGeom.reserve(next.hingeGeom.size() + more);
+    }
     auto opposite = [&](uint32_t t, uint32_t e0, uint32_t e1) {
       for (int k = 0; k < 3; ++k) {
         const uint32_t v = T[3 * t + k];
@@ -243,93 +268,121 @@ Model Model::build(const drape_scene_desc& scene) {
   }
   for (uint32_t i = 0; i < n; ++i) next.updateMass(i);
   for (std::size_t h = 0; h < next.hinges.size(); ++h) next.hinges[h].K = next.hingeStiffness(h);
-  next.buildStructure();
   next.buildIncidence();
+  next.buildStructure();
   return next;
 }
 
-void Model::buildStructure() {
-  const std::size_t n = x.size();
-  // Every coupled (row, col) pair as one 64-bit key; sorting and deduplicating gives the CSR rows directly.
-  std::vector<uint64_t> keys;
-  keys.reserve(n + 9 * stretch.size() + 16 * hinges.size() + 4 * seams.size());
-  for (uint32_t i = 0; i < n; ++i) keys.push_back((static_cast<uint64_t>(i) << 32) | i);
-  auto couple = [&](const uint32_t* vs, int m) {
-    for (int a = 0; a < m; ++a)
-      for (int b = 0; b < m; ++b) keys.push_back((static_cast<uint64_t>(vs[a]) << 32) | vs[b]);
-  };
-  for (const auto& t : stretch) couple(t.v.data(), 3);
-  for (const auto& h : hinges) couple(h.v.data(), 4);
+// Calls f(vertices, count) for every term's vertex set: stretch terms, hinges, then seam springs.
+template <class F>
+void Model::forEachTerm(F&& f) const {
+  for (const auto& t : stretch) f(t.v.data(), 3);
+  for (const auto& h : hinges) f(h.v.data(), 4);
   for (const auto& s : seams) {
     const uint32_t ab[2] = {s.a, s.b};
-    couple(ab, 2);
+    f(ab, 2);
   }
-  std::sort(keys.begin(), keys.end());
-  keys.erase(std::unique(keys.begin(), keys.end()), keys.end());
-  rowStart.assign(n + 1, 0);
-  colIndex.resize(keys.size());
-  for (std::size_t k = 0; k < keys.size(); ++k) {
-    colIndex[k] = static_cast<uint32_t>(keys[k]);
-    ++rowStart[(keys[k] >> 32) + 1];
+}
+
+// Vertex set of the term an incidence entry names; returns its size.
+int Model::termVertices(uint32_t code, uint32_t ab[4]) const {
+  const uint32_t kind = code >> 30, term = (code >> 2) & 0x0FFFFFFFu;
+  if (kind == 0) {
+    std::copy(stretch[term].v.begin(), stretch[term].v.end(), ab);
+    return 3;
   }
-  for (std::size_t i = 0; i < n; ++i) rowStart[i + 1] += rowStart[i];
-  diagSlot.resize(n);
-  for (uint32_t i = 0; i < n; ++i) diagSlot[i] = slot(i, i);
-  auto slotsFor = [&](const uint32_t* vs, int m, uint32_t* out) {
-    for (int a = 0; a < m; ++a)
-      for (int b = 0; b < m; ++b) out[a * m + b] = slot(vs[a], vs[b]);
-  };
-  stretchSlots.resize(stretch.size());
-  for (std::size_t k = 0; k < stretch.size(); ++k) slotsFor(stretch[k].v.data(), 3, stretchSlots[k].data());
-  hingeSlots.resize(hinges.size());
-  for (std::size_t k = 0; k < hinges.size(); ++k) slotsFor(hinges[k].v.data(), 4, hingeSlots[k].data());
-  seamSlots.resize(seams.size());
-  for (std::size_t k = 0; k < seams.size(); ++k) {
-    const uint32_t ab[2] = {seams[k].a, seams[k].b};
-    slotsFor(ab, 2, seamSlots[k].data());
+  if (kind == 1) {
+    std::copy(hinges[term].v.begin(), hinges[term].v.end(), ab);
+    return 4;
   }
-  contactForce.assign(n, 0.0);
-  maxRowSlots = 0;
-  for (std::size_t i = 0; i < n; ++i) maxRowSlots = std::max(maxRowSlots, rowStart[i + 1] - rowStart[i]);
+  ab[0] = seams[term].a;
+  ab[1] = seams[term].b;
+  return 2;
 }
 
 void Model::buildIncidence() {
   const std::size_t n = x.size();
+  if (stretch.size() >= (1u << 28) || hinges.size() >= (1u << 28) || seams.size() >= (1u << 28))
+    throw std::invalid_argument("too many terms for the incidence encoding");
   incStart.assign(n + 1, 0);
-  for (const auto& t : stretch)
-    for (auto v : t.v) ++incStart[v + 1];
-  for (const auto& h : hinges)
-    for (auto v : h.v) ++incStart[v + 1];
-  for (const auto& s : seams) {
-    ++incStart[s.a + 1];
-    ++incStart[s.b + 1];
-  }
+  forEachTerm([&](const uint32_t* vs, int m) {
+    for (int a = 0; a < m; ++a) ++incStart[vs[a] + 1];
+  });
   for (std::size_t i = 0; i < n; ++i) incStart[i + 1] += incStart[i];
   incEntry.assign(incStart[n], 0);
   incLocal.assign(incStart[n], 0);
+  // Entries in the reference's gather order (gpu_solver_core.cpp:184-224): stretch (t, a) in term order, then hinges,
+  // then seams.
   std::vector<uint32_t> fill(incStart.begin(), incStart.end() - 1);
-  auto add = [&](uint32_t kind, uint32_t term, uint32_t a, uint32_t particle, const uint32_t* slots, int N) {
-    const uint32_t e = fill[particle]++;
-    incEntry[e] = (kind << 30) | (term << 2) | a;
-    uint32_t packed = 0;
-    for (int b = 0; b < N; ++b) packed |= (slots[a * N + b] - rowStart[particle]) << (8 * b);
-    incLocal[e] = packed;
+  auto add = [&](uint32_t kind, uint32_t term, const uint32_t* vs, int m) {
+    for (int a = 0; a < m; ++a) incEntry[fill[vs[a]]++] = (kind << 30) | (term << 2) | static_cast<uint32_t>(a);
   };
-  if (stretch.size() >= (1u << 28) || hinges.size() >= (1u << 28) || seams.size() >= (1u << 28))
-    throw std::invalid_argument("too many terms for the incidence encoding");
-  if (maxRowSlots > kMaxRowSlots)
-    throw std::invalid_argument("a particle couples to " + std::to_string(maxRowSlots) + " particles; the CUDA solver supports " +
-                                std::to_string(kMaxRowSlots));
-  for (uint32_t t = 0; t < stretch.size(); ++t)
-    for (uint32_t a = 0; a < 3; ++a) add(0, t, a, stretch[t].v[a], stretchSlots[t].data(), 3);
-  for (uint32_t h = 0; h < hinges.size(); ++h)
-    for (uint32_t a = 0; a < 4; ++a) add(1, h, a, hinges[h].v[a], hingeSlots[h].data(), 4);
+  for (uint32_t t = 0; t < stretch.size(); ++t) add(0, t, stretch[t].v.data(), 3);
+  for (uint32_t h = 0; h < hinges.size(); ++h) add(1, h, hinges[h].v.data(), 4);
   for (uint32_t k = 0; k < seams.size(); ++k) {
     const uint32_t ab[2] = {seams[k].a, seams[k].b};
-    for (uint32_t a = 0; a < 2; ++a) add(2, k, a, ab[a], seamSlots[k].data(), 2);
+    add(2, k, ab, 2);
   }
   maxRowEntries = 0;
   for (std::size_t i = 0; i < n; ++i) maxRowEntries = std::max(maxRowEntries, incStart[i + 1] - incStart[i]);
+}
+
+void Model::buildStructure() {
+  const std::size_t n = x.size();
+  // One pass over the rows, each from its incidence entries. Row i's columns: i itself and every vertex of every term
+  // that contains i, deduplicated with a stamp array and sorted -- the sorted unique coupled columns of the reference's
+  // per-row vectors (sim_model.cpp:41-74). Then where[c] = the slot of column c in row i, which gives each incident
+  // term's slots of row i and the entry's row-local slot positions with one load per lookup (the reference finds
+  // them by binary search, sim_model.cpp:35-39; the slots are the same).
+  rowStart.assign(n + 1, 0);
+  colIndex.clear();
+  colIndex.reserve(incStart[n] + n);
+  slotRow.clear();
+  slotRow.reserve(incStart[n] + n);
+  diagSlot.resize(n);
+  stretchSlots.resize(stretch.size());
+  hingeSlots.resize(hinges.size());
+  seamSlots.resize(seams.size());
+  std::vector<uint32_t> stamp(n, UINT32_MAX), where(n, 0);
+  maxRowSlots = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const uint32_t rs = static_cast<uint32_t>(colIndex.size());
+    stamp[i] = i;
+    colIndex.push_back(i);
+    uint32_t vs[4];
+    for (uint32_t e = incStart[i]; e < incStart[i + 1]; ++e) {
+      const int m = termVertices(incEntry[e], vs);
+      for (int b = 0; b < m; ++b)
+        if (stamp[vs[b]] != i) {
+          stamp[vs[b]] = i;
+          colIndex.push_back(vs[b]);
+        }
+    }
+    std::sort(colIndex.begin() + rs, colIndex.end());
+    rowStart[i + 1] = static_cast<uint32_t>(colIndex.size());
+    slotRow.resize(colIndex.size(), i);
+    maxRowSlots = std::max<uint32_t>(maxRowSlots, rowStart[i + 1] - rs);
+    for (uint32_t k = rs; k < rowStart[i + 1]; ++k) where[colIndex[k]] = k;
+    diagSlot[i] = where[i];
+    for (uint32_t e = incStart[i]; e < incStart[i + 1]; ++e) {
+      const uint32_t code = incEntry[e], kind = code >> 30, term = (code >> 2) & 0x0FFFFFFFu, a = code & 3u;
+      const int m = termVertices(code, vs);
+      uint32_t* out = kind == 0 ? stretchSlots[term].data() : (kind == 1 ? hingeSlots[term].data() : seamSlots[term].data());
+      uint32_t packed = 0;
+      for (int b = 0; b < m; ++b) {
+        const uint32_t sl = where[vs[b]];
+        out[a * m + b] = sl;
+        packed |= ((sl - rs) & 0xFFu) << (8 * b);
+      }
+      incLocal[e] = packed;
+    }
+  }
+  colIndex.shrink_to_fit();
+  slotRow.shrink_to_fit();
+  contactForce.assign(n, 0.0);
+  if (maxRowSlots > kMaxRowSlots)
+    throw std::invalid_argument("a particle couples to " + std::to_string(maxRowSlots) + " particles; the CUDA solver supports " +
+                                std::to_string(kMaxRowSlots));
 }
 
 void Model::updateFabric(const std::string& id, const drape_fabric* pieceFabric, uint32_t count) {

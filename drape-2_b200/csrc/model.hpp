@@ -7,8 +7,8 @@
 //   - hinges in lexicographic (min, max) edge order, each edge's triangles in insertion order (= std::map iteration,
 //     sim_model.cpp:124-146), then per garment the seam springs interleaved with their seam hinges
 //     (sim_model.cpp:147-175);
-//   - rows = sorted unique coupled columns (self + every term's vertex set), slots found by lower_bound
-//     (sim_model.cpp:35-74).
+//   - rows = sorted unique coupled columns (self + every term's vertex set), each term's slots = the positions of its
+//     vertices' columns in their rows (sim_model.cpp:35-74).
 #pragma once
 
 #include <array>
@@ -60,8 +60,11 @@ struct Model {
 
   drape_settings settings{};
   bool hasBody = false;
-  drape_field_desc field{};      // values points into fieldValues
-  std::vector<float> fieldValues;
+  drape_field_desc field{};      // values = nullptr; the samples are fieldData()[0, fieldCount)
+  std::vector<float> fieldValues;  // the model's own copy of the samples (build with copyField), else empty
+  const float* fieldSource = nullptr;  // without a copy: the caller's samples, valid while the build call runs
+  std::size_t fieldCount = 0;          // samples in the field (0: no body)
+  const float* fieldData() const { return fieldValues.empty() ? fieldSource : fieldValues.data(); }
   std::vector<Garment> garments;
   std::vector<drape_fabric> fabrics;
   std::vector<Vec3f> x, v;
@@ -76,6 +79,7 @@ struct Model {
   std::vector<double> hingeGeom;
   std::vector<Seam> seams;
   std::vector<uint32_t> rowStart, colIndex, diagSlot;
+  std::vector<uint32_t> slotRow;  // the row of each block slot
   std::vector<std::array<uint32_t, 9>> stretchSlots;
   std::vector<std::array<uint32_t, 16>> hingeSlots;
   std::vector<std::array<uint32_t, 4>> seamSlots;
@@ -88,7 +92,9 @@ struct Model {
   std::vector<uint32_t> incStart, incEntry, incLocal;
   uint32_t maxRowSlots = 0, maxRowEntries = 0;
 
-  static Model build(const drape_scene_desc& scene);  // throws invalid_argument / out_of_range like sim_model.cpp
+  // Throws invalid_argument / out_of_range like sim_model.cpp. Without copyField the model keeps no copy of the
+  // collision field: fieldSource points at the scene's samples, which the caller uploads before the scene goes away.
+  static Model build(const drape_scene_desc& scene, bool copyField = true);
   void updateFabric(const std::string& id, const drape_fabric* pieceFabric, uint32_t count);
   void setPhase(const std::string& id, int phase);
   std::size_t garmentIndex(const std::string& id) const;  // throws std::out_of_range for unknown ids
@@ -97,8 +103,11 @@ struct Model {
   uint32_t slot(uint32_t row, uint32_t col) const;
 
  private:
+  template <class F>
+  void forEachTerm(F&& f) const;
+  int termVertices(uint32_t code, uint32_t ab[4]) const;
+  void buildIncidence();  // entry codes; then buildStructure: rows, slot maps, row-local slot positions
   void buildStructure();
-  void buildIncidence();
 };
 
 }  // namespace drape_b200

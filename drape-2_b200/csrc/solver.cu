@@ -2,7 +2,7 @@
 //
 // The driver plays the role of the reference's GpuSolverCore (libs/sim/src/gpu/gpu_solver_core.cpp:41-407): it owns
 // the model (model.hpp), the device buffers and one CUDA stream, and issues per substep
-//   k_begin, then per Newton iteration k_activate, k_assemble, k_solve (cooperative), then k_finish, k_advance_clock.
+//   k_begin, then per Newton iteration k_activate, k_terms, k_assemble, k_solve (cooperative), then k_finish, k_advance_clock.
 // Unlike the reference driver there is no host round trip inside a substep: energies, slope, line search and the
 // Newton stop test are decided on the device. The host synchronises once per step() to read the work counters and the
 // error status (the bounded grid barrier's timeout).
@@ -76,7 +76,7 @@ struct drape_solver {
   DBuf<dcu::Stretch> stretch;
   DBuf<dcu::Hinge> hinge;
   DBuf<dcu::Seam> seam;
-  DBuf<uint32_t> rowStart, colIndex, diagSlot, incStart, incEntry, incLocal;
+  DBuf<uint32_t> rowStart, colIndex, diagSlot, incStart, incEntry, incLocal, slotRow;
   DBuf<float> fieldValues, blocks;
   DBuf<float4> x, v, xStart, yRel, u, grad, step, r, z, p0, p1, ap, apFull, resid, fExt, pinPos, precond;
   DBuf<float4> stretchDer, hingeDer;
@@ -150,8 +150,6 @@ struct drape_solver {
     if (!prop.cooperativeLaunch) throw std::runtime_error("cuda: device does not support cooperative launch");
     numSMs = prop.multiProcessorCount;
     CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-    CK(cudaFuncSetAttribute(dcu::k_assemble, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                            static_cast<int>(dcu::kAssembleSmem)));
     // The solve kernels keep their rows' matrix blocks in shared memory: as many slots as the opt-in limit leaves.
     const void* solveKernels[] = {reinterpret_cast<const void*>(dcu::k_solve<false>),
                                   reinterpret_cast<const void*>(dcu::k_solve<true>),
@@ -206,7 +204,7 @@ struct drape_solver {
 
   void build(const drape_scene_desc& scene) {
     use();
-    Model next = Model::build(scene);
+    Model next = Model::build(scene, false);  // the field is uploaded from the scene's samples below
     built = false;
     m = std::move(next);
     const uint32_t n = static_cast<uint32_t>(m.x.size());
@@ -225,8 +223,11 @@ struct drape_solver {
     incStart.upload(m.incStart, s);
     incEntry.upload(m.incEntry, s);
     incLocal.upload(m.incLocal, s);
-    if (!m.fieldValues.empty()) {
-      fieldValues.upload(m.fieldValues, s);
+    slotRow.upload(m.slotRow, s);
+    if (m.fieldCount > 0) {
+      fieldValues.upload(m.fieldData(), m.fieldCount, s);
+      CK(cudaStreamSynchronize(s));  // the copy has read the caller's samples; the model keeps no pointer to them
+      m.fieldSource = nullptr;
     } else {
       fieldValues.alloc(1);
     }
@@ -265,6 +266,7 @@ struct drape_solver {
     d.incStart = incStart.p;
     d.incEntry = incEntry.p;
     d.incLocal = incLocal.p;
+    d.slotRow = slotRow.p;
     d.x = x.p;
     d.v = v.p;
     d.xStart = xStart.p;
@@ -292,8 +294,8 @@ struct drape_solver {
     dev = d;
     netGraph.reset();
     if (learnedOn) bindNet();
-    assembleGrid = static_cast<int>(std::max<uint32_t>(1, std::min<uint32_t>((n + dcu::kAssembleWarps - 1) / dcu::kAssembleWarps,
-                                                                           static_cast<uint32_t>(numSMs) * 16)));
+    assembleGrid = static_cast<int>(std::max<uint32_t>(1, std::min<uint32_t>((B + dcu::kAssembleThreads - 1) / dcu::kAssembleThreads,
+                                                                           static_cast<uint32_t>(numSMs) * 64)));
     const size_t terms = m.stretch.size() + m.hinges.size();
     termsGrid = static_cast<int>(std::max<size_t>(1, std::min<size_t>((terms + dcu::kTermThreads - 1) / dcu::kTermThreads,
                                                                       static_cast<size_t>(numSMs) * 16)));
@@ -422,7 +424,7 @@ struct drape_solver {
       dcu::k_terms<<<termsGrid, dcu::kTermThreads, 0, stream>>>(d);
       profStop(e, 2);
       e = profStart();
-      dcu::k_assemble<<<assembleGrid, dcu::kAssembleWarps * dcu::kWarp, dcu::kAssembleSmem, stream>>>(d);
+      dcu::k_assemble<<<assembleGrid, dcu::kAssembleThreads, 0, stream>>>(d);
       CK(cudaGetLastError());
       profStop(e, 2);
       if (learnedOn && netGraph && netNewtonCounter++ % static_cast<uint64_t>(precondRefresh) == 0) {
@@ -1147,7 +1149,7 @@ int drape_cuda_capture_system(drape_solver* s, double h, float* blocks, float* g
     dcu::k_begin<<<pg, 256, 0, s->stream>>>(d);
     dcu::k_activate<<<pg, 256, 0, s->stream>>>(d);
     dcu::k_terms<<<s->termsGrid, dcu::kTermThreads, 0, s->stream>>>(d);
-    dcu::k_assemble<<<s->assembleGrid, dcu::kAssembleWarps * dcu::kWarp, dcu::kAssembleSmem, s->stream>>>(d);
+    dcu::k_assemble<<<s->assembleGrid, dcu::kAssembleThreads, 0, s->stream>>>(d);
     CK(cudaGetLastError());
     const size_t B = s->m.colIndex.size(), SP = s->dev.P.slotsPadded;
     std::vector<float> planes(9 * SP);

@@ -23,8 +23,8 @@ constexpr int kTermThreads = 256;  // k_terms block size
 
 __global__ void __launch_bounds__(kTermThreads) k_terms(Dev D) { termsRows(D, blockIdx.x, gridDim.x); }
 
-__global__ void __launch_bounds__(kAssembleWarps * kWarp) k_assemble(Dev D) {
-  assembleRows(D, blockIdx.x, gridDim.x);
+__global__ void __launch_bounds__(kAssembleThreads) k_assemble(Dev D) {
+  assembleSlots(D, blockIdx.x, gridDim.x);
 }
 
 // One Newton iteration's persistent solve; the whole grid is one group.
