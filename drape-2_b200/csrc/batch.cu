@@ -465,7 +465,7 @@ struct drape_batch {
   DBuf<dcu::Stretch> stretch;
   DBuf<dcu::Hinge> hinge;
   DBuf<dcu::Seam> seam, saveSeam;
-  DBuf<uint32_t> rowStart, colIndex, diagSlot, incStart, incEntry, incLocal, slotRow, tslot;
+  DBuf<uint32_t> rowStart, colIndex, diagSlot, incStart, incEntry, offSlot, offStart, offContrib, tslot;
   DBuf<uint32_t> starts, bases;  // point and assembly prefixes; pBase and kBase
   DBuf<float> fieldValues, blocks, snapGap;
   DBuf<float4> x, v, xStart, yRel, u, grad, step, r, z, p0, p1, ap, apFull, resid, fExt, pinPos, precond;
@@ -563,8 +563,8 @@ struct drape_batch {
     pBase.assign(G, 0);
     sBase.assign(G, 0);
     kBase.assign(G, 0);
-    std::vector<uint32_t> tBase(G), hBase(G), eBase(G), fabBase(G), fieldBase(G), rBase(G);
-    uint32_t n = 0, b = 0, t = 0, h = 0, k = 0, e = 0, fab = 0, fv = 0;
+    std::vector<uint32_t> tBase(G), hBase(G), eBase(G), fabBase(G), fieldBase(G), rBase(G), cBase(G);
+    uint32_t n = 0, b = 0, t = 0, h = 0, k = 0, e = 0, fab = 0, fv = 0, cc = 0;
     for (uint32_t g = 0; g < G; ++g) {
       const Model& m = models[g];
       pBase[g] = n;
@@ -576,12 +576,14 @@ struct drape_batch {
       fabBase[g] = fab;
       fieldBase[g] = fv;
       rBase[g] = n + g;
+      cBase[g] = cc;
       n += static_cast<uint32_t>(m.x.size());
       b += static_cast<uint32_t>(m.colIndex.size());
       t += static_cast<uint32_t>(m.stretch.size());
       h += static_cast<uint32_t>(m.hinges.size());
       k += static_cast<uint32_t>(m.seams.size());
       e += static_cast<uint32_t>(m.incEntry.size());
+      cc += static_cast<uint32_t>(m.offContrib.size());
       fab += static_cast<uint32_t>(dmodel::fabrics(m).size());
       fv += static_cast<uint32_t>(std::max<size_t>(m.fieldValues.size(), 1));
     }
@@ -595,7 +597,7 @@ struct drape_batch {
     std::vector<dcu::Stretch> hs;
     std::vector<dcu::Hinge> hh;
     std::vector<dcu::Seam> hk;
-    std::vector<uint32_t> hrs, hci, hds, his, hie, hil, hsr, hts;
+    std::vector<uint32_t> hrs, hci, hds, his, hie, hos, hoS, hoc, hts;
     std::vector<float> hfv;
     std::vector<float4> hx, hv, hfe, hpp;
     for (uint32_t g = 0; g < G; ++g) {
@@ -613,8 +615,9 @@ struct drape_batch {
       append(hds, m.diagSlot);
       append(his, m.incStart);
       append(hie, m.incEntry);
-      append(hil, m.incLocal);
-      append(hsr, m.slotRow);
+      append(hos, m.offSlot);
+      append(hoS, m.offStart);
+      append(hoc, m.offContrib);
       append(hts, net::transposedSlots(m.rowStart, cols));
       if (m.fieldValues.empty()) hfv.push_back(0.0f); else append(hfv, m.fieldValues);
       std::vector<float4> xs, vs, fe, pp;
@@ -636,8 +639,9 @@ struct drape_batch {
     diagSlot.upload(hds, s);
     incStart.upload(his, s);
     incEntry.upload(hie, s);
-    incLocal.upload(hil, s);
-    slotRow.upload(hsr, s);
+    offSlot.upload(hos, s);
+    offStart.upload(hoS, s);
+    offContrib.upload(hoc, s);
     tslot.upload(hts, s);
     fieldValues.upload(hfv, s);
     blocks.alloc(static_cast<size_t>(SP) * 9);
@@ -700,8 +704,9 @@ struct drape_batch {
       d.diagSlot = diagSlot.p + pb;
       d.incStart = incStart.p + rBase[g];
       d.incEntry = incEntry.p + eBase[g];
-      d.incLocal = incLocal.p + eBase[g];
-      d.slotRow = slotRow.p + sBase[g];
+      d.offSlot = offSlot.p + (sBase[g] - pBase[g]);
+      d.offStart = offStart.p + (sBase[g] - pBase[g] + g);
+      d.offContrib = offContrib.p + cBase[g];
       for (auto [dst, src] : {std::pair<float4**, float4*>{&d.x, x.p}, {&d.v, v.p}, {&d.xStart, xStart.p},
                               {&d.yRel, yRel.p}, {&d.u, u.p}, {&d.grad, grad.p}, {&d.step, step.p}, {&d.r, r.p},
                               {&d.z, z.p}, {&d.p0, p0.p}, {&d.p1, p1.p}, {&d.ap, ap.p}, {&d.apFull, apFull.p},

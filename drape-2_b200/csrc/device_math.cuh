@@ -211,8 +211,9 @@ __device__ inline void stretchRowFrom(float4 d, const StretchDer& o, int a, floa
   }
 }
 
-// Block (a, b) of a stretch term's Hessian and the gradient of vertex a, read from the term's record in global memory:
-// the operations stretchRowFrom performs for H[b] of row a and for its g, in the same order.
+// Block (a, b) of a stretch term's Hessian and, with Grad, the gradient of vertex a, read from the term's record in
+// global memory: the operations stretchRowFrom performs for H[b] of row a and for its g, in the same order.
+template <bool Grad>
 __device__ inline void stretchBlockFrom(float4 d, const float4* __restrict__ rec, int a, int b, float3& g, M3& H) {
   zero(H);
   g = mk(0, 0, 0);
@@ -227,7 +228,7 @@ __device__ inline void stretchBlockFrom(float4 d, const float4* __restrict__ rec
     const float gs = wn.w, hs = ws.x, ts = ws.y;
     const float ca = coef(d, which, a), cb = coef(d, which, b);
     const float3 gra = n * ca, grb = n * cb;
-    g += gra * gs;
+    if (Grad) g += gra * gs;
     addOuter(H, hs, gra, grb);
     if (ts != 0.0f) addProjector(H, ts * ca * cb, n);
   }
@@ -236,7 +237,7 @@ __device__ inline void stretchBlockFrom(float4 d, const float4* __restrict__ rec
     const float3 dfu = xyz(w4), dfv = xyz(w5);
     const float3 gra = dfu * coef(d, 0, a) + dfv * coef(d, 1, a);
     const float3 grb = dfu * coef(d, 0, b) + dfv * coef(d, 1, b);
-    g += gra * w4.w;
+    if (Grad) g += gra * w4.w;
     addOuter(H, w5.w, gra, grb);
   }
 }
@@ -293,11 +294,13 @@ __device__ inline void hingeRowFrom(const HingeDer& o, int a, float3& g, M3 H[4]
   }
 }
 
-// Block (a, b) of a hinge term's Hessian and the gradient of vertex a from its record (hingeRowFrom's operations).
+// Block (a, b) of a hinge term's Hessian and, with Grad, the gradient of vertex a from its record (hingeRowFrom's
+// operations).
+template <bool Grad>
 __device__ inline void hingeBlockFrom(const float4* __restrict__ rec, int a, int b, float3& g, M3& H) {
   const float4 wa = rec[a], wb = rec[b];
-  const float KC = rec[0].w, K = rec[1].w;
-  g = xyz(wa) * KC;
+  const float K = rec[1].w;
+  if (Grad) g = xyz(wa) * rec[0].w;
   zero(H);
   addOuter(H, K, xyz(wa), xyz(wb));
 }

@@ -114,8 +114,9 @@ struct Dev {
   const uint32_t* diagSlot;
   const uint32_t* incStart;
   const uint32_t* incEntry;
-  const uint32_t* incLocal;
-  const uint32_t* slotRow;   // row of each block slot
+  const uint32_t* offSlot;   // the off-diagonal slots in slot order: row << 6 | row-local position
+  const uint32_t* offStart;  // per off-diagonal slot: its contributions [offStart[k], offStart[k + 1]) of offContrib
+  const uint32_t* offContrib;  // incidence entry << 2 | block of the entry's term, in gather order
   float4 *x, *v, *xStart, *yRel, *u, *grad, *step, *r, *z, *p0, *p1, *ap, *apFull, *resid;
   float4* stretchDer;      // per stretch term: its StretchDer record (6 float4), written by termsRows
   float4* hingeDer;        // per hinge term: its HingeDer record (4 float4)
@@ -377,11 +378,12 @@ __device__ inline void activateRows(const Dev& D, uint32_t rank, uint32_t size) 
 
 // ---------------------------------------------------------------------------------------------------------------
 // Assembly in two passes. termsRows evaluates every stretch and hinge term once into a derivative record;
-// assembleSlots then gives every block slot (i, j) one thread, which walks row i's incidence list (the reference's
-// fixed gather order, gpu_solver_core.cpp:184-224) and adds block (a, b) of each incident term that couples i (its
-// vertex a) with j (its vertex b), formed from the term's record. The diagonal slot's thread starts from the
-// particle's own inertia and friction term and also sums the row's gradient. Every slot's sum runs in the same order
-// as the reference's gather; deterministic, no atomics, no shared memory.
+// assembleSlots then gives every block slot (i, j) one thread, which adds block (a, b) of each incident term that
+// couples i (its vertex a) with j (its vertex b), formed from the term's record, in row i's incidence order (the
+// reference's fixed gather order, gpu_solver_core.cpp:184-224). The diagonal slot walks row i's whole incidence list
+// (every entry's block (a, a)) after the particle's own inertia and friction term and also sums the row's gradient;
+// an off-diagonal slot walks its own contribution list (the reference's per-slot gather list). Deterministic, no
+// atomics, no shared memory.
 
 __device__ inline float3 relPos(const Dev& D, uint32_t v0, uint32_t vk) {
   return (ld3(D.xStart, vk) - ld3(D.xStart, v0)) + ld3(D.u, vk);
@@ -430,84 +432,101 @@ __device__ inline void termsRows(const Dev& D, uint32_t rank, uint32_t size) {
   }
 }
 
-// Block (a, b) of the term an incidence entry names, and the gradient of its vertex a (seam springs, a few hundred
-// per garment, are evaluated here; stretch and hinge terms come from their records).
+// Block (a, b) of the term an incidence entry names, and with Grad the gradient of its vertex a (seam springs, a few
+// hundred per garment, are evaluated here; stretch and hinge terms come from their records).
+template <bool Grad>
 __device__ inline void entryBlock(const Dev& D, uint32_t code, int b, float3& g, M3& H) {
   const uint32_t kind = code >> 30, term = (code >> 2) & 0x0FFFFFFFu;
   const int a = static_cast<int>(code & 3u);
   if (kind == 0) {
-    stretchBlockFrom(D.stretch[term].d, D.stretchDer + 6ull * term, a, b, g, H);
+    stretchBlockFrom<Grad>(D.stretch[term].d, D.stretchDer + 6ull * term, a, b, g, H);
   } else if (kind == 1) {
-    hingeBlockFrom(D.hingeDer + 4ull * term, a, b, g, H);
+    hingeBlockFrom<Grad>(D.hingeDer + 4ull * term, a, b, g, H);
   } else {
     const Seam sp = D.seam[term];
     M3 H2[2];
     seamRow(D.P.seamStiffness, seamTarget(D, sp), ld3(D.u, sp.a), relPos(D, sp.a, sp.b), a, g, H2);
-    H = H2[b & 1];
+    H = b == 0 ? H2[0] : H2[1];
   }
 }
 
+// Diagonal slot of row i: the particle's own inertia and friction term, then block (a, a) of every incident entry
+// (vertex a of an entry is i itself); also the row's gradient, the block-Jacobi inverse and the contact release.
+__device__ inline void diagonalSlot(const Dev& D, uint32_t i, uint32_t SP) {
+  const uint32_t s = D.diagSlot[i];
+  const Particle pa = D.particle[i];
+  const Contact c = D.contact[i];
+  M3 acc;
+  zero(acc);
+  float3 gAcc = mk(0, 0, 0);
+  // The particle's own term: inertia 1/2 (m/h^2)|u - yRel|^2 and friction (kernels.h:104-129).
+  if (pa.pinned == 0u) {
+    const float k = pa.mass * D.P.invH2;
+    gAcc = (ld3(D.u, i) - ld3(D.yRel, i)) * k;
+    acc.m[0] = acc.m[4] = acc.m[8] = k;
+  }
+  if (c.frictionLambda > 0.0f)
+    frictionRow(ld3(D.u, i), xyz(c.normal), D.fabric[pa.fabric].friction * c.frictionLambda,
+                D.P.frictionSlip * D.P.h, gAcc, acc);
+  const uint32_t ee = D.incStart[i + 1];
+  for (uint32_t e = D.incStart[i]; e < ee; ++e) {
+    const uint32_t code = D.incEntry[e];
+    float3 g;
+    M3 H;
+    entryBlock<true>(D, code, static_cast<int>(code & 3u), g, H);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) acc.m[k] += H.m[k];
+    gAcc += g;
+  }
+#pragma unroll
+  for (int k = 0; k < 9; ++k) D.blocks[k * SP + s] = acc.m[k];
+  // Block-Jacobi inverse of the diagonal block (kernels.h:237-249); zero for pinned particles.
+  M3 inv;
+  if (pa.pinned != 0u) {
+    zero(inv);
+  } else {
+    bool ok = false;
+    inv = invertSpd(acc, ok);
+  }
+  D.precond[3 * i + 0] = make_float4(inv.m[0], inv.m[1], inv.m[2], 0.0f);
+  D.precond[3 * i + 1] = make_float4(inv.m[3], inv.m[4], inv.m[5], 0.0f);
+  D.precond[3 * i + 2] = make_float4(inv.m[6], inv.m[7], inv.m[8], 0.0f);
+  // Gradient (pinned rows zero) and contact release (kernels.h:204-231).
+  const float3 gi = pa.pinned != 0u ? mk(0, 0, 0) : gAcc;
+  D.grad[i] = f4(gi);
+  if (c.active != 0u && dot(gi, xyz(c.normal)) < 0.0f) D.contact[i].active = 0u;
+}
+
+// Off-diagonal slot k (offSlot[k] = row << 6 | row-local position): its contributions (incidence entry, block b of
+// the entry's term) in gather order.
+__device__ inline void offDiagonalSlot(const Dev& D, uint32_t k, uint32_t SP) {
+  const uint32_t packed = D.offSlot[k];
+  const uint32_t s = D.rowStart[packed >> 6] + (packed & 63u);
+  M3 acc;
+  zero(acc);
+  const uint32_t ce = D.offStart[k + 1];
+  for (uint32_t c = D.offStart[k]; c < ce; ++c) {
+    const uint32_t v = D.offContrib[c];
+    float3 g;
+    M3 H;
+    entryBlock<false>(D, D.incEntry[v >> 2], static_cast<int>(v & 3u), g, H);
+#pragma unroll
+    for (int q = 0; q < 9; ++q) acc.m[q] += H.m[q];
+  }
+#pragma unroll
+  for (int q = 0; q < 9; ++q) D.blocks[q * SP + s] = acc.m[q];
+}
+
+// Thread k of the n + (B - n) assembly threads: the diagonal slot of row k for k < n, else off-diagonal slot k - n, so
+// that the diagonal slots (every incident entry) and the off-diagonal ones (a few entries each) fill separate warps.
 __device__ inline void assembleSlots(const Dev& D, uint32_t rank, uint32_t size) {
   if (D.ctl->newtonDone) return;
-  const uint32_t SP = D.P.slotsPadded;
-  for (uint32_t s = rank * blockDim.x + threadIdx.x; s < D.P.nBlocks; s += size * blockDim.x) {
-    const uint32_t i = D.slotRow[s];
-    const uint32_t rs = D.rowStart[i];
-    const bool diag = D.diagSlot[i] == s;
-    M3 acc;
-    zero(acc);
-    float3 gAcc = mk(0, 0, 0);
-    Particle pa{};
-    Contact c{};
-    if (diag) {
-      // The particle's own term: inertia 1/2 (m/h^2)|u - yRel|^2 and friction (kernels.h:104-129).
-      pa = D.particle[i];
-      c = D.contact[i];
-      if (pa.pinned == 0u) {
-        const float k = pa.mass * D.P.invH2;
-        gAcc = (ld3(D.u, i) - ld3(D.yRel, i)) * k;
-        acc.m[0] = acc.m[4] = acc.m[8] = k;
-      }
-      if (c.frictionLambda > 0.0f)
-        frictionRow(ld3(D.u, i), xyz(c.normal), D.fabric[pa.fabric].friction * c.frictionLambda,
-                    D.P.frictionSlip * D.P.h, gAcc, acc);
-    }
-    // The entry touches this slot where one of its N packed row-local positions equals ours (the N positions of an
-    // entry are distinct; the unused high bytes are masked off).
-    const uint32_t mine = (s - rs) * 0x01010101u;
-    const uint32_t ee = D.incStart[i + 1];
-    for (uint32_t e = D.incStart[i]; e < ee; ++e) {
-      const uint32_t code = D.incEntry[e];
-      const uint32_t kind = code >> 30;
-      const uint32_t valid = kind == 1 ? 0xFFFFFFFFu : (kind == 0 ? 0x00FFFFFFu : 0x0000FFFFu);
-      const uint32_t hit = __vcmpeq4(D.incLocal[e], mine) & valid;
-      if (hit == 0u) continue;
-      float3 g;
-      M3 H;
-      entryBlock(D, code, (__ffs(hit) - 1) >> 3, g, H);
-#pragma unroll
-      for (int k = 0; k < 9; ++k) acc.m[k] += H.m[k];
-      gAcc += g;
-    }
-#pragma unroll
-    for (int k = 0; k < 9; ++k) D.blocks[k * SP + s] = acc.m[k];
-    if (diag) {
-      // Block-Jacobi inverse of the diagonal block (kernels.h:237-249); zero for pinned particles.
-      M3 inv;
-      if (pa.pinned != 0u) {
-        zero(inv);
-      } else {
-        bool ok = false;
-        inv = invertSpd(acc, ok);
-      }
-      D.precond[3 * i + 0] = make_float4(inv.m[0], inv.m[1], inv.m[2], 0.0f);
-      D.precond[3 * i + 1] = make_float4(inv.m[3], inv.m[4], inv.m[5], 0.0f);
-      D.precond[3 * i + 2] = make_float4(inv.m[6], inv.m[7], inv.m[8], 0.0f);
-      // Gradient (pinned rows zero) and contact release (kernels.h:204-231).
-      const float3 gi = pa.pinned != 0u ? mk(0, 0, 0) : gAcc;
-      D.grad[i] = f4(gi);
-      if (c.active != 0u && dot(gi, xyz(c.normal)) < 0.0f) D.contact[i].active = 0u;
-    }
+  const uint32_t n = D.P.n, SP = D.P.slotsPadded;
+  for (uint32_t k = rank * blockDim.x + threadIdx.x; k < D.P.nBlocks; k += size * blockDim.x) {
+    if (k < n)
+      diagonalSlot(D, k, SP);
+    else
+      offDiagonalSlot(D, k - n, SP);
   }
 }
 

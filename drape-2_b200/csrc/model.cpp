@@ -284,6 +284,12 @@ void Model::forEachTerm(F&& f) const {
   }
 }
 
+// Vertex count of the term an incidence entry names (3 stretch, 4 hinge, 2 seam).
+int Model::entryArity(uint32_t code) {
+  const uint32_t kind = code >> 30;
+  return kind == 0 ? 3 : (kind == 1 ? 4 : 2);
+}
+
 // Vertex set of the term an incidence entry names; returns its size.
 int Model::termVertices(uint32_t code, uint32_t ab[4]) const {
   const uint32_t kind = code >> 30, term = (code >> 2) & 0x0FFFFFFFu;
@@ -337,8 +343,14 @@ void Model::buildStructure() {
   rowStart.assign(n + 1, 0);
   colIndex.clear();
   colIndex.reserve(incStart[n] + n);
-  slotRow.clear();
-  slotRow.reserve(incStart[n] + n);
+  offSlot.clear();
+  offSlot.reserve(incStart[n]);
+  offStart.clear();
+  offStart.reserve(incStart[n] + 1);
+  offContrib.clear();
+  offContrib.reserve(2 * static_cast<std::size_t>(incStart[n]));
+  if (n >= (1u << 26)) throw std::invalid_argument("too many particles for the slot encoding");
+  if (incStart[n] >= (1u << 29)) throw std::invalid_argument("too many term incidences for the contribution encoding");
   diagSlot.resize(n);
   stretchSlots.resize(stretch.size());
   hingeSlots.resize(hinges.size());
@@ -360,8 +372,13 @@ void Model::buildStructure() {
     }
     std::sort(colIndex.begin() + rs, colIndex.end());
     rowStart[i + 1] = static_cast<uint32_t>(colIndex.size());
-    slotRow.resize(colIndex.size(), i);
-    maxRowSlots = std::max<uint32_t>(maxRowSlots, rowStart[i + 1] - rs);
+    const uint32_t L = rowStart[i + 1] - rs;
+    maxRowSlots = std::max<uint32_t>(maxRowSlots, L);
+    if (L > kMaxRowSlots)
+      throw std::invalid_argument("a particle couples to " + std::to_string(L) + " particles; the CUDA solver supports " +
+                                  std::to_string(kMaxRowSlots));
+    for (uint32_t k = rs; k < rowStart[i + 1]; ++k)
+      if (colIndex[k] != i) offSlot.push_back((i << 6) | (k - rs));
     for (uint32_t k = rs; k < rowStart[i + 1]; ++k) where[colIndex[k]] = k;
     diagSlot[i] = where[i];
     for (uint32_t e = incStart[i]; e < incStart[i + 1]; ++e) {
@@ -376,13 +393,35 @@ void Model::buildStructure() {
       }
       incLocal[e] = packed;
     }
+    // Contribution lists of the row's off-diagonal slots, in slot order: entry e's block b lands in row-local slot
+    // byte b of incLocal[e]; each list keeps the incidence (gather) order.
+    uint32_t cnt[kMaxRowSlots] = {};
+    uint32_t pos[kMaxRowSlots];
+    for (uint32_t e = incStart[i]; e < incStart[i + 1]; ++e) {
+      const int m = entryArity(incEntry[e]);
+      for (int b = 0; b < m; ++b) ++cnt[(incLocal[e] >> (8 * b)) & 0xFFu];
+    }
+    const uint32_t dl = diagSlot[i] - rs;
+    uint32_t next = static_cast<uint32_t>(offContrib.size());
+    for (uint32_t t = 0; t < L; ++t) {
+      if (t == dl) continue;
+      offStart.push_back(next);
+      pos[t] = next;
+      next += cnt[t];
+    }
+    offContrib.resize(next);
+    for (uint32_t e = incStart[i]; e < incStart[i + 1]; ++e) {
+      const int m = entryArity(incEntry[e]);
+      for (int b = 0; b < m; ++b) {
+        const uint32_t t = (incLocal[e] >> (8 * b)) & 0xFFu;
+        if (t != dl) offContrib[pos[t]++] = (e << 2) | static_cast<uint32_t>(b);
+      }
+    }
   }
+  offStart.push_back(static_cast<uint32_t>(offContrib.size()));
   colIndex.shrink_to_fit();
-  slotRow.shrink_to_fit();
+  offSlot.shrink_to_fit();
   contactForce.assign(n, 0.0);
-  if (maxRowSlots > kMaxRowSlots)
-    throw std::invalid_argument("a particle couples to " + std::to_string(maxRowSlots) + " particles; the CUDA solver supports " +
-                                std::to_string(kMaxRowSlots));
 }
 
 void Model::updateFabric(const std::string& id, const drape_fabric* pieceFabric, uint32_t count) {

@@ -79,7 +79,9 @@ struct Model {
   std::vector<double> hingeGeom;
   std::vector<Seam> seams;
   std::vector<uint32_t> rowStart, colIndex, diagSlot;
-  std::vector<uint32_t> slotRow;  // the row of each block slot
+  // The off-diagonal slots in slot order (row << 6 | row-local position) and, per such slot k, the contributions
+  // [offStart[k], offStart[k + 1]) of offContrib in gather order: incidence entry e << 2 | block b of its term.
+  std::vector<uint32_t> offSlot, offStart, offContrib;
   std::vector<std::array<uint32_t, 9>> stretchSlots;
   std::vector<std::array<uint32_t, 16>> hingeSlots;
   std::vector<std::array<uint32_t, 4>> seamSlots;
@@ -106,6 +108,7 @@ struct Model {
   template <class F>
   void forEachTerm(F&& f) const;
   int termVertices(uint32_t code, uint32_t ab[4]) const;
+  static int entryArity(uint32_t code);
   void buildIncidence();  // entry codes; then buildStructure: rows, slot maps, row-local slot positions
   void buildStructure();
 };

@@ -76,7 +76,7 @@ struct drape_solver {
   DBuf<dcu::Stretch> stretch;
   DBuf<dcu::Hinge> hinge;
   DBuf<dcu::Seam> seam;
-  DBuf<uint32_t> rowStart, colIndex, diagSlot, incStart, incEntry, incLocal, slotRow;
+  DBuf<uint32_t> rowStart, colIndex, diagSlot, incStart, incEntry, offSlot, offStart, offContrib;
   DBuf<float> fieldValues, blocks;
   DBuf<float4> x, v, xStart, yRel, u, grad, step, r, z, p0, p1, ap, apFull, resid, fExt, pinPos, precond;
   DBuf<float4> stretchDer, hingeDer;
@@ -222,8 +222,9 @@ struct drape_solver {
     diagSlot.upload(m.diagSlot, s);
     incStart.upload(m.incStart, s);
     incEntry.upload(m.incEntry, s);
-    incLocal.upload(m.incLocal, s);
-    slotRow.upload(m.slotRow, s);
+    offSlot.upload(m.offSlot, s);
+    offStart.upload(m.offStart, s);
+    offContrib.upload(m.offContrib, s);
     if (m.fieldCount > 0) {
       fieldValues.upload(m.fieldData(), m.fieldCount, s);
       CK(cudaStreamSynchronize(s));  // the copy has read the caller's samples; the model keeps no pointer to them
@@ -265,8 +266,9 @@ struct drape_solver {
     d.diagSlot = diagSlot.p;
     d.incStart = incStart.p;
     d.incEntry = incEntry.p;
-    d.incLocal = incLocal.p;
-    d.slotRow = slotRow.p;
+    d.offSlot = offSlot.p;
+    d.offStart = offStart.p;
+    d.offContrib = offContrib.p;
     d.x = x.p;
     d.v = v.p;
     d.xStart = xStart.p;
