@@ -176,36 +176,34 @@ struct GridSync {
   // The whole grid as one group.
   __device__ void init(Control* c, unsigned long long lim) { init(c, lim, blockIdx.x, gridDim.x); }
 
-  // blockSynced: the caller has just passed a __syncthreads after every thread's writes of this phase and only
-  // thread 0 publishes after it (the case of gridReduce), so the leading block barrier can be skipped.
-  __device__ bool sync(bool blockSynced = false) {
-    __shared__ int ok;
-    target += size;
-    if (!blockSynced) __syncthreads();
-    if (threadIdx.x == 0) {
-      unsigned long long* counter = &ctl->barrierArrivals;
-      asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(counter), "l"(1ull) : "memory");
-      int good = 1;
-      unsigned int spins = 0;
-      const unsigned long long start = globalTimerNs();
-      for (;;) {
-        unsigned long long seen;
-        asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(seen) : "l"(counter) : "memory");
-        if (seen >= target) break;
-        if ((++spins & 31u) == 0) {
-          if (*reinterpret_cast<volatile int*>(&ctl->error) != 0) {
-            good = 0;
-            break;
-          }
-          if (globalTimerNs() - start > limitNs) {
-            atomicExch(&ctl->error, 1);
-            good = 0;
-            break;
-          }
+  // One thread's arrival for the whole block (release: the block's writes before it, ordered by the caller, become
+  // visible) and its bounded wait for the group (acquire). The caller advances `target` first. Returns 0 when the
+  // limit ran out or another block raised the error flag.
+  __device__ int arriveAndWait() const {
+    unsigned long long* counter = &ctl->barrierArrivals;
+    asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(counter), "l"(1ull) : "memory");
+    unsigned int spins = 0;
+    const unsigned long long start = globalTimerNs();
+    for (;;) {
+      unsigned long long seen;
+      asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(seen) : "l"(counter) : "memory");
+      if (seen >= target) return 1;
+      if ((++spins & 31u) == 0) {
+        if (*reinterpret_cast<volatile int*>(&ctl->error) != 0) return 0;
+        if (globalTimerNs() - start > limitNs) {
+          atomicExch(&ctl->error, 1);
+          return 0;
         }
       }
-      ok = good;
     }
+  }
+
+  // A barrier of the whole group (no data).
+  __device__ bool sync() {
+    __shared__ int ok;
+    target += size;
+    __syncthreads();
+    if (threadIdx.x == 0) ok = arriveAndWait();
     __syncthreads();
     return ok != 0;
   }
@@ -247,33 +245,82 @@ __device__ inline void blockSum(double (&v)[K], double* out) {
   blockReduce<K, false>(v, out);
 }
 
-// Grid-wide FP64 sums (or maxima): every block publishes its block total and passes the barrier; then thread t of
-// every block reads the totals of blocks t, t + blockDim, ... and the block combines them in its fixed tree, so every
-// block obtains bit-identical results and takes the same branches. Returns false when the barrier gave up.
+// a + b, or the larger of the two.
+template <bool Max>
+__device__ __forceinline__ double combine(double a, double b) {
+  return Max ? fmax(a, b) : a + b;
+}
+
+// Grid-wide FP64 sums (or maxima). The warps' sums meet in shared memory; warp 0 combines them, publishes the block
+// total, arrives at the group barrier and waits, then reads every block's total (lane l: blocks l, l + 32, ..., all
+// loads issued before the first add) and combines them in a fixed order; the other warps wait at one block barrier
+// meanwhile. Every block obtains bit-identical results and takes the same branches. Two block barriers per call: `red`
+// is rewritten only after the closing barrier, by which warp 0 has read it, and `res` only after the next call's first
+// barrier, by which every warp has read it. Returns false when the barrier gave up.
 template <int K, bool Max = false>
 __device__ inline bool gridReduce(const Dev& D, GridSync& gs, double (&v)[K], double (&out)[K]) {
+  constexpr int kLoads = 5;  // partials a lane loads at a time (160 blocks per round: one round for one block per SM)
+  __shared__ double red[K][32];
   __shared__ double res[K];
+  __shared__ int ok;
+  constexpr double kIdentity = Max ? -INFINITY : 0.0;
   double* half = D.partials + static_cast<size_t>(gs.parity) * gs.size * kPartialStride;
   gs.parity ^= 1u;
-  {
-    double blk[K];
-    blockReduce<K, Max>(v, blk);
-    if (threadIdx.x == 0)
+  gs.target += gs.size;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
 #pragma unroll
-      for (int k = 0; k < K; ++k) half[gs.rank * kPartialStride + k] = blk[k];
-  }
-  if (!gs.sync(true)) return false;
-  double s[K];
+  for (int k = 0; k < K; ++k)
 #pragma unroll
-  for (int k = 0; k < K; ++k) s[k] = Max ? -INFINITY : 0.0;
-  for (unsigned int b = threadIdx.x; b < gs.size; b += blockDim.x)
+    for (int o = 16; o > 0; o >>= 1) v[k] = combine<Max>(v[k], __shfl_down_sync(0xffffffffu, v[k], o));
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k) red[k][w] = v[k];
+  __syncthreads();
+  if (w == 0) {
+    double s[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      const double x = __ldcg(half + b * kPartialStride + k);
-      s[k] = Max ? fmax(s[k], x) : s[k] + x;
+      s[k] = lane < nw ? red[k][lane] : kIdentity;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s[k] = combine<Max>(s[k], __shfl_down_sync(0xffffffffu, s[k], o));
     }
-  blockReduce<K, Max>(s, res);
+    int good = 0;
+    if (lane == 0) {
+#pragma unroll
+      for (int k = 0; k < K; ++k) half[gs.rank * kPartialStride + k] = s[k];
+      good = gs.arriveAndWait();
+    }
+    good = __shfl_sync(0xffffffffu, good, 0);
+    __syncwarp();  // the other lanes' reads below follow lane 0's acquire
+    if (good) {
+      double t[K];
+#pragma unroll
+      for (int k = 0; k < K; ++k) t[k] = kIdentity;
+      for (unsigned int b0 = 0; b0 < gs.size; b0 += 32 * kLoads) {
+        double x[kLoads][K];
+#pragma unroll
+        for (int j = 0; j < kLoads; ++j) {
+          const unsigned int b = b0 + 32 * j + lane;
+#pragma unroll
+          for (int k = 0; k < K; ++k) x[j][k] = b < gs.size ? __ldcg(half + b * kPartialStride + k) : kIdentity;
+        }
+#pragma unroll
+        for (int j = 0; j < kLoads; ++j)
+#pragma unroll
+          for (int k = 0; k < K; ++k) t[k] = combine<Max>(t[k], x[j][k]);
+      }
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t[k] = combine<Max>(t[k], __shfl_down_sync(0xffffffffu, t[k], o));
+      if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < K; ++k) res[k] = t[k];
+    }
+    if (lane == 0) ok = good;
+  }
   __syncthreads();
+  if (!ok) return false;
 #pragma unroll
   for (int k = 0; k < K; ++k) out[k] = res[k];
   return true;
