@@ -631,7 +631,7 @@ __device__ inline double energyPartial(const Dev& D, const GridSync& gs, double 
 // iteration's SpMV reads them from there.
 //
 // The PCG follows the reference's order (cpu_solver.cpp:169-213): two grid reductions per iteration (p.Ap, then
-// r.r with r.z); the direction update p = z + beta p is folded into the next SpMV.
+// r.r with r.z); the direction update p = z + beta p is folded into the next SpMV (A p = A z + beta A pPrev).
 
 __device__ __forceinline__ M3 loadPrecond(const Dev& D, uint32_t i) {
   const float4 a = D.precond[3 * i], b = D.precond[3 * i + 1], c = D.precond[3 * i + 2];
@@ -815,19 +815,19 @@ __device__ inline void directionProducts(const Dev& D, const SmemMatrix& A, uint
   }
 }
 
-// One PCG iteration's product with the direction update folded in (p_j = z_j + beta * pPrev_j): writes p_i (pCur),
-// Ap_i (apFull) and the contact-filtered Ap_i (ap); returns this thread's share of p . filtered Ap.
+// One PCG iteration's product for the direction p = z + beta * pPrev without materialising p first: the rows gather
+// only z_j and add beta times their previous product A pPrev (apFull). Writes p_i (pCur), Ap_i (apFull) and the
+// contact-filtered Ap_i (ap); returns this thread's share of p . filtered Ap.
 template <int RL>
 __device__ inline double directionStep(const Dev& D, const SmemMatrix& A, uint32_t r0, uint32_t r1,
                                        const float4* pPrev, float4* pCur, float fb, bool first) {
   double vpap = 0.0;
   directionProducts<RL>(
-      D, A, r0, r1,
-      [&](uint32_t j) {
-        const float3 zj = ld3(D.z, j);
-        return first ? zj : zj + ld3(pPrev, j) * fb;
-      },
-      [&](uint32_t i, float3 pi, float3 acc) {
+      D, A, r0, r1, [&](uint32_t j) { return ld3(D.z, j); },
+      [&](uint32_t i, float3 zi, float3 az) {
+        // A p = A z + beta A pPrev: the previous direction's product is this row's apFull.
+        const float3 pi = first ? zi : zi + ld3(pPrev, i) * fb;
+        const float3 acc = first ? az : az + ld3(D.apFull, i) * fb;
         pCur[i] = f4(pi);
         const float3 filtered = filterContact(D.contact[i], acc);
         D.apFull[i] = f4(acc);
