@@ -111,18 +111,33 @@ __global__ void k_stats(Dev D, double* part, unsigned int* done, StatsOut* out) 
     last = atomicAdd(done, 1u) == gridDim.x - 1;
   }
   __syncthreads();
-  if (last && threadIdx.x == 0) {
-    __threadfence();
+  if (!last) return;
+  // The last block combines the blocks' rows: thread t reads rows t, t + blockDim, ... (their loads in flight
+  // together across the block), then fixed-shape block reductions.
+  __threadfence();
+  double sum3[3] = {0.0, 0.0, 0.0}, max2[2] = {0.0, 0.0};
+  int nonFinite = 0;
+  for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+    const double* row = part + b * 8;
+    sum3[0] += __ldcg(row + 0);
+    sum3[1] += __ldcg(row + 1);
+    max2[0] = fmax(max2[0], __ldcg(row + 2));
+    max2[1] = fmax(max2[1], __ldcg(row + 3));
+    sum3[2] += __ldcg(row + 4);
+    nonFinite |= __ldcg(row + 5) != 0.0;
+  }
+  __shared__ double tot3[3], tot2[2];
+  blockSum<3>(sum3, tot3);
+  blockReduce<2, true>(max2, tot2);
+  nonFinite = __syncthreads_or(nonFinite);
+  if (threadIdx.x == 0) {
     StatsOut s{};
-    for (unsigned int b = 0; b < gridDim.x; ++b) {
-      const double* row = part + b * 8;
-      s.kineticEnergy += __ldcg(row + 0);
-      s.sumV2 += __ldcg(row + 1);
-      s.maxSeamGap = fmax(s.maxSeamGap, __ldcg(row + 2));
-      s.maxPenetration = fmax(s.maxPenetration, __ldcg(row + 3));
-      s.moving += static_cast<unsigned long long>(__ldcg(row + 4));
-      s.nonFinite |= __ldcg(row + 5) != 0.0;
-    }
+    s.kineticEnergy = tot3[0];
+    s.sumV2 = tot3[1];
+    s.moving = static_cast<unsigned long long>(tot3[2]);
+    s.maxSeamGap = tot2[0];
+    s.maxPenetration = tot2[1];
+    s.nonFinite = nonFinite != 0;
     *out = s;
     *done = 0;
   }
