@@ -1091,6 +1091,30 @@ int drape_model_structure(const drape_model* dm, uint32_t* row_start, uint32_t* 
   });
 }
 
+int drape_model_gather_sizes(const drape_model* dm, uint32_t sizes[4]) {
+  return guarded(nullptr, [&] {
+    if (!dm || !sizes) throw std::invalid_argument("null model or sizes");
+    const Model& m = dm->m;
+    sizes[0] = static_cast<uint32_t>(m.x.size());
+    sizes[1] = static_cast<uint32_t>(m.incEntry.size());
+    sizes[2] = static_cast<uint32_t>(m.offSlot.size());
+    sizes[3] = static_cast<uint32_t>(m.offContrib.size());
+  });
+}
+
+int drape_model_gather_lists(const drape_model* dm, uint32_t* inc_start, uint32_t* inc_entry, uint32_t* off_slot,
+                             uint32_t* off_start, uint32_t* off_contrib) {
+  return guarded(nullptr, [&] {
+    if (!dm) throw std::invalid_argument("null model");
+    const Model& m = dm->m;
+    if (inc_start) std::copy(m.incStart.begin(), m.incStart.end(), inc_start);
+    if (inc_entry) std::copy(m.incEntry.begin(), m.incEntry.end(), inc_entry);
+    if (off_slot) std::copy(m.offSlot.begin(), m.offSlot.end(), off_slot);
+    if (off_start) std::copy(m.offStart.begin(), m.offStart.end(), off_start);
+    if (off_contrib) std::copy(m.offContrib.begin(), m.offContrib.end(), off_contrib);
+  });
+}
+
 int drape_cuda_contact_candidates(drape_solver* s, const float* x_start, uint8_t* near_flag, float* normal,
                                   float* offset) {
   return guarded(s, [&] {

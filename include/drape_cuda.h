@@ -144,6 +144,14 @@ int drape_model_structure_sizes(const drape_model* m, uint32_t sizes[5]);
 int drape_model_structure(const drape_model* m, uint32_t* row_start, uint32_t* col_index, uint32_t* diag_slot,
                           uint32_t* stretch_slots, uint32_t* hinge_slots, uint32_t* seam_slots, uint32_t* stretch_v,
                           uint32_t* hinge_v, uint32_t* seam_ab);
+/* The assembly's gather lists, in place of the reference's per-particle and per-slot gather lists
+   (gpu_solver_core.cpp:184-224): per particle its incidence entries (term kind << 30 | term << 2 | vertex a) in
+   gather order; per off-diagonal block slot, in slot order, the slot (row << 6 | row-local position) and its
+   contributions (incidence entry << 2 | block b of the entry's term) in gather order. sizes: particles, incidence
+   entries, off-diagonal slots, contributions. Any output pointer may be null. */
+int drape_model_gather_sizes(const drape_model* m, uint32_t sizes[4]);
+int drape_model_gather_lists(const drape_model* m, uint32_t* inc_start, uint32_t* inc_entry, uint32_t* off_slot,
+                             uint32_t* off_start, uint32_t* off_contrib);
 
 /* Contact candidates (kernels.h:55-82 / cpu_solver.cpp:247-263) for given substep-start positions (3 floats per
    particle), computed by the device's contact-setup code path: near flag, normal (3 floats), plane offset. The solver

@@ -130,3 +130,70 @@ def test_build_errors_match_reference(cuda_mod, oracle_mod, bad, exc):
     if bad != "triangle":
         with pytest.raises(exc):
             oracle_mod.OracleSolver().build(scene)
+
+
+def product_gather_lists(cuda_mod, scene):
+    """The product's gather lists (drape_model_gather_lists) re-expressed in the reference's contribution numbering:
+    per particle [i, then the term-gradient index of each incidence entry]; per block slot [i for a diagonal slot,
+    then the term-block index of each contribution] (gpu_solver_core.cpp:184-224)."""
+    L = cuda_mod.load()
+    L.drape_model_build.argtypes = [C.POINTER(drape_scene_desc), C.POINTER(C.c_void_p)]
+    L.drape_model_destroy.argtypes = [C.c_void_p]
+    L.drape_model_last_error.restype = C.c_char_p
+    L.drape_model_gather_sizes.argtypes = [C.c_void_p, C.POINTER(C.c_uint32)]
+    L.drape_model_gather_lists.argtypes = [C.c_void_p] + [C.POINTER(C.c_uint32)] * 5
+    desc = SceneDesc(scene)
+    h = C.c_void_p()
+    code = L.drape_model_build(desc.ptr(), C.byref(h))
+    if code != 0:
+        cuda_mod._raise(code, L.drape_model_last_error())
+    try:
+        sz = (C.c_uint32 * 4)()
+        assert L.drape_model_gather_sizes(h, sz) == 0
+        n, E, O, NC = list(sz)
+        inc_start, inc_entry = np.zeros(n + 1, np.uint32), np.zeros(E, np.uint32)
+        off_slot, off_start, off_contrib = np.zeros(O, np.uint32), np.zeros(O + 1, np.uint32), np.zeros(NC, np.uint32)
+        arrs = [inc_start, inc_entry, off_slot, off_start, off_contrib]
+        assert L.drape_model_gather_lists(h, *[a.ctypes.data_as(C.POINTER(C.c_uint32)) for a in arrs]) == 0
+    finally:
+        L.drape_model_destroy(h)
+    return inc_start, inc_entry, off_slot, off_start, off_contrib
+
+
+@pytest.mark.parametrize("name", ["sheet_40x40", "sewn_pair", "tube_variant", "two_garments"])
+def test_assembly_gather_lists_match_reference(cuda_mod, oracle_mod, name):
+    """Bit-exact: every gradient row and every block slot of the product's assembly sums the same contributions in the
+    same order as the reference's gather lists (the oracle's restatement of gpu_solver_core.cpp:184-224)."""
+    scene = SCENES[name]()
+    inc_start, inc_entry, off_slot, off_start, off_contrib = product_gather_lists(cuda_mod, scene)
+    o = oracle_mod.OracleSolver()
+    o.build(scene)
+    st = o.structure()
+    n, Sn, H = len(st["diag_slot"]), len(st["stretch_v"]), len(st["hinge_v"])
+    kind, term, a = inc_entry >> 30, (inc_entry >> 2) & 0x0FFFFFFF, (inc_entry & 3).astype(np.int64)
+    term = term.astype(np.int64)
+    # Reference numbering: gradients n + 3t + a | n + 3S + 4h + a | n + 3S + 4H + 2k + a; blocks n + 9t + 3a + b |
+    # n + 9S + 16h + 4a + b | n + 9S + 16H + 4k + 2a + b.
+    gbase = np.where(kind == 0, n + 3 * term, np.where(kind == 1, n + 3 * Sn + 4 * term, n + 3 * Sn + 4 * H + 2 * term))
+    grad_ref = gbase + a
+    arity = np.where(kind == 0, 3, np.where(kind == 1, 4, 2))
+    bbase = np.where(kind == 0, n + 9 * term, np.where(kind == 1, n + 9 * Sn + 16 * term, n + 9 * Sn + 16 * H + 4 * term))
+    for i in range(n):
+        e0, e1 = inc_start[i], inc_start[i + 1]
+        got = [i] + list(grad_ref[e0:e1])
+        ref = list(st["grad_idx"][st["grad_start"][i]:st["grad_start"][i + 1]])
+        assert got == ref, i
+    B = len(st["col_index"])
+    per_slot = [None] * B
+    for i in range(n):  # diagonal slots: the own term, then block (a, a) of every incidence entry
+        e = np.arange(inc_start[i], inc_start[i + 1])
+        per_slot[st["diag_slot"][i]] = [i] + list(bbase[e] + arity[e] * a[e] + a[e])
+    rs = st["row_start"]
+    for k in range(len(off_slot)):
+        row, t = int(off_slot[k]) >> 6, int(off_slot[k]) & 63
+        c = off_contrib[off_start[k]:off_start[k + 1]].astype(np.int64)
+        e, b = c >> 2, c & 3
+        per_slot[rs[row] + t] = list(bbase[e] + arity[e] * a[e] + b)
+    for s in range(B):
+        ref = list(st["block_idx"][st["block_start"][s]:st["block_start"][s + 1]])
+        assert per_slot[s] == ref, s
