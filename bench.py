@@ -395,6 +395,30 @@ def bake_leg(peak):
     return out
 
 
+def mesh_leg():
+    """The pattern mesher (drape_mesh_build, host code; the reference's buildSimMesh): the tube workload's two
+    0.55 x 0.7 m panels sewn along both side edges, meshed at the reference's three particle distances, wall time
+    per mesh (best of 3) on one host core."""
+    from drape_b200 import mesher as M
+    a, b = M.rectangle_piece("front", 0.55, 0.7), M.rectangle_piece("back", 0.55, 0.7)
+    pat = M.Pattern([a, b], [M.SeamSpec("left", M.segment_edge(a, "left", "left", False),
+                                        M.segment_edge(b, "right", "right", True)),
+                             M.SeamSpec("right", M.segment_edge(a, "right", "right", False),
+                                        M.segment_edge(b, "left", "left", True))])
+    out = {}
+    for q in ("draft", "standard", "fine"):
+        h = M.particle_distance(q)
+        best, m = None, None
+        for _ in range(3):
+            t0 = time.perf_counter()
+            m = M.build_sim_mesh(pat, h)
+            dt = time.perf_counter() - t0
+            best = dt if best is None else min(best, dt)
+        out[q] = {"particle_distance_m": h, "vertices": int(len(m.rest)), "triangles": int(len(m.triangles)),
+                  "seam_pairs": int(len(m.seam_pairs)), "ms": 1000.0 * best}
+    return out
+
+
 def run_profile_case(args):
     """One small case for an ncu capture (not a benchmark line): "spmv" times the standalone SpMV on the tiled tube
     system; "batch" builds the first --batch-garments tubes of the batched workload and runs --batch-frames frames
@@ -639,6 +663,7 @@ def main():
         line["batch"] = batch_leg(args, local, world, rank, max_over_ranks, peak)
     if rank == 0:
         line["bake"] = bake_leg(peak)
+        line["mesh"] = mesh_leg()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.workload)
     if rank == 0:

@@ -13,7 +13,7 @@ LIB_DIR = os.path.join(ROOT, "lib")
 LIB = os.path.join(LIB_DIR, "libdrape_cuda.so")
 OBJ_DIR = os.path.join(LIB_DIR, "obj")
 
-SOURCES = ["solver.cu", "batch.cu", "learned.cu", "bake.cu", "model.cpp"]
+SOURCES = ["solver.cu", "batch.cu", "learned.cu", "bake.cu", "model.cpp", "mesher.cpp"]
 HEADERS = ["kernels.cuh", "device_math.cuh", "model.hpp", "learned.hpp", "umma.cuh", "device_model.hpp",
            "device_buffer.hpp", "solver_kernels.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -22,7 +22,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 def _inputs():
     files = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
-    headers = ("drape_cuda.h", "drape_scene.h", "drape_precond.h", "drape_batch.h", "drape_bake.h")
+    headers = ("drape_cuda.h", "drape_scene.h", "drape_precond.h", "drape_batch.h", "drape_bake.h", "drape_mesh.h")
     files += [os.path.join(REPO, "include", h) for h in headers]
     return files
 

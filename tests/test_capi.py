@@ -15,7 +15,7 @@ def declared_functions():
     for h in sorted(os.listdir(os.path.join(ROOT, "include"))):
         src = open(os.path.join(ROOT, "include", h)).read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-        names.update(re.findall(r"\b((?:drape_cuda|drape_model|drape_precond|drape_batch)_[a-z0-9_]+)\s*\(", src))
+        names.update(re.findall(r"\b((?:drape_cuda|drape_model|drape_precond|drape_batch|drape_bake|drape_mesh)_[a-z0-9_]+)\s*\(", src))
     return sorted(names)
 
 
@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol(cuda_mod):
     for name in declared_functions():
         assert hasattr(lib, name), name
     out = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True, text=True, check=True).stdout
-    exported = set(re.findall(r" T ((?:drape_cuda|drape_model|drape_precond|drape_batch)_\w+)", out))
+    exported = set(re.findall(r" T ((?:drape_cuda|drape_model|drape_precond|drape_batch|drape_bake|drape_mesh)_\w+)", out))
     assert set(declared_functions()) <= exported
 
 
