@@ -96,7 +96,7 @@ struct drape_solver {
     cudaEvent_t a, b;
     int kind;
   };
-  bool profiling = false;
+  int profiling = 0;  // 0 off, 1 every kernel, 2 k_solve only
   std::vector<cudaEvent_t> eventPool;
   std::vector<Pending> pending;
   drape_profile prof{};
@@ -111,9 +111,10 @@ struct drape_solver {
     eventPool.pop_back();
     return e;
   }
-  // Records a start event when profiling; returns it (or nullptr).
-  cudaEvent_t profStart() {
-    if (!profiling) return nullptr;
+  // Records a start event when profiling kernels of this kind (1: all kernels, 2: only k_solve, kind 3); returns it
+  // (or nullptr).
+  cudaEvent_t profStart(int kind) {
+    if (profiling == 0 || (profiling == 2 && kind != 3)) return nullptr;
     cudaEvent_t a = takeEvent();
     CK(cudaEventRecord(a, stream));
     return a;
@@ -414,31 +415,31 @@ struct drape_solver {
     d.P.learnedSwitch = precondSwitch;
     const uint32_t n = d.P.n;
     const int pg = std::max(1, static_cast<int>(std::min<uint32_t>((n + 255) / 256, static_cast<uint32_t>(pointGrid))));
-    cudaEvent_t e = profStart();
+    cudaEvent_t e = profStart(0);
     dcu::k_begin<<<pg, 256, 0, stream>>>(d);
     CK(cudaGetLastError());
     profStop(e, 0);
     for (int it = 0; it < iterations; ++it) {
-      e = profStart();
+      e = profStart(1);
       dcu::k_activate<<<pg, 256, 0, stream>>>(d);
       profStop(e, 1);
-      e = profStart();
+      e = profStart(2);
       dcu::k_terms<<<termsGrid, dcu::kTermThreads, 0, stream>>>(d);
       profStop(e, 2);
-      e = profStart();
+      e = profStart(2);
       dcu::k_assemble<<<assembleGrid, dcu::kAssembleThreads, 0, stream>>>(d);
       CK(cudaGetLastError());
       profStop(e, 2);
       if (learnedOn && netGraph && netNewtonCounter++ % static_cast<uint64_t>(precondRefresh) == 0) {
-        e = profStart();
+        e = profStart(6);
         net->forwardOn(net->graphOf(*netGraph), stream, false, &ctl.p->error);
         profStop(e, 6);
       }
-      e = profStart();
+      e = profStart(3);
       launchSolve(d);
       profStop(e, 3);
     }
-    e = profStart();
+    e = profStart(4);
     dcu::k_finish<<<pg, 256, 0, stream>>>(d);
     dcu::k_advance_clock<<<1, 32, 0, stream>>>(d);
     CK(cudaGetLastError());
@@ -478,7 +479,7 @@ struct drape_solver {
     use();
     drape_stats st{};
     if (m.x.empty()) return st;
-    cudaEvent_t e = profStart();
+    cudaEvent_t e = profStart(5);
     dcu::k_stats<<<statsGrid, 256, 0, stream>>>(dev, statsPartials.p, statsDone.p, statsOut.p);
     CK(cudaGetLastError());
     profStop(e, 5);
@@ -992,7 +993,7 @@ int drape_cuda_profile(drape_solver* s, int enable) {
     s->use();
     CK(cudaStreamSynchronize(s->stream));
     s->collectProfile();
-    s->profiling = enable != 0;
+    s->profiling = enable == 2 ? 2 : (enable != 0 ? 1 : 0);
     if (s->profiling) {
       s->prof = drape_profile{};
       const drape_counters c = s->counters();

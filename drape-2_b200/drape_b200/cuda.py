@@ -278,8 +278,10 @@ class CudaSolver:
         self._check(self.L.drape_cuda_stream(self.h, C.byref(p)))
         return p.value or 0
 
-    def profile(self, enable: bool) -> None:
-        self._check(self.L.drape_cuda_profile(self.h, 1 if enable else 0))
+    def profile(self, enable, solve_only: bool = False) -> None:
+        """Per-kernel CUDA-event timing on the solver's stream: every kernel, or (solve_only) k_solve alone, which
+        adds two events a Newton iteration instead of two around every launch."""
+        self._check(self.L.drape_cuda_profile(self.h, (2 if solve_only else 1) if enable else 0))
 
     def profile_read(self) -> dict:
         p = drape_profile()

@@ -121,7 +121,9 @@ typedef struct drape_profile {
   int64_t cg_iterations;        /* PCG iterations inside the profiled solve launches */
   int64_t energy_evaluations;   /* FP64 energy passes (E(0) and every line-search trial) */
 } drape_profile;
-int drape_cuda_profile(drape_solver* s, int enable); /* enabling also clears the accumulated figures */
+/* enable: 0 off, 1 every kernel, 2 k_solve only (two events a launch, for timing a drape with little overhead);
+   enabling also clears the accumulated figures. */
+int drape_cuda_profile(drape_solver* s, int enable);
 int drape_cuda_profile_read(const drape_solver* s, drape_profile* out);
 
 /* Bytes copied host -> device and device -> host by this solver since creation. */
