@@ -4,7 +4,9 @@
 #include <algorithm>
 #include <cmath>
 #include <numeric>
+#include <exception>
 #include <stdexcept>
+#include <thread>
 
 namespace drape_b200 {
 
@@ -333,94 +335,157 @@ void Model::buildIncidence() {
   for (std::size_t i = 0; i < n; ++i) maxRowEntries = std::max(maxRowEntries, incStart[i + 1] - incStart[i]);
 }
 
+namespace {
+
+// Runs f(c) for c in [0, chunks) on up to `chunks` threads (the calling thread takes chunk 0); the first exception a
+// chunk throws is rethrown after all have finished.
+template <class F>
+void parallelChunks(std::size_t chunks, F&& f) {
+  if (chunks <= 1) {
+    if (chunks == 1) f(0);
+    return;
+  }
+  std::vector<std::exception_ptr> errors(chunks);
+  std::vector<std::thread> pool;
+  for (std::size_t c = 1; c < chunks; ++c)
+    pool.emplace_back([&, c] {
+      try {
+        f(c);
+      } catch (...) {
+        errors[c] = std::current_exception();
+      }
+    });
+  try {
+    f(0);
+  } catch (...) {
+    errors[0] = std::current_exception();
+  }
+  for (auto& t : pool) t.join();
+  for (auto& e : errors)
+    if (e) std::rethrow_exception(e);
+}
+
+}  // namespace
+
 void Model::buildStructure() {
   const std::size_t n = x.size();
-  // One pass over the rows, each from its incidence entries. Row i's columns: i itself and every vertex of every term
-  // that contains i, deduplicated with a stamp array and sorted -- the sorted unique coupled columns of the reference's
-  // per-row vectors (sim_model.cpp:41-74). Then where[c] = the slot of column c in row i, which gives each incident
-  // term's slots of row i and the entry's row-local slot positions with one load per lookup (the reference finds
-  // them by binary search, sim_model.cpp:35-39; the slots are the same).
-  rowStart.assign(n + 1, 0);
-  colIndex.clear();
-  colIndex.reserve(incStart[n] + n);
-  offSlot.clear();
-  offSlot.reserve(incStart[n]);
-  offStart.clear();
-  offStart.reserve(incStart[n] + 1);
-  offContrib.clear();
-  offContrib.reserve(2 * static_cast<std::size_t>(incStart[n]));
+  // Row i's columns: i itself and every vertex of every term that contains i, deduplicated with a stamp array and
+  // sorted -- the sorted unique coupled columns of the reference's per-row vectors (sim_model.cpp:41-74). Each term's
+  // slots are the positions of its vertices' columns in their rows (the reference finds them by binary search,
+  // sim_model.cpp:35-39; the slots are the same). Rows are built in chunks on several threads, each chunk into its
+  // own buffers with row-local positions; a prefix sum over the row sizes then places every chunk.
   if (n >= (1u << 26)) throw std::invalid_argument("too many particles for the slot encoding");
   if (incStart[n] >= (1u << 29)) throw std::invalid_argument("too many term incidences for the contribution encoding");
-  diagSlot.resize(n);
+  rowStart.assign(n + 1, 0);
+  diagSlot.assign(n, 0);
   stretchSlots.resize(stretch.size());
   hingeSlots.resize(hinges.size());
   seamSlots.resize(seams.size());
-  std::vector<uint32_t> stamp(n, UINT32_MAX), where(n, 0);
-  maxRowSlots = 0;
-  for (uint32_t i = 0; i < n; ++i) {
-    const uint32_t rs = static_cast<uint32_t>(colIndex.size());
-    stamp[i] = i;
-    colIndex.push_back(i);
-    uint32_t vs[4];
-    for (uint32_t e = incStart[i]; e < incStart[i + 1]; ++e) {
-      const int m = termVertices(incEntry[e], vs);
-      for (int b = 0; b < m; ++b)
-        if (stamp[vs[b]] != i) {
-          stamp[vs[b]] = i;
-          colIndex.push_back(vs[b]);
-        }
-    }
-    std::sort(colIndex.begin() + rs, colIndex.end());
-    rowStart[i + 1] = static_cast<uint32_t>(colIndex.size());
-    const uint32_t L = rowStart[i + 1] - rs;
-    maxRowSlots = std::max<uint32_t>(maxRowSlots, L);
-    if (L > kMaxRowSlots)
-      throw std::invalid_argument("a particle couples to " + std::to_string(L) + " particles; the CUDA solver supports " +
-                                  std::to_string(kMaxRowSlots));
-    for (uint32_t k = rs; k < rowStart[i + 1]; ++k)
-      if (colIndex[k] != i) offSlot.push_back((i << 6) | (k - rs));
-    for (uint32_t k = rs; k < rowStart[i + 1]; ++k) where[colIndex[k]] = k;
-    diagSlot[i] = where[i];
-    for (uint32_t e = incStart[i]; e < incStart[i + 1]; ++e) {
-      const uint32_t code = incEntry[e], kind = code >> 30, term = (code >> 2) & 0x0FFFFFFFu, a = code & 3u;
-      const int m = termVertices(code, vs);
-      uint32_t* out = kind == 0 ? stretchSlots[term].data() : (kind == 1 ? hingeSlots[term].data() : seamSlots[term].data());
-      uint32_t packed = 0;
-      for (int b = 0; b < m; ++b) {
-        const uint32_t sl = where[vs[b]];
-        out[a * m + b] = sl;
-        packed |= ((sl - rs) & 0xFFu) << (8 * b);
-      }
-      incLocal[e] = packed;
-    }
-    // Contribution lists of the row's off-diagonal slots, in slot order: entry e's block b lands in row-local slot
-    // byte b of incLocal[e]; each list keeps the incidence (gather) order.
-    uint32_t cnt[kMaxRowSlots] = {};
-    uint32_t pos[kMaxRowSlots];
-    for (uint32_t e = incStart[i]; e < incStart[i + 1]; ++e) {
-      const int m = entryArity(incEntry[e]);
-      for (int b = 0; b < m; ++b) ++cnt[(incLocal[e] >> (8 * b)) & 0xFFu];
-    }
-    const uint32_t dl = diagSlot[i] - rs;
-    uint32_t next = static_cast<uint32_t>(offContrib.size());
-    for (uint32_t t = 0; t < L; ++t) {
-      if (t == dl) continue;
-      offStart.push_back(next);
-      pos[t] = next;
-      next += cnt[t];
-    }
-    offContrib.resize(next);
-    for (uint32_t e = incStart[i]; e < incStart[i + 1]; ++e) {
-      const int m = entryArity(incEntry[e]);
-      for (int b = 0; b < m; ++b) {
-        const uint32_t t = (incLocal[e] >> (8 * b)) & 0xFFu;
-        if (t != dl) offContrib[pos[t]++] = (e << 2) | static_cast<uint32_t>(b);
-      }
-    }
+  struct Chunk {
+    uint32_t r0 = 0, r1 = 0;
+    std::vector<uint32_t> cols, offSlot, offStart, offContrib;
+    uint32_t maxL = 0;
+  };
+  const std::size_t threads = std::max<std::size_t>(1, std::min<std::size_t>(16, std::thread::hardware_concurrency()));
+  const std::size_t chunkCount = std::max<std::size_t>(1, std::min(threads, (n + 8191) / 8192));
+  std::vector<Chunk> chunks(chunkCount);
+  for (std::size_t c = 0; c < chunkCount; ++c) {
+    chunks[c].r0 = static_cast<uint32_t>(n * c / chunkCount);
+    chunks[c].r1 = static_cast<uint32_t>(n * (c + 1) / chunkCount);
   }
-  offStart.push_back(static_cast<uint32_t>(offContrib.size()));
-  colIndex.shrink_to_fit();
-  offSlot.shrink_to_fit();
+  // Pass 1: per row, the sorted columns, the row-local slot positions of its incidence entries (incLocal), its
+  // diagonal position (kept in diagSlot until pass 2) and its off-diagonal slots' contribution lists in slot order
+  // (entry e's block b lands in row-local slot byte b of incLocal[e]; each list keeps the incidence order).
+  parallelChunks(chunkCount, [&](std::size_t c) {
+    Chunk& ch = chunks[c];
+    std::vector<uint32_t> stamp(n, UINT32_MAX), where(n, 0);
+    uint32_t vs[4];
+    for (uint32_t i = ch.r0; i < ch.r1; ++i) {
+      const std::size_t rs = ch.cols.size();
+      stamp[i] = i;
+      ch.cols.push_back(i);
+      for (uint32_t e = incStart[i]; e < incStart[i + 1]; ++e) {
+        const int m = termVertices(incEntry[e], vs);
+        for (int b = 0; b < m; ++b)
+          if (stamp[vs[b]] != i) {
+            stamp[vs[b]] = i;
+            ch.cols.push_back(vs[b]);
+          }
+      }
+      std::sort(ch.cols.begin() + static_cast<std::ptrdiff_t>(rs), ch.cols.end());
+      const uint32_t L = static_cast<uint32_t>(ch.cols.size() - rs);
+      ch.maxL = std::max(ch.maxL, L);
+      if (L > kMaxRowSlots)
+        throw std::invalid_argument("a particle couples to " + std::to_string(L) + " particles; the CUDA solver supports " +
+                                    std::to_string(kMaxRowSlots));
+      rowStart[i + 1] = L;
+      for (uint32_t t = 0; t < L; ++t) where[ch.cols[rs + t]] = t;
+      const uint32_t dl = where[i];
+      diagSlot[i] = dl;
+      for (uint32_t t = 0; t < L; ++t)
+        if (t != dl) ch.offSlot.push_back((i << 6) | t);
+      uint32_t cnt[kMaxRowSlots] = {};
+      for (uint32_t e = incStart[i]; e < incStart[i + 1]; ++e) {
+        const int m = termVertices(incEntry[e], vs);
+        uint32_t packed = 0;
+        for (int b = 0; b < m; ++b) {
+          const uint32_t t = where[vs[b]];
+          packed |= t << (8 * b);
+          ++cnt[t];
+        }
+        incLocal[e] = packed;
+      }
+      uint32_t pos[kMaxRowSlots];
+      uint32_t next = static_cast<uint32_t>(ch.offContrib.size());
+      for (uint32_t t = 0; t < L; ++t) {
+        if (t == dl) continue;
+        ch.offStart.push_back(next);
+        pos[t] = next;
+        next += cnt[t];
+      }
+      ch.offContrib.resize(next);
+      for (uint32_t e = incStart[i]; e < incStart[i + 1]; ++e) {
+        const int m = entryArity(incEntry[e]);
+        for (int b = 0; b < m; ++b) {
+          const uint32_t t = (incLocal[e] >> (8 * b)) & 0xFFu;
+          if (t != dl) ch.offContrib[pos[t]++] = (e << 2) | static_cast<uint32_t>(b);
+        }
+      }
+    }
+  });
+  maxRowSlots = 0;
+  for (const Chunk& ch : chunks) maxRowSlots = std::max(maxRowSlots, ch.maxL);
+  for (std::size_t i = 0; i < n; ++i) rowStart[i + 1] += rowStart[i];
+  std::vector<std::size_t> offBase(chunkCount + 1, 0), contribBase(chunkCount + 1, 0);
+  for (std::size_t c = 0; c < chunkCount; ++c) {
+    offBase[c + 1] = offBase[c] + chunks[c].offSlot.size();
+    contribBase[c + 1] = contribBase[c] + chunks[c].offContrib.size();
+  }
+  colIndex.assign(rowStart[n], 0);
+  offSlot.assign(offBase[chunkCount], 0);
+  offStart.assign(offBase[chunkCount] + 1, 0);
+  offContrib.assign(contribBase[chunkCount], 0);
+  offStart[offBase[chunkCount]] = static_cast<uint32_t>(contribBase[chunkCount]);
+  // Pass 2: every chunk into place; global slots of the diagonal and of every term's blocks.
+  parallelChunks(chunkCount, [&](std::size_t c) {
+    const Chunk& ch = chunks[c];
+    std::copy(ch.cols.begin(), ch.cols.end(), colIndex.begin() + rowStart[ch.r0]);
+    std::copy(ch.offSlot.begin(), ch.offSlot.end(), offSlot.begin() + static_cast<std::ptrdiff_t>(offBase[c]));
+    for (std::size_t k = 0; k < ch.offStart.size(); ++k)
+      offStart[offBase[c] + k] = static_cast<uint32_t>(contribBase[c] + ch.offStart[k]);
+    std::copy(ch.offContrib.begin(), ch.offContrib.end(),
+              offContrib.begin() + static_cast<std::ptrdiff_t>(contribBase[c]));
+    for (uint32_t i = ch.r0; i < ch.r1; ++i) {
+      const uint32_t rs = rowStart[i];
+      diagSlot[i] += rs;
+      for (uint32_t e = incStart[i]; e < incStart[i + 1]; ++e) {
+        const uint32_t code = incEntry[e], kind = code >> 30, term = (code >> 2) & 0x0FFFFFFFu, a = code & 3u;
+        const int m = entryArity(code);
+        uint32_t* out = kind == 0 ? stretchSlots[term].data() : (kind == 1 ? hingeSlots[term].data() : seamSlots[term].data());
+        for (int b = 0; b < m; ++b) out[a * m + b] = rs + ((incLocal[e] >> (8 * b)) & 0xFFu);
+      }
+    }
+  });
   contactForce.assign(n, 0.0);
 }
 
