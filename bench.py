@@ -92,11 +92,12 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_id: str):
+    def __init__(self, gpu_id: str, period_ms: int = 200):
         self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", gpu_id], stdout=self.file, stderr=subprocess.DEVNULL)
+                                          "-lms", str(period_ms), "-i", gpu_id], stdout=self.file,
+                                         stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
 
@@ -494,6 +495,7 @@ def main():
                     help="run one small case for a profiler capture instead of the benchmark")
     ap.add_argument("--spmv-tiles", type=int, default=12)
     ap.add_argument("--batch-frames", type=int, default=6)
+    ap.add_argument("--clock-period-ms", type=int, default=200, help="nvidia-smi clock sampling period")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -560,7 +562,7 @@ def main():
     solver.profile(True, solve_only=True)  # events around k_solve only: the timed drapes carry two events a launch
     barrier()
     torch.cuda.synchronize()
-    sampler = ClockSampler(gpu_id)
+    sampler = ClockSampler(gpu_id, args.clock_period_ms)
     times, results = [], []
     for _ in range(args.steps):
         for seed in range(SEEDS):
@@ -660,6 +662,7 @@ def main():
                   "frames_per_seed": [int(r.frames_run) for r in results[-SEEDS:]],
                   "settled_per_seed": [bool(r.settled) for r in results[-SEEDS:]],
                   "settle_s_per_seed": [float(t) for t in times[-SEEDS:]],
+                  "settle_s_median": float(np.median(times)),
                   "frames_mean": float(np.mean([r.frames_run for r in results])),
                   "assembly_seconds": float(results[-1].assembly_seconds),
                   "retries": int(sum(r.retries for r in results)),

@@ -448,11 +448,26 @@ struct drape_solver {
       if (g.phase == DRAPE_PHASE_ASSEMBLING) g.assemblyTime += h;
   }
 
+  // Waits for the stream by polling it: the per-frame waits of stepping and of the drape runner wake up without the
+  // scheduling delay a blocking synchronise can take on a busy host.
+  void waitStream() {
+    for (;;) {
+      const cudaError_t e = cudaStreamQuery(stream);
+      if (e == cudaSuccess) return;
+      if (e != cudaErrorNotReady) CK(e);
+    }
+  }
+
   void readControl() {
     CK(cudaMemcpyAsync(hCtl.p, ctl.p, sizeof(dcu::Control), cudaMemcpyDeviceToHost, stream));
-    CK(cudaStreamSynchronize(stream));
+    waitStream();
     d2hBytes += sizeof(dcu::Control);
     collectProfile();
+    checkControl();
+  }
+
+  // After the control block has reached hCtl: a device error status becomes std::runtime_error("cuda: ...").
+  void checkControl() {
     if (hCtl.p->error != 0) {
       const int e = hCtl.p->error;
       resetControlAfterError();
@@ -474,19 +489,47 @@ struct drape_solver {
     readControl();
   }
 
-  drape_stats stats() {
-    requireBuilt();
-    use();
-    drape_stats st{};
-    if (m.x.empty()) return st;
+  void enqueueStats() {
     cudaEvent_t e = profStart(5);
     dcu::k_stats<<<statsGrid, 256, 0, stream>>>(dev, statsPartials.p, statsDone.p, statsOut.p);
     CK(cudaGetLastError());
     profStop(e, 5);
     CK(cudaMemcpyAsync(hStats.p, statsOut.p, sizeof(dcu::StatsOut), cudaMemcpyDeviceToHost, stream));
-    CK(cudaStreamSynchronize(stream));
     d2hBytes += sizeof(dcu::StatsOut);
+  }
+
+  drape_stats stats() {
+    requireBuilt();
+    use();
+    if (m.x.empty()) return drape_stats{};
+    enqueueStats();
+    waitStream();
     collectProfile();
+    return hostStats();
+  }
+
+  // One frame and its statistics with one host synchronisation (the drape runner's per-frame pair of calls).
+  drape_stats advanceWithStats(double dt, int substeps, int iterations) {
+    requireBuilt();
+    use();
+    if (failAfter == 0) throw std::runtime_error("cuda: injected device failure");
+    if (failAfter > 0) --failAfter;
+    if (m.x.empty()) return drape_stats{};
+    const int sub = std::max(1, substeps);
+    const double h = dt / sub;
+    const int its = std::max(1, iterations);
+    for (int k = 0; k < sub; ++k) enqueueSubstep(h, its);
+    CK(cudaMemcpyAsync(hCtl.p, ctl.p, sizeof(dcu::Control), cudaMemcpyDeviceToHost, stream));
+    d2hBytes += sizeof(dcu::Control);
+    enqueueStats();
+    waitStream();
+    collectProfile();
+    checkControl();
+    return hostStats();
+  }
+
+  drape_stats hostStats() const {
+    drape_stats st{};
     const dcu::StatsOut& s = *hStats.p;
     st.has_non_finite = s.nonFinite;
     st.kinetic_energy = s.kineticEnergy;
@@ -658,12 +701,11 @@ drape_drape_result drapeToRest(drape_solver& s, const std::vector<std::string>& 
       state = DRAPE_STATE_TIMED_OUT;
       break;
     }
-    s.advance(o.frame_dt, substeps, o.iterations);
+    const drape_stats st = s.advanceWithStats(o.frame_dt, substeps, o.iterations);
     ++result.frames_run;
     ++keptFrames;
     time += o.frame_dt;
     phaseTime += o.frame_dt;
-    const drape_stats st = s.stats();
     riseFrames = st.kinetic_energy > lastEnergy ? riseFrames + 1 : 0;
     lastEnergy = st.kinetic_energy;
     if (st.has_non_finite || riseFrames >= o.energy_rise_frames) {
