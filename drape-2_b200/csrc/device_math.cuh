@@ -2,7 +2,7 @@
 // energies in FP64), the collision field and the post-solve push-out.
 //
 // The term formulas restate the reference's double-precision math (libs/sim/src/energies.cpp:11-110, stretch.hpp:15-49,
-// bending.hpp:29-51), organised for owner-computes assembly: a call returns one vertex's gradient and its row of
+// bending.hpp:29-51), organised for the assembly: a term's derivative record once, then any vertex's gradient and
 // Hessian blocks. The collision-field sampling uses explicitly rounded IEEE operations in the reference's FP32 order
 // (libs/sim/kernels/term_math.h:203-243 restating collision_field.cpp:8-41) so that the contact-candidate decisions
 // (phi < r + reach, |grad| < 1e-4) are bit-identical to the reference's 32-bit path on identical inputs.
@@ -126,8 +126,8 @@ __device__ __forceinline__ float coef(float4 d, int column, int k) {
 // for C > 0 and the one-sided strain limit at limitScale K; energies.cpp:27-62, stretch.hpp:15-49) at x[0..2]
 // (relative to vertex 0), in two parts: stretchDerivs evaluates the term once and keeps what every vertex's row needs
 // (per direction the unit vector n = f / |f| and the gradient, Gauss-Newton and tension scales; for the bias the
-// derivatives of n_u . n_v with respect to f_u and f_v and its scales), and stretchRowFrom forms the gradient of
-// vertex a and its Hessian row from that record and the term's dmInv coefficients.
+// derivatives of n_u . n_v with respect to f_u and f_v and its scales), and stretchBlockFrom forms any block (a, b)
+// of its Hessian and the gradient of vertex a from that record and the term's dmInv coefficients.
 struct StretchDer {
   float4 w[6];  // warp: (n, gs), (hs, ts, flags, -); weft: (n, gs), (hs, ts, -, -); bias: (dfu, K c), (dfv, K)
 };
@@ -178,41 +178,8 @@ __device__ inline void stretchDerivs(const StretchIn& t, const float3 x[3], Stre
   o.w[1].z = __uint_as_float(flags);
 }
 
-__device__ inline void stretchRowFrom(float4 d, const StretchDer& o, int a, float3& g, M3 H[3]) {
-  g = mk(0, 0, 0);
-#pragma unroll
-  for (int b = 0; b < 3; ++b) zero(H[b]);
-  const uint32_t flags = __float_as_uint(o.w[1].z);
-#pragma unroll
-  for (int which = 0; which < 2; ++which) {
-    if (!(flags & (which == 0 ? kStretchWarp : kStretchWeft))) continue;
-    const float3 n = xyz(o.w[2 * which]);
-    const float gs = o.w[2 * which].w, hs = o.w[2 * which + 1].x, ts = o.w[2 * which + 1].y;
-    float3 gr[3];
-#pragma unroll
-    for (int b = 0; b < 3; ++b) gr[b] = n * coef(d, which, b);
-    g += gr[a] * gs;
-    const float ca = coef(d, which, a);
-#pragma unroll
-    for (int b = 0; b < 3; ++b) {
-      addOuter(H[b], hs, gr[a], gr[b]);
-      if (ts != 0.0f) addProjector(H[b], ts * ca * coef(d, which, b), n);
-    }
-  }
-  if (flags & kStretchBias) {
-    const float3 dfu = xyz(o.w[4]), dfv = xyz(o.w[5]);
-    const float Kc = o.w[4].w, K = o.w[5].w;
-    float3 gr[3];
-#pragma unroll
-    for (int b = 0; b < 3; ++b) gr[b] = dfu * coef(d, 0, b) + dfv * coef(d, 1, b);
-    g += gr[a] * Kc;
-#pragma unroll
-    for (int b = 0; b < 3; ++b) addOuter(H[b], K, gr[a], gr[b]);
-  }
-}
-
 // Block (a, b) of a stretch term's Hessian and, with Grad, the gradient of vertex a, read from the term's record in
-// global memory: the operations stretchRowFrom performs for H[b] of row a and for its g, in the same order.
+// global memory: per direction K (grad_a C)(grad_b C)^T plus the tension projector, then the bias part.
 template <bool Grad>
 __device__ inline void stretchBlockFrom(float4 d, const float4* __restrict__ rec, int a, int b, float3& g, M3& H) {
   zero(H);
@@ -266,7 +233,7 @@ __device__ inline float dihedral(const float3 x[4], float3 g[4]) {
 }
 
 // Hinge term 1/2 K (theta - theta0)^2 with a Gauss-Newton Hessian (energies.cpp:64-69), in two parts: hingeDerivs
-// evaluates theta and its gradient once per term, hingeRowFrom forms vertex a's gradient and Hessian row.
+// evaluates theta and its gradient once per term, hingeBlockFrom forms vertex a's gradient and any Hessian block.
 struct HingeDer {
   float4 w[4];  // gradient of theta at vertex k (xyz); w[0].w = K (theta - rest), w[1].w = K
 };
@@ -281,21 +248,8 @@ __device__ inline void hingeDerivs(float K, float rest, const float3 x[4], Hinge
   o.w[3] = f4(gr[3]);
 }
 
-__device__ inline void hingeRowFrom(const HingeDer& o, int a, float3& g, M3 H[4]) {
-  float3 gr[4];
-#pragma unroll
-  for (int k = 0; k < 4; ++k) gr[k] = xyz(o.w[k]);
-  const float KC = o.w[0].w, K = o.w[1].w;
-  g = gr[a] * KC;
-#pragma unroll
-  for (int b = 0; b < 4; ++b) {
-    zero(H[b]);
-    addOuter(H[b], K, gr[a], gr[b]);
-  }
-}
-
-// Block (a, b) of a hinge term's Hessian and, with Grad, the gradient of vertex a from its record (hingeRowFrom's
-// operations).
+// Block (a, b) of a hinge term's Hessian, K (grad_a theta)(grad_b theta)^T, and with Grad the gradient of vertex a,
+// K (theta - rest) grad_a theta, from its record.
 template <bool Grad>
 __device__ inline void hingeBlockFrom(const float4* __restrict__ rec, int a, int b, float3& g, M3& H) {
   const float4 wa = rec[a], wb = rec[b];

@@ -1,9 +1,9 @@
 // Device data layout and kernels of one implicit-Euler substep (predict / contact setup, contact activation,
-// owner-computes term assembly, persistent PCG + line search, finish), plus statistics.
+// term records and slot-parallel assembly, persistent PCG + line search, finish), plus statistics.
 //
 // Reference algorithm: CpuSolver::Impl::substep (libs/sim/src/cpu_solver.cpp:230-314) in the displacement form of the
 // reference's 32-bit GPU path (u = x - xStart, term positions relative to the term's first vertex;
-// libs/sim/kernels/kernels.h:30-448). Per Newton iteration this file runs three launches instead of the reference's
+// libs/sim/kernels/kernels.h:30-448). Per Newton iteration this file runs four launches instead of the reference's
 // ~40 + 13 per CG iteration dispatches with host round trips (gpu_solver_core.cpp:325-407):
 //   k_activate   contact activation (kernels.h:85-99)
 //   k_terms      every stretch and hinge term evaluated once into a derivative record (kernels.h:137-176)

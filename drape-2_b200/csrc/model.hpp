@@ -1,5 +1,5 @@
 // Host-side scene model of the CUDA solver: particles, energy terms, the block-CSR Hessian pattern with each term's
-// slot map, and the per-particle incidence lists the owner-computes assembly kernel walks.
+// slot map, the per-particle incidence lists and the per-slot contribution lists the assembly kernel walks.
 //
 // Restates drape::sim::SimModel (libs/sim/src/sim_model.hpp:20-83, sim_model.cpp:12-274) without Eigen. The integer
 // artefacts (hinge order, rowStart / colIndex / diagSlot, stretchSlots / hingeSlots / seamSlots) are built with sorts

@@ -4,8 +4,8 @@
 // the model (model.hpp), the device buffers and one CUDA stream, and issues per substep
 //   k_begin, then per Newton iteration k_activate, k_terms, k_assemble, k_solve (cooperative), then k_finish, k_advance_clock.
 // Unlike the reference driver there is no host round trip inside a substep: energies, slope, line search and the
-// Newton stop test are decided on the device. The host synchronises once per step() to read the work counters and the
-// error status (the bounded grid barrier's timeout).
+// Newton stop test are decided on the device. The host waits once per step() (once per frame in the drape runner, with
+// the frame's statistics) to read the work counters and the error status (the bounded grid barrier's timeout).
 #include <cuda_runtime.h>
 
 #include <algorithm>
