@@ -179,3 +179,40 @@ def test_mesh_drives_the_solver_model(cuda_mod):
         assert H > 0 and B > n
     finally:
         L.drape_model_destroy(h)
+
+
+def _polygon_piece(pid, pts, grain=(0.0, 1.0)):
+    pts = [np.asarray(p, np.float64) for p in pts]
+    return M.Piece(pid, [(f"e{i}", M.line(pts[i], pts[(i + 1) % len(pts)])) for i in range(len(pts))], grain, "body")
+
+
+@pytest.mark.parametrize("h", [0.02, 0.01, 0.005])
+def test_concave_piece_keeps_its_notch(h):
+    """An L-shaped piece: the triangulation covers the outline exactly (area to 1e-9) and no triangle crosses the
+    notch (every centroid lies inside the L), so the outline constraint and the removal of the outside hold."""
+    pts = [(0, 0), (0.3, 0), (0.3, 0.1), (0.1, 0.1), (0.1, 0.3), (0, 0.3)]
+    m = M.build_sim_mesh(single(_polygon_piece("L", pts, (0.6, 0.8))), h)
+    assert abs(tri_areas(m).sum() - (0.3 * 0.1 + 0.1 * 0.2)) < 1e-9
+    c = m.rest[m.triangles].mean(axis=1)
+    inside = ((c[:, 0] <= 0.3) & (c[:, 1] <= 0.1)) | ((c[:, 0] <= 0.1) & (c[:, 1] <= 0.3))
+    assert inside.all() and (c >= 0).all()
+    assert (tri_areas(m) > 0).all() and min_angle_deg(m) >= 15.0
+
+
+def test_every_outline_edge_is_a_mesh_edge():
+    """The outline samples, in order, are joined by mesh edges (the constraint edges of the triangulation)."""
+    pat = two_rects_sewn()
+    pat.pieces.append(M.disc_piece(0.07, "disc"))
+    m = M.build_sim_mesh(pat, 0.01)
+    edges = set()
+    for t in m.triangles:
+        for k in range(3):
+            a, b = int(t[k]), int(t[(k + 1) % 3])
+            edges.add((min(a, b), max(a, b)))
+    for pi in range(len(pat.pieces)):
+        idx = np.nonzero((m.vertex_piece == pi) & (m.boundary == 1))[0]
+        # Boundary vertices come first in each piece, in outline order.
+        assert np.array_equal(idx, np.arange(idx[0], idx[0] + len(idx)))
+        for k in range(len(idx)):
+            a, b = int(idx[k]), int(idx[(k + 1) % len(idx)])
+            assert (min(a, b), max(a, b)) in edges, (pi, k)
