@@ -279,3 +279,21 @@ def test_drape_to_rest_ends_a_marginal_drape_in_a_terminal_state(gpu):
     st = s.stats()
     assert not st.has_non_finite
     assert st.max_body_penetration <= 0.002
+
+@pytest.mark.gpu
+def test_profile_solve_only_times_k_solve_alone(gpu):
+    """drape_cuda_profile(s, 2): events around k_solve only (two a Newton iteration), every other kernel untimed."""
+    s = gpu.CudaSolver(0)
+    s.build(S.sheet_on_sphere(cg_tolerance=1e-2, max_cg=50))
+    s.profile(True, solve_only=True)
+    for _ in range(3):
+        s.step(1 / 60, 1, 2)
+    s.stats()
+    p = s.profile_read()
+    s.profile(False)
+    assert p["launches"]["k_solve"] == 6 and p["milliseconds"]["k_solve"] > 0
+    assert all(v == 0 for k, v in p["launches"].items() if k != "k_solve")
+    s.profile(True)
+    s.step(1 / 60, 1, 2)
+    p = s.profile_read()
+    assert p["launches"]["k_solve"] == 2 and p["launches"]["k_begin"] == 1 and p["launches"]["k_assemble"] == 4
