@@ -681,6 +681,9 @@ def main():
     peak, _ = measured_peaks()
     solver.restore(init)
     line["spmv"] = spmv_leg(CU, solver, peak)
+    big = spmv_leg(CU, solver, peak, tiles=24)  # twice the matrix (568 MB), the HBM-resident regime of the batch
+    line["spmv"]["larger_matrix"] = {k: big[k] for k in ("matrix_mb", "ms_per_launch", "achieved", "frac",
+                                                          "max_rel_error_vs_host")}
     if args.batch_garments > 0:
         line["batch"] = batch_leg(args, local, world, rank, max_over_ranks, peak)
     if rank == 0:
