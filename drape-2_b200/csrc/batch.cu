@@ -1463,6 +1463,7 @@ int drape_batch_drape_to_rest(drape_batch* b, const drape_drape_options* options
       o.snapshot_every = 30;
       o.max_retries = 3;
       o.energy_rise_frames = 60;
+      o.frames_per_wait = 1;
     }
     if (o.frame_dt <= 0 || o.snapshot_every < 1 || o.substeps < 1)
       throw std::invalid_argument("frame_dt, substeps and snapshot_every must be positive");

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -60,6 +61,7 @@ struct drape_solver {
   int solveGrid = 0, pointGrid = 0, assembleGrid = 0, termsGrid = 0, statsGrid = 0;
   unsigned long long barrierLimitNs = 2000000000ull;  // 2 s
   int failAfter = -1;
+  static constexpr int kFrameSlots = 32;  // most frames one advanceFrames call runs before its host wait
   uint32_t solveSmemCap = 0;       // block slots one solve block can keep in shared memory
   // Learned preconditioner: the solver's own copy of the network and its workspace on this solver's CSR.
   std::unique_ptr<net::Network> net;
@@ -86,7 +88,7 @@ struct drape_solver {
   DBuf<dcu::StatsOut> statsOut;
   DBuf<unsigned int> statsDone;
   HostPinned<dcu::Control> hCtl;
-  HostPinned<dcu::StatsOut> hStats;
+  HostPinned<dcu::StatsOut> hStats;  // one slot per frame of a multi-frame advance
   DBuf<int> cgLog;
   dcu::Dev dev{};
   uint64_t h2dBytes = 0, d2hBytes = 0;
@@ -173,11 +175,11 @@ struct drape_solver {
     pointGrid = numSMs * 8;
     statsGrid = numSMs * 2;
     hCtl.alloc();
-    hStats.alloc();
+    hStats.alloc(kFrameSlots);
     ctl.alloc(1);
     partials.alloc(2 * static_cast<size_t>(solveGrid) * dcu::kPartialStride);  // two halves, alternating
     statsPartials.alloc(static_cast<size_t>(statsGrid) * 8);
-    statsOut.alloc(1);
+    statsOut.alloc(kFrameSlots);
     statsDone.alloc(1);
     cgLog.alloc(dcu::kCgLogCapacity);
   }
@@ -489,12 +491,12 @@ struct drape_solver {
     readControl();
   }
 
-  void enqueueStats() {
+  void enqueueStats(int slot = 0) {
     cudaEvent_t e = profStart(5);
-    dcu::k_stats<<<statsGrid, 256, 0, stream>>>(dev, statsPartials.p, statsDone.p, statsOut.p);
+    dcu::k_stats<<<statsGrid, 256, 0, stream>>>(dev, statsPartials.p, statsDone.p, statsOut.p + slot);
     CK(cudaGetLastError());
     profStop(e, 5);
-    CK(cudaMemcpyAsync(hStats.p, statsOut.p, sizeof(dcu::StatsOut), cudaMemcpyDeviceToHost, stream));
+    CK(cudaMemcpyAsync(hStats.p + slot, statsOut.p + slot, sizeof(dcu::StatsOut), cudaMemcpyDeviceToHost, stream));
     d2hBytes += sizeof(dcu::StatsOut);
   }
 
@@ -508,29 +510,43 @@ struct drape_solver {
     return hostStats();
   }
 
-  // One frame and its statistics with one host synchronisation (the drape runner's per-frame pair of calls).
-  drape_stats advanceWithStats(double dt, int substeps, int iterations) {
+  // `frames` frames, each followed by its statistics, with one host synchronisation at the end: out[f] is the state
+  // after frame f. One frame is the drape runner's per-frame pair of calls (advance, stats); several let the runner
+  // keep the device busy across frames and decide on their statistics afterwards.
+  void advanceFrames(double dt, int substeps, int iterations, int frames, drape_stats* out) {
     requireBuilt();
     use();
+    if (frames < 1 || frames > kFrameSlots) throw std::invalid_argument("frames per advance out of range");
     if (failAfter == 0) throw std::runtime_error("cuda: injected device failure");
-    if (failAfter > 0) --failAfter;
-    if (m.x.empty()) return drape_stats{};
+    if (failAfter > 0) failAfter = std::max(0, failAfter - frames);
+    if (m.x.empty()) {
+      for (int f = 0; f < frames; ++f) out[f] = drape_stats{};
+      return;
+    }
     const int sub = std::max(1, substeps);
     const double h = dt / sub;
     const int its = std::max(1, iterations);
-    for (int k = 0; k < sub; ++k) enqueueSubstep(h, its);
+    for (int f = 0; f < frames; ++f) {
+      for (int k = 0; k < sub; ++k) enqueueSubstep(h, its);
+      enqueueStats(f);
+    }
     CK(cudaMemcpyAsync(hCtl.p, ctl.p, sizeof(dcu::Control), cudaMemcpyDeviceToHost, stream));
     d2hBytes += sizeof(dcu::Control);
-    enqueueStats();
     waitStream();
     collectProfile();
     checkControl();
-    return hostStats();
+    for (int f = 0; f < frames; ++f) out[f] = hostStats(f);
   }
 
-  drape_stats hostStats() const {
+  drape_stats advanceWithStats(double dt, int substeps, int iterations) {
     drape_stats st{};
-    const dcu::StatsOut& s = *hStats.p;
+    advanceFrames(dt, substeps, iterations, 1, &st);
+    return st;
+  }
+
+  drape_stats hostStats(int slot = 0) const {
+    drape_stats st{};
+    const dcu::StatsOut& s = hStats.p[slot];
     st.has_non_finite = s.nonFinite;
     st.kinetic_energy = s.kineticEnergy;
     st.rms_speed = s.moving ? std::sqrt(s.sumV2 / static_cast<double>(s.moving)) : 0.0;
@@ -668,6 +684,7 @@ drape_drape_options defaultOptions() {
   o.snapshot_every = 30;
   o.max_retries = 3;
   o.energy_rise_frames = 60;
+  o.frames_per_wait = 10;
   return o;
 }
 
@@ -695,68 +712,122 @@ drape_drape_result drapeToRest(drape_solver& s, const std::vector<std::string>& 
   auto finished = [&] {
     return state == DRAPE_STATE_SETTLED || state == DRAPE_STATE_FAILED || state == DRAPE_STATE_TIMED_OUT;
   };
+  // Frames run in batches of up to frames_per_wait with one host wait each. A batch ends where a decision is known in
+  // advance to fall (the next snapshot frame, the time limits, the first frame that can complete the settle hold), so
+  // those decisions land on its last frame. A decision that cannot be foreseen (the seam gap closing, a failure) on an
+  // earlier frame j discards the batch's later frames: the state after frame j is rebuilt by restoring the batch's
+  // start and replaying its first j + 1 frames, which the deterministic step reproduces bit for bit. The outcome is
+  // the one-frame-per-wait runner's, frame for frame. The learned preconditioner refreshes on a Newton-iteration
+  // count, which a replay would shift, so it keeps one frame per wait.
+  const int perWait = s.learnedOn ? 1 : std::clamp(o.frames_per_wait, 1, drape_solver::kFrameSlots);
+  drape_solver::DeviceSnapshot batchStart;
+  drape_stats frameStats[drape_solver::kFrameSlots], replayStats[drape_solver::kFrameSlots];
+  // The last two frames' seam gaps while Assembling: a batch stops at the frame where their trend meets
+  // seam_gap_done, so the phase change seldom needs a replay.
+  double gapPrev = NAN, gapLast = NAN;
+  auto framesInBatch = [&] {
+    const int settleIn = phase == DRAPE_PHASE_SETTLING ? std::max(1, o.settle_hold_frames - stillFrames) : INT_MAX;
+    int gapIn = INT_MAX;
+    if (phase == DRAPE_PHASE_ASSEMBLING && gapPrev > gapLast && gapLast >= o.seam_gap_done)
+      gapIn = static_cast<int>(std::min(1e6, std::max(1.0, std::ceil((gapLast - o.seam_gap_done) / (gapPrev - gapLast)))));
+    double t = time, pt = phaseTime;
+    int k = 0, kept = keptFrames;
+    for (;;) {
+      ++k;
+      ++kept;
+      t += o.frame_dt;
+      pt += o.frame_dt;
+      if (k >= perWait || kept % o.snapshot_every == 0 || t >= o.max_sim_seconds - kTimeEps || k >= settleIn || k >= gapIn ||
+          (phase == DRAPE_PHASE_ASSEMBLING && pt >= o.max_assembly_seconds - kTimeEps))
+        break;
+    }
+    return s.failAfter > 0 ? std::min(k, s.failAfter) : k;
+  };
+  // Makes frame j the batch's last: the device state becomes the one after frame j.
+  auto endBatchAt = [&](int j, int& k) {
+    if (j + 1 >= k) return;
+    s.restoreFrom(batchStart);
+    const int injected = s.failAfter;
+    s.failAfter = -1;
+    s.advanceFrames(o.frame_dt, substeps, o.iterations, j + 1, replayStats);
+    s.failAfter = injected;
+    k = j + 1;
+  };
   while (!finished()) {
     if (time >= o.max_sim_seconds - kTimeEps) {
       result.simulated_seconds = time;
       state = DRAPE_STATE_TIMED_OUT;
       break;
     }
-    const drape_stats st = s.advanceWithStats(o.frame_dt, substeps, o.iterations);
-    ++result.frames_run;
-    ++keptFrames;
-    time += o.frame_dt;
-    phaseTime += o.frame_dt;
-    riseFrames = st.kinetic_energy > lastEnergy ? riseFrames + 1 : 0;
-    lastEnergy = st.kinetic_energy;
-    if (st.has_non_finite || riseFrames >= o.energy_rise_frames) {
-      ++result.retries;
-      if (result.retries > o.max_retries) {
-        result.retries = o.max_retries;
-        result.failed = 1;
-        result.simulated_seconds = time;
-        state = DRAPE_STATE_FAILED;
-        break;
-      }
-      s.restoreFrom(saved.snap);
-      time = saved.time;
-      phase = saved.phase;
-      phaseTime = saved.phaseTime;
-      keptFrames = static_cast<int>(saved.time / o.frame_dt + 0.5);
-      substeps *= 2;
-      resetCounters();
-      state = phase == DRAPE_PHASE_ASSEMBLING ? DRAPE_STATE_ASSEMBLING : DRAPE_STATE_SETTLING;
-      continue;
-    }
-    if (phase == DRAPE_PHASE_ASSEMBLING) {
-      if (st.max_seam_gap < o.seam_gap_done || phaseTime >= o.max_assembly_seconds - kTimeEps) {
-        result.assembly_end_seam_gap = st.max_seam_gap;
-        result.assembly_seconds = time;
-        phase = DRAPE_PHASE_SETTLING;
-        setAll(phase);
-        phaseTime = 0;
+    int k = framesInBatch();
+    if (k > 1) s.saveTo(batchStart);
+    s.advanceFrames(o.frame_dt, substeps, o.iterations, k, frameStats);
+    for (int j = 0; j < k && !finished(); ++j) {
+      const drape_stats& st = frameStats[j];
+      ++result.frames_run;
+      ++keptFrames;
+      time += o.frame_dt;
+      phaseTime += o.frame_dt;
+      riseFrames = st.kinetic_energy > lastEnergy ? riseFrames + 1 : 0;
+      lastEnergy = st.kinetic_energy;
+      if (st.has_non_finite || riseFrames >= o.energy_rise_frames) {
+        ++result.retries;
+        if (result.retries > o.max_retries) {
+          endBatchAt(j, k);
+          result.retries = o.max_retries;
+          result.failed = 1;
+          result.simulated_seconds = time;
+          state = DRAPE_STATE_FAILED;
+          break;
+        }
+        s.restoreFrom(saved.snap);
+        time = saved.time;
+        phase = saved.phase;
+        phaseTime = saved.phaseTime;
+        keptFrames = static_cast<int>(saved.time / o.frame_dt + 0.5);
+        substeps *= 2;
         resetCounters();
-      }
-    } else {
-      stillFrames = st.rms_speed < o.settle_rms_speed ? stillFrames + 1 : 0;
-      if (stillFrames >= o.settle_hold_frames) {
-        result.settled = 1;
-        result.simulated_seconds = time;
-        state = DRAPE_STATE_SETTLED;
+        gapPrev = gapLast = NAN;
+        state = phase == DRAPE_PHASE_ASSEMBLING ? DRAPE_STATE_ASSEMBLING : DRAPE_STATE_SETTLING;
         break;
       }
+      if (phase == DRAPE_PHASE_ASSEMBLING) {
+        gapPrev = gapLast;
+        gapLast = st.max_seam_gap;
+        if (st.max_seam_gap < o.seam_gap_done || phaseTime >= o.max_assembly_seconds - kTimeEps) {
+          endBatchAt(j, k);
+          result.assembly_end_seam_gap = st.max_seam_gap;
+          result.assembly_seconds = time;
+          phase = DRAPE_PHASE_SETTLING;
+          setAll(phase);
+          phaseTime = 0;
+          resetCounters();
+        }
+      } else {
+        stillFrames = st.rms_speed < o.settle_rms_speed ? stillFrames + 1 : 0;
+        if (stillFrames >= o.settle_hold_frames) {
+          endBatchAt(j, k);
+          result.settled = 1;
+          result.simulated_seconds = time;
+          state = DRAPE_STATE_SETTLED;
+          break;
+        }
+      }
+      if (keptFrames % o.snapshot_every == 0) {
+        endBatchAt(j, k);
+        s.saveTo(saved.snap);
+        saved.time = time;
+        saved.phase = phase;
+        saved.phaseTime = phaseTime;
+      }
+      if (time >= o.max_sim_seconds - kTimeEps) {
+        endBatchAt(j, k);
+        result.simulated_seconds = time;
+        state = DRAPE_STATE_TIMED_OUT;
+        break;
+      }
+      state = phase == DRAPE_PHASE_ASSEMBLING ? DRAPE_STATE_ASSEMBLING : DRAPE_STATE_SETTLING;
     }
-    if (keptFrames % o.snapshot_every == 0) {
-      s.saveTo(saved.snap);
-      saved.time = time;
-      saved.phase = phase;
-      saved.phaseTime = phaseTime;
-    }
-    if (time >= o.max_sim_seconds - kTimeEps) {
-      result.simulated_seconds = time;
-      state = DRAPE_STATE_TIMED_OUT;
-      break;
-    }
-    state = phase == DRAPE_PHASE_ASSEMBLING ? DRAPE_STATE_ASSEMBLING : DRAPE_STATE_SETTLING;
   }
   return result;
 }

@@ -109,6 +109,7 @@ class drape_drape_options(C.Structure):
         ("snapshot_every", C.c_int32),
         ("max_retries", C.c_int32),
         ("energy_rise_frames", C.c_int32),
+        ("frames_per_wait", C.c_int32),
     ]
 
 

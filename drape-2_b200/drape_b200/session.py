@@ -31,13 +31,14 @@ class DrapeOptions:
     snapshot_every: int = 30
     max_retries: int = 3
     energy_rise_frames: int = 60
+    frames_per_wait: int = 10  # device frames per host wait in the C runner (same outcome for every value)
 
     def to_c(self):
         from .scene import drape_drape_options
         return drape_drape_options(self.substeps, self.iterations, self.frame_dt, self.max_assembly_seconds,
                                    self.seam_gap_done, self.settle_rms_speed, self.settle_hold_frames,
                                    self.max_sim_seconds, self.snapshot_every, self.max_retries,
-                                   self.energy_rise_frames)
+                                   self.energy_rise_frames, self.frames_per_wait)
 
 
 @dataclass

@@ -108,6 +108,10 @@ typedef struct drape_drape_options {
   int32_t snapshot_every;      /* 30 */
   int32_t max_retries;         /* 3 */
   int32_t energy_rise_frames;  /* 60 */
+  /* Frames the device runs per host wait (1 = the reference's one frame per wait; default 10). Not a reference option:
+   * the runner replays a batch's discarded frames where a decision falls inside it, so every value gives the same
+   * outcome, frame for frame. The learned preconditioner and the batch runner keep one wait per frame. */
+  int32_t frames_per_wait;     /* 10 */
 } drape_drape_options;
 
 enum { DRAPE_STATE_ASSEMBLING = 0, DRAPE_STATE_SETTLING, DRAPE_STATE_SETTLED, DRAPE_STATE_FAILED, DRAPE_STATE_TIMED_OUT };
