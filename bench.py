@@ -615,7 +615,7 @@ def main():
     # End to end through the C ABI with host buffers: build from host arrays (H2D), drape, read positions (D2H), for
     # the same seeded start states.
     e2e_steps = args.e2e_steps or args.steps
-    e2e_times, h2d, d2h, e2e_frames = [], [], [], []
+    e2e_times, e2e_build, h2d, d2h, e2e_frames = [], [], [], [], []
     garment = scene.garments[0]
     own = garment.initial_positions
     for _ in range(e2e_steps):
@@ -627,6 +627,7 @@ def main():
             start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             start.record(stream)
             solver.build(scene)
+            e2e_build.append(time.perf_counter() - t0)
             e2e_frames.append(int(solver.drape_to_rest([gid]).frames_run))
             out = np.empty((sizes["n"], 3), np.float32)
             solver.read_positions(out)
@@ -654,6 +655,8 @@ def main():
         "e2e": {"value": e2e_value, "unit": "s", "h2d_bytes_per_step": int(sum(h2d) / e2e_steps),
                 "d2h_bytes_per_step": int(sum(d2h) / e2e_steps), "drapes": len(e2e_times),
                 "frames_per_seed": e2e_frames[-SEEDS:], "frames_mean": float(np.mean(e2e_frames)),
+                "s_per_seed": [round(t, 4) for t in e2e_times[-SEEDS:]],
+                "build_s_per_seed": [round(t, 4) for t in e2e_build[-SEEDS:]],
                 "note": "mean seconds per drape; bytes per step of 16 drapes"},
         "roofline": roofline,
         "clocks": clocks,

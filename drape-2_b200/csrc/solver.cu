@@ -193,6 +193,8 @@ struct drape_solver {
         cudaEventDestroy(p.b);
       }
       for (auto e : eventPool) cudaEventDestroy(e);
+      for (auto& g : frameGraphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
       cudaStreamDestroy(stream);
     }
   }
@@ -402,13 +404,85 @@ struct drape_solver {
   }
 
   void launchSolve(const dcu::Dev& d) {
-    void* args[] = {const_cast<dcu::Dev*>(&d)};
-    void* kernel = learnedOn && netGraph ? reinterpret_cast<void*>(dcu::k_solve<true>)
-                                         : reinterpret_cast<void*>(dcu::k_solve<false>);
-    CK(cudaLaunchCooperativeKernel(kernel, dim3(solveGrid), dim3(dcu::kSolveThreads), args, solveSmemBytes, stream));
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(solveGrid);
+    cfg.blockDim = dim3(dcu::kSolveThreads);
+    cfg.dynamicSmemBytes = solveSmemBytes;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;  // co-resident blocks for the grid barrier; capturable in a graph
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CK(learnedOn && netGraph ? cudaLaunchKernelEx(&cfg, dcu::k_solve<true>, d)
+                             : cudaLaunchKernelEx(&cfg, dcu::k_solve<false>, d));
   }
 
-  void enqueueSubstep(double h, int iterations) {
+  // Frame graphs: one frame's launches (its substeps, then the statistics into slot f) captured once per slot and
+  // replayed, one graph launch a frame instead of a dozen kernel launches. A graph is recaptured when the device view
+  // or a launch parameter it was captured with changes; profiling and the learned preconditioner launch directly.
+  struct FrameGraph {
+    cudaGraphExec_t exec = nullptr;
+    dcu::Dev dev{};
+    double h = 0;
+    int substeps = 0, iterations = 0, precondSwitch = 0;
+    unsigned long long barrierLimitNs = 0;
+  };
+  FrameGraph frameGraphs[kFrameSlots];
+  bool frameGraphsUsable = true;
+
+  bool launchFrameGraph(double h, int substeps, int iterations, int slot) {
+    if (!frameGraphsUsable || profiling != 0 || (learnedOn && netGraph)) return false;
+    FrameGraph& g = frameGraphs[slot];
+    if (!g.exec || g.h != h || g.substeps != substeps || g.iterations != iterations ||
+        g.precondSwitch != precondSwitch || g.barrierLimitNs != barrierLimitNs ||
+        std::memcmp(&g.dev, &dev, sizeof(dcu::Dev)) != 0) {
+      if (g.exec) CK(cudaGraphExecDestroy(g.exec));
+      g.exec = nullptr;
+      const uint64_t bytes = d2hBytes;
+      cudaGraph_t graph = nullptr;
+      CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      try {
+        for (int k = 0; k < substeps; ++k) enqueueSubstep(h, iterations, false);
+        enqueueStats(slot);
+      } catch (...) {
+        cudaStreamEndCapture(stream, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        frameGraphsUsable = false;
+        d2hBytes = bytes;
+        return false;
+      }
+      d2hBytes = bytes;
+      if (cudaStreamEndCapture(stream, &graph) != cudaSuccess || !graph ||
+          cudaGraphInstantiate(&g.exec, graph, 0) != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        g.exec = nullptr;
+        frameGraphsUsable = false;
+        return false;
+      }
+      cudaGraphDestroy(graph);
+      g.dev = dev;
+      g.h = h;
+      g.substeps = substeps;
+      g.iterations = iterations;
+      g.precondSwitch = precondSwitch;
+      g.barrierLimitNs = barrierLimitNs;
+    }
+    CK(cudaGraphLaunch(g.exec, stream));
+    d2hBytes += sizeof(dcu::StatsOut);
+    for (int k = 0; k < substeps; ++k) advanceHostClock(h);
+    return true;
+  }
+
+  // The host copy of the Assembling garments' clocks, which k_advance_clock advances on the device.
+  void advanceHostClock(double h) {
+    for (auto& g : m.garments)
+      if (g.phase == DRAPE_PHASE_ASSEMBLING) g.assemblyTime += h;
+  }
+
+  void enqueueSubstep(double h, int iterations, bool hostClock = true) {
     dcu::Dev d = dev;
     d.P.h = static_cast<float>(h);
     d.P.invH2 = static_cast<float>(1.0 / (h * h));
@@ -446,8 +520,7 @@ struct drape_solver {
     dcu::k_advance_clock<<<1, 32, 0, stream>>>(d);
     CK(cudaGetLastError());
     profStop(e, 4);
-    for (auto& g : m.garments)
-      if (g.phase == DRAPE_PHASE_ASSEMBLING) g.assemblyTime += h;
+    if (hostClock) advanceHostClock(h);
   }
 
   // Waits for the stream by polling it: the per-frame waits of stepping and of the drape runner wake up without the
@@ -527,6 +600,7 @@ struct drape_solver {
     const double h = dt / sub;
     const int its = std::max(1, iterations);
     for (int f = 0; f < frames; ++f) {
+      if (launchFrameGraph(h, sub, its, f)) continue;
       for (int k = 0; k < sub; ++k) enqueueSubstep(h, its);
       enqueueStats(f);
     }

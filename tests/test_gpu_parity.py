@@ -299,10 +299,12 @@ def test_profile_solve_only_times_k_solve_alone(gpu):
     assert p["launches"]["k_solve"] == 2 and p["launches"]["k_begin"] == 1 and p["launches"]["k_assemble"] == 4
 
 
-def _drape_with(gpu, scene, gid, frames_per_wait):
+def _drape_with(gpu, scene, gid, frames_per_wait, direct=False):
     from drape_b200.session import DrapeOptions
     s = gpu.CudaSolver(0)
     s.build(scene)
+    if direct:
+        s.profile(True)  # timed launches, one by one, instead of the frame graphs
     res = s.drape_to_rest([gid], DrapeOptions(frames_per_wait=frames_per_wait).to_c())
     fields = {f: getattr(res, f) for f, _ in type(res)._fields_}
     return fields, s.snapshot()
@@ -312,10 +314,11 @@ def _drape_with(gpu, scene, gid, frames_per_wait):
 def test_drape_to_rest_frame_batches_match_one_frame_per_wait(gpu, scene_name):
     """frames_per_wait only changes how often the host waits: batches of 10 and of 7 frames (whose discarded frames
     are replayed where a decision falls inside a batch) end in the same state, bit for bit, with the same result as
-    one frame per wait. The 10k tube covers the phase change and the settle hold; the marginal tube the time limit or
-    the restore-and-retry path."""
+    one frame per wait. The reference run launches every kernel directly (profiling on), the batched runs replay
+    frame graphs, so the graphs are checked too. The 10k tube covers the phase change and the settle hold; the
+    marginal tube the time limit or the restore-and-retry path."""
     scene = S.tube_10k() if scene_name == "tube_10k" else S.seamed_tube(24, 30, field_n=64, field_cell=0.008)
-    ref_res, ref_snap = _drape_with(gpu, scene, "tube", 1)
+    ref_res, ref_snap = _drape_with(gpu, scene, "tube", 1, direct=True)
     assert ref_res["frames_run"] > 0
     for fpw in (10, 7):
         res, snap = _drape_with(gpu, scene, "tube", fpw)
