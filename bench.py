@@ -111,7 +111,7 @@ class ClockSampler:
             self.proc.kill()
         self.file.flush()
         self.file.seek(0)
-        sm, smax, reasons = [], [], set()
+        sm, smax, reasons, masks, power = [], [], set(), {}, []
         names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
         for line in self.file.read().splitlines():
             parts = [p.strip() for p in line.split(",")]
@@ -125,9 +125,15 @@ class ClockSampler:
             for name, val in zip(names, parts[5:9]):
                 if val.lower().startswith("active"):
                     reasons.add(name)
+            masks[parts[4]] = masks.get(parts[4], 0) + 1
+            try:
+                power.append(float(parts[3]))
+            except ValueError:
+                pass
         os.unlink(self.file.name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "sm_mhz_min": min(sm) if sm else None,
+                "power_w_max": max(power) if power else None, "active_masks": masks}
 
 
 def dist_setup():
