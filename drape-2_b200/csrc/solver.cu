@@ -1133,7 +1133,10 @@ int drape_cuda_drape_to_rest(drape_solver* s, const char* const* garments, uint3
     std::vector<std::string> ids;
     for (uint32_t k = 0; k < garment_count; ++k) ids.emplace_back(garments[k] ? garments[k] : "");
     for (const auto& id : ids) s->m.garmentIndex(id);
-    *out = drapeToRest(*s, ids, options ? *options : defaultOptions());
+    const drape_drape_options o = options ? *options : defaultOptions();
+    if (!(o.frame_dt > 0) || o.snapshot_every < 1 || o.substeps < 1)
+      throw std::invalid_argument("frame_dt, substeps and snapshot_every must be positive");
+    *out = drapeToRest(*s, ids, o);
   });
 }
 

@@ -253,6 +253,10 @@ def test_errors_map_to_reference_exceptions(gpu):
     snap["velocities"] = snap["velocities"][:-1]
     with pytest.raises(ValueError):
         s.restore(snap)
+    from drape_b200.session import DrapeOptions
+    for bad in (dict(snapshot_every=0), dict(substeps=0), dict(frame_dt=0.0)):
+        with pytest.raises(ValueError, match="must be positive"):
+            s.drape_to_rest(["sheet"], DrapeOptions(**bad).to_c())
 
 
 def test_drape_to_rest_settles_the_10k_tube(gpu):
