@@ -32,6 +32,10 @@ typedef struct oracle_solver oracle_solver;
 /* Return codes: 0 ok, -1 std::invalid_argument, -2 std::out_of_range, -3 other error. */
 oracle_solver* oracle_create(int full_fp64);
 void oracle_destroy(oracle_solver* s);
+/* Host threads of the oracle's parallel loops (<= 0: all processors). Every count gives bit-identical results: each
+   per-slot and per-particle sum keeps the serial scatter's order and every energy and dot-product sum is serial. */
+void oracle_set_threads(int threads);
+int oracle_threads(void);
 const char* oracle_last_error(const oracle_solver* s);
 
 int oracle_build(oracle_solver* s, const drape_scene_desc* scene);

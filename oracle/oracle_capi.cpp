@@ -2,6 +2,8 @@
 #include "oracle_impl.hpp"
 #include "bake_impl.hpp"
 
+#include <omp.h>
+
 // ---------------------------------------------------------------------------------------------------------------
 // C API.
 
@@ -59,6 +61,10 @@ oracle_solver* oracle_create(int full_fp64) {
 }
 
 void oracle_destroy(oracle_solver* s) { delete s; }
+
+// Host threads of the oracle's parallel loops (results are identical for every count).
+void oracle_set_threads(int threads) { omp_set_num_threads(threads > 0 ? threads : omp_get_num_procs()); }
+int oracle_threads(void) { return omp_get_max_threads(); }
 
 const char* oracle_last_error(const oracle_solver* s) { return s ? s->error.c_str() : "null solver"; }
 

@@ -834,6 +834,7 @@ struct Solver {
     frictionLambda.assign(n, 0.0);
     contactNear.assign(n, 0);
     contactActive.assign(n, 0);
+    buildGatherLists();
   }
 
   double contactGap(std::size_t i, V3d pos) const { return contactOffset[i] - dot(contactNormal[i], pos - xStart[i]); }
@@ -842,78 +843,186 @@ struct Solver {
       if (contactActive[i]) vec[i] -= contactNormal[i] * dot(contactNormal[i], vec[i]);
   }
 
-  template <int N, class Eval>
-  void addTerm(const uint32_t* vs, const uint32_t* slots, const std::vector<V3d>& pos, bool withDerivatives,
-               double& energy, Eval&& eval) {
-    V3d xs[N];
-    for (int a = 0; a < N; ++a) xs[a] = pos[vs[a]];
-    TermEval<N> te;
-    eval(xs, te);
-    energy += te.energy;
-    if (!withDerivatives) return;
-    for (int a = 0; a < N; ++a) {
-      grad[vs[a]] += te.grad[a];
-      for (int b = 0; b < N; ++b) blocks[slots[a * N + b]] += te.hess[a][b];
+  // Parallel evaluation with the serial oracle's arithmetic, bit for bit. The reference CpuSolver scatters each term's
+  // gradient and Hessian blocks into the shared arrays in term order (cpu_solver.cpp:76-90, :92-145) and sums the
+  // energy and the dot products in index order (:161-165). Here every term is evaluated independently (in parallel)
+  // into its own record; each block slot and each particle then adds its contributions in exactly the order the
+  // serial scatter would (inertia first, then stretch, hinge and seam terms in term order, friction last), and every
+  // energy and dot-product sum runs serially in index order over per-item values computed in parallel. The results
+  // are therefore identical for any thread count, the single-threaded run included.
+  std::vector<TermEval<3>> stretchEval;
+  std::vector<TermEval<4>> hingeEval;
+  std::vector<TermEval<2>> seamEval;
+  std::vector<TermEval<1>> frictionEval;
+  std::vector<double> eInertia, eStretch, eHinge, eSeam, eFriction, dotTmp;
+  // Contribution lists: entry = kind (2 bits: 0 stretch, 1 hinge, 2 seam) << 30 | local (4 bits) << 26 | term.
+  std::vector<uint32_t> slotListStart, slotList, gradListStart, gradList;
+  std::vector<int32_t> slotDiag;  // the particle whose diagonal block a slot holds, or -1
+
+  static uint32_t entry(uint32_t kind, uint32_t local, uint32_t term) { return kind << 30 | local << 26 | term; }
+
+  template <class Fn>
+  void forEachContribution(Fn&& fn) const {  // fn(kind, term, a, b, N, slot): in the serial scatter's order
+    for (std::size_t k = 0; k < m.stretch.size(); ++k)
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) fn(0u, k, a, b, 3, m.stretchSlots[k][a * 3 + b], m.stretch[k].v[a]);
+    for (std::size_t k = 0; k < m.hinges.size(); ++k)
+      for (int a = 0; a < 4; ++a)
+        for (int b = 0; b < 4; ++b) fn(1u, k, a, b, 4, m.hingeSlots[k][a * 4 + b], m.hinges[k].v[a]);
+    for (std::size_t k = 0; k < m.seams.size(); ++k) {
+      const uint32_t ab[2] = {m.seams[k].a, m.seams[k].b};
+      for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) fn(2u, k, a, b, 2, m.seamSlots[k][a * 2 + b], ab[a]);
     }
   }
 
+  void buildGatherLists() {
+    const std::size_t n = m.x.size(), B = m.colIndex.size();
+    if (m.stretch.size() >= (1u << 26) || m.hinges.size() >= (1u << 26) || m.seams.size() >= (1u << 26))
+      throw std::invalid_argument("oracle: too many terms for the gather lists");
+    slotListStart.assign(B + 1, 0);
+    gradListStart.assign(n + 1, 0);
+    forEachContribution([&](uint32_t, std::size_t, int, int b, int, uint32_t slot, uint32_t va) {
+      ++slotListStart[slot + 1];
+      if (b == 0) ++gradListStart[va + 1];
+    });
+    for (std::size_t s = 0; s < B; ++s) slotListStart[s + 1] += slotListStart[s];
+    for (std::size_t i = 0; i < n; ++i) gradListStart[i + 1] += gradListStart[i];
+    slotList.assign(slotListStart[B], 0);
+    gradList.assign(gradListStart[n], 0);
+    std::vector<uint32_t> sFill(slotListStart.begin(), slotListStart.end() - 1);
+    std::vector<uint32_t> gFill(gradListStart.begin(), gradListStart.end() - 1);
+    forEachContribution([&](uint32_t kind, std::size_t k, int a, int b, int N, uint32_t slot, uint32_t va) {
+      slotList[sFill[slot]++] = entry(kind, static_cast<uint32_t>(a * N + b), static_cast<uint32_t>(k));
+      if (b == 0) gradList[gFill[va]++] = entry(kind, static_cast<uint32_t>(a), static_cast<uint32_t>(k));
+    });
+    slotDiag.assign(B, -1);
+    for (std::size_t i = 0; i < n; ++i) slotDiag[m.diagSlot[i]] = static_cast<int32_t>(i);
+    stretchEval.resize(m.stretch.size());
+    hingeEval.resize(m.hinges.size());
+    seamEval.resize(m.seams.size());
+    frictionEval.resize(n);
+    eInertia.resize(n);
+    eStretch.resize(m.stretch.size());
+    eHinge.resize(m.hinges.size());
+    eSeam.resize(m.seams.size());
+    eFriction.resize(n);
+    dotTmp.resize(n);
+  }
+
+  const M3& hessOf(uint32_t e) const {
+    const uint32_t kind = e >> 30, local = (e >> 26) & 15u, k = e & ((1u << 26) - 1);
+    if (kind == 0) return stretchEval[k].hess[local / 3][local % 3];
+    if (kind == 1) return hingeEval[k].hess[local / 4][local % 4];
+    return seamEval[k].hess[local / 2][local % 2];
+  }
+  const V3d& gradOf(uint32_t e) const {
+    const uint32_t kind = e >> 30, local = (e >> 26) & 15u, k = e & ((1u << 26) - 1);
+    if (kind == 0) return stretchEval[k].grad[local];
+    if (kind == 1) return hingeEval[k].grad[local];
+    return seamEval[k].grad[local];
+  }
+
+  template <int N>
+  static void gatherTerm(const uint32_t* vs, const std::vector<V3d>& pos, V3d* xs) {
+    for (int a = 0; a < N; ++a) xs[a] = pos[vs[a]];
+  }
+
   double evaluate(const std::vector<V3d>& pos, double invH2, bool withDerivatives) {
-    const std::size_t n = pos.size();
-    double energy = 0;
-    if (withDerivatives) {
-      std::fill(grad.begin(), grad.end(), V3d{});
-      std::fill(blocks.begin(), blocks.end(), M3{});
-    }
-    for (std::size_t i = 0; i < n; ++i) {
-      if (m.pinned[i]) continue;
-      const double k = m.mass[i] * invH2;
-      const V3d d = pos[i] - y[i];
-      energy += 0.5 * k * sqnorm(d);
-      if (withDerivatives) {
-        grad[i] += k * d;
-        blocks[m.diagSlot[i]] += k * M3::identity();
-      }
-    }
+    const std::ptrdiff_t n = static_cast<std::ptrdiff_t>(pos.size());
+    const std::ptrdiff_t S = static_cast<std::ptrdiff_t>(m.stretch.size());
+    const std::ptrdiff_t H = static_cast<std::ptrdiff_t>(m.hinges.size());
+    const std::ptrdiff_t K = static_cast<std::ptrdiff_t>(m.seams.size());
     const double limitScale = m.settings.strainLimitStiffnessScale;
-    for (std::size_t k = 0; k < m.stretch.size(); ++k) {
-      const auto& t = m.stretch[k];
-      addTerm<3>(t.v.data(), m.stretchSlots[k].data(), pos, withDerivatives, energy, [&](const V3d* xs, TermEval<3>& te) {
+    const double slipEps = m.settings.frictionSlipSpeed * substepH;
+#pragma omp parallel
+    {
+#pragma omp for schedule(static) nowait
+      for (std::ptrdiff_t i = 0; i < n; ++i) {
+        eInertia[i] = 0;
+        if (m.pinned[i]) continue;
+        const double k = m.mass[i] * invH2;
+        const V3d d = pos[i] - y[i];
+        eInertia[i] = 0.5 * k * sqnorm(d);
+      }
+#pragma omp for schedule(static) nowait
+      for (std::ptrdiff_t k = 0; k < S; ++k) {
+        const auto& t = m.stretch[k];
+        V3d xs[3];
+        gatherTerm<3>(t.v.data(), pos, xs);
+        TermEval<3> local;
+        TermEval<3>& te = withDerivatives ? (stretchEval[k] = TermEval<3>{}) : local;
         evalStretchTerm(t.dmInv, t.area, xs, m.fabrics[t.fabric], limitScale, te);
-      });
-    }
-    for (std::size_t k = 0; k < m.hinges.size(); ++k) {
-      const auto& h = m.hinges[k];
-      addTerm<4>(h.v.data(), m.hingeSlots[k].data(), pos, withDerivatives, energy,
-                 [&](const V3d* xs, TermEval<4>& te) { evalHingeTerm(h.K, h.restAngle, xs, te); });
-    }
-    for (std::size_t k = 0; k < m.seams.size(); ++k) {
-      const auto& s = m.seams[k];
-      const double target = m.seamTarget(s);
-      const uint32_t ab[2] = {s.a, s.b};
-      addTerm<2>(ab, m.seamSlots[k].data(), pos, withDerivatives, energy,
-                 [&](const V3d* xs, TermEval<2>& te) { evalSeamTerm(xs, target, m.settings.seamStiffness, te); });
-    }
-    for (std::size_t i = 0; i < n; ++i) {
-      if (frictionLambda[i] <= 0) continue;
-      TermEval<1> te;
-      evalFrictionTerm(pos[i], xStart[i], contactNormal[i], m.fabrics[m.pFabric[i]].friction * frictionLambda[i],
-                       m.settings.frictionSlipSpeed * substepH, te);
-      energy += te.energy;
+        eStretch[k] = te.energy;
+      }
+#pragma omp for schedule(static) nowait
+      for (std::ptrdiff_t k = 0; k < H; ++k) {
+        const auto& h = m.hinges[k];
+        V3d xs[4];
+        gatherTerm<4>(h.v.data(), pos, xs);
+        TermEval<4> local;
+        TermEval<4>& te = withDerivatives ? (hingeEval[k] = TermEval<4>{}) : local;
+        evalHingeTerm(h.K, h.restAngle, xs, te);
+        eHinge[k] = te.energy;
+      }
+#pragma omp for schedule(static) nowait
+      for (std::ptrdiff_t k = 0; k < K; ++k) {
+        const auto& s = m.seams[k];
+        const uint32_t ab[2] = {s.a, s.b};
+        V3d xs[2];
+        gatherTerm<2>(ab, pos, xs);
+        TermEval<2> local;
+        TermEval<2>& te = withDerivatives ? (seamEval[k] = TermEval<2>{}) : local;
+        evalSeamTerm(xs, m.seamTarget(s), m.settings.seamStiffness, te);
+        eSeam[k] = te.energy;
+      }
+#pragma omp for schedule(static)
+      for (std::ptrdiff_t i = 0; i < n; ++i) {
+        eFriction[i] = 0;
+        if (frictionLambda[i] <= 0) continue;
+        TermEval<1> local;
+        TermEval<1>& te = withDerivatives ? (frictionEval[i] = TermEval<1>{}) : local;
+        evalFrictionTerm(pos[i], xStart[i], contactNormal[i], m.fabrics[m.pFabric[i]].friction * frictionLambda[i],
+                         slipEps, te);
+        eFriction[i] = te.energy;
+      }
       if (withDerivatives) {
-        grad[i] += te.grad[0];
-        blocks[m.diagSlot[i]] += te.hess[0][0];
+        const std::ptrdiff_t B = static_cast<std::ptrdiff_t>(blocks.size());
+#pragma omp for schedule(static) nowait
+        for (std::ptrdiff_t s = 0; s < B; ++s) {
+          M3 acc{};
+          const int32_t i = slotDiag[s];
+          if (i >= 0 && !m.pinned[i]) acc += (m.mass[i] * invH2) * M3::identity();
+          for (uint32_t e = slotListStart[s]; e < slotListStart[s + 1]; ++e) acc += hessOf(slotList[e]);
+          if (i >= 0 && frictionLambda[i] > 0) acc += frictionEval[i].hess[0][0];
+          blocks[s] = acc;
+        }
+#pragma omp for schedule(static)
+        for (std::ptrdiff_t i = 0; i < n; ++i) {
+          V3d acc{};
+          if (!m.pinned[i]) acc += (m.mass[i] * invH2) * (pos[i] - y[i]);
+          for (uint32_t e = gradListStart[i]; e < gradListStart[i + 1]; ++e) acc += gradOf(gradList[e]);
+          if (frictionLambda[i] > 0) acc += frictionEval[i].grad[0];
+          grad[i] = m.pinned[i] ? V3d{} : acc;
+        }
       }
     }
-    if (withDerivatives) {
-      for (std::size_t i = 0; i < n; ++i)
-        if (m.pinned[i]) grad[i] = V3d{};
-    }
+    // The energy in the serial order: inertia (unpinned particles), stretch, hinge, seam terms, friction.
+    double energy = 0;
+    for (std::ptrdiff_t i = 0; i < n; ++i)
+      if (!m.pinned[i]) energy += eInertia[i];
+    for (std::ptrdiff_t k = 0; k < S; ++k) energy += eStretch[k];
+    for (std::ptrdiff_t k = 0; k < H; ++k) energy += eHinge[k];
+    for (std::ptrdiff_t k = 0; k < K; ++k) energy += eSeam[k];
+    for (std::ptrdiff_t i = 0; i < n; ++i)
+      if (frictionLambda[i] > 0) energy += eFriction[i];
     return energy;
   }
 
   void multiply(const std::vector<V3d>& in, std::vector<V3d>& out) const {
-    const std::size_t n = in.size();
-    for (std::size_t i = 0; i < n; ++i) {
+    const std::ptrdiff_t n = static_cast<std::ptrdiff_t>(in.size());
+#pragma omp parallel for schedule(static)
+    for (std::ptrdiff_t i = 0; i < n; ++i) {
       V3d acc;
       if (!m.pinned[i]) {
         for (uint32_t s = m.rowStart[i]; s < m.rowStart[i + 1]; ++s) {
@@ -925,68 +1034,88 @@ struct Solver {
     }
   }
 
-  static double vdot(const std::vector<V3d>& a, const std::vector<V3d>& b) {
+  // a . b summed in index order (the per-particle products in parallel, the sum serial).
+  double vdot(const std::vector<V3d>& a, const std::vector<V3d>& b) {
+    const std::ptrdiff_t n = static_cast<std::ptrdiff_t>(a.size());
+    if (dotTmp.size() < a.size()) dotTmp.resize(a.size());
+#pragma omp parallel for schedule(static)
+    for (std::ptrdiff_t i = 0; i < n; ++i) dotTmp[i] = dot(a[i], b[i]);
     double s = 0;
-    for (std::size_t i = 0; i < a.size(); ++i) s += dot(a[i], b[i]);
+    for (std::ptrdiff_t i = 0; i < n; ++i) s += dotTmp[i];
     return s;
   }
 
+  void filterRow(std::vector<V3d>& vec, std::ptrdiff_t i) const {
+    if (contactActive[i]) vec[i] -= contactNormal[i] * dot(contactNormal[i], vec[i]);
+  }
+
   void solveLinear() {
-    const std::size_t n = grad.size();
-    for (std::size_t i = 0; i < n; ++i) {
+    const std::ptrdiff_t n = static_cast<std::ptrdiff_t>(grad.size());
+#pragma omp parallel for schedule(static)
+    for (std::ptrdiff_t i = 0; i < n; ++i) {
       if (m.pinned[i]) {
         precond[i] = M3{};
-        continue;
+      } else {
+        bool ok = false;
+        const M3 inv = invertSymmetric(blocks[m.diagSlot[i]], ok);
+        precond[i] = ok ? inv : M3::identity();
       }
-      bool ok = false;
-      const M3 inv = invertSymmetric(blocks[m.diagSlot[i]], ok);
-      precond[i] = ok ? inv : M3::identity();
-    }
-    for (std::size_t i = 0; i < n; ++i) {
       step[i] = V3d{};
       resid[i] = -grad[i];
       r[i] = resid[i];
+      filterRow(r, i);
+      z[i] = precond[i] * r[i];
+      filterRow(z, i);
+      p[i] = z[i];
     }
-    filter(r);
-    for (std::size_t i = 0; i < n; ++i) z[i] = precond[i] * r[i];
-    filter(z);
-    p = z;
     double rz = vdot(r, z);
     const double r0 = std::sqrt(vdot(r, r));
     for (int it = 0; r0 > 0 && it < m.settings.maxCgIterations; ++it) {
       multiply(p, apFull);
-      ap = apFull;
-      filter(ap);
+#pragma omp parallel for schedule(static)
+      for (std::ptrdiff_t i = 0; i < n; ++i) {
+        ap[i] = apFull[i];
+        filterRow(ap, i);
+      }
       const double pAp = vdot(p, ap);
       if (!(pAp > 0)) break;
       const double alpha = rz / pAp;
       ++counters.cg_iterations;
-      for (std::size_t i = 0; i < n; ++i) {
+#pragma omp parallel for schedule(static)
+      for (std::ptrdiff_t i = 0; i < n; ++i) {
         step[i] += alpha * p[i];
         r[i] -= alpha * ap[i];
         resid[i] -= alpha * apFull[i];
       }
       if (std::sqrt(vdot(r, r)) <= m.settings.cgTolerance * r0) break;
-      for (std::size_t i = 0; i < n; ++i) z[i] = precond[i] * r[i];
-      filter(z);
+#pragma omp parallel for schedule(static)
+      for (std::ptrdiff_t i = 0; i < n; ++i) {
+        z[i] = precond[i] * r[i];
+        filterRow(z, i);
+      }
       const double rzNew = vdot(r, z);
       const double beta = rzNew / rz;
       rz = rzNew;
-      for (std::size_t i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
+#pragma omp parallel for schedule(static)
+      for (std::ptrdiff_t i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
     }
-    for (std::size_t i = 0; i < n; ++i)
+#pragma omp parallel for schedule(static)
+    for (std::ptrdiff_t i = 0; i < n; ++i)
       m.contactForce[i] = contactActive[i] ? std::max(0.0, -dot(resid[i], contactNormal[i])) : 0.0;
   }
 
   double evaluateWithContact(double invH2) {
-    for (std::size_t i = 0; i < xd.size(); ++i) {
+    const std::ptrdiff_t n = static_cast<std::ptrdiff_t>(xd.size());
+#pragma omp parallel for schedule(static)
+    for (std::ptrdiff_t i = 0; i < n; ++i) {
       if (!contactNear[i]) continue;
       const double c = contactGap(i, xd[i]);
       if (c > -kContactSnap) contactActive[i] = 1;
       if (contactActive[i] && c > 0) xd[i] += c * contactNormal[i];
     }
     const double e = evaluate(xd, invH2, true);
-    for (std::size_t i = 0; i < xd.size(); ++i)
+#pragma omp parallel for schedule(static)
+    for (std::ptrdiff_t i = 0; i < n; ++i)
       if (contactActive[i] && dot(grad[i], contactNormal[i]) < 0) contactActive[i] = 0;
     return e;
   }
@@ -994,21 +1123,20 @@ struct Solver {
   // Predict and contact setup (cpu_solver.cpp:234-263).
   void beginSubstep(double h) {
     const V3d gravity = m.settings.gravity;
-    const std::size_t n = m.x.size();
-    for (std::size_t i = 0; i < n; ++i) {
+    const std::ptrdiff_t n = static_cast<std::ptrdiff_t>(m.x.size());
+    substepH = h;
+#pragma omp parallel for schedule(static)
+    for (std::ptrdiff_t i = 0; i < n; ++i) {
       xStart[i] = m.x[i];
       const V3d vel = m.v[i];
       if (m.pinned[i]) {
         y[i] = xStart[i];
         xd[i] = xStart[i];
-        continue;
+      } else {
+        const V3d g = m.garments[m.pGarment[i]].phase == Settling ? gravity : V3d{};
+        y[i] = xStart[i] + h * vel + h * h * (g + m.fExt[i] / m.mass[i]);
+        xd[i] = xStart[i] + h * vel;
       }
-      const V3d g = m.garments[m.pGarment[i]].phase == Settling ? gravity : V3d{};
-      y[i] = xStart[i] + h * vel + h * h * (g + m.fExt[i] / m.mass[i]);
-      xd[i] = xStart[i] + h * vel;
-    }
-    substepH = h;
-    for (std::size_t i = 0; i < n; ++i) {
       contactNear[i] = 0;
       contactActive[i] = 0;
       frictionLambda[i] = 0;
@@ -1029,7 +1157,7 @@ struct Solver {
 
   void substep(double h, int newtonIterations) {
     const double invH2 = 1.0 / (h * h);
-    const std::size_t n = m.x.size();
+    const std::ptrdiff_t n = static_cast<std::ptrdiff_t>(m.x.size());
     ++counters.substeps;
     beginSubstep(h);
     for (int it = 0; it < newtonIterations; ++it) {
@@ -1040,47 +1168,50 @@ struct Solver {
       if (!(slope < 0)) break;
       double alpha = 1.0;
       for (int ls = 0; ls < 20; ++ls) {
-        for (std::size_t i = 0; i < n; ++i) trial[i] = xd[i] + alpha * step[i];
+#pragma omp parallel for schedule(static)
+        for (std::ptrdiff_t i = 0; i < n; ++i) trial[i] = xd[i] + alpha * step[i];
         if (evaluate(trial, invH2, false) <= e0 + 1e-4 * alpha * slope) break;
         alpha *= 0.5;
         ++counters.line_search_halvings;
       }
-      double maxMove = 0;
-      for (std::size_t i = 0; i < n; ++i) {
+      double maxMove = 0;  // a maximum: the same for any grouping
+#pragma omp parallel for schedule(static) reduction(max : maxMove)
+      for (std::ptrdiff_t i = 0; i < n; ++i) {
         xd[i] += alpha * step[i];
         const V3d d = alpha * step[i];
         maxMove = std::max(maxMove, std::max(std::abs(d.x), std::max(std::abs(d.y), std::abs(d.z))));
       }
-      for (std::size_t i = 0; i < n; ++i) frictionLambda[i] = contactActive[i] ? m.contactForce[i] : 0.0;
+#pragma omp parallel for schedule(static)
+      for (std::ptrdiff_t i = 0; i < n; ++i) frictionLambda[i] = contactActive[i] ? m.contactForce[i] : 0.0;
       if (maxMove < 1e-9) break;
     }
-    for (std::size_t i = 0; i < n; ++i) m.x[i] = m.state(xd[i]);
-    if (m.hasBody) {
-      for (std::size_t i = 0; i < n; ++i) {
-        if (m.pinned[i]) continue;
-        const double radius = m.contactRadius(i);
-        if (m.body.sample(m.x[i]) >= radius - kContactSnap) continue;
-        const bool flat = isZero(m.body.gradient(m.x[i]));
-        if (m.fp64) {
-          if (flat) {
-            m.x[i] = landOnBodyD(m.body, radius, xStart[i], m.x[i]);
-          } else {
-            collideBodyD(m.body, radius, m.fabrics[m.pFabric[i]].friction, xStart[i], m.x[i]);
-          }
+#pragma omp parallel for schedule(static)
+    for (std::ptrdiff_t i = 0; i < n; ++i) {
+      m.x[i] = m.state(xd[i]);
+      if (!m.hasBody || m.pinned[i]) continue;
+      const double radius = m.contactRadius(i);
+      if (m.body.sample(m.x[i]) >= radius - kContactSnap) continue;
+      const bool flat = isZero(m.body.gradient(m.x[i]));
+      if (m.fp64) {
+        if (flat) {
+          m.x[i] = landOnBodyD(m.body, radius, xStart[i], m.x[i]);
         } else {
-          if (flat) {
-            m.x[i] = tod(landOnBodyF(m.body, static_cast<float>(radius), tof(xStart[i]), tof(m.x[i])));
-          } else {
-            V3f xf = tof(m.x[i]);
-            collideBodyF(m.body, static_cast<float>(radius), static_cast<float>(m.fabrics[m.pFabric[i]].friction),
-                         tof(xStart[i]), xf);
-            m.x[i] = tod(xf);
-          }
+          collideBodyD(m.body, radius, m.fabrics[m.pFabric[i]].friction, xStart[i], m.x[i]);
+        }
+      } else {
+        if (flat) {
+          m.x[i] = tod(landOnBodyF(m.body, static_cast<float>(radius), tof(xStart[i]), tof(m.x[i])));
+        } else {
+          V3f xf = tof(m.x[i]);
+          collideBodyF(m.body, static_cast<float>(radius), static_cast<float>(m.fabrics[m.pFabric[i]].friction),
+                       tof(xStart[i]), xf);
+          m.x[i] = tod(xf);
         }
       }
     }
     for (const auto& [i, pos] : m.pins) m.x[i] = pos;
-    for (std::size_t i = 0; i < n; ++i) {
+#pragma omp parallel for schedule(static)
+    for (std::ptrdiff_t i = 0; i < n; ++i) {
       double c = m.settings.dampingScale * m.fabrics[m.pFabric[i]].damping;
       if (m.garments[m.pGarment[i]].phase == Assembling) c += m.settings.assemblyExtraDamping;
       if (m.fp64) {
@@ -1093,7 +1224,6 @@ struct Solver {
     for (auto& g : m.garments)
       if (g.phase == Assembling) g.assemblyTime += h;
   }
-
   void advance(double dt, int substeps, int iterations) {
     const int s = std::max(1, substeps);
     const double h = dt / s;
