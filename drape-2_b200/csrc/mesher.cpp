@@ -1,19 +1,19 @@
-// Pattern -> simulation mesh (include/drape_mesh.h): the reference's buildSimMesh
-// (libs/garment/src/sim_mesh_builder.cpp:196-323) on the host.
+// Pattern -> simulation mesh (include/drape_mesh.h) on the host, for the reference's buildSimMesh contract
+// (libs/garment/src/sim_mesh_builder.cpp:196-323; pattern rules libs/garment/src/validate.cpp:25-87).
 //
-// Steps per piece, as the reference: validate the pattern (libs/garment/src/validate.cpp:25-87); sample the outline
-// at arc-length positions: every seam side with its seam's step count, the free spans between breakpoints (start,
-// corners > 10 degrees, seam ends) with round(length / h) steps (:215-259); add the grain-aligned hexagonal lattice
-// points inside the outline and at least h / 2 from it (:124-160); triangulate boundary + lattice with the outline as
-// constraint and drop the outside (:268-281); three Jacobi Laplacian smoothing passes of the interior that never flip a
-// triangle (:166-194); vertex areas as a third of the incident triangle areas; seam pairs A_k <-> B_k (:305-322).
+// Per piece: validate the pattern; walk the outline once into boundary stations (each seam side one run with its
+// seam's station count, the free stretches between seam sides split at the corners into runs of ceil(length / h)
+// steps); fill the interior with a grain-aligned hexagonal lattice, row by row in the grain frame, keeping points
+// inside the outline and at least h / 2 from it; triangulate stations and lattice with the outline as constraint and
+// drop the outside; relax the interior vertices toward their incident triangles' centroids without letting any
+// incident angle shrink; vertex areas are a third of the incident triangle areas; seam pairs join station k of the
+// two sides.
 //
 // The constrained Delaunay triangulation is this file's own (the reference uses the CDT 1.4.5 library, absent here):
 // Lawson incremental insertion (point location by walking, split of the containing triangle or edge, legalising flips
 // with the in-circle test), constraint edges recovered by flipping the edges that cross them (Sloan 1993), then a
-// flood fill from the enclosing triangle's corners that stops at constraint edges removes the outside. On the
-// lattice-plus-outline inputs of this mesher the Delaunay triangulation is unique away from the outline, so the
-// triangles match any correct CDT there; the order of vertices and triangles is this file's.
+// flood fill from the enclosing triangle's corners that stops at constraint edges removes the outside. Vertex and
+// triangle order are this file's.
 #include "../../include/drape_mesh.h"
 
 #include <algorithm>
@@ -608,7 +608,12 @@ class Cdt {
 };
 
 // ---------------------------------------------------------------------------------------------------------------
-// The mesher (sim_mesh_builder.cpp:196-323).
+// The mesher. Per piece: the outline is walked into boundary stations (in outline order, from arc length 0), a
+// grain-aligned hexagonal lattice fills the interior, the stations and the lattice are triangulated with the outline
+// as constraint, and the interior vertices are relaxed. The output follows the reference's SimMesh contract
+// (libs/garment/src/sim_mesh_builder.cpp:196-323): seam sides carry the same station count on both pieces so seam
+// pairs match one to one, outline corners are vertices, lattice edges follow the grain's 60-degree directions,
+// vertex areas are a third of the incident triangle areas.
 
 struct Mesh {
   std::vector<V2> rest;
@@ -621,110 +626,139 @@ struct Mesh {
   std::vector<std::array<uint32_t, 4>> seamPairs;
 };
 
-constexpr double kEps = 1e-9;
+constexpr double kArcEps = 1e-9;
 
-int stepsCeil(double len, double h) { return std::max(1, static_cast<int>(std::ceil(len / h - 1e-9))); }
-int stepsRound(double len, double h) { return std::max(1, static_cast<int>(std::lround(len / h))); }
+// Stations on a run of outline: the fewest equal arc steps no longer than h (at least one).
+int stationsFor(double length, double h) { return std::max(1, static_cast<int>(std::ceil(length / h - kArcEps))); }
 
-// Sorted unique arc positions of one outline's samples.
-struct Samples {
-  double perimeter = 0;
-  std::vector<double> s;
-  double wrap(double x) const { return x >= perimeter - kEps ? 0.0 : x; }
-  void add(double x) { s.push_back(wrap(x)); }
-  void finish() {
-    std::sort(s.begin(), s.end());
-    std::vector<double> u;
-    for (double x : s)
-      if (u.empty() || x - u.back() > kEps) u.push_back(x);
-    s.swap(u);
-  }
-  std::size_t index(double x) const {
-    x = wrap(x);
-    const auto it = std::lower_bound(s.begin(), s.end(), x - kEps);
-    if (it == s.end() || std::abs(*it - x) > kEps) throw MeshError("internal: boundary sample not found");
-    return static_cast<std::size_t>(it - s.begin());
-  }
-};
-
-// Outline positions where the tangent turns by more than 10 degrees.
-std::vector<double> corners(const Outline& o) {
+// Arc positions of the segment joints where the outline's direction turns by more than 10 degrees (the reference's
+// corner rule).
+std::vector<double> turningPoints(const Outline& o) {
   std::vector<double> out;
   const std::size_t n = o.seg.size();
   for (std::size_t i = 0; i < n; ++i) {
-    const Cubic& prev = o.seg[(i + n - 1) % n];
-    const Cubic& next = o.seg[i];
-    V2 tin = prev.derivative(1.0), tout = next.derivative(0.0);
-    if (norm(tin) < 1e-14) tin = prev.p[3] - prev.p[0];
-    if (norm(tout) < 1e-14) tout = next.p[3] - next.p[0];
-    const double c = std::clamp(dot(unit(tin), unit(tout)), -1.0, 1.0);
-    if (std::acos(c) * 180.0 / kPi > 10.0) out.push_back(o.start[i]);
+    const Cubic& before = o.seg[(i + n - 1) % n];
+    const Cubic& after = o.seg[i];
+    V2 din = before.derivative(1.0), dout = after.derivative(0.0);
+    if (norm(din) < 1e-14) din = before.p[3] - before.p[0];  // degenerate end tangents: use the chords
+    if (norm(dout) < 1e-14) dout = after.p[3] - after.p[0];
+    const double turn = std::acos(std::clamp(dot(unit(din), unit(dout)), -1.0, 1.0));
+    if (turn > 10.0 * kPi / 180.0) out.push_back(o.start[i]);
   }
   return out;
 }
 
-// Outline edges bucketed into square cells of size h, for the lattice's distance-to-outline test.
-class EdgeBuckets {
- public:
-  EdgeBuckets(const std::vector<V2>& poly, double cell) : poly_(poly), cell_(cell) {
-    for (std::size_t i = 0; i < poly.size(); ++i) {
-      const V2 a = poly[i], b = poly[(i + 1) % poly.size()];
-      const int x0 = cellOf(std::min(a.x, b.x) - cell), x1 = cellOf(std::max(a.x, b.x) + cell);
-      const int y0 = cellOf(std::min(a.y, b.y) - cell), y1 = cellOf(std::max(a.y, b.y) + cell);
-      for (int x = x0; x <= x1; ++x)
-        for (int y = y0; y <= y1; ++y) cells_[key(x, y)].push_back(static_cast<uint32_t>(i));
-    }
-  }
-  double nearest(V2 p) const {  // +inf when no edge is within a cell
-    const auto it = cells_.find(key(cellOf(p.x), cellOf(p.y)));
-    if (it == cells_.end()) return std::numeric_limits<double>::infinity();
-    double best = std::numeric_limits<double>::infinity();
-    for (uint32_t i : it->second) best = std::min(best, pointSegmentDistance(p, poly_[i], poly_[(i + 1) % poly_.size()]));
-    return best;
-  }
-
- private:
-  int cellOf(double v) const { return static_cast<int>(std::floor(v / cell_)); }
-  static int64_t key(int x, int y) { return (static_cast<int64_t>(x) << 32) ^ static_cast<uint32_t>(y); }
-  const std::vector<V2>& poly_;
-  double cell_;
-  std::unordered_map<int64_t, std::vector<uint32_t>> cells_;
+// A stretch of outline sampled as one unit: [a, b] in arc length with `count` equal steps. A seam side is one run
+// (seam >= 0, side 0 or 1) whatever corners it covers, so both of its pieces sample it at the same fractions.
+struct Run {
+  double a = 0, b = 0;
+  int count = 1;
+  int seam = -1, side = 0;
 };
 
-// Hexagonal lattice aligned with the grain (rows h sqrt(3)/2 apart, odd rows shifted by h/2), inside the polygon
-// (even-odd crossings along each row) and at least h/2 from its edges.
-std::vector<V2> lattice(const std::vector<V2>& poly, V2 grain, double h) {
-  const V2 u = unit(grain), v{-u.y, u.x};
-  std::vector<V2> loc(poly.size());
-  double umin = 1e300, umax = -1e300, vmin = 1e300, vmax = -1e300;
-  for (std::size_t i = 0; i < poly.size(); ++i) {
-    loc[i] = {dot(poly[i], u), dot(poly[i], v)};
-    umin = std::min(umin, loc[i].x);
-    umax = std::max(umax, loc[i].x);
-    vmin = std::min(vmin, loc[i].y);
-    vmax = std::max(vmax, loc[i].y);
-  }
-  const double rowStep = std::sqrt(3.0) / 2.0 * h;
-  const EdgeBuckets buckets(poly, h);
-  std::vector<V2> out;
-  std::vector<double> xs;
-  for (int j = static_cast<int>(std::floor(vmin / rowStep)) - 1; j <= static_cast<int>(std::ceil(vmax / rowStep)) + 1;
-       ++j) {
-    const double vy = j * rowStep;
-    xs.clear();
-    for (std::size_t k = 0; k < loc.size(); ++k) {
-      const V2 a = loc[k], b = loc[(k + 1) % loc.size()];
-      if ((a.y > vy) != (b.y > vy)) xs.push_back(a.x + (vy - a.y) * (b.x - a.x) / (b.y - a.y));
+struct BoundaryWalk {
+  std::vector<V2> points;  // stations in outline order; station 0 at arc length 0
+  std::map<std::pair<int, int>, std::vector<uint32_t>> seamStations;  // (seam, side) -> stations 0..count
+};
+
+// Walks the outline once: the gaps between this piece's seam sides are split at the turning points into free runs of
+// stationsFor(length, h) steps; every run emits its start and interior stations, so the stations come out in outline
+// order, and each seam side records its station indices as it is emitted (the last one is the next run's first, or
+// station 0 where the outline closes).
+BoundaryWalk walkBoundary(const Outline& o, std::vector<Run> seamRuns, double h) {
+  const double perimeter = o.perimeter();
+  std::sort(seamRuns.begin(), seamRuns.end(), [](const Run& x, const Run& y) { return x.a < y.a; });
+  const std::vector<double> turns = turningPoints(o);
+  std::vector<Run> runs;
+  auto addFree = [&](double a, double b) {
+    if (b - a <= kArcEps) return;
+    double from = a;
+    for (double t : turns) {
+      if (t <= from + kArcEps || t >= b - kArcEps) continue;
+      runs.push_back({from, t, stationsFor(t - from, h)});
+      from = t;
     }
-    std::sort(xs.begin(), xs.end());
-    const double shift = ((j % 2) + 2) % 2 == 1 ? 0.5 : 0.0;
-    for (int i = static_cast<int>(std::floor(umin / h)) - 1; i <= static_cast<int>(std::ceil(umax / h)) + 1; ++i) {
-      const double ux = (i + shift) * h;
-      const auto below = std::lower_bound(xs.begin(), xs.end(), ux) - xs.begin();
-      if (below % 2 == 0) continue;
-      const V2 p = ux * u + vy * v;
-      if (buckets.nearest(p) < 0.5 * h) continue;
-      out.push_back(p);
+    runs.push_back({from, b, stationsFor(b - from, h)});
+  };
+  double cursor = 0.0;
+  for (const Run& s : seamRuns) {
+    addFree(cursor, s.a);
+    runs.push_back(s);
+    cursor = std::max(cursor, s.b);
+  }
+  addFree(cursor, perimeter);
+  BoundaryWalk w;
+  std::vector<std::pair<const Run*, uint32_t>> pending;  // seam runs and their first station
+  for (const Run& r : runs) {
+    const uint32_t first = static_cast<uint32_t>(w.points.size());
+    for (int k = 0; k < r.count; ++k) w.points.push_back(o.pointAt(r.a + (r.b - r.a) * k / r.count));
+    if (r.seam >= 0) pending.emplace_back(&r, first);
+  }
+  const uint32_t total = static_cast<uint32_t>(w.points.size());
+  for (const auto& [r, first] : pending) {
+    std::vector<uint32_t>& v = w.seamStations[{r->seam, r->side}];
+    for (int k = 0; k <= r->count; ++k) v.push_back((first + static_cast<uint32_t>(k)) % total);
+  }
+  return w;
+}
+
+// The hexagonal lattice aligned with `grain` (rows along the grain, h sqrt(3)/2 apart, every other row shifted by
+// h/2), restricted to the points inside the closed polygon `poly` (nonzero winding) that keep at least h/2 from every
+// polygon edge. Work happens in the grain frame, row by row: each polygon edge is listed under the rows its
+// h/2-neighbourhood reaches, so a row sees exactly the edges that can cross it or come within h/2 of it; the winding
+// of a lattice point is the signed count of those edges crossing the row beyond it.
+std::vector<V2> grainLattice(const std::vector<V2>& poly, V2 grain, double h) {
+  const V2 gu = unit(grain), gv{-gu.y, gu.x};
+  const std::size_t n = poly.size();
+  std::vector<V2> q(n);
+  double vLo = 1e300, vHi = -1e300, uLo = 1e300, uHi = -1e300;
+  for (std::size_t i = 0; i < n; ++i) {
+    q[i] = {dot(poly[i], gu), dot(poly[i], gv)};
+    uLo = std::min(uLo, q[i].x);
+    uHi = std::max(uHi, q[i].x);
+    vLo = std::min(vLo, q[i].y);
+    vHi = std::max(vHi, q[i].y);
+  }
+  const double pitch = h * std::sqrt(0.75), clearance = 0.5 * h;
+  const int jLo = static_cast<int>(std::floor(vLo / pitch)), jHi = static_cast<int>(std::ceil(vHi / pitch));
+  std::vector<std::vector<uint32_t>> rowEdges(static_cast<std::size_t>(jHi - jLo + 1));
+  for (std::size_t k = 0; k < n; ++k) {
+    const V2 a = q[k], b = q[(k + 1) % n];
+    const int r0 = std::max(jLo, static_cast<int>(std::ceil((std::min(a.y, b.y) - clearance) / pitch)));
+    const int r1 = std::min(jHi, static_cast<int>(std::floor((std::max(a.y, b.y) + clearance) / pitch)));
+    for (int j = r0; j <= r1; ++j) rowEdges[static_cast<std::size_t>(j - jLo)].push_back(static_cast<uint32_t>(k));
+  }
+  std::vector<V2> out;
+  std::vector<std::pair<double, int>> hits;  // (u of the crossing, winding contribution)
+  for (int j = jLo; j <= jHi; ++j) {
+    const std::vector<uint32_t>& edges = rowEdges[static_cast<std::size_t>(j - jLo)];
+    const double v = j * pitch;
+    hits.clear();
+    int winding = 0;
+    for (uint32_t k : edges) {
+      const V2 a = q[k], b = q[(k + 1) % n];
+      if ((a.y <= v) == (b.y <= v)) continue;
+      const int dir = b.y > a.y ? 1 : -1;
+      hits.emplace_back(a.x + (v - a.y) * (b.x - a.x) / (b.y - a.y), dir);
+      winding += dir;
+    }
+    if (hits.empty()) continue;
+    std::sort(hits.begin(), hits.end());
+    const double shift = (j % 2 != 0) ? 0.5 * h : 0.0;
+    const int iLo = static_cast<int>(std::ceil((uLo - shift) / h)), iHi = static_cast<int>(std::floor((uHi - shift) / h));
+    std::size_t next = 0;
+    for (int i = iLo; i <= iHi; ++i) {
+      const double u = i * h + shift;
+      while (next < hits.size() && hits[next].first <= u) winding -= hits[next++].second;
+      if (winding == 0) continue;
+      const V2 p{u, v};
+      bool clear = true;
+      for (uint32_t k : edges)
+        if (pointSegmentDistance(p, q[k], q[(k + 1) % n]) < clearance) {
+          clear = false;
+          break;
+        }
+      if (clear) out.push_back(u * gu + v * gv);
     }
   }
   return out;
@@ -732,35 +766,61 @@ std::vector<V2> lattice(const std::vector<V2>& poly, V2 grain, double h) {
 
 double triArea(V2 a, V2 b, V2 c) { return 0.5 * cross3(a, b, c); }
 
-// Jacobi Laplacian smoothing of the interior vertices; a move that leaves an incident triangle with area <= 1e-14
-// is undone.
-void smooth(std::vector<V2>& pts, const std::vector<std::array<uint32_t, 3>>& tris, std::size_t boundaryCount,
-            int iterations) {
-  std::vector<std::vector<uint32_t>> nbrs(pts.size()), incident(pts.size());
+// Largest corner cosine of a triangle: the smaller its smallest angle, the larger this is.
+double largestCosine(V2 a, V2 b, V2 c) {
+  auto cosAt = [](V2 p, V2 x, V2 y) {
+    const V2 e = x - p, f = y - p;
+    return dot(e, f) / std::max(1e-300, norm(e) * norm(f));
+  };
+  return std::max(cosAt(a, b, c), std::max(cosAt(b, c, a), cosAt(c, a, b)));
+}
+
+// Centroidal relaxation of the interior vertices [firstInterior, pts.size()), `sweeps` Gauss-Seidel passes: a vertex
+// moves to the area-weighted mean of its incident triangles' centroids. The move is kept only if every incident
+// triangle stays counter-clockwise (area > 1e-14) and the smallest angle among them does not shrink; otherwise half
+// the move is tried, then none. A vertex inside an undistorted hexagonal patch is its own target and stays put.
+void relaxInterior(std::vector<V2>& pts, const std::vector<std::array<uint32_t, 3>>& tris, std::size_t firstInterior,
+                   int sweeps) {
+  std::vector<uint32_t> start(pts.size() + 1, 0), list;
+  for (const auto& t : tris)
+    for (uint32_t v : t) ++start[v + 1];
+  for (std::size_t i = 0; i < pts.size(); ++i) start[i + 1] += start[i];
+  list.resize(start.back());
+  std::vector<uint32_t> fill(start.begin(), start.end() - 1);
   for (uint32_t t = 0; t < tris.size(); ++t)
-    for (int k = 0; k < 3; ++k) {
-      incident[tris[t][k]].push_back(t);
-      nbrs[tris[t][k]].push_back(tris[t][(k + 1) % 3]);
-      nbrs[tris[t][k]].push_back(tris[t][(k + 2) % 3]);
+    for (uint32_t v : tris[t]) list[fill[v]++] = t;
+  auto worst = [&](std::size_t i, double& minArea) {
+    double c = -1.0;
+    minArea = 1e300;
+    for (uint32_t e = start[i]; e < start[i + 1]; ++e) {
+      const auto& t = tris[list[e]];
+      minArea = std::min(minArea, triArea(pts[t[0]], pts[t[1]], pts[t[2]]));
+      c = std::max(c, largestCosine(pts[t[0]], pts[t[1]], pts[t[2]]));
     }
-  for (auto& n : nbrs) {
-    std::sort(n.begin(), n.end());
-    n.erase(std::unique(n.begin(), n.end()), n.end());
-  }
-  for (int it = 0; it < iterations; ++it) {
-    const std::vector<V2> prev = pts;
-    for (std::size_t i = boundaryCount; i < pts.size(); ++i) {
-      if (nbrs[i].empty()) continue;
-      V2 mean{0, 0};
-      for (uint32_t n : nbrs[i]) mean = mean + prev[n];
-      mean = (1.0 / static_cast<double>(nbrs[i].size())) * mean;
-      const V2 old = pts[i];
-      pts[i] = mean;
-      for (uint32_t t : incident[i])
-        if (triArea(pts[tris[t][0]], pts[tris[t][1]], pts[tris[t][2]]) <= 1e-14) {
-          pts[i] = old;
-          break;
-        }
+    return c;
+  };
+  for (int sweep = 0; sweep < sweeps; ++sweep) {
+    for (std::size_t i = firstInterior; i < pts.size(); ++i) {
+      if (start[i] == start[i + 1]) continue;
+      double weight = 0;
+      V2 target{0, 0};
+      for (uint32_t e = start[i]; e < start[i + 1]; ++e) {
+        const auto& t = tris[list[e]];
+        const double a = std::abs(triArea(pts[t[0]], pts[t[1]], pts[t[2]]));
+        target = target + (a / 3.0) * (pts[t[0]] + pts[t[1]] + pts[t[2]]);
+        weight += a;
+      }
+      if (!(weight > 0)) continue;
+      target = (1.0 / weight) * target;
+      const V2 home = pts[i];
+      double area = 0;
+      const double before = worst(i, area);
+      for (double step : {1.0, 0.5}) {
+        pts[i] = home + step * (target - home);
+        const double after = worst(i, area);
+        if (area > 1e-14 && after <= before + 1e-12) break;
+        pts[i] = home;
+      }
     }
   }
 }
@@ -773,78 +833,49 @@ Mesh build(const Pattern& pat, double h) {
     for (const auto& [rule, text] : issues) msg += " [" + rule + "] " + text + ";";
     throw MeshError(msg);
   }
-  struct Side {
-    double start, end;
-    int steps;
-  };
-  std::vector<std::vector<Side>> sides(pat.pieces.size());
-  std::vector<int> seamSteps(pat.seams.size());
+  // Every seam gets one station count (from its longer side) and places a run of it on each side's piece.
+  std::vector<int> seamCount(pat.seams.size());
+  std::vector<std::vector<Run>> pieceSeamRuns(pat.pieces.size());
   for (std::size_t s = 0; s < pat.seams.size(); ++s) {
     const Seam& sm = pat.seams[s];
-    const int steps = stepsCeil(std::max(sm.a.end - sm.a.start, sm.b.end - sm.b.start), h);
-    seamSteps[s] = steps;
-    for (const EdgeRef* e : {&sm.a, &sm.b}) sides[pat.find(e->piece)].push_back({e->start, e->end, steps});
+    seamCount[s] = stationsFor(std::max(sm.a.end - sm.a.start, sm.b.end - sm.b.start), h);
+    const EdgeRef* sides[2] = {&sm.a, &sm.b};
+    for (int side = 0; side < 2; ++side)
+      pieceSeamRuns[static_cast<std::size_t>(pat.find(sides[side]->piece))].push_back(
+          {sides[side]->start, sides[side]->end, seamCount[s], static_cast<int>(s), side});
   }
   Mesh mesh;
-  std::vector<Samples> loops(pat.pieces.size());
-  std::vector<uint32_t> loopOffset(pat.pieces.size());
+  std::map<std::pair<int, int>, std::vector<uint32_t>> seamVertices;  // (seam, side) -> mesh vertices
   for (std::size_t pi = 0; pi < pat.pieces.size(); ++pi) {
     const Piece& piece = pat.pieces[pi];
-    const Outline& o = piece.outline;
-    Samples& loop = loops[pi];
-    loop.perimeter = o.perimeter();
-    std::vector<double> breaks{0.0};
-    for (double c : corners(o)) breaks.push_back(c);
-    for (const Side& sd : sides[pi]) {
-      breaks.push_back(sd.start);
-      breaks.push_back(sd.end);
-    }
-    for (double& b : breaks) b = loop.wrap(b);
-    std::sort(breaks.begin(), breaks.end());
-    breaks.erase(std::unique(breaks.begin(), breaks.end(), [](double a, double b) { return b - a <= kEps; }),
-                 breaks.end());
-    for (const Side& sd : sides[pi])
-      for (int k = 0; k <= sd.steps; ++k) loop.add(sd.start + (sd.end - sd.start) * k / sd.steps);
-    for (std::size_t b = 0; b < breaks.size(); ++b) {
-      const double s0 = breaks[b], s1 = b + 1 < breaks.size() ? breaks[b + 1] : loop.perimeter;
-      const double mid = 0.5 * (s0 + s1);
-      bool inSeam = false;
-      for (const Side& sd : sides[pi]) inSeam = inSeam || (mid > sd.start && mid < sd.end);
-      if (inSeam) continue;
-      const int n = stepsRound(s1 - s0, h);
-      for (int k = 0; k < n; ++k) loop.add(s0 + (s1 - s0) * k / n);
-    }
-    loop.finish();
-
-    std::vector<V2> pts;
-    for (double s : loop.s) pts.push_back(o.pointAt(s));
+    const BoundaryWalk walk = walkBoundary(piece.outline, pieceSeamRuns[pi], h);
+    std::vector<V2> pts = walk.points;
     const std::size_t boundaryCount = pts.size();
     const V2 grain = unit(piece.grain);
-    for (const V2& p : lattice(pts, grain, h)) pts.push_back(p);
+    const std::vector<V2> inner = grainLattice(walk.points, grain, h);
+    pts.insert(pts.end(), inner.begin(), inner.end());
     {
-      std::vector<std::pair<std::pair<double, double>, std::size_t>> sorted(pts.size());
-      for (std::size_t i = 0; i < pts.size(); ++i) sorted[i] = {{pts[i].x, pts[i].y}, i};
-      std::sort(sorted.begin(), sorted.end());
+      std::vector<V2> sorted = pts;
+      std::sort(sorted.begin(), sorted.end(), [](V2 a, V2 b) { return a.x < b.x || (a.x == b.x && a.y < b.y); });
       for (std::size_t i = 1; i < sorted.size(); ++i)
-        if (sorted[i].first == sorted[i - 1].first)
+        if (sorted[i].x == sorted[i - 1].x && sorted[i].y == sorted[i - 1].y)
           throw MeshError("piece '" + piece.id + "': duplicate mesh vertices");
     }
     Cdt cdt(pts);
     cdt.insertAll();
-    std::vector<std::pair<int, int>> edges;
+    std::vector<std::pair<int, int>> loop(boundaryCount);
     for (std::size_t i = 0; i < boundaryCount; ++i)
-      edges.emplace_back(static_cast<int>(i), static_cast<int>((i + 1) % boundaryCount));
-    cdt.constrain(edges);
+      loop[i] = {static_cast<int>(i), static_cast<int>((i + 1) % boundaryCount)};
+    cdt.constrain(loop);
     std::vector<std::array<uint32_t, 3>> tris;
     for (const auto& t : cdt.inside()) {
       std::array<uint32_t, 3> tri{static_cast<uint32_t>(t[0]), static_cast<uint32_t>(t[1]), static_cast<uint32_t>(t[2])};
       if (triArea(pts[tri[0]], pts[tri[1]], pts[tri[2]]) < 0) std::swap(tri[1], tri[2]);
       tris.push_back(tri);
     }
-    smooth(pts, tris, boundaryCount, 3);
+    relaxInterior(pts, tris, boundaryCount, 3);
 
-    const uint32_t offset = static_cast<uint32_t>(mesh.rest.size());
-    loopOffset[pi] = offset;
+    const uint32_t base = static_cast<uint32_t>(mesh.rest.size());
     for (std::size_t i = 0; i < pts.size(); ++i) {
       mesh.rest.push_back(pts[i]);
       mesh.vertexPiece.push_back(static_cast<uint32_t>(pi));
@@ -854,22 +885,25 @@ Mesh build(const Pattern& pat, double h) {
     for (const auto& t : tris) {
       const double area = triArea(pts[t[0]], pts[t[1]], pts[t[2]]);
       if (!(area > 1e-12)) throw MeshError("piece '" + piece.id + "': degenerate triangle");
-      mesh.triangles.push_back({t[0] + offset, t[1] + offset, t[2] + offset});
+      mesh.triangles.push_back({t[0] + base, t[1] + base, t[2] + base});
       mesh.trianglePiece.push_back(static_cast<uint32_t>(pi));
-      for (uint32_t v : t) mesh.vertexArea[v + offset] += area / 3.0;
+      for (uint32_t v : t) mesh.vertexArea[base + v] += area / 3.0;
     }
     mesh.pieceGrain.push_back(grain);
+    for (const auto& [key, stations] : walk.seamStations) {
+      std::vector<uint32_t>& dst = seamVertices[key];
+      for (uint32_t v : stations) dst.push_back(base + v);
+    }
   }
+  // Seam pairs: station k of each side, counted from the side's far end when the side is reversed.
   for (std::size_t s = 0; s < pat.seams.size(); ++s) {
-    const Seam& sm = pat.seams[s];
-    const int n = seamSteps[s];
-    auto vertexAt = [&](const EdgeRef& e, int k) {
-      const std::size_t pi = static_cast<std::size_t>(pat.find(e.piece));
-      const int kk = e.reversed ? n - k : k;
-      return loopOffset[pi] + static_cast<uint32_t>(loops[pi].index(e.start + (e.end - e.start) * kk / n));
-    };
+    const int n = seamCount[s];
+    const std::vector<uint32_t>& a = seamVertices.at({static_cast<int>(s), 0});
+    const std::vector<uint32_t>& b = seamVertices.at({static_cast<int>(s), 1});
+    const bool ra = pat.seams[s].a.reversed, rb = pat.seams[s].b.reversed;
     for (int k = 0; k <= n; ++k)
-      mesh.seamPairs.push_back({vertexAt(sm.a, k), vertexAt(sm.b, k), static_cast<uint32_t>(s), static_cast<uint32_t>(k)});
+      mesh.seamPairs.push_back({a[static_cast<std::size_t>(ra ? n - k : k)], b[static_cast<std::size_t>(rb ? n - k : k)],
+                                static_cast<uint32_t>(s), static_cast<uint32_t>(k)});
   }
   return mesh;
 }
