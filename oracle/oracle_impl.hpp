@@ -22,6 +22,9 @@
 
 namespace oracle {
 
+// Loops over fewer items than this run on the calling thread (a parallel region costs more than they do).
+constexpr std::ptrdiff_t kParallelMin = 4096;
+
 // ---------------------------------------------------------------------------------------------------------------
 // Fixed-size math.
 
@@ -935,7 +938,7 @@ struct Solver {
     const std::ptrdiff_t K = static_cast<std::ptrdiff_t>(m.seams.size());
     const double limitScale = m.settings.strainLimitStiffnessScale;
     const double slipEps = m.settings.frictionSlipSpeed * substepH;
-#pragma omp parallel
+#pragma omp parallel if (n + S + H >= kParallelMin)
     {
 #pragma omp for schedule(static) nowait
       for (std::ptrdiff_t i = 0; i < n; ++i) {
@@ -1021,7 +1024,7 @@ struct Solver {
 
   void multiply(const std::vector<V3d>& in, std::vector<V3d>& out) const {
     const std::ptrdiff_t n = static_cast<std::ptrdiff_t>(in.size());
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) if (n >= kParallelMin)
     for (std::ptrdiff_t i = 0; i < n; ++i) {
       V3d acc;
       if (!m.pinned[i]) {
@@ -1038,7 +1041,7 @@ struct Solver {
   double vdot(const std::vector<V3d>& a, const std::vector<V3d>& b) {
     const std::ptrdiff_t n = static_cast<std::ptrdiff_t>(a.size());
     if (dotTmp.size() < a.size()) dotTmp.resize(a.size());
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) if (n >= kParallelMin)
     for (std::ptrdiff_t i = 0; i < n; ++i) dotTmp[i] = dot(a[i], b[i]);
     double s = 0;
     for (std::ptrdiff_t i = 0; i < n; ++i) s += dotTmp[i];
@@ -1051,7 +1054,7 @@ struct Solver {
 
   void solveLinear() {
     const std::ptrdiff_t n = static_cast<std::ptrdiff_t>(grad.size());
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) if (n >= kParallelMin)
     for (std::ptrdiff_t i = 0; i < n; ++i) {
       if (m.pinned[i]) {
         precond[i] = M3{};
@@ -1072,7 +1075,7 @@ struct Solver {
     const double r0 = std::sqrt(vdot(r, r));
     for (int it = 0; r0 > 0 && it < m.settings.maxCgIterations; ++it) {
       multiply(p, apFull);
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) if (n >= kParallelMin)
       for (std::ptrdiff_t i = 0; i < n; ++i) {
         ap[i] = apFull[i];
         filterRow(ap, i);
@@ -1081,14 +1084,14 @@ struct Solver {
       if (!(pAp > 0)) break;
       const double alpha = rz / pAp;
       ++counters.cg_iterations;
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) if (n >= kParallelMin)
       for (std::ptrdiff_t i = 0; i < n; ++i) {
         step[i] += alpha * p[i];
         r[i] -= alpha * ap[i];
         resid[i] -= alpha * apFull[i];
       }
       if (std::sqrt(vdot(r, r)) <= m.settings.cgTolerance * r0) break;
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) if (n >= kParallelMin)
       for (std::ptrdiff_t i = 0; i < n; ++i) {
         z[i] = precond[i] * r[i];
         filterRow(z, i);
@@ -1096,17 +1099,17 @@ struct Solver {
       const double rzNew = vdot(r, z);
       const double beta = rzNew / rz;
       rz = rzNew;
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) if (n >= kParallelMin)
       for (std::ptrdiff_t i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
     }
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) if (n >= kParallelMin)
     for (std::ptrdiff_t i = 0; i < n; ++i)
       m.contactForce[i] = contactActive[i] ? std::max(0.0, -dot(resid[i], contactNormal[i])) : 0.0;
   }
 
   double evaluateWithContact(double invH2) {
     const std::ptrdiff_t n = static_cast<std::ptrdiff_t>(xd.size());
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) if (n >= kParallelMin)
     for (std::ptrdiff_t i = 0; i < n; ++i) {
       if (!contactNear[i]) continue;
       const double c = contactGap(i, xd[i]);
@@ -1114,7 +1117,7 @@ struct Solver {
       if (contactActive[i] && c > 0) xd[i] += c * contactNormal[i];
     }
     const double e = evaluate(xd, invH2, true);
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) if (n >= kParallelMin)
     for (std::ptrdiff_t i = 0; i < n; ++i)
       if (contactActive[i] && dot(grad[i], contactNormal[i]) < 0) contactActive[i] = 0;
     return e;
@@ -1125,7 +1128,7 @@ struct Solver {
     const V3d gravity = m.settings.gravity;
     const std::ptrdiff_t n = static_cast<std::ptrdiff_t>(m.x.size());
     substepH = h;
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) if (n >= kParallelMin)
     for (std::ptrdiff_t i = 0; i < n; ++i) {
       xStart[i] = m.x[i];
       const V3d vel = m.v[i];
@@ -1168,24 +1171,24 @@ struct Solver {
       if (!(slope < 0)) break;
       double alpha = 1.0;
       for (int ls = 0; ls < 20; ++ls) {
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) if (n >= kParallelMin)
         for (std::ptrdiff_t i = 0; i < n; ++i) trial[i] = xd[i] + alpha * step[i];
         if (evaluate(trial, invH2, false) <= e0 + 1e-4 * alpha * slope) break;
         alpha *= 0.5;
         ++counters.line_search_halvings;
       }
       double maxMove = 0;  // a maximum: the same for any grouping
-#pragma omp parallel for schedule(static) reduction(max : maxMove)
+#pragma omp parallel for schedule(static) reduction(max : maxMove) if (n >= kParallelMin)
       for (std::ptrdiff_t i = 0; i < n; ++i) {
         xd[i] += alpha * step[i];
         const V3d d = alpha * step[i];
         maxMove = std::max(maxMove, std::max(std::abs(d.x), std::max(std::abs(d.y), std::abs(d.z))));
       }
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) if (n >= kParallelMin)
       for (std::ptrdiff_t i = 0; i < n; ++i) frictionLambda[i] = contactActive[i] ? m.contactForce[i] : 0.0;
       if (maxMove < 1e-9) break;
     }
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) if (n >= kParallelMin)
     for (std::ptrdiff_t i = 0; i < n; ++i) {
       m.x[i] = m.state(xd[i]);
       if (!m.hasBody || m.pinned[i]) continue;
@@ -1210,7 +1213,7 @@ struct Solver {
       }
     }
     for (const auto& [i, pos] : m.pins) m.x[i] = pos;
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) if (n >= kParallelMin)
     for (std::ptrdiff_t i = 0; i < n; ++i) {
       double c = m.settings.dampingScale * m.fabrics[m.pFabric[i]].damping;
       if (m.garments[m.pGarment[i]].phase == Assembling) c += m.settings.assemblyExtraDamping;
