@@ -1,20 +1,21 @@
 #!/usr/bin/env python
 """Benchmark of the cloth solver's Newton-step hot path on B200: drape settle time.
 
-One step = sixteen drapes of the seamed-tube workload to rest (its own start state and fifteen with every coordinate
-moved by a seeded uniform +-1 um), each run by the solver's drape runner (DrapeSession semantics,
+One step = one drape of the seamed-tube workload to rest, run by the solver's drape runner (DrapeSession semantics,
 libs/sim/src/drape_session.cpp:32-95: Assembling until the seams close, then Settling until the RMS speed stays below
-2 mm/s for 60 frames). The metric is the mean device time to settle one drape; PCG iterations per Newton step are
-reported beside it.
+2 mm/s for 60 frames). Step k drapes start state k mod 16: the workload's own (k = 0) or one with every coordinate
+moved by a seeded uniform +-1 um. The metric is the mean device time to settle one drape; PCG iterations per Newton
+step are reported beside it.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference] [--workload tube60k|tube10k]
 
 --impl cuda (default): the CUDA library through its C ABI, inputs resident in HBM (value) and through the full
   host-buffer path (e2e: build from host arrays, drape, read positions back). For N > 1 every rank drapes its own
-  replica (one drape does not shard); value is the slowest rank's settle time.
---impl reference: the reference solver's CPU algorithm (the oracle's restatement of CpuSolver, single-threaded like
-  the reference) timed on a bounded sample of frames of the same workload, extrapolated to the frames the reference
-  path needs to settle (tests/golden/settle_frames.json, made by tests/golden/make_settle_frames.py).
+  replica (one drape does not shard); value is the slowest rank's mean settle time.
+--impl reference: the reference solver's CPU algorithm (the oracle's restatement of CpuSolver, float particle state
+  and double solve, its loops spread over all host threads with results identical to one thread) drapes the
+  workload's own start state to rest once, timed whole: the K steps are K consecutive slices of that one drape's
+  frames, so value is the measured wall time of the whole CPU drape.
 """
 from __future__ import annotations
 
@@ -49,7 +50,7 @@ SETTLE_FIXTURE = os.path.join(ROOT, "tests", "golden", "settle_frames.json")
 # 2 mm/s threshold for hundreds of frames (332-1110 frames over such start states on the 60k tube), so one drape
 # alone does not measure the solver.
 SEEDS = 16
-SEED_DESC = ("each step drapes 16 start states: the workload's own and 15 with every coordinate moved by uniform "
+SEED_DESC = ("step k drapes start state k mod 16: the workload's own (0) or one with every coordinate moved by uniform "
              "+-1 um (numpy default_rng(seed), seeds 1-15); value and e2e are means over all of them")
 
 
@@ -143,117 +144,268 @@ def dist_setup():
     return world, rank, local
 
 
-def reference_settle_seconds(workload: str, repeats: int):
-    """The reference CPU path's settle time on this host: the first `sample` frames of the drape are timed here
-    (`repeats` times, the fastest kept), and the full drape's wall time recorded by tests/golden/make_settle_frames.py
-    on its machine is scaled by the ratio of the two sample times. Returns (seconds, description, fixture)."""
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def reference_drape(workload: str, steps: int, warmup_frames: int, threads: int = 0) -> dict:
+    """The reference CPU path (the oracle's faithful restatement of CpuSolver: float particle state, double solve,
+    block-Jacobi PCG with the workload's cap and tolerance) drapes the workload's own start state to rest, timed whole
+    on the host. Its loops run on `threads` host threads (0: all); the per-slot, per-particle and energy/dot sums keep
+    the serial order, so the drape is the single-threaded one bit for bit. `warmup_frames` frames of a separate solver
+    run first, untimed. Returns the wall time, the frame count, per-frame wall times folded into `steps` consecutive
+    slices of equal frame count, the counters and the threads used."""
     import oracle as O
     from drape_b200 import session as SS
-    with open(SETTLE_FIXTURE) as f:
-        fx = json.load(f)[workload]
+    L = O.lib()
+    L.oracle_set_threads(threads)
+    used = int(L.oracle_threads())
     scene = make_scene(workload)
-    sample = int(fx["sample_frames"])
-    best = None
-    for _ in range(max(1, repeats)):
-        o = O.OracleSolver()
-        o.build(scene)
-        sess = SS.DrapeSession(o, [scene.garments[0].id])
-        t0 = time.perf_counter()
-        for _ in range(sample):
-            sess.advance()
-        dt = time.perf_counter() - t0
-        best = dt if best is None else min(best, dt)
-    value = float(fx["total_seconds"]) * best / float(fx["sample_seconds"])
-    desc = (f"first {sample} frames of the drape timed on this host ({best:.2f} s, one thread); the full drape "
-            f"({fx['frames']} frames to settle, {fx['total_seconds']:.1f} s where the fixture was made, sample "
-            f"{fx['sample_seconds']:.2f} s) scaled by the sample ratio")
-    return value, desc, fx
+    gid = scene.garments[0].id
+    if warmup_frames > 0:
+        w = O.OracleSolver()
+        w.build(scene)
+        w.set_phase(gid, 0)
+        for _ in range(warmup_frames):
+            w.step(1.0 / 60.0, 1, 2)
+        del w
+    o = O.OracleSolver()
+    o.build(scene)
+    sess = SS.DrapeSession(o, [gid])
+    frame_s = []
+    t0 = time.perf_counter()
+    while not sess.finished():
+        f0 = time.perf_counter()
+        sess.advance()
+        frame_s.append(time.perf_counter() - f0)
+    total = time.perf_counter() - t0
+    c = o.counters()
+    k = max(1, steps)
+    bounds = [round(i * len(frame_s) / k) for i in range(k + 1)]
+    step_s = [float(sum(frame_s[bounds[i]:bounds[i + 1]])) for i in range(k)]
+    r = sess.result
+    return {"seconds": total, "frames": int(r.frames_run), "settled": bool(r.settled), "step_s": step_s,
+            "newton_iterations": int(c.newton_iterations), "cg_iterations": int(c.cg_iterations),
+            "line_search_halvings": int(c.line_search_halvings), "threads": used, "cpu": cpu_model(),
+            "host_cpus": os.cpu_count()}
 
 
 def run_reference(args):
-    """The reference CPU path (oracle restatement of CpuSolver, float state, double solve, one thread)."""
+    """The reference CPU path timed whole: one drape of the workload's own start state to rest (see reference_drape).
+    Under torchrun only rank 0 runs it."""
     world, rank, _ = dist_setup()
     if rank != 0:
         return 0
-    value, desc, fx = reference_settle_seconds(args.workload, args.warmup + args.steps)
+    r = reference_drape(args.workload, args.steps, args.warmup)
+    value = r["seconds"]
+    sample = (f"one whole drape of the workload's own start state to rest: {r['frames']} frames, settled "
+              f"{r['settled']}, timed from its first frame to the frame that settles it, on {r['threads']} host "
+              f"threads ({r['cpu']}, {r['host_cpus']} logical CPUs); the {args.steps} steps are consecutive slices "
+              f"of its frames")
     line = {
         "metric": METRIC, "value": value, "unit": "s", "impl": "reference", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": value * 1000.0, "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "warmup": args.warmup, "ms_per_step": value * 1000.0 / max(1, args.steps), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOADS[args.workload]["desc"],
-                   "solver": "CpuSolver restatement (float particle state, double solve), block-Jacobi PCG"},
-        "cpu_baseline": {"value": value, "unit": "s", "cores": 1, "kind": "port", "sample": desc},
+                   "solver": "CpuSolver restatement (float particle state, double solve), block-Jacobi PCG",
+                   "step": "1/K of one whole CPU drape's frames (the K steps together are the drape, timed whole); "
+                           "warm-up: W frames of a separate solver"},
+        "cpu_baseline": {"value": value, "unit": "s", "cores": r["threads"], "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "frames_to_settle": int(fx["frames"]),
-        "pcg_iters_per_newton": {"mean": fx["cg_iterations"] / max(1, fx["newton_iterations"]), "cap": 50},
+        "frames_to_settle": r["frames"], "settled": r["settled"],
+        "step_s": [round(t, 3) for t in r["step_s"]],
+        "pcg_iters_per_newton": {"mean": r["cg_iterations"] / max(1, r["newton_iterations"]), "cap": 50},
+        "line_search_halvings": r["line_search_halvings"],
     }
     print(json.dumps(line))
     return 0
 
 
-def learned_leg(CU, device, scene, gid, init, flush, args, jacobi_value, jacobi_final, max_over_ranks):
-    """The same drape with the learned preconditioner (shipped trained weights, the network run on every Newton
-    iteration, PCG cap and tolerance unchanged), on the same GPU, from the same initial state, L2 flushed the same
-    way. Reports its settle time beside block-Jacobi's, its PCG iterations per Newton iteration, and how far its
-    settled shape lies from the block-Jacobi drape's."""
+def precond_leg(CU, device, args, flush, max_over_ranks, cap: int = 1000, tol: float = 1e-2, seeds: int = 2):
+    """Block-Jacobi against the learned preconditioner on the same GPU and the same 60k tube drapes, with the PCG
+    stopped by its tolerance (the reference's 1e-2) under a cap of `cap` iterations that the solves are not meant to
+    reach, so that PCG iterations per Newton step measure convergence, not the cap (the reference's own cap of 50
+    binds on almost every 60k solve). Each preconditioner drapes the first `seeds` start states of the timed steps
+    to rest after one warm-up drape, L2 flushed between drapes. The learned drape uses the shipped trained weights
+    (drape_b200/weights/tube.npy) with the network run every `refresh` Newton iterations; block-Jacobi stays its
+    fallback. Reports per preconditioner: mean settle seconds, frames, ms per frame, PCG iterations per Newton step
+    (mean, p50, p95, max), whether any solve reached the cap, and the settled shape's distance from block-Jacobi's."""
     import torch
     from drape_b200 import learned as LR
-    p = LR.LearnedPreconditioner(device, LR.load_weights("tube"))
-    s = CU.CudaSolver(device)
-    s.set_precond(p)
-    s.build(scene)
-    s.restore(init)
-    stream = torch.cuda.ExternalStream(s.stream_handle())
+    from drape_b200 import scenes as S
+    from drape_b200.scene import Settings
+    scene = S.tube_60k(settings=Settings(max_cg_iterations=cap, cg_tolerance=tol))
+    gid = scene.garments[0].id
+    out, finals = {}, {}
+    for name in ("jacobi", "learned"):
+        s = CU.CudaSolver(device)
+        net = None
+        if name == "learned":
+            net = LR.LearnedPreconditioner(device, LR.load_weights("tube"))
+            s.set_precond(net)
+            s.set_precond_schedule(refresh_every=args.refresh_every)
+        else:
+            s.set_pcg_variant(args.pcg_variant)
+        s.build(scene)
+        init = s.snapshot()
+        base32 = np.ascontiguousarray(init["positions"], np.float32)
+        stream = torch.cuda.ExternalStream(s.stream_handle())
 
-    def drape():
-        s.restore(init)
-        with torch.cuda.stream(stream):
-            flush.fill_(1.0)
-        torch.cuda.synchronize()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        res = s.drape_to_rest([gid])
-        b.record(stream)
-        b.synchronize()
-        return a.elapsed_time(b) / 1000.0, res
+        def drape(seed):
+            snap = dict(init)
+            snap["positions"] = seeded_positions(base32, seed)
+            s.restore(snap)
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            r = s.drape_to_rest([gid])
+            e1.record(stream)
+            e1.synchronize()
+            return e0.elapsed_time(e1) / 1000.0, r
 
-    drape()  # warm-up
-    s.reset_counters()
-    s.profile(True, solve_only=True)  # timed like the block-Jacobi drapes
-    times, results = [], []
-    for _ in range(max(1, min(args.steps, 2))):
-        t, r = drape()
-        times.append(t)
-        results.append(r)
-    s.profile(False)
-    c = s.counters()
-    hist = s.cg_history()
-    d = np.linalg.norm(s.positions().astype(np.float64) - jacobi_final, axis=1)
-    # Kernel shares: 120 frames from the initial state with every kernel (the network included) timed.
-    s.restore(init)
-    s.profile(True)
-    for _ in range(120):
-        s.step(1.0 / 60.0, 1, 2)
-    prof = s.profile_read()
-    s.profile(False)
-    value = max_over_ranks(statistics.mean(times))
-    total_ms = sum(prof["milliseconds"].values())
-    out = {
-        "precond": "learned (trained weights drape_b200/weights/tube.npy), network run every Newton iteration",
-        "settle_s": value, "jacobi_settle_s": jacobi_value,
-        "speedup_vs_jacobi": jacobi_value / value if value else None,
-        "frames": int(results[-1].frames_run), "settled": bool(results[-1].settled),
-        "ms_per_frame": 1000.0 * statistics.mean(t / max(1, r.frames_run) for t, r in zip(times, results)),
-        "pcg_iters_per_newton": {"mean": float(np.mean(hist)) if len(hist) else None,
-                                 "p50": float(np.percentile(hist, 50)) if len(hist) else None,
-                                 "p95": float(np.percentile(hist, 95)) if len(hist) else None},
-        "learned_solves": int(c.learned_solves), "jacobi_fallbacks": int(c.precond_fallbacks),
-        "kernel_share": {k: (v / total_ms if total_ms else 0.0) for k, v in prof["milliseconds"].items()},
-        "kernel_share_sample": "120 frames from the initial state, every kernel timed",
-        "settled_shape_vs_jacobi_m": {"max": float(d.max()), "rms": float(np.sqrt(np.mean(d * d)))},
-    }
-    s.close()
-    p.close()
+        drape(0)  # warm-up
+        s.reset_counters()
+        times, res = [], []
+        for k in range(seeds):
+            t, r = drape(k)
+            times.append(t)
+            res.append(r)
+        c = s.counters()
+        hist = np.asarray(s.cg_history(), np.int64)
+        finals[name] = s.positions().astype(np.float64)  # the last timed drape's settled shape
+        value = max_over_ranks(statistics.mean(times))
+        out[name] = {"settle_s": value, "settle_s_per_drape": [round(t, 4) for t in times],
+                     "frames": [int(r.frames_run) for r in res], "settled": [bool(r.settled) for r in res],
+                     "ms_per_frame": 1000.0 * sum(times) / max(1, sum(r.frames_run for r in res)),
+                     "pcg_iters_per_newton": {"mean": float(hist.mean()) if len(hist) else None,
+                                              "p50": float(np.percentile(hist, 50)) if len(hist) else None,
+                                              "p95": float(np.percentile(hist, 95)) if len(hist) else None,
+                                              "max": int(hist.max()) if len(hist) else None},
+                     "cap_reached": bool(len(hist) and int(hist.max()) >= cap),
+                     "newton_iterations": int(c.newton_iterations),
+                     "us_per_pcg_iteration": c.pcg_nanoseconds / 1000.0 / max(1, c.cg_iterations)}
+        if name == "learned":
+            out[name].update({"learned_solves": int(c.learned_solves), "jacobi_fallbacks": int(c.precond_fallbacks),
+                              "network_every_newton_iterations": args.refresh_every})
+        else:
+            out[name]["pcg"] = "pipelined" if args.pcg_variant == 1 else "reference order"
+        s.close()
+        if net is not None:
+            net.close()
+    d = np.linalg.norm(finals["learned"] - finals["jacobi"], axis=1)
+    jm, lm = out["jacobi"]["pcg_iters_per_newton"]["mean"], out["learned"]["pcg_iters_per_newton"]["mean"]
+    out.update({
+        "workload": f"60k seamed tube drape to rest, PCG tolerance {tol} with a cap of {cap}, {seeds} start states",
+        "speedup_vs_jacobi": out["jacobi"]["settle_s"] / out["learned"]["settle_s"] if out["learned"]["settle_s"]
+        else None,
+        "pcg_iteration_ratio": (jm / lm) if (jm and lm) else None,
+        "settled_shape_learned_vs_jacobi_mm": {"max": 1e3 * float(d.max()), "rms": 1e3 * float(np.sqrt(np.mean(d * d)))},
+    })
+    return out
+
+
+DEVIATION_FIXTURE = os.path.join(ROOT, "tests", "golden", "deviation.npz")
+
+
+def _seam_gap_penetration(scene, x: np.ndarray):
+    """Largest seam-pair distance and largest depth below the body's surface (m) of positions x, as SimModel::stats
+    reports them (sim_model.cpp:222-241), from the scene's own seam pairs and sampled field."""
+    x = np.asarray(x, np.float64)
+    gap, off = 0.0, 0
+    for g in scene.garments:
+        if g.seam_pairs is not None and len(g.seam_pairs):
+            sp = np.asarray(g.seam_pairs, np.int64)
+            gap = max(gap, float(np.linalg.norm(x[off + sp[:, 0]] - x[off + sp[:, 1]], axis=1).max()))
+        off += g.vertex_count
+    pen = float(np.max(-scene.body.sample(x))) if scene.body is not None else 0.0
+    return gap, pen
+
+
+def deviation_leg(CU, device, jacobi_final=None, variant=0):
+    """Deviation of the CUDA path from the oracle on the workloads' configurations, next to the oracle's own
+    self-spread (its faithful run against a faithful run from a start moved by a seeded uniform +-1 um per coordinate:
+    what a 1 mm bar can mean on that scene, libs/sim/tests/test_gpu_parity.cpp:12-20). The oracle's end states come
+    from tests/golden/deviation.npz (made by tests/golden/make_deviation.py); the CUDA path runs the same frames here.
+      c1       sheet on sphere, 120 frames, PCG tolerance 1e-6 (cap 3000)
+      c2       10k tube from its start, 300 frames (Assembling for the oracle drape's assembly frames, then Settling)
+      c3       60k tube, 60 frames continued from the faithful oracle's settled state (the reference's
+               continue-from-settled parity case)
+      c3drape  60k tube: the settled shape of the CUDA drape (the workload's own start state) against the oracle's
+               settled shapes
+    Each entry: max and RMS vertex distance to the faithful oracle (float state, double solve: the reference
+    CpuSolver) and to the full-FP64 oracle, the seam gap and body penetration of each result, the self-spread."""
+    from drape_b200 import scenes as S
+    try:
+        F = np.load(DEVIATION_FIXTURE)
+    except OSError as e:
+        return {"unavailable": f"no oracle fixture: {e}"}
+
+    def dist(a, b):
+        d = np.linalg.norm(np.asarray(a, np.float64) - np.asarray(b, np.float64), axis=1)
+        return {"max_mm": 1e3 * float(d.max()), "rms_mm": 1e3 * float(np.sqrt(np.mean(d * d)))}
+
+    def entry(name, scene, x, desc):
+        fa, f64 = F[f"{name}_faithful"], F[f"{name}_fp64"]
+        gap, pen = _seam_gap_penetration(scene, x)
+        ogap, open_ = _seam_gap_penetration(scene, fa)
+        gap64, pen64 = _seam_gap_penetration(scene, f64)
+        return {"config": desc, "particles": int(len(x)),
+                "vs_oracle_faithful": dist(x, fa), "vs_oracle_fp64": dist(x, f64),
+                "oracle_self_spread": {"max_mm": 1e3 * float(F[f"{name}_spread_max"]),
+                                       "rms_mm": 1e3 * float(F[f"{name}_spread_rms"])},
+                "oracle_faithful_vs_fp64": {"max_mm": 1e3 * float(F[f"{name}_faithful_vs_fp64_max"]),
+                                            "rms_mm": 1e3 * float(F[f"{name}_faithful_vs_fp64_rms"])},
+                "seam_gap_mm": {"cuda": 1e3 * gap, "oracle_faithful": 1e3 * ogap, "oracle_fp64": 1e3 * gap64},
+                "penetration_mm": {"cuda": 1e3 * pen, "oracle_faithful": 1e3 * open_, "oracle_fp64": 1e3 * pen64}}
+
+    def run(scene, frames, start=None, settle_after=None):
+        s = CU.CudaSolver(device)
+        s.set_pcg_variant(variant)
+        s.build(scene)
+        if start is not None:
+            s.restore(start)
+        gids = [g.id for g in scene.garments]
+        for f in range(frames):
+            if settle_after is not None and f == 0:
+                for g in gids:
+                    s.set_phase(g, 0)  # Assembling
+            if settle_after is not None and f == settle_after:
+                for g in gids:
+                    s.set_phase(g, 1)  # Settling
+            s.step(1.0 / 60.0, 1, 2)
+        x = s.positions().astype(np.float64)
+        s.close()
+        return x
+
+    out = {}
+    sc = S.sheet_on_sphere(cg_tolerance=1e-6, max_cg=3000)
+    out["c1"] = entry("c1", sc, run(sc, 120), "sheet 40x40 dropped on the sphere, 120 frames, PCG tol 1e-6 cap 3000")
+    sc = S.tube_10k()
+    asm = int(F["c2_assembly_frames"])
+    out["c2"] = entry("c2", sc, run(sc, 300, settle_after=asm),
+                      f"10k seamed tube from its start, 300 frames (Assembling {asm} frames, then Settling)")
+    sc = S.tube_60k()
+    start = {k: F[f"c3_start_{k}"] for k in ("positions", "velocities", "phases", "assembly_time", "seam_start_gap",
+                                              "contact_force")}
+    out["c3"] = entry("c3", sc, run(sc, 60, start=start),
+                      f"60k seamed tube, 60 frames continued from the faithful oracle's settled state "
+                      f"({int(F['c3_start_frames'])} oracle frames to settle)")
+    if jacobi_final is not None:
+        out["c3drape"] = entry("c3drape", sc, jacobi_final,
+                               "60k seamed tube: settled shape of the CUDA drape (block-Jacobi, the workload's own "
+                               f"start) vs the oracle's settled shapes (faithful {int(F['c3drape_frames_faithful'])}, "
+                               f"FP64 {int(F['c3drape_frames_fp64'])} frames)")
+    out["bar_mm"] = 1.0
+    out["pcg"] = "pipelined" if variant == 1 else "reference order"
     return out
 
 
@@ -479,23 +631,31 @@ def run_profile_case(args):
 
 
 def cpu_baseline(workload: str):
-    try:
-        value, desc, _ = reference_settle_seconds(workload, 1)
-    except (OSError, KeyError) as e:
-        return {"value": None, "unit": "s", "cores": 1, "kind": "port", "sample": f"no settle fixture: {e}"}
-    return {"value": value, "unit": "s", "cores": 1, "kind": "port", "sample": desc}
+    """The reference CPU path on this host's cores (reference_drape): one whole drape of the workload's own start
+    state to rest, timed whole."""
+    r = reference_drape(workload, 1, 0)
+    sample = (f"one whole drape of the workload's own start state to rest ({r['frames']} frames, settled "
+              f"{r['settled']}) on {r['threads']} host threads ({r['cpu']}, {r['host_cpus']} logical CPUs), "
+              f"timed whole")
+    return {"value": r["seconds"], "unit": "s", "cores": r["threads"], "kind": "port", "sample": sample,
+            "frames": r["frames"], "pcg_iters_per_newton": r["cg_iterations"] / max(1, r["newton_iterations"])}
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=16)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="tube60k")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=1, help="end-to-end steps (0: same as --steps)")
+    ap.add_argument("--e2e-steps", type=int, default=0, help="end-to-end steps (0: same as --steps)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner leg")
+    ap.add_argument("--refresh-every", type=int, default=1,
+                    help="learned leg: run the network every this many Newton iterations")
+    ap.add_argument("--no-deviation", action="store_true", help="skip the deviation-from-the-oracle leg")
+    ap.add_argument("--pcg-variant", type=int, choices=[0, 1], default=0,
+                    help="block-Jacobi PCG form: 0 the reference's order, 1 pipelined (one grid exchange an iteration)")
     ap.add_argument("--batch-garments", type=int, default=64, help="garments of the batched leg (0: skip it)")
     ap.add_argument("--profile-case", choices=["spmv", "batch", "bake", "drape"], default=None,
                     help="run one small case for a profiler capture instead of the benchmark")
@@ -534,6 +694,7 @@ def main():
     scene = make_scene(args.workload)
     gid = scene.garments[0].id
     solver = CU.CudaSolver(local)
+    solver.set_pcg_variant(args.pcg_variant)
     solver.build(scene)
     st = solver.structure()
     sizes = dict(n=len(st["diag_slot"]), B=len(st["col_index"]), S=len(st["stretch_v"]), H=len(st["hinge_v"]),
@@ -569,12 +730,17 @@ def main():
     barrier()
     torch.cuda.synchronize()
     sampler = ClockSampler(gpu_id, args.clock_period_ms)
-    times, results = [], []
-    for _ in range(args.steps):
-        for seed in range(SEEDS):
-            t, res = one_drape(seed)
-            times.append(t)
-            results.append(res)
+    times, results, per_drape = [], [], []
+    last = solver.counters()
+    for k in range(args.steps):
+        t, res = one_drape(k % SEEDS)
+        times.append(t)
+        results.append(res)
+        c = solver.counters()  # host read after the drape's end event, outside the timed events
+        per_drape.append({"newton": c.newton_iterations - last.newton_iterations,
+                          "cg": c.cg_iterations - last.cg_iterations,
+                          "halvings": c.line_search_halvings - last.line_search_halvings})
+        last = c
     barrier()
     torch.cuda.synchronize()
     clocks = sampler.stop()
@@ -611,10 +777,29 @@ def main():
     launches_timed = sum(share_prof["launches"].values()) / max(1, share_res.frames_run) * \
         sum(r.frames_run for r in results)
     total_ms = sum(share_prof["milliseconds"].values())
+    # The bound that k_solve actually meets: its matrix (36 B a block slot) lives in shared memory and L2, so its time
+    # per PCG iteration is set by the grid-wide exchanges. The PCG loop's own device time (%globaltimer, block 0) per
+    # iteration is set beside the measured floor of the same exchanges on the same grid with no other work.
+    pcg_us = counters.pcg_nanoseconds / 1000.0 / max(1, counters.cg_iterations)
+    floor_mode = 2 if args.pcg_variant == 1 else 0
+    floor_us = statistics.median(CU.reduction_floor(local, floor_mode, 4000) for _ in range(3))
+    latency = {"kernel": "k_solve PCG loop", "us_per_pcg_iteration": pcg_us, "floor_us": floor_us,
+               "floor": ("one three-value FP64 grid reduction per iteration (pipelined PCG)" if floor_mode == 2 else
+                         "two FP64 grid reductions per iteration (reference-order PCG)"),
+               "frac_of_floor": floor_us / pcg_us if pcg_us else None,
+               "onchip_bytes_per_iteration": ab["pcg_iter"],
+               "onchip_gbs": ab["pcg_iter"] / (pcg_us * 1e-6) / 1e9 if pcg_us else None,
+               "note": "floor = drape_cuda_reduction_floor on the solve's grid (one 1024-thread block per SM), "
+                       "median of 3 x 4000 rounds; us_per_pcg_iteration = in-kernel PCG time / PCG iterations over "
+                       "the timed drapes (CG init amortised); onchip_gbs = the iteration's algorithmic bytes over its "
+                       "time, served from shared memory and L2"}
     roofline = {"bound": "hbm", "kernel": "k_solve", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak if peak else None, "peak_source": peak_kind,
                 "traffic": traffic, "algorithmic_bytes_per_launch": solve_bytes / solve_launches,
                 "avg_launch_ms": solve_ms / solve_launches,
+                "bound_note": "HBM is not what limits k_solve: its DRAM traffic is a small part of its algorithmic "
+                              "bytes (the matrix sits in shared memory and L2); the limit is grid-exchange latency, "
+                              "see the line's k_solve_latency object",
                 "kernel_share": {k: (v / total_ms if total_ms else 0.0) for k, v in share_prof["milliseconds"].items()},
                 "kernel_share_sample": "one extra drape of the workload's own start state, every kernel timed"}
 
@@ -624,26 +809,25 @@ def main():
     e2e_times, e2e_build, h2d, d2h, e2e_frames = [], [], [], [], []
     garment = scene.garments[0]
     own = garment.initial_positions
-    for _ in range(e2e_steps):
-        for seed in range(SEEDS):
-            garment.initial_positions = seed_positions[seed].astype(np.float64)
-            torch.cuda.synchronize()
-            b0 = solver.transfer_bytes()
-            t0 = time.perf_counter()
-            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            start.record(stream)
-            solver.build(scene)
-            e2e_build.append(time.perf_counter() - t0)
-            e2e_frames.append(int(solver.drape_to_rest([gid]).frames_run))
-            out = np.empty((sizes["n"], 3), np.float32)
-            solver.read_positions(out)
-            end.record(stream)
-            end.synchronize()
-            wall = time.perf_counter() - t0
-            e2e_times.append(max(wall, start.elapsed_time(end) / 1000.0))
-            b1 = solver.transfer_bytes()
-            h2d.append(b1[0] - b0[0])
-            d2h.append(b1[1] - b0[1])
+    for k in range(e2e_steps):
+        garment.initial_positions = seed_positions[k % SEEDS].astype(np.float64)
+        torch.cuda.synchronize()
+        b0 = solver.transfer_bytes()
+        t0 = time.perf_counter()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        solver.build(scene)
+        e2e_build.append(time.perf_counter() - t0)
+        e2e_frames.append(int(solver.drape_to_rest([gid]).frames_run))
+        out = np.empty((sizes["n"], 3), np.float32)
+        solver.read_positions(out)
+        end.record(stream)
+        end.synchronize()
+        wall = time.perf_counter() - t0
+        e2e_times.append(max(wall, start.elapsed_time(end) / 1000.0))
+        b1 = solver.transfer_bytes()
+        h2d.append(b1[0] - b0[0])
+        d2h.append(b1[1] - b0[1])
     garment.initial_positions = own
     e2e_value = max_over_ranks(statistics.mean(e2e_times))
     solver.restore(init)
@@ -654,23 +838,30 @@ def main():
         "ms_per_step": value * 1000.0, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64", "data": "synthetic",
         "config": {"workload": WORKLOADS[args.workload]["desc"], "precond": "block-Jacobi",
+                   "pcg": ("pipelined (one grid exchange per iteration)" if args.pcg_variant == 1 else
+                           "reference order (two grid exchanges per iteration)"),
                    "start_states": SEED_DESC,
                    "precision": "FP32 blocks/SpMV/vectors, FP64 dots, FP64 energy/slope/line search",
                    "l2": "256 MB buffer written between timed drapes (L2 flushed)",
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e_value, "unit": "s", "h2d_bytes_per_step": int(sum(h2d) / e2e_steps),
                 "d2h_bytes_per_step": int(sum(d2h) / e2e_steps), "drapes": len(e2e_times),
-                "frames_per_seed": e2e_frames[-SEEDS:], "frames_mean": float(np.mean(e2e_frames)),
-                "s_per_seed": [round(t, 4) for t in e2e_times[-SEEDS:]],
-                "build_s_per_seed": [round(t, 4) for t in e2e_build[-SEEDS:]],
-                "note": "mean seconds per drape; bytes per step of 16 drapes"},
+                "frames_per_step": e2e_frames, "frames_mean": float(np.mean(e2e_frames)),
+                "s_per_step": [round(t, 4) for t in e2e_times],
+                "build_s_per_step": [round(t, 4) for t in e2e_build],
+                "note": "mean seconds per drape (one drape per step, the same start states as the timed steps); "
+                        "bytes per step"},
         "roofline": roofline,
+        "k_solve_latency": latency,
         "clocks": clocks,
         "gpu_launches": int(launches_timed),
         "drape": {"drapes_timed": drapes,
-                  "frames_per_seed": [int(r.frames_run) for r in results[-SEEDS:]],
-                  "settled_per_seed": [bool(r.settled) for r in results[-SEEDS:]],
-                  "settle_s_per_seed": [float(t) for t in times[-SEEDS:]],
+                  "frames_per_step": [int(r.frames_run) for r in results],
+                  "settled_per_step": [bool(r.settled) for r in results],
+                  "settle_s_per_step": [round(float(t), 4) for t in times],
+                  "ms_per_frame_per_step": [round(1000.0 * t / max(1, r.frames_run), 3)
+                                            for t, r in zip(times, results)],
+                  "work_per_step": per_drape,
                   "settle_s_median": float(np.median(times)),
                   "frames_mean": float(np.mean([r.frames_run for r in results])),
                   "assembly_seconds": float(results[-1].assembly_seconds),
@@ -684,9 +875,12 @@ def main():
                                  "cap": 50},
         "sizes": sizes,
     }
+    jac_final = solver.positions().astype(np.float64)
+    if rank == 0 and not args.no_deviation:
+        line["deviation"] = deviation_leg(CU, local, jac_final if args.workload == "tube60k" else None,
+                                          args.pcg_variant)
     if not args.no_learned:
-        jac_final = solver.positions().astype(np.float64)
-        line["precond"] = learned_leg(CU, local, scene, gid, init, flush, args, value, jac_final, max_over_ranks)
+        line["precond"] = precond_leg(CU, local, args, flush, max_over_ranks)
     peak, _ = measured_peaks()
     solver.restore(init)
     line["spmv"] = spmv_leg(CU, solver, peak)

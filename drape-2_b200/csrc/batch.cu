@@ -1301,7 +1301,7 @@ struct drape_batch {
     BCK(cudaStreamSynchronize(stream));
     for (auto& x : c) {
       x.substeps = x.newtonIterations = x.cgIterations = x.lineSearchHalvings = x.energyEvaluations = 0;
-      x.learnedSolves = x.precondFallbacks = 0;
+      x.learnedSolves = x.precondFallbacks = x.pcgNs = 0;
     }
     BCK(cudaMemcpyAsync(ctl.p, c.data(), sizeof(dcu::Control) * G, cudaMemcpyHostToDevice, stream));
     BCK(cudaStreamSynchronize(stream));
@@ -1319,6 +1319,7 @@ struct drape_batch {
     out.line_search_halvings = c.lineSearchHalvings;
     out.precond_fallbacks = c.precondFallbacks;
     out.learned_solves = c.learnedSolves;
+    out.pcg_nanoseconds = c.pcgNs;
     return out;
   }
 

@@ -81,6 +81,7 @@ struct Control {
   int lastCg;
   int pad;
   long long learnedSolves, precondFallbacks;  // PCG solves with the learned preconditioner; of those, restarted
+  long long pcgNs;  // %globaltimer nanoseconds inside the PCG solves (block 0's view: CG init to the last iteration)
 };
 
 constexpr unsigned int kCgLogCapacity = 1u << 16;  // PCG iterations per Newton iteration, ring buffer
@@ -95,6 +96,8 @@ struct Params {
   uint32_t n, nStretch, nHinge, nSeam, nBlocks, nGarments, slotsPadded;
   uint32_t smemSlots;   // k_solve: block slots a block keeps in shared memory
   int learnedSwitch;    // k_solve<true>: block-Jacobi iterations before the learned preconditioner takes over
+  int pcgVariant;       // the solve kernel chosen for block-Jacobi: 0 reference order, 1 pipelined (kept in the view
+                        // so that captured frame graphs are recaptured when it changes)
   unsigned long long barrierLimitNs;
 };
 
@@ -118,6 +121,7 @@ struct Dev {
   const uint32_t* offStart;  // per off-diagonal slot: its contributions [offStart[k], offStart[k + 1]) of offContrib
   const uint32_t* offContrib;  // incidence entry << 2 | block of the entry's term, in gather order
   float4 *x, *v, *xStart, *yRel, *u, *grad, *step, *r, *z, *p0, *p1, *ap, *apFull, *resid;
+  float4 *pm0, *pm1, *pz;  // pipelined PCG only: the two m = M w buffers and z = A q (null where not allocated)
   float4* stretchDer;      // per stretch term: its StretchDer record (6 float4), written by termsRows
   float4* hingeDer;        // per hinge term: its HingeDer record (4 float4)
   const float* Lf;         // learned factor L: 9 planes of slotsPadded floats on lower slots (k_solve<true>)
@@ -911,6 +915,106 @@ __device__ inline int pcgReferenceOrder(const Dev& D, GridSync& gs, const SmemMa
   return it;
 }
 
+// Pipelined contact-filtered block-Jacobi PCG (Ghysels and Vanroose, "Hiding global synchronization latency in the
+// preconditioned conjugate gradient algorithm", Parallel Computing 40 (2014) 224-238, Alg. 3). In exact arithmetic
+// its iterates, iteration count and stopping tests are those of pcgReferenceOrder (operator F A F, preconditioner
+// F M F, the same |r| <= tol |r0| and p.Ap <= 0 tests): besides u = M r and w = A u it carries s = A p, q = M s and
+// z = A q by recurrence, so each iteration is one pass over the rows and ONE grid exchange instead of two. The pass
+// forms n = F A m for the m = F M w of the previous exchange (the only gather), updates the row's z, q, s, p, x, r,
+// u, w and forms the next exchange's FP64 partials (r.u, w.u, r.r) and the next m; the exchange (gridReduce<3>)
+// publishes partials and m together. m alternates between two buffers: a block cannot pass the next exchange before
+// every block has arrived at it, hence before any block still gathers the m it would overwrite. The unfiltered
+// residual for the contact force, resid = -grad - A step, is formed once after the loop. Vectors: x = step, r = r,
+// u = z, w = ap, s = apFull, p = p0, q = p1, z = pz, m = pm0 / pm1. Returns the iteration count, or -1 when a grid
+// barrier gave up.
+template <int PL>
+__device__ inline int pcgPipelined(const Dev& D, GridSync& gs, const SmemMatrix& A) {
+  uint32_t r0i, r1i;
+  blockRange(D.P.n, gs.rank, gs.size, r0i, r1i);
+  float4 *x = D.step, *r = D.r, *u = D.z, *w = D.ap, *s = D.apFull, *p = D.p0, *q = D.p1, *zq = D.pz;
+  float4* const mBuf[2] = {D.pm0, D.pm1};
+  // x = 0, r = F(-grad), u = F(M r); u is gathered next, so a plain barrier publishes it.
+  for (uint32_t i = r0i + threadIdx.x; i < r1i; i += blockDim.x) {
+    const Contact c = D.contact[i];
+    const float3 ri = filterContact(c, -ld3(D.grad, i));
+    x[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    r[i] = f4(ri);
+    u[i] = f4(filterContact(c, mul(loadPrecond(D, i), ri)));
+  }
+  if (!gs.sync()) return -1;
+  // w = F A u, the first partials and m.
+  double t[3];
+  {
+    double v[3] = {0.0, 0.0, 0.0};
+    directionProducts<PL>(
+        D, A, r0i, r1i, [&](uint32_t j) { return ld3(u, j); },
+        [&](uint32_t i, float3 ui, float3 au) {
+          const Contact c = D.contact[i];
+          const float3 wi = filterContact(c, au);
+          const float3 ri = ld3(r, i);
+          w[i] = f4(wi);
+          v[0] += dotd3(ri, ui);
+          v[1] += dotd3(wi, ui);
+          v[2] += dotd3(ri, ri);
+          mBuf[0][i] = f4(filterContact(c, mul(loadPrecond(D, i), wi)));
+        });
+    if (!gridReduce<3>(D, gs, v, t)) return -1;
+  }
+  const double r0 = sqrt(t[2]);
+  double gammaPrev = 0.0, alphaPrev = 0.0;
+  int it = 0;
+  while (it < D.P.maxCg) {
+    if (!(r0 > 0.0)) break;
+    if (it > 0 && sqrt(t[2]) <= D.P.cgTolerance * r0) break;
+    const double gamma = t[0], delta = t[1];
+    const double beta = it == 0 ? 0.0 : gamma / gammaPrev;
+    const double pAp = it == 0 ? delta : delta - beta * gamma / alphaPrev;
+    if (!(pAp > 0.0)) break;
+    const double alpha = gamma / pAp;
+    const float fa = static_cast<float>(alpha), fb = static_cast<float>(beta);
+    const bool first = it == 0;
+    const float4* mCur = mBuf[it & 1];
+    float4* mNext = mBuf[(it + 1) & 1];
+    double v[3] = {0.0, 0.0, 0.0};
+    directionProducts<PL>(
+        D, A, r0i, r1i, [&](uint32_t j) { return ld3(mCur, j); },
+        [&](uint32_t i, float3 mi, float3 am) {
+          const Contact c = D.contact[i];
+          const float3 ni = filterContact(c, am);
+          const float3 ui0 = ld3(u, i), wi0 = ld3(w, i);
+          const float3 zi = first ? ni : ni + ld3(zq, i) * fb;
+          const float3 qi = first ? mi : mi + ld3(q, i) * fb;
+          const float3 si = first ? wi0 : wi0 + ld3(s, i) * fb;
+          const float3 pi = first ? ui0 : ui0 + ld3(p, i) * fb;
+          const float3 ri = ld3(r, i) - si * fa;
+          const float3 ui = ui0 - qi * fa;
+          const float3 wi = wi0 - zi * fa;
+          x[i] = f4(ld3(x, i) + pi * fa);
+          zq[i] = f4(zi);
+          q[i] = f4(qi);
+          s[i] = f4(si);
+          p[i] = f4(pi);
+          r[i] = f4(ri);
+          u[i] = f4(ui);
+          w[i] = f4(wi);
+          v[0] += dotd3(ri, ui);
+          v[1] += dotd3(wi, ui);
+          v[2] += dotd3(ri, ri);
+          mNext[i] = f4(filterContact(c, mul(loadPrecond(D, i), wi)));
+        });
+    ++it;
+    gammaPrev = gamma;
+    alphaPrev = alpha;
+    if (!gridReduce<3>(D, gs, v, t)) return -1;
+  }
+  // resid = -grad - A step over unpinned rows and columns (the reference-order PCG's recurrence, formed directly). Every
+  // exit of the loop follows a grid exchange, whose barrier has published every block's last x.
+  directionProducts<PL>(
+      D, A, r0i, r1i, [&](uint32_t j) { return ld3(x, j); },
+      [&](uint32_t i, float3, float3 ax) { D.resid[i] = f4(-ld3(D.grad, i) - ax); });
+  return it;
+}
+
 // z = F(L L^T r) over this block's rows, with L the learned factor (planes D.Lf, lower slots) and y = L^T r kept in
 // D.ap between the two products; returns false when a grid barrier gave up. Adds r.z of its rows to *rz.
 template <int RL>
@@ -1058,12 +1162,31 @@ __device__ inline int pcgLearned(const Dev& D, GridSync& gs, const SmemMatrix& A
 // first (0: none), then, when the solve has not converged, the learned preconditioner from the current iterate within
 // the remaining iteration budget; a learned phase that stalls is followed by a full block-Jacobi solve. Returns the
 // total iteration count of all phases, or -1 when a barrier gave up.
-template <bool Learned, int PL>
+// Variant (block-Jacobi only): 0 the reference's order (pcgReferenceOrder), 1 pipelined (pcgPipelined; needs the
+// pm0/pm1/pz vectors). A compile-time choice, so each solve kernel carries one PCG's registers.
+template <bool Learned, int PL, int Variant>
+__device__ inline int pcgSolveStaged(const Dev& D, GridSync& gs, const SmemMatrix& A);
+
+template <bool Learned, int PL, int Variant = 0>
 __device__ inline int pcgSolve(const Dev& D, GridSync& gs) {
   uint32_t r0i, r1i;
   blockRange(D.P.n, gs.rank, gs.size, r0i, r1i);
   const SmemMatrix A = stageMatrix(D, r0i, r1i);
-  if (!Learned) return pcgReferenceOrder<PL>(D, gs, A);
+  const unsigned long long t0 = globalTimerNs();
+  const int it = pcgSolveStaged<Learned, PL, Variant>(D, gs, A);
+  if (gs.rank == 0 && threadIdx.x == 0) D.ctl->pcgNs += static_cast<long long>(globalTimerNs() - t0);
+  return it;
+}
+
+template <bool Learned, int PL, int Variant>
+__device__ inline int pcgSolveStaged(const Dev& D, GridSync& gs, const SmemMatrix& A) {
+  if constexpr (!Learned) {
+    if constexpr (Variant == 1) {
+      return pcgPipelined<PL>(D, gs, A);
+    } else {
+      return pcgReferenceOrder<PL>(D, gs, A);
+    }
+  }
   int first = 0;
   double r0 = 0.0;
   const int sw = D.P.learnedSwitch;
@@ -1083,13 +1206,13 @@ __device__ inline int pcgSolve(const Dev& D, GridSync& gs) {
 // One Newton iteration's solve for the blocks of one group (the whole grid for one solver, or a garment's blocks in
 // a batched launch); gs is initialised. PL: the scheme of the PCG's product A p (lanes per row, or 0 for
 // slot-parallel; see directionProducts), also the lanes of the learned factor's products when positive.
-template <bool Learned, int PL>
+template <bool Learned, int PL, int Variant = 0>
 __device__ inline void solveGroup(const Dev& D, GridSync& gs) {
   Control* ctl = D.ctl;
   const uint32_t n = D.P.n;
   uint32_t r0i, r1i;
   blockRange(n, gs.rank, gs.size, r0i, r1i);
-  const int it = pcgSolve<Learned, PL>(D, gs);
+  const int it = pcgSolve<Learned, PL, Variant>(D, gs);
   if (it < 0) return;
   if (gs.rank == 0 && threadIdx.x == 0) {
     if (D.cgLog) D.cgLog[static_cast<unsigned long long>(ctl->newtonIterations) % kCgLogCapacity] = it;

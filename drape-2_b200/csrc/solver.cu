@@ -69,6 +69,7 @@ struct drape_solver {
   bool learnedOn = false;
   int precondRefresh = 1;           // run the network on every precondRefresh-th Newton iteration
   int precondSwitch = 0;            // block-Jacobi iterations before the learned preconditioner takes over
+  int pcgVariant = 0;               // block-Jacobi PCG: 0 the reference's order, 1 pipelined (drape_cuda_set_pcg_variant)
   uint64_t netNewtonCounter = 0;
   size_t solveSmemBytes = 0;       // dynamic shared memory of the solve launch for the built scene
 
@@ -81,6 +82,7 @@ struct drape_solver {
   DBuf<uint32_t> rowStart, colIndex, diagSlot, incStart, incEntry, offSlot, offStart, offContrib;
   DBuf<float> fieldValues, blocks;
   DBuf<float4> x, v, xStart, yRel, u, grad, step, r, z, p0, p1, ap, apFull, resid, fExt, pinPos, precond;
+  DBuf<float4> pm0, pm1, pz;  // the pipelined PCG's extra vectors
   DBuf<float4> stretchDer, hingeDer;
   DBuf<dcu::Contact> contact;
   DBuf<double> partials, statsPartials;
@@ -154,8 +156,9 @@ struct drape_solver {
     numSMs = prop.multiProcessorCount;
     CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     // The solve kernels keep their rows' matrix blocks in shared memory: as many slots as the opt-in limit leaves.
-    const void* solveKernels[] = {reinterpret_cast<const void*>(dcu::k_solve<false>),
-                                  reinterpret_cast<const void*>(dcu::k_solve<true>),
+    const void* solveKernels[] = {reinterpret_cast<const void*>(dcu::k_solve<false, 0>),
+                                  reinterpret_cast<const void*>(dcu::k_solve<false, 1>),
+                                  reinterpret_cast<const void*>(dcu::k_solve<true, 0>),
                                   reinterpret_cast<const void*>(dcu::k_pcg_only)};
     size_t staticSmem = 0;
     for (const void* k : solveKernels) {
@@ -238,7 +241,8 @@ struct drape_solver {
       fieldValues.alloc(1);
     }
     blocks.alloc(static_cast<size_t>(SP) * 9);
-    for (DBuf<float4>* b : {&x, &v, &xStart, &yRel, &u, &grad, &step, &r, &z, &p0, &p1, &ap, &apFull, &resid, &fExt, &pinPos})
+    for (DBuf<float4>* b : {&x, &v, &xStart, &yRel, &u, &grad, &step, &r, &z, &p0, &p1, &ap, &apFull, &resid, &fExt, &pinPos,
+                            &pm0, &pm1, &pz})
       b->alloc(n);
     precond.alloc(static_cast<size_t>(n) * 3);
     stretchDer.alloc(std::max<size_t>(1, 6 * m.stretch.size()));
@@ -288,6 +292,10 @@ struct drape_solver {
     d.ap = ap.p;
     d.apFull = apFull.p;
     d.resid = resid.p;
+    d.pm0 = pm0.p;
+    d.pm1 = pm1.p;
+    d.pz = pz.p;
+    d.P.pcgVariant = pcgVariant;
     d.stretchDer = stretchDer.p;
     d.hingeDer = hingeDer.p;
     d.fExt = fExt.p;
@@ -414,8 +422,13 @@ struct drape_solver {
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    CK(learnedOn && netGraph ? cudaLaunchKernelEx(&cfg, dcu::k_solve<true>, d)
-                             : cudaLaunchKernelEx(&cfg, dcu::k_solve<false>, d));
+    if (learnedOn && netGraph) {
+      CK(cudaLaunchKernelEx(&cfg, dcu::k_solve<true, 0>, d));
+    } else if (d.P.pcgVariant == 1) {
+      CK(cudaLaunchKernelEx(&cfg, dcu::k_solve<false, 1>, d));
+    } else {
+      CK(cudaLaunchKernelEx(&cfg, dcu::k_solve<false, 0>, d));
+    }
   }
 
   // Frame graphs: one frame's launches (its substeps, then the statistics into slot f) captured once per slot and
@@ -640,6 +653,7 @@ struct drape_solver {
     c.line_search_halvings = hCtl.p->lineSearchHalvings;
     c.precond_fallbacks = hCtl.p->precondFallbacks;
     c.learned_solves = hCtl.p->learnedSolves;
+    c.pcg_nanoseconds = hCtl.p->pcgNs;
     return c;
   }
 
@@ -649,7 +663,7 @@ struct drape_solver {
     CK(cudaStreamSynchronize(stream));
     dcu::Control c = *hCtl.p;
     c.substeps = c.newtonIterations = c.cgIterations = c.lineSearchHalvings = c.energyEvaluations = 0;
-    c.learnedSolves = c.precondFallbacks = 0;
+    c.learnedSolves = c.precondFallbacks = c.pcgNs = 0;
     *hCtl.p = c;
     CK(cudaMemcpyAsync(ctl.p, hCtl.p, sizeof(dcu::Control), cudaMemcpyHostToDevice, stream));
     CK(cudaStreamSynchronize(stream));
@@ -971,7 +985,7 @@ int drape_cuda_is_available(void) {
     cudaDeviceProp prop{};
     if (cudaGetDeviceProperties(&prop, d) == cudaSuccess && prop.major == 10) {
       cudaFuncAttributes attr{};
-      if (cudaFuncGetAttributes(&attr, dcu::k_solve<false>) == cudaSuccess) return 1;
+      if (cudaFuncGetAttributes(&attr, dcu::k_solve<false, 0>) == cudaSuccess) return 1;
       cudaGetLastError();
     }
   }
@@ -1546,6 +1560,15 @@ int drape_cuda_set_precond_schedule(drape_solver* s, int refresh_every, int jaco
   });
 }
 
+int drape_cuda_set_pcg_variant(drape_solver* s, int variant) {
+  return guarded(s, [&] {
+    need(s);
+    if (variant != 0 && variant != 1) throw std::invalid_argument("PCG variant must be 0 (reference order) or 1 (pipelined)");
+    s->pcgVariant = variant;
+    s->dev.P.pcgVariant = variant;  // the frame graphs compare the device view and recapture
+  });
+}
+
 int drape_cuda_set_barrier_limit(drape_solver* s, uint64_t nanoseconds) {
   return guarded(s, [&] {
     need(s);
@@ -1566,6 +1589,38 @@ int drape_cuda_test_barrier_timeout(int device, int blocks, uint64_t nanoseconds
     CK(cudaGetLastError());
     CK(cudaDeviceSynchronize());
     CK(cudaMemcpy(status, out.p, sizeof(int), cudaMemcpyDeviceToHost));
+  });
+}
+
+int drape_cuda_reduction_floor(int device, int mode, int iterations, double* ns_per_iteration) {
+  return guarded(nullptr, [&] {
+    if (!ns_per_iteration || mode < 0 || mode > 3 || iterations < 1 || iterations > 1000000)
+      throw std::invalid_argument("bad argument");
+    CK(cudaSetDevice(device));
+    int sms = 0;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    DBuf<dcu::Control> c;
+    DBuf<double> partials;
+    DBuf<unsigned long long> out;
+    c.alloc(1);
+    partials.alloc(2 * static_cast<size_t>(sms) * dcu::kPartialStride);
+    out.alloc(1);
+    dcu::Dev d{};
+    d.ctl = c.p;
+    d.partials = partials.p;
+    d.P.barrierLimitNs = 2000000000ull;
+    unsigned long long* o = out.p;
+    void* args[] = {&d, &mode, &iterations, &o};
+    CK(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(dcu::k_reduction_floor), dim3(sms),
+                                   dim3(dcu::kSolveThreads), args, 0, nullptr));
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
+    unsigned long long ns = 0;
+    dcu::Control h{};
+    CK(cudaMemcpy(&ns, out.p, sizeof(ns), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&h, c.p, sizeof(h), cudaMemcpyDeviceToHost));
+    if (h.error || ns == 0) throw std::runtime_error("cuda: a grid barrier timed out");
+    *ns_per_iteration = static_cast<double>(ns) / iterations;
   });
 }
 
@@ -1614,17 +1669,26 @@ constexpr int kNoAllocMaxDevices = 64;
 NoAllocDevice g_noAlloc[kNoAllocMaxDevices];
 std::mutex g_noAllocMutex;
 
-// Once per device, with that device current: the device address of the scratch array and the SM count.
-NoAllocDevice& noAllocScratch(int device) {
+// The device address of the scratch array and the SM count, with `device` current. The SM count is looked up once per
+// device. The address is looked up again on every call made outside a stream capture (cudaGetSymbolAddress allocates
+// nothing), so a context that another framework re-created, or a cudaDeviceReset, leaves no stale address behind;
+// during a capture the address from the last uncaptured call is used.
+NoAllocDevice& noAllocScratch(int device, cudaStream_t stream) {
   if (device < 0 || device >= kNoAllocMaxDevices) throw std::runtime_error("cuda: device index out of range");
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(stream, &capture));
   std::lock_guard<std::mutex> lock(g_noAllocMutex);
   NoAllocDevice& d = g_noAlloc[device];
-  if (!d.ready) {
+  if (!d.ready || capture == cudaStreamCaptureStatusNone) {
+    if (!d.ready && capture != cudaStreamCaptureStatusNone)
+      throw std::runtime_error("cuda: the first no-allocation PCG call on a device must come before any capture");
     void* p = nullptr;
     CK(cudaGetSymbolAddress(&p, g_pcgScratch));
-    CK(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, device));
-    if (d.sms < 1 || static_cast<uint32_t>(d.sms) > kNoAllocMaxBlocks)
-      throw std::runtime_error("cuda: unsupported SM count for the no-allocation PCG");
+    if (!d.ready) {
+      CK(cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, device));
+      if (d.sms < 1 || static_cast<uint32_t>(d.sms) > kNoAllocMaxBlocks)
+        throw std::runtime_error("cuda: unsupported SM count for the no-allocation PCG");
+    }
     d.scratch = static_cast<unsigned char*>(p);
     d.ready = true;
   }
@@ -1635,18 +1699,27 @@ NoAllocDevice& noAllocScratch(int device) {
 
 namespace dcu {
 
+// Error code in Control::error for a caller's block-CSR structure that the no-allocation PCG refuses: row_start not
+// non-decreasing from 0 to `slots`, a column index >= n, or a row without its diagonal block.
+constexpr int kNoAllocBadStructure = 3;
+
+// Clears the control block and the iteration output before the structure check can raise an error in it.
+__global__ void k_noalloc_clear(Control* ctl, int* iterations) {
+  *ctl = Control{};
+  *iterations = 0;
+}
+
 // Converts the caller's flags into the solver's layouts inside the scratch (particle pinned flags, contact state,
-// columns with the pinned bit, diagonal slots) and clears the control block and the iteration output.
-__global__ void k_noalloc_prepare(uint32_t n, const uint32_t* __restrict__ rowStart,
+// columns with the pinned bit, diagonal slots) and checks the structure on the way. Every read and write stays in
+// bounds whatever the caller passed: slot indices are clamped to [0, slots) and column indices are checked against n
+// before they index `pinned`; a violation raises kNoAllocBadStructure and leaves in-range placeholders behind, which
+// the solve never reads because it does not start.
+__global__ void k_noalloc_prepare(uint32_t n, uint32_t slots, const uint32_t* __restrict__ rowStart,
                                   const uint32_t* __restrict__ colIndex, const uint8_t* __restrict__ pinned,
                                   const uint8_t* __restrict__ active, const float4* __restrict__ normals,
-                                  Particle* particle, Contact* contact, uint32_t* cols, uint32_t* diag, Control* ctl,
-                                  int* iterations) {
+                                  Particle* particle, Contact* contact, uint32_t* cols, uint32_t* diag, Control* ctl) {
   const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
-  if (tid == 0) {
-    *ctl = Control{};
-    *iterations = 0;
-  }
+  if (tid == 0 && (rowStart[0] != 0u || rowStart[n] != slots)) atomicExch(&ctl->error, kNoAllocBadStructure);
   for (uint32_t i = tid; i < n; i += stride) {
     particle[i] = Particle{1.0f, 0u, 0u, pinned[i] ? 1u : 0u};
     Contact c{};
@@ -1655,18 +1728,62 @@ __global__ void k_noalloc_prepare(uint32_t n, const uint32_t* __restrict__ rowSt
     if (normals) c.normal = make_float4(normals[i].x, normals[i].y, normals[i].z, 0.0f);
     contact[i] = c;
     const uint32_t rs = rowStart[i], re = rowStart[i + 1];
-    uint32_t d = re;
-    for (uint32_t s = rs; s < re; ++s) {
+    bool bad = rs > re || re > slots;
+    const uint32_t lo = min(rs, slots), hi = min(max(rs, re), slots);
+    uint32_t d = slots;
+    for (uint32_t s = lo; s < hi; ++s) {
       const uint32_t j = colIndex[s];
-      cols[s] = (j < n && pinned[j]) ? (j | kPinnedBit) : j;
+      if (j >= n) {
+        bad = true;
+        cols[s] = 0u;
+        continue;
+      }
+      cols[s] = pinned[j] ? (j | kPinnedBit) : j;
       if (j == i) d = s;
     }
+    if (d == slots) {
+      bad = true;
+      d = 0u;  // slots >= n >= 1 (checked on the host), so slot 0 exists
+    }
     diag[i] = d;
+    if (bad) atomicExch(&ctl->error, kNoAllocBadStructure);
   }
 }
 
+// k_pcg_precondition and k_pcg_only of the allocating entry point, skipped once the structure check has failed (every
+// block reads the same flag, written by an earlier kernel on the stream, so the cooperative launch returns as a whole).
+__global__ void k_noalloc_precondition(Dev D, const uint32_t* __restrict__ diag) {
+  if (*reinterpret_cast<volatile int*>(&D.ctl->error) != 0) return;
+  const uint32_t SP = D.P.slotsPadded;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < D.P.n; i += gridDim.x * blockDim.x) {
+    M3 A;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) A.m[k] = D.blocks[k * SP + diag[i]];
+    M3 inv;
+    if (D.particle[i].pinned != 0u) {
+      zero(inv);
+    } else {
+      bool ok = false;
+      inv = invertSpd(A, ok);
+    }
+    D.precond[3 * i + 0] = make_float4(inv.m[0], inv.m[1], inv.m[2], 0.0f);
+    D.precond[3 * i + 1] = make_float4(inv.m[3], inv.m[4], inv.m[5], 0.0f);
+    D.precond[3 * i + 2] = make_float4(inv.m[6], inv.m[7], inv.m[8], 0.0f);
+  }
+}
+
+__global__ void __launch_bounds__(kSolveThreads, 1) k_noalloc_pcg(Dev D) {
+  if (*reinterpret_cast<volatile int*>(&D.ctl->error) != 0) return;
+  GridSync gs;
+  gs.init(D.ctl, D.P.barrierLimitNs);
+  const int it = pcgSolve<false, kRowLanes>(D, gs);
+  if (it >= 0 && blockIdx.x == 0 && threadIdx.x == 0) D.ctl->lastCg = it;
+}
+
+// -2: the structure check failed; -1: a grid barrier gave up waiting; else the PCG iteration count.
 __global__ void k_noalloc_finish(const Control* ctl, int* iterations) {
-  *iterations = ctl->error ? -1 : ctl->lastCg;
+  const int e = ctl->error;
+  *iterations = e == kNoAllocBadStructure ? -2 : (e ? -1 : ctl->lastCg);
 }
 
 }  // namespace dcu
@@ -1687,10 +1804,11 @@ extern "C" int drape_cuda_pcg_noalloc(uint32_t n, uint32_t slots, const uint32_t
     if (slots > DRAPE_PCG_NOALLOC_MAX_SLOTS)
       throw std::invalid_argument("pcg_noalloc: " + std::to_string(slots) + " block slots exceed the limit of " +
                                   std::to_string(DRAPE_PCG_NOALLOC_MAX_SLOTS));
+    if (slots < n) throw std::invalid_argument("pcg_noalloc: fewer block slots than rows (every row has a diagonal)");
     if (slots_padded < slots) throw std::invalid_argument("pcg_noalloc: slots_padded < row_start[n]");
     int device = 0;
     CK(cudaGetDevice(&device));
-    NoAllocDevice& nd = noAllocScratch(device);
+    NoAllocDevice& nd = noAllocScratch(device, st);
     unsigned char* base = nd.scratch;
     using L = NoAllocLayout;
     auto* vec = reinterpret_cast<float4*>(base + L::vectors);
@@ -1723,16 +1841,18 @@ extern "C" int drape_cuda_pcg_noalloc(uint32_t n, uint32_t slots, const uint32_t
     d.ctl = reinterpret_cast<dcu::Control*>(base + L::control);
     auto* diag = reinterpret_cast<uint32_t*>(base + L::diag);
     const int pg = std::max(1, static_cast<int>((n + 255) / 256));
-    dcu::k_noalloc_prepare<<<pg, 256, 0, st>>>(
-        n, d_row_start, d_col_index, d_pinned, d_active, static_cast<const float4*>(d_normals),
-        reinterpret_cast<dcu::Particle*>(base + L::particle), d.contact, reinterpret_cast<uint32_t*>(base + L::cols),
-        diag, d.ctl, d_iterations);
+    dcu::k_noalloc_clear<<<1, 1, 0, st>>>(d.ctl, d_iterations);
     CK(cudaGetLastError());
-    dcu::k_pcg_precondition<<<pg, 256, 0, st>>>(d, diag);
+    dcu::k_noalloc_prepare<<<pg, 256, 0, st>>>(
+        n, slots, d_row_start, d_col_index, d_pinned, d_active, static_cast<const float4*>(d_normals),
+        reinterpret_cast<dcu::Particle*>(base + L::particle), d.contact, reinterpret_cast<uint32_t*>(base + L::cols),
+        diag, d.ctl);
+    CK(cudaGetLastError());
+    dcu::k_noalloc_precondition<<<pg, 256, 0, st>>>(d, diag);
     CK(cudaGetLastError());
     void* args[] = {&d};
-    CK(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(dcu::k_pcg_only), dim3(nd.sms), dim3(dcu::kSolveThreads),
-                                   args, 0, st));
+    CK(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(dcu::k_noalloc_pcg), dim3(nd.sms),
+                                   dim3(dcu::kSolveThreads), args, 0, st));
     dcu::k_noalloc_finish<<<1, 1, 0, st>>>(d.ctl, d_iterations);
     CK(cudaGetLastError());
   });

@@ -29,12 +29,13 @@ __global__ void __launch_bounds__(kAssembleThreads, 5) k_assemble(Dev D) {
 }
 
 // One Newton iteration's persistent solve; the whole grid is one group.
-template <bool Learned>
+// Variant: the block-Jacobi PCG's form (0 reference order, 1 pipelined; see pcgSolveStaged).
+template <bool Learned, int Variant = 0>
 __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(Dev D) {
   if (D.ctl->newtonDone) return;
   GridSync gs;
   gs.init(D.ctl, D.P.barrierLimitNs);
-  solveGroup<Learned, kRowLanes>(D, gs);
+  solveGroup<Learned, kRowLanes, Variant>(D, gs);
 }
 
 __global__ void k_finish(Dev D) { finishRows(D, blockIdx.x, gridDim.x); }
@@ -239,6 +240,39 @@ __global__ void k_barrier_probe(Control* ctl, unsigned long long limitNs, int* o
   gs.target += 1;  // one arrival that never comes
   const bool released = gs.sync();
   if (threadIdx.x == 0 && blockIdx.x == 0) *out = released ? 0 : ctl->error;
+}
+
+// The persistent solve's synchronisation floor: `iterations` rounds of grid-wide exchanges on the solve's grid, with no
+// other work, timed by block 0 with %globaltimer (nanoseconds for all rounds in *ns, or 0 if a barrier gave up).
+//   mode 0: gridReduce<1> + gridReduce<2>  (a reference-order PCG iteration's two reductions: p.Ap, then r.r and r.z)
+//   mode 1: gridReduce<3> + a plain barrier (one merged reduction plus the direction's exchange before the next SpMV)
+//   mode 2: gridReduce<3> alone
+//   mode 3: two plain barriers
+// Each round feeds its result into the next, so no round can be skipped or overlapped.
+__global__ void __launch_bounds__(kSolveThreads, 1) k_reduction_floor(Dev D, int mode, int iterations,
+                                                                       unsigned long long* ns) {
+  GridSync gs;
+  gs.init(D.ctl, D.P.barrierLimitNs);
+  double x = 1e-3 * threadIdx.x;
+  const unsigned long long t0 = globalTimerNs();
+  for (int it = 0; it < iterations; ++it) {
+    if (mode == 0) {
+      double a[1] = {x}, b[1];
+      if (!gridReduce<1>(D, gs, a, b)) return;
+      double c[2] = {x, b[0]}, d[2];
+      if (!gridReduce<2>(D, gs, c, d)) return;
+      x = 1e-9 * d[1];
+    } else if (mode == 1 || mode == 2) {
+      double a[3] = {x, 2.0 * x, 1.0}, b[3];
+      if (!gridReduce<3>(D, gs, a, b)) return;
+      if (mode == 1 && !gs.sync()) return;
+      x = 1e-9 * b[0];
+    } else {
+      if (!gs.sync() || !gs.sync()) return;
+      x += 1e-9;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *ns = (x > -1.0) ? globalTimerNs() - t0 : 0ull;
 }
 
 }  // namespace dcu

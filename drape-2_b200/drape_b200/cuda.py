@@ -83,6 +83,8 @@ def load(build_if_missing: bool = True):
     L.drape_cuda_precond_factor.argtypes = [C.c_void_p, _P(_f)]
     L.drape_cuda_test_barrier_timeout.argtypes = [C.c_int, C.c_int, C.c_uint64, _P(C.c_int)]
     L.drape_cuda_inject_failure.argtypes = [C.c_void_p, C.c_int]
+    L.drape_cuda_set_pcg_variant.argtypes = [C.c_void_p, C.c_int]
+    L.drape_cuda_reduction_floor.argtypes = [C.c_int, C.c_int, C.c_int, _P(_d)]
     L.drape_cuda_cg_history.argtypes = [C.c_void_p, _P(_i32), C.c_size_t, _P(C.c_size_t)]
     L.drape_cuda_stream.argtypes = [C.c_void_p, _P(C.c_void_p)]
     L.drape_cuda_profile.argtypes = [C.c_void_p, C.c_int]
@@ -312,6 +314,10 @@ class CudaSolver:
     def set_precond_schedule(self, refresh_every: int = 1, jacobi_first: int = 0) -> None:
         self._check(self.L.drape_cuda_set_precond_schedule(self.h, int(refresh_every), int(jacobi_first)))
 
+    def set_pcg_variant(self, variant: int) -> None:
+        """0: the reference-order block-Jacobi PCG (default); 1: pipelined, one grid exchange per iteration."""
+        self._check(self.L.drape_cuda_set_pcg_variant(self.h, int(variant)))
+
     def inject_failure(self, steps: int) -> None:
         self._check(self.L.drape_cuda_inject_failure(self.h, int(steps)))
 
@@ -343,3 +349,13 @@ def test_barrier_timeout(device: int = 0, blocks: int = 2, nanoseconds: int = 20
     st = C.c_int(-1)
     _raise(L.drape_cuda_test_barrier_timeout(device, blocks, nanoseconds, C.byref(st)), L.drape_cuda_last_error(None))
     return st.value
+
+
+def reduction_floor(device: int = 0, mode: int = 0, iterations: int = 2000) -> float:
+    """Device microseconds per round of the persistent solve's grid-wide exchanges with no other work
+    (drape_cuda_reduction_floor): mode 0 = the two FP64 reductions of a reference-order PCG iteration, 1 = one merged
+    reduction plus a plain barrier, 2 = one merged reduction, 3 = two plain barriers."""
+    L = load()
+    ns = C.c_double(0.0)
+    _raise(L.drape_cuda_reduction_floor(device, mode, iterations, C.byref(ns)), L.drape_cuda_last_error(None))
+    return ns.value / 1000.0

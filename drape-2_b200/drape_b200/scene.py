@@ -93,7 +93,7 @@ class drape_stats(C.Structure):
 class drape_counters(C.Structure):
     _fields_ = [(name, C.c_int64) for name in (
         "substeps", "newton_iterations", "cg_iterations", "line_search_halvings", "precond_fallbacks",
-        "learned_solves")]
+        "learned_solves", "pcg_nanoseconds")]
 
 
 class drape_drape_options(C.Structure):

@@ -2,7 +2,7 @@
  * C ABI of the B200 cloth-solver hot path (libdrape_cuda.so).
  *
  * One opaque handle is one solver: the reference's drape::sim::Solver (libs/sim/include/drape/sim/solver.hpp:85-98)
- * with its state on one GPU. A reference-side CudaSolver (see INTEGRATION.md) forwards each Solver method to the
+ * with its state on one GPU. A reference-side CudaSolver forwards each Solver method to the
  * entry point named beside it, and registers itself as a SolverBackend in makeSolver / isAvailable / backendName
  * (libs/sim/include/drape/sim/solver_factory.hpp:12-20, libs/sim/src/solver_factory.cpp:16-61), so the GPU/CPU switch
  * (libs/session/include/drape/session/sim_controller.hpp:25) can select it.
@@ -193,11 +193,15 @@ int drape_cuda_spmv_device(uint32_t n, const uint32_t* d_row_start, const uint32
    Inputs and outputs are the caller's device buffers: row_start (n + 1) and col_index (slots = row_start[n], passed
    by value as `slots`) as u32; blocks as 9 planes of slots_padded floats (component 3 * row + col); pinned and
    active as one u8 per particle (active may be NULL); normals, grad, step and resid as float4 per particle (normals
-   may be NULL). The iteration count is written to *d_iterations in device memory (-1 if the bounded grid barrier
-   gave up). The work is queued on `stream` (a cudaStream_t, NULL for the legacy default stream) without
-   synchronising; the return value reports argument and launch errors.
+   may be NULL). The iteration count is written to *d_iterations in device memory: -1 if the bounded grid barrier
+   gave up, -2 if the device-side structure check refused the system (row_start not non-decreasing from 0 to
+   `slots`, a column index >= n, or a row without its diagonal block; the allocating entry point throws for the
+   same cases). Nothing is solved then and step/resid are left as they were. The work is queued on `stream` (a
+   cudaStream_t, NULL for the legacy default stream) without synchronising; the return value reports argument and
+   launch errors (slots < n is refused on the host).
    The first call on a device does a one-time set-up for that device (it looks up the array's device address with
-   the device current); make that first call before any stream capture. Every call shares the one array, which keeps
+   the device current); make that first call before any stream capture. Later calls made outside a capture look the
+   address up again, so a re-created context is picked up. Every call shares the one array, which keeps
    the last call's contents; each call clears what must start at zero. Calls whose work overlaps on the GPU (other
    streams, other host threads, other devices' calls on the same device) race on the array: serialise them. */
 #define DRAPE_PCG_NOALLOC_MAX_PARTICLES 8192u
@@ -208,10 +212,22 @@ int drape_cuda_pcg_noalloc(uint32_t n, uint32_t slots, const uint32_t* d_row_sta
                            const uint8_t* d_active, const void* d_normals, const void* d_grad, int max_iterations,
                            double tolerance, void* d_step, void* d_resid, int32_t* d_iterations, void* stream);
 
+/* The block-Jacobi PCG's form (no reference counterpart; both solve the reference's contact-filtered system with its
+   stopping tests, cpu_solver.cpp:169-213): 0 (the default) the reference's order, two grid-wide exchanges per
+   iteration; 1 pipelined (Ghysels and Vanroose 2014), the same iterates in exact arithmetic with one exchange per
+   iteration and three more work vectors, rounding differently. The learned preconditioner always runs its own PCG. */
+int drape_cuda_set_pcg_variant(drape_solver* s, int variant);
+
 /* The bounded wait of the device grid barrier, in nanoseconds (0 restores the default of 2 s). A kernel whose barrier
    waits longer sets the handle's error status and returns instead of hanging; the step then fails with
    DRAPE_DEVICE_ERROR and the solver stays usable. */
 int drape_cuda_set_barrier_limit(drape_solver* s, uint64_t nanoseconds);
+/* Measurement hook (no reference counterpart): the synchronisation floor of the persistent solve on `device`: the
+   solve's grid (one 1024-thread block per SM, cooperative) runs `iterations` rounds of grid-wide exchanges with no
+   other work and *ns_per_iteration gets the device time per round (%globaltimer, block 0). mode 0: the two FP64 grid
+   reductions of a reference-order PCG iteration; 1: one three-value reduction plus a plain barrier; 2: one three-value
+   reduction; 3: two plain barriers. */
+int drape_cuda_reduction_floor(int device, int mode, int iterations, double* ns_per_iteration);
 /* Test hook: runs a grid barrier that can only end by its time limit (it waits for one more block than it has) on
    `blocks` blocks with the given limit, and returns the status the blocks read back in *status (0: released, which
    cannot happen; 1: timed out). Exercises the bounded wait without a device fault. */

@@ -134,6 +134,7 @@ typedef struct drape_counters {
   int64_t line_search_halvings;
   int64_t precond_fallbacks; /* learned preconditioner abandoned for block-Jacobi */
   int64_t learned_solves;    /* PCG solves that started with the learned preconditioner */
+  int64_t pcg_nanoseconds;   /* device time inside the PCG solves (CG init to the last iteration; %globaltimer) */
 } drape_counters;
 
 #ifdef __cplusplus

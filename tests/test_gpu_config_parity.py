@@ -1,0 +1,187 @@
+"""Config-level parity of the CUDA path with the oracle, through the C ABI.
+
+Restates the reference's GPU-vs-CPU parity tests (libs/sim/tests/test_gpu_parity.cpp:52-80): after 60 frames the
+CUDA solver's particles lie within 1 mm of the faithful oracle's (the reference CpuSolver restated: float particle
+state, double solve), on scenes the oracle itself reproduces to well under 1 mm when its start moves by 1 um; each
+case prints that self-spread beside the difference (test_gpu_parity.cpp:55-63). The flat hanging sheet is the
+reference's exception: an out-of-plane nudge buckles it, so its self-spread is large while a faithful port stays close
+(there the print is informational). The reference's third case continues the settled tee; its CDT-meshed tee is not
+buildable here, so the settled seamed tubes take its place (the 10k tube settled live by the oracle, the 60k tube from
+the committed oracle-settled state of tests/golden/deviation.npz).
+
+The workloads' own configurations (the 40 x 40 sheet dropped on the sphere, 120 frames at PCG tolerance 1e-6; the
+10k tube draped from its start for 300 frames) are drops onto a body, where the oracle's own 1 um self-spread is
+centimetres (131 mm and 6 mm, tests/golden/deviation.npz); there the bar is the oracle's own spread: the CUDA result
+lies no further from the oracle than three times the oracle's distance from itself under the 1 um nudge, or 1 mm.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from drape_b200 import scenes as S
+from drape_b200 import session as SS
+from drape_b200.scene import Scene
+
+pytestmark = pytest.mark.gpu
+FIXTURE = os.path.join(os.path.dirname(__file__), "golden", "deviation.npz")
+BAR_M = 1e-3
+SNAP_KEYS = ("positions", "velocities", "phases", "assembly_time", "seam_start_gap", "contact_force")
+
+
+def perturbed(snap, amount=1e-6, seed=1):
+    s = dict(snap)
+    x = np.asarray(s["positions"], np.float64)
+    s["positions"] = (x + amount * np.random.default_rng(seed).uniform(-1.0, 1.0, x.shape)).astype(np.float32)
+    return s
+
+
+def cuda_solver(gpu, variant):
+    def make():
+        s = gpu.CudaSolver(0)
+        s.set_pcg_variant(variant)
+        return s
+    return make
+
+
+def end_positions(make, scene, frames, start=None, perturb=0.0, settle_after=None):
+    s = make()
+    s.build(scene)
+    if start is not None:
+        s.restore(start)
+    if perturb:
+        s.restore(perturbed(s.snapshot(), perturb))
+    gids = [g.id for g in scene.garments]
+    for f in range(frames):
+        if settle_after is not None and f == 0:
+            for g in gids:
+                s.set_phase(g, 0)
+        if settle_after is not None and f == settle_after:
+            for g in gids:
+                s.set_phase(g, 1)
+        s.step(1.0 / 60.0, 1, 2)
+    assert not s.stats().has_non_finite
+    x = s.positions().astype(np.float64)
+    if hasattr(s, "close"):
+        s.close()
+    return x
+
+
+def max_distance(a, b):
+    return float(np.linalg.norm(a - b, axis=1).max())
+
+
+_ORACLE_RUNS = {}
+
+
+def oracle_runs(oracle_mod, key, scene, start):
+    """The oracle's 60-frame end positions and its 1 um self-spread for one scene (cached across the PCG variants)."""
+    if key not in _ORACLE_RUNS:
+        ref = end_positions(oracle_mod.OracleSolver, scene, 60, start)
+        spread = max_distance(end_positions(oracle_mod.OracleSolver, scene, 60, start, perturb=1e-6), ref)
+        _ORACLE_RUNS[key] = (ref, spread)
+    return _ORACLE_RUNS[key]
+
+
+def expect_parity(gpu, oracle_mod, key, scene, variant, start=None, informational_spread=False):
+    ref, spread = oracle_runs(oracle_mod, key, scene, start)
+    x = end_positions(cuda_solver(gpu, variant), scene, 60, start)
+    apart = max_distance(x, ref)
+    d = np.linalg.norm(x - ref, axis=1)
+    rms = float(np.sqrt(np.mean(d * d)))
+    print(f"parity ({key}, pcg variant {variant}): oracle self-spread {spread * 1e3:.3f} mm"
+          f"{' (informational)' if informational_spread else ''}, cuda vs oracle {apart * 1e3:.3f} mm "
+          f"(rms {rms * 1e3:.3f} mm)")
+    return apart, rms, spread
+
+
+VARIANTS = [0, 1]  # the reference-order PCG and the pipelined one
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_hanging_sheet_60_frames(gpu, oracle_mod, variant):
+    apart, _, _ = expect_parity(gpu, oracle_mod, "hanging", S.hanging_sheet(), variant, informational_spread=True)
+    assert apart < BAR_M, apart
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_patch_on_sphere_60_frames(gpu, oracle_mod, variant):
+    apart, _, _ = expect_parity(gpu, oracle_mod, "patch", Scene([S.centred_sheet(0.004, 0.004, 0.2)],
+                                                               S.sphere_field()), variant)
+    assert apart < BAR_M, apart
+
+
+_SETTLED_10K = {}
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_tube10k_from_settled_60_frames(gpu, oracle_mod, variant):
+    """The oracle drapes the 10k tube to rest (the DrapeSession criterion); 60 more frames run on both solvers from
+    that state: every term, seams, body contact and friction at once. A settled drape still creeps, so the max
+    distance is held to the oracle's own self-spread (three times it, or 1 mm) and the RMS distance to 1 mm."""
+    scene = S.tube_10k()
+    if "start" not in _SETTLED_10K:
+        o = oracle_mod.OracleSolver()
+        o.build(scene)
+        res = SS.drape_to_rest(o, ["tube"])
+        assert res.settled
+        _SETTLED_10K["start"] = o.snapshot()
+    apart, rms, spread = expect_parity(gpu, oracle_mod, "tube10k", scene, variant, start=_SETTLED_10K["start"])
+    assert rms < BAR_M, rms
+    assert apart <= max(BAR_M, 3.0 * spread), (apart, spread)
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_tube60k_from_settled_60_frames(gpu, variant):
+    """The 60k workload tube, 60 frames from the faithful oracle's settled state (committed with the oracle's end
+    state after the same 60 frames and its self-spread: 5.9 mm max, 0.39 mm RMS). Bars as for the 10k tube."""
+    F = np.load(FIXTURE)
+    scene = S.tube_60k()
+    start = {k: F[f"c3_start_{k}"] for k in SNAP_KEYS}
+    x = end_positions(cuda_solver(gpu, variant), scene, int(F["c3_frames"]), start)
+    ref = F["c3_faithful"].astype(np.float64)
+    apart = max_distance(x, ref)
+    d = np.linalg.norm(x - ref, axis=1)
+    rms = float(np.sqrt(np.mean(d * d)))
+    spread = float(F["c3_spread_max"])
+    print(f"parity (tube60k, pcg variant {variant}): oracle self-spread {spread * 1e3:.3f} mm "
+          f"(rms {float(F['c3_spread_rms']) * 1e3:.3f}), cuda vs oracle {apart * 1e3:.3f} mm (rms {rms * 1e3:.3f}), "
+          f"cuda vs FP64 oracle {max_distance(x, F['c3_fp64'].astype(np.float64)) * 1e3:.3f} mm")
+    assert rms < BAR_M, rms
+    assert apart <= max(BAR_M, 3.0 * spread), (apart, spread)
+
+
+def test_pipelined_pcg_tracks_reference_order_one_frame(gpu):
+    """One frame of the 10k tube drop with each PCG form: the pipelined one is the reference-order PCG up to rounding
+    (same Newton and PCG iteration counts within one per solve, positions within 1e-5 m)."""
+    out = []
+    for variant in VARIANTS:
+        s = cuda_solver(gpu, variant)()
+        s.build(S.tube_10k())
+        s.set_phase("tube", 0)
+        s.step(1.0 / 60.0, 1, 2)
+        c = s.counters()
+        out.append((s.positions().astype(np.float64), c.newton_iterations, c.cg_iterations, s.cg_history()))
+        s.close()
+    (x0, n0, _, h0), (x1, n1, _, h1) = out
+    assert n0 == n1
+    assert np.abs(np.asarray(h0) - np.asarray(h1)).max() <= 1, (h0, h1)
+    assert np.abs(x0 - x1).max() < 1e-5
+
+
+@pytest.mark.parametrize("name", ["c1", "c2"])
+def test_workload_drops_within_the_oracles_own_spread(gpu, name):
+    """The workloads' drop configurations (see the module docstring): CUDA vs oracle no further than 3x the oracle's
+    1 um self-spread (or 1 mm)."""
+    F = np.load(FIXTURE)
+    if name == "c1":
+        scene = S.sheet_on_sphere(cg_tolerance=float(F["c1_cg_tolerance"]), max_cg=int(F["c1_max_cg"]))
+        x = end_positions(cuda_solver(gpu, 0), scene, int(F["c1_frames"]))
+    else:
+        scene = S.tube_10k()
+        x = end_positions(cuda_solver(gpu, 0), scene, int(F["c2_frames"]), settle_after=int(F["c2_assembly_frames"]))
+    apart = max_distance(x, F[f"{name}_faithful"].astype(np.float64))
+    spread = float(F[f"{name}_spread_max"])
+    print(f"{name}: oracle self-spread {spread * 1e3:.3f} mm, cuda vs oracle {apart * 1e3:.3f} mm, "
+          f"cuda vs FP64 oracle {max_distance(x, F[f'{name}_fp64'].astype(np.float64)) * 1e3:.3f} mm")
+    assert apart <= max(BAR_M, 3.0 * spread), (apart, spread)
