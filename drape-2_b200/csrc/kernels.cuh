@@ -932,7 +932,6 @@ __device__ inline int pcgPipelined(const Dev& D, GridSync& gs, const SmemMatrix&
   uint32_t r0i, r1i;
   blockRange(D.P.n, gs.rank, gs.size, r0i, r1i);
   float4 *x = D.step, *r = D.r, *u = D.z, *w = D.ap, *s = D.apFull, *p = D.p0, *q = D.p1, *zq = D.pz;
-  float4* const mBuf[2] = {D.pm0, D.pm1};
   // x = 0, r = F(-grad), u = F(M r); u is gathered next, so a plain barrier publishes it.
   for (uint32_t i = r0i + threadIdx.x; i < r1i; i += blockDim.x) {
     const Contact c = D.contact[i];
@@ -956,7 +955,7 @@ __device__ inline int pcgPipelined(const Dev& D, GridSync& gs, const SmemMatrix&
           v[0] += dotd3(ri, ui);
           v[1] += dotd3(wi, ui);
           v[2] += dotd3(ri, ri);
-          mBuf[0][i] = f4(filterContact(c, mul(loadPrecond(D, i), wi)));
+          D.pm0[i] = f4(filterContact(c, mul(loadPrecond(D, i), wi)));
         });
     if (!gridReduce<3>(D, gs, v, t)) return -1;
   }
@@ -973,30 +972,31 @@ __device__ inline int pcgPipelined(const Dev& D, GridSync& gs, const SmemMatrix&
     const double alpha = gamma / pAp;
     const float fa = static_cast<float>(alpha), fb = static_cast<float>(beta);
     const bool first = it == 0;
-    const float4* mCur = mBuf[it & 1];
-    float4* mNext = mBuf[(it + 1) & 1];
+    const float4* mCur = (it & 1) ? D.pm1 : D.pm0;
+    float4* mNext = (it & 1) ? D.pm0 : D.pm1;
     double v[3] = {0.0, 0.0, 0.0};
     directionProducts<PL>(
         D, A, r0i, r1i, [&](uint32_t j) { return ld3(mCur, j); },
         [&](uint32_t i, float3 mi, float3 am) {
+          // Each recurrence is formed and stored in turn (z, w, s, r, q, u, p, x), so that only r, u and w stay live.
           const Contact c = D.contact[i];
-          const float3 ni = filterContact(c, am);
-          const float3 ui0 = ld3(u, i), wi0 = ld3(w, i);
-          const float3 zi = first ? ni : ni + ld3(zq, i) * fb;
-          const float3 qi = first ? mi : mi + ld3(q, i) * fb;
-          const float3 si = first ? wi0 : wi0 + ld3(s, i) * fb;
-          const float3 pi = first ? ui0 : ui0 + ld3(p, i) * fb;
-          const float3 ri = ld3(r, i) - si * fa;
-          const float3 ui = ui0 - qi * fa;
-          const float3 wi = wi0 - zi * fa;
-          x[i] = f4(ld3(x, i) + pi * fa);
+          const float3 zi = first ? filterContact(c, am) : filterContact(c, am) + ld3(zq, i) * fb;
           zq[i] = f4(zi);
-          q[i] = f4(qi);
-          s[i] = f4(si);
-          p[i] = f4(pi);
-          r[i] = f4(ri);
-          u[i] = f4(ui);
+          const float3 wi0 = ld3(w, i);
+          const float3 wi = wi0 - zi * fa;
           w[i] = f4(wi);
+          const float3 si = first ? wi0 : wi0 + ld3(s, i) * fb;
+          s[i] = f4(si);
+          const float3 ri = ld3(r, i) - si * fa;
+          r[i] = f4(ri);
+          const float3 qi = first ? mi : mi + ld3(q, i) * fb;
+          q[i] = f4(qi);
+          const float3 ui0 = ld3(u, i);
+          const float3 ui = ui0 - qi * fa;
+          u[i] = f4(ui);
+          const float3 pi = first ? ui0 : ui0 + ld3(p, i) * fb;
+          p[i] = f4(pi);
+          x[i] = f4(ld3(x, i) + pi * fa);
           v[0] += dotd3(ri, ui);
           v[1] += dotd3(wi, ui);
           v[2] += dotd3(ri, ri);
