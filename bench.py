@@ -600,8 +600,26 @@ def run_profile_case(args):
         s.build(make_scene("tube60k"))
         print(json.dumps(spmv_leg(CU, s, peak, tiles=args.spmv_tiles)))
         return 0
+    if args.profile_case == "learned":
+        # One forward and one backward of the network (k_layer, k_bw_layer, ...) on a captured 10k-tube system.
+        from drape_b200 import learned as LR
+        s = CU.CudaSolver(0)
+        s.build(make_scene("tube10k"))
+        for _ in range(20):
+            s.step(1.0 / 60.0, 1, 2)
+        sysm = s.capture_system(1.0 / 60.0)
+        n = len(sysm["diag_slot"])
+        p = LR.LearnedPreconditioner(0, LR.load_weights("tube"))
+        sid = p.add_sample(sysm["row_start"], sysm["col_index"], sysm["blocks"], np.zeros(n, np.uint8),
+                           sysm["active"], np.random.default_rng(0).standard_normal((1, n, 3)).astype(np.float32))
+        p.forward(sid)
+        loss, grad = p.loss_grad(sid)
+        print(json.dumps({"case": "learned", "particles": n, "block_slots": int(len(sysm["col_index"])),
+                          "loss": float(loss), "grad_norm": float(np.linalg.norm(grad))}))
+        return 0
     if args.profile_case == "drape":
         s = CU.CudaSolver(0)
+        s.set_pcg_variant(args.pcg_variant)
         s.build(make_scene(args.workload))
         for _ in range(args.batch_frames):
             s.step(1.0 / 60.0, 1, 2)
@@ -658,7 +676,7 @@ def main():
     ap.add_argument("--pcg-variant", type=int, choices=[0, 1], default=0,
                     help="block-Jacobi PCG form: 0 the reference's order, 1 pipelined (one grid exchange an iteration)")
     ap.add_argument("--batch-garments", type=int, default=64, help="garments of the batched leg (0: skip it)")
-    ap.add_argument("--profile-case", choices=["spmv", "batch", "bake", "drape"], default=None,
+    ap.add_argument("--profile-case", choices=["spmv", "batch", "bake", "drape", "learned"], default=None,
                     help="run one small case for a profiler capture instead of the benchmark")
     ap.add_argument("--spmv-tiles", type=int, default=12)
     ap.add_argument("--batch-frames", type=int, default=6)
