@@ -370,16 +370,23 @@ __global__ void __launch_bounds__(kThreads) k_layer(Graph g, const __nv_bfloat16
   for (uint32_t tile = blockIdx.x; tile < g.nTiles; tile += gridDim.x) {
     const TileRows tr = tileRows(g, tile);
     tileSlotInfo(g, tr, S.slotRow, S.rowFirst, true);
-    // X_msg: [h_j; eps_s] per message slot.
-    for (int k = t; k < 128 * 16; k += kThreads) {
-      const int q = k / 16, c = k % 16;
-      uint4 v = zero4();
-      if (S.slotRow[q] >= 0) {
-        const uint32_t s = tr.s0 + q;
-        v = c < 8 ? reinterpret_cast<const uint4*>(hin + 64 * static_cast<size_t>(colOf(g, s)))[c]
-                  : reinterpret_cast<const uint4*>(g.eps + 64 * static_cast<size_t>(s))[c - 8];
+    // X_msg: [h_j; eps_s] per message slot. Thread t owns 16-byte chunk c = t % 16 of slots q = t / 16 + 8 i; its 16
+    // gathers are all issued before the first store into the tile, so they are in flight together.
+    {
+      const int c = t % 16;
+      uint4 v[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int q = t / 16 + 8 * i;
+        v[i] = zero4();
+        if (S.slotRow[q] >= 0) {
+          const uint32_t s = tr.s0 + q;
+          v[i] = c < 8 ? reinterpret_cast<const uint4*>(hin + 64 * static_cast<size_t>(colOf(g, s)))[c]
+                       : reinterpret_cast<const uint4*>(g.eps + 64 * static_cast<size_t>(s))[c - 8];
+        }
       }
-      st16(S.x, q, c, 128, v);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) st16(S.x, t / 16 + 8 * i, c, 128, v[i]);
     }
     if (!T.run([&] { umma::gemmIssue(T.tmem, S.x, S.wm, 128, 64, 128, false); })) break;
     {
@@ -473,17 +480,27 @@ __global__ void __launch_bounds__(kThreads) k_output(Graph g, const __nv_bfloat1
   for (uint32_t tile = blockIdx.x; tile < g.nTiles; tile += gridDim.x) {
     const TileRows tr = tileRows(g, tile);
     tileSlotInfo(g, tr, S.slotRow, S.rowFirst, false);
-    for (int k = t; k < 128 * 24; k += kThreads) {
-      const int q = k / 24, c = k % 24;
-      uint4 v = zero4();
-      const int sr = S.slotRow[q];
-      if (sr >= 0) {
-        const uint32_t s = tr.s0 + q;
-        if (c < 8) v = reinterpret_cast<const uint4*>(h + 64 * static_cast<size_t>(tr.r0 + sr))[c];
-        else if (c < 16) v = reinterpret_cast<const uint4*>(h + 64 * static_cast<size_t>(colOf(g, s)))[c - 8];
-        else v = reinterpret_cast<const uint4*>(g.eps + 64 * static_cast<size_t>(s))[c - 16];
+    // [h_i; h_j; eps_s] per lower slot, in two rounds of 12 chunks a thread: each round's gathers are issued before
+    // its first store into the tile (12 loads in flight at a moderate register count).
+    for (int round = 0; round < 2; ++round) {
+      uint4 v[12];
+#pragma unroll
+      for (int i = 0; i < 12; ++i) {
+        const int k = t + kThreads * (12 * round + i), q = k / 24, c = k % 24;
+        v[i] = zero4();
+        const int sr = S.slotRow[q];
+        if (sr >= 0) {
+          const uint32_t s = tr.s0 + q;
+          if (c < 8) v[i] = reinterpret_cast<const uint4*>(h + 64 * static_cast<size_t>(tr.r0 + sr))[c];
+          else if (c < 16) v[i] = reinterpret_cast<const uint4*>(h + 64 * static_cast<size_t>(colOf(g, s)))[c - 8];
+          else v[i] = reinterpret_cast<const uint4*>(g.eps + 64 * static_cast<size_t>(s))[c - 16];
+        }
       }
-      st16(S.x, q, c, 192, v);
+#pragma unroll
+      for (int i = 0; i < 12; ++i) {
+        const int k = t + kThreads * (12 * round + i);
+        st16(S.x, k / 24, k % 24, 192, v[i]);
+      }
     }
     if (!T.run([&] { umma::gemmIssue(T.tmem, S.x, S.w, 128, 16, 192, false); })) break;
     float o[16];
@@ -926,14 +943,22 @@ __global__ void __launch_bounds__(kThreads) k_bw_layer(Graph g, const __nv_bfloa
     const int nq = static_cast<int>(tr.s1 - tr.s0);
     const bool acc = !first;
     // --- node part: u = W_u [h; a] + b_u, gu = GH (u > 0).
-    for (int k = t; k < 128 * 16; k += kThreads) {
-      const int r = k / 16, c = k % 16;
-      uint4 v = zero4();
-      if (r < R)
-        v = c < 8 ? reinterpret_cast<const uint4*>(hl + 64 * static_cast<size_t>(tr.r0 + r))[c]
-                  : reinterpret_cast<const uint4*>(agg + 64 * static_cast<size_t>(tr.r0 + r))[c - 8];
-      st16(S.x, r, c, 128, v);
-      st16T(S.xt, r, c, 128, v);
+    {  // thread t: chunk c = t % 16 of rows t / 16 + 8 i, all loads in flight before the stores
+      const int c = t % 16;
+      uint4 v[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int r = t / 16 + 8 * i;
+        v[i] = zero4();
+        if (r < R)
+          v[i] = c < 8 ? reinterpret_cast<const uint4*>(hl + 64 * static_cast<size_t>(tr.r0 + r))[c]
+                       : reinterpret_cast<const uint4*>(agg + 64 * static_cast<size_t>(tr.r0 + r))[c - 8];
+      }
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        st16(S.x, t / 16 + 8 * i, c, 128, v[i]);
+        st16T(S.xt, t / 16 + 8 * i, c, 128, v[i]);
+      }
     }
     if (!(good = T.run([&] { umma::gemmIssue(T.tmem + kU, S.x, S.wu, 128, 64, 128, false); }))) break;
     {
@@ -981,16 +1006,24 @@ __global__ void __launch_bounds__(kThreads) k_bw_layer(Graph g, const __nv_bfloa
     }
     __syncthreads();
     // --- message part: v = W_m [h_j; eps_s] + b_m, gv = (ga_i / 8) (v > 0).
-    for (int k = t; k < 128 * 16; k += kThreads) {
-      const int q = k / 16, c = k % 16;
-      uint4 v = zero4();
-      if (S.slotRow[q] >= 0) {
-        const uint32_t s = tr.s0 + q;
-        v = c < 8 ? reinterpret_cast<const uint4*>(hl + 64 * static_cast<size_t>(colOf(g, s)))[c]
-                  : reinterpret_cast<const uint4*>(g.eps + 64 * static_cast<size_t>(s))[c - 8];
+    {  // thread t: chunk c = t % 16 of slots t / 16 + 8 i, all 16 gathers in flight before the stores
+      const int c = t % 16;
+      uint4 v[16];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int q = t / 16 + 8 * i;
+        v[i] = zero4();
+        if (S.slotRow[q] >= 0) {
+          const uint32_t s = tr.s0 + q;
+          v[i] = c < 8 ? reinterpret_cast<const uint4*>(hl + 64 * static_cast<size_t>(colOf(g, s)))[c]
+                       : reinterpret_cast<const uint4*>(g.eps + 64 * static_cast<size_t>(s))[c - 8];
+        }
       }
-      st16(S.x, q, c, 128, v);
-      st16T(S.xt, q, c, 128, v);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        st16(S.x, t / 16 + 8 * i, c, 128, v[i]);
+        st16T(S.xt, t / 16 + 8 * i, c, 128, v[i]);
+      }
     }
     if (!(good = T.run([&] { umma::gemmIssue(T.tmem + kU, S.x, S.wm, 128, 64, 128, false); }))) break;
     float gv[64];
