@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
+#include <thread>
 #include <climits>
 #include <cmath>
 #include <cstring>
@@ -538,11 +540,19 @@ struct drape_solver {
 
   // Waits for the stream by polling it: the per-frame waits of stepping and of the drape runner wake up without the
   // scheduling delay a blocking synchronise can take on a busy host.
+  // Polls for up to waitSpinUs microseconds, then sleeps 20 us between polls: a drape's waits (one per batch of
+  // frames, ~14 ms of device work) do not keep a host core busy, which a CPU-quota-limited host would throttle while
+  // the device drains its queue. waitSpinUs = UINT32_MAX polls without sleeping.
+  uint32_t waitSpinUs = 200;
   void waitStream() {
+    const auto start = std::chrono::steady_clock::now();
     for (;;) {
       const cudaError_t e = cudaStreamQuery(stream);
       if (e == cudaSuccess) return;
       if (e != cudaErrorNotReady) CK(e);
+      if (waitSpinUs != UINT32_MAX &&
+          std::chrono::steady_clock::now() - start > std::chrono::microseconds(waitSpinUs))
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
     }
   }
 
@@ -1557,6 +1567,13 @@ int drape_cuda_set_precond_schedule(drape_solver* s, int refresh_every, int jaco
     if (jacobi_first < 0) throw std::invalid_argument("jacobi_first must be >= 0");
     s->precondRefresh = refresh_every;
     s->precondSwitch = jacobi_first;
+  });
+}
+
+int drape_cuda_set_host_wait(drape_solver* s, uint32_t spin_microseconds) {
+  return guarded(s, [&] {
+    need(s);
+    s->waitSpinUs = spin_microseconds;
   });
 }
 

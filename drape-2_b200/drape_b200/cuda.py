@@ -84,6 +84,7 @@ def load(build_if_missing: bool = True):
     L.drape_cuda_test_barrier_timeout.argtypes = [C.c_int, C.c_int, C.c_uint64, _P(C.c_int)]
     L.drape_cuda_inject_failure.argtypes = [C.c_void_p, C.c_int]
     L.drape_cuda_set_pcg_variant.argtypes = [C.c_void_p, C.c_int]
+    L.drape_cuda_set_host_wait.argtypes = [C.c_void_p, C.c_uint32]
     L.drape_cuda_reduction_floor.argtypes = [C.c_int, C.c_int, C.c_int, _P(_d)]
     L.drape_cuda_cg_history.argtypes = [C.c_void_p, _P(_i32), C.c_size_t, _P(C.c_size_t)]
     L.drape_cuda_stream.argtypes = [C.c_void_p, _P(C.c_void_p)]
@@ -313,6 +314,10 @@ class CudaSolver:
 
     def set_precond_schedule(self, refresh_every: int = 1, jacobi_first: int = 0) -> None:
         self._check(self.L.drape_cuda_set_precond_schedule(self.h, int(refresh_every), int(jacobi_first)))
+
+    def set_host_wait(self, spin_microseconds: int) -> None:
+        """Host wait: poll for up to spin_microseconds, then sleep between polls (2**32 - 1: poll only)."""
+        self._check(self.L.drape_cuda_set_host_wait(self.h, int(spin_microseconds)))
 
     def set_pcg_variant(self, variant: int) -> None:
         """0: the reference-order block-Jacobi PCG (default); 1: pipelined, one grid exchange per iteration."""

@@ -212,6 +212,10 @@ int drape_cuda_pcg_noalloc(uint32_t n, uint32_t slots, const uint32_t* d_row_sta
                            const uint8_t* d_active, const void* d_normals, const void* d_grad, int max_iterations,
                            double tolerance, void* d_step, void* d_resid, int32_t* d_iterations, void* stream);
 
+/* How the host waits for the solver's stream (no reference counterpart): it polls for up to `spin_microseconds`, then
+   sleeps 20 us between polls (default 200; UINT32_MAX polls without sleeping). Results do not depend on it. */
+int drape_cuda_set_host_wait(drape_solver* s, uint32_t spin_microseconds);
+
 /* The block-Jacobi PCG's form (no reference counterpart; both solve the reference's contact-filtered system with its
    stopping tests, cpu_solver.cpp:169-213): 0 (the default) the reference's order, two grid-wide exchanges per
    iteration; 1 pipelined (Ghysels and Vanroose 2014), the same iterates in exact arithmetic with one exchange per
