@@ -329,3 +329,18 @@ def test_drape_to_rest_frame_batches_match_one_frame_per_wait(gpu, scene_name):
         assert res == ref_res, (fpw, res, ref_res)
         for key in ("positions", "velocities", "contact_force", "phases", "assembly_time", "seam_start_gap"):
             assert np.array_equal(snap[key], ref_snap[key]), (fpw, key)
+
+
+def test_host_wait_mode_does_not_change_results(gpu):
+    """The host's wait for the stream (poll only, or poll then sleep) changes when the host sees the work done, never
+    the work: 20 frames of the sheet drop give bit-identical positions either way."""
+    out = []
+    for spin in (2**32 - 1, 0, 200):
+        s = gpu.CudaSolver(0)
+        s.set_host_wait(spin)
+        s.build(S.sheet_on_sphere(cg_tolerance=1e-2, max_cg=50))
+        for _ in range(20):
+            s.step(1 / 60, 1, 2)
+        out.append(s.positions())
+        s.close()
+    assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])
