@@ -417,7 +417,7 @@ def deviation_leg(CU, device, jacobi_final=None, variant=0):
                                f"start) vs the oracle's settled shapes (faithful {int(F['c3drape_frames_faithful'])}, "
                                f"FP64 {int(F['c3drape_frames_fp64'])} frames)")
     out["bar_mm"] = 1.0
-    out["pcg"] = "pipelined" if variant == 1 else "reference order"
+    out["pcg"] = {0: "reference order", 1: "pipelined", 2: "Chronopoulos-Gear"}[variant]
     return out
 
 
@@ -685,8 +685,9 @@ def main():
     ap.add_argument("--refresh-every", type=int, default=1,
                     help="learned leg: run the network every this many Newton iterations")
     ap.add_argument("--no-deviation", action="store_true", help="skip the deviation-from-the-oracle leg")
-    ap.add_argument("--pcg-variant", type=int, choices=[0, 1], default=0,
-                    help="block-Jacobi PCG form: 0 the reference's order, 1 pipelined (one grid exchange an iteration)")
+    ap.add_argument("--pcg-variant", type=int, choices=[0, 1, 2], default=0,
+                    help="block-Jacobi PCG form: 0 the reference's order, 1 pipelined (one grid exchange an iteration), "
+                         "2 Chronopoulos-Gear (one reduction and one plain barrier)")
     ap.add_argument("--batch-garments", type=int, default=64, help="garments of the batched leg (0: skip it)")
     ap.add_argument("--profile-case", choices=["spmv", "batch", "bake", "drape", "learned"], default=None,
                     help="run one small case for a profiler capture instead of the benchmark")
@@ -818,11 +819,13 @@ def main():
     # per PCG iteration is set by the grid-wide exchanges. The PCG loop's own device time (%globaltimer, block 0) per
     # iteration is set beside the measured floor of the same exchanges on the same grid with no other work.
     pcg_us = counters.pcg_nanoseconds / 1000.0 / max(1, counters.cg_iterations)
-    floor_mode = 2 if args.pcg_variant == 1 else 0
+    floor_mode = {0: 0, 1: 2, 2: 1}[args.pcg_variant]
     floor_us = statistics.median(CU.reduction_floor(local, floor_mode, 4000) for _ in range(3))
     latency = {"kernel": "k_solve PCG loop", "us_per_pcg_iteration": pcg_us, "floor_us": floor_us,
-               "floor": ("one three-value FP64 grid reduction per iteration (pipelined PCG)" if floor_mode == 2 else
-                         "two FP64 grid reductions per iteration (reference-order PCG)"),
+               "floor": {0: "two FP64 grid reductions per iteration (reference-order PCG)",
+                         2: "one three-value FP64 grid reduction per iteration (pipelined PCG)",
+                         1: "one three-value FP64 grid reduction and one plain barrier per iteration "
+                            "(Chronopoulos-Gear PCG)"}[floor_mode],
                "frac_of_floor": floor_us / pcg_us if pcg_us else None,
                "onchip_bytes_per_iteration": ab["pcg_iter"],
                "onchip_gbs": ab["pcg_iter"] / (pcg_us * 1e-6) / 1e9 if pcg_us else None,
@@ -875,8 +878,10 @@ def main():
         "ms_per_step": value * 1000.0, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64", "data": "synthetic",
         "config": {"workload": WORKLOADS[args.workload]["desc"], "precond": "block-Jacobi",
-                   "pcg": ("pipelined (one grid exchange per iteration)" if args.pcg_variant == 1 else
-                           "reference order (two grid exchanges per iteration)"),
+                   "pcg": {0: "reference order (two grid reductions per iteration)",
+                           1: "pipelined (one grid reduction per iteration)",
+                           2: "Chronopoulos-Gear (one grid reduction and one plain barrier per iteration)"}[
+                               args.pcg_variant],
                    "start_states": SEED_DESC,
                    "precision": "FP32 blocks/SpMV/vectors, FP64 dots, FP64 energy/slope/line search",
                    "l2": "256 MB buffer written between timed drapes (L2 flushed)",

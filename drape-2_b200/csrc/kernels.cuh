@@ -96,7 +96,7 @@ struct Params {
   uint32_t n, nStretch, nHinge, nSeam, nBlocks, nGarments, slotsPadded;
   uint32_t smemSlots;   // k_solve: block slots a block keeps in shared memory
   int learnedSwitch;    // k_solve<true>: block-Jacobi iterations before the learned preconditioner takes over
-  int pcgVariant;       // the solve kernel chosen for block-Jacobi: 0 reference order, 1 pipelined (kept in the view
+  int pcgVariant;       // the solve kernel chosen for block-Jacobi: 0 reference order, 1 pipelined, 2 Chronopoulos-Gear (kept in the view
                         // so that captured frame graphs are recaptured when it changes)
   unsigned long long barrierLimitNs;
 };
@@ -1015,6 +1015,78 @@ __device__ inline int pcgPipelined(const Dev& D, GridSync& gs, const SmemMatrix&
   return it;
 }
 
+// Contact-filtered block-Jacobi PCG in the Chronopoulos-Gear form ("s-step iterative methods for symmetric linear
+// systems", J. Comput. Appl. Math. 25 (1989) 153-168): the same iterates and stopping tests as pcgReferenceOrder in
+// exact arithmetic. Each iteration forms w = F A z exactly (the only gather), reduces r.z, w.z and r.r in one FP64 grid
+// reduction, and takes alpha = (r.z) / (w.z - beta (r.z) / alpha_prev) (= r.z / p.Ap) with beta = (r.z) / (r.z)_prev;
+// A p is carried as s = w + beta s, as the reference-order form carries it. The exchange that publishes the new z is a
+// plain barrier instead of the reference order's second reduction. resid = -grad - A step is formed after the loop.
+// Vectors: x = step, r = r, z = z, p = p0, s = ap, w = apFull. Returns the iteration count, or -1 when a grid barrier
+// gave up.
+template <int PL>
+__device__ inline int pcgSingleReduction(const Dev& D, GridSync& gs, const SmemMatrix& A) {
+  uint32_t r0i, r1i;
+  blockRange(D.P.n, gs.rank, gs.size, r0i, r1i);
+  float4 *x = D.step, *r = D.r, *z = D.z, *p = D.p0, *s = D.ap, *w = D.apFull;
+  for (uint32_t i = r0i + threadIdx.x; i < r1i; i += blockDim.x) {
+    const Contact c = D.contact[i];
+    const float3 ri = filterContact(c, -ld3(D.grad, i));
+    x[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    r[i] = f4(ri);
+    z[i] = f4(filterContact(c, mul(loadPrecond(D, i), ri)));
+  }
+  if (!gs.sync()) return -1;
+  double r0 = 0.0, gammaPrev = 0.0, alphaPrev = 0.0;
+  int it = 0;
+  while (true) {
+    // w = F A z and the three partials.
+    double v[3] = {0.0, 0.0, 0.0};
+    directionProducts<PL>(
+        D, A, r0i, r1i, [&](uint32_t j) { return ld3(z, j); },
+        [&](uint32_t i, float3 zi, float3 az) {
+          const float3 wi = filterContact(D.contact[i], az);
+          const float3 ri = ld3(r, i);
+          w[i] = f4(wi);
+          v[0] += dotd3(ri, zi);
+          v[1] += dotd3(wi, zi);
+          v[2] += dotd3(ri, ri);
+        });
+    double t[3];
+    if (!gridReduce<3>(D, gs, v, t)) return -1;
+    if (it == 0) r0 = sqrt(t[2]);
+    if (!(r0 > 0.0)) break;
+    if (it > 0 && sqrt(t[2]) <= D.P.cgTolerance * r0) break;
+    if (it >= D.P.maxCg) break;
+    const double gamma = t[0];
+    const double beta = it == 0 ? 0.0 : gamma / gammaPrev;
+    const double pAp = it == 0 ? t[1] : t[1] - beta * gamma / alphaPrev;
+    if (!(pAp > 0.0)) break;
+    const double alpha = gamma / pAp;
+    const float fa = static_cast<float>(alpha), fb = static_cast<float>(beta);
+    const bool first = it == 0;
+    for (uint32_t i = r0i + threadIdx.x; i < r1i; i += blockDim.x) {
+      const Contact c = D.contact[i];
+      const float3 pi = first ? ld3(z, i) : ld3(z, i) + ld3(p, i) * fb;
+      p[i] = f4(pi);
+      const float3 si = first ? ld3(w, i) : ld3(w, i) + ld3(s, i) * fb;
+      s[i] = f4(si);
+      x[i] = f4(ld3(x, i) + pi * fa);
+      const float3 ri = ld3(r, i) - si * fa;
+      r[i] = f4(ri);
+      z[i] = f4(filterContact(c, mul(loadPrecond(D, i), ri)));
+    }
+    ++it;
+    gammaPrev = gamma;
+    alphaPrev = alpha;
+    if (!gs.sync()) return -1;
+  }
+  // resid = -grad - A step over unpinned rows and columns; the last exchange has published every block's x.
+  directionProducts<PL>(
+      D, A, r0i, r1i, [&](uint32_t j) { return ld3(x, j); },
+      [&](uint32_t i, float3, float3 ax) { D.resid[i] = f4(-ld3(D.grad, i) - ax); });
+  return it;
+}
+
 // z = F(L L^T r) over this block's rows, with L the learned factor (planes D.Lf, lower slots) and y = L^T r kept in
 // D.ap between the two products; returns false when a grid barrier gave up. Adds r.z of its rows to *rz.
 template <int RL>
@@ -1163,7 +1235,8 @@ __device__ inline int pcgLearned(const Dev& D, GridSync& gs, const SmemMatrix& A
 // the remaining iteration budget; a learned phase that stalls is followed by a full block-Jacobi solve. Returns the
 // total iteration count of all phases, or -1 when a barrier gave up.
 // Variant (block-Jacobi only): 0 the reference's order (pcgReferenceOrder), 1 pipelined (pcgPipelined; needs the
-// pm0/pm1/pz vectors). A compile-time choice, so each solve kernel carries one PCG's registers.
+// pm0/pm1/pz vectors), 2 Chronopoulos-Gear (pcgSingleReduction). A compile-time choice, so each solve kernel carries
+// one PCG's registers.
 template <bool Learned, int PL, int Variant>
 __device__ inline int pcgSolveStaged(const Dev& D, GridSync& gs, const SmemMatrix& A);
 
@@ -1183,6 +1256,8 @@ __device__ inline int pcgSolveStaged(const Dev& D, GridSync& gs, const SmemMatri
   if constexpr (!Learned) {
     if constexpr (Variant == 1) {
       return pcgPipelined<PL>(D, gs, A);
+    } else if constexpr (Variant == 2) {
+      return pcgSingleReduction<PL>(D, gs, A);
     } else {
       return pcgReferenceOrder<PL>(D, gs, A);
     }

@@ -160,6 +160,7 @@ struct drape_solver {
     // The solve kernels keep their rows' matrix blocks in shared memory: as many slots as the opt-in limit leaves.
     const void* solveKernels[] = {reinterpret_cast<const void*>(dcu::k_solve<false, 0>),
                                   reinterpret_cast<const void*>(dcu::k_solve<false, 1>),
+                                  reinterpret_cast<const void*>(dcu::k_solve<false, 2>),
                                   reinterpret_cast<const void*>(dcu::k_solve<true, 0>),
                                   reinterpret_cast<const void*>(dcu::k_pcg_only)};
     size_t staticSmem = 0;
@@ -428,6 +429,8 @@ struct drape_solver {
       CK(cudaLaunchKernelEx(&cfg, dcu::k_solve<true, 0>, d));
     } else if (d.P.pcgVariant == 1) {
       CK(cudaLaunchKernelEx(&cfg, dcu::k_solve<false, 1>, d));
+    } else if (d.P.pcgVariant == 2) {
+      CK(cudaLaunchKernelEx(&cfg, dcu::k_solve<false, 2>, d));
     } else {
       CK(cudaLaunchKernelEx(&cfg, dcu::k_solve<false, 0>, d));
     }
@@ -1580,7 +1583,8 @@ int drape_cuda_set_host_wait(drape_solver* s, uint32_t spin_microseconds) {
 int drape_cuda_set_pcg_variant(drape_solver* s, int variant) {
   return guarded(s, [&] {
     need(s);
-    if (variant != 0 && variant != 1) throw std::invalid_argument("PCG variant must be 0 (reference order) or 1 (pipelined)");
+    if (variant < 0 || variant > 2)
+      throw std::invalid_argument("PCG variant must be 0 (reference order), 1 (pipelined) or 2 (Chronopoulos-Gear)");
     s->pcgVariant = variant;
     s->dev.P.pcgVariant = variant;  // the frame graphs compare the device view and recapture
   });

@@ -216,10 +216,12 @@ int drape_cuda_pcg_noalloc(uint32_t n, uint32_t slots, const uint32_t* d_row_sta
    sleeps 20 us between polls (default 200; UINT32_MAX polls without sleeping). Results do not depend on it. */
 int drape_cuda_set_host_wait(drape_solver* s, uint32_t spin_microseconds);
 
-/* The block-Jacobi PCG's form (no reference counterpart; both solve the reference's contact-filtered system with its
-   stopping tests, cpu_solver.cpp:169-213): 0 (the default) the reference's order, two grid-wide exchanges per
-   iteration; 1 pipelined (Ghysels and Vanroose 2014), the same iterates in exact arithmetic with one exchange per
-   iteration and three more work vectors, rounding differently. The learned preconditioner always runs its own PCG. */
+/* The block-Jacobi PCG's form (no reference counterpart; each solves the reference's contact-filtered system with its
+   stopping tests, cpu_solver.cpp:169-213): 0 (the default) the reference's order, two grid-wide reductions per
+   iteration; 1 pipelined (Ghysels and Vanroose 2014), one reduction per iteration and three more work vectors, its
+   FP32 recurrences drifting further from the products they stand for; 2 Chronopoulos-Gear, one reduction and one plain
+   barrier per iteration with the reference order's recurrences. All three give the same iterates in exact
+   arithmetic and round differently. The learned preconditioner always runs its own PCG. */
 int drape_cuda_set_pcg_variant(drape_solver* s, int variant);
 
 /* The bounded wait of the device grid barrier, in nanoseconds (0 restores the default of 2 s). A kernel whose barrier

@@ -95,7 +95,7 @@ def expect_parity(gpu, oracle_mod, key, scene, variant, start=None, informationa
     return apart, rms, spread
 
 
-VARIANTS = [0, 1]  # the reference-order PCG (the parity path) and the pipelined one
+VARIANTS = [0, 1, 2]  # the reference-order PCG (the parity path), the pipelined one, the Chronopoulos-Gear one
 # The pipelined PCG carries A p, M A p and A M A p by FP32 recurrences whose rounding drifts from the products they
 # stand for (its Newton steps take about 4x the reference order's line-search halvings on the 60k drape); on a settled
 # drape's 60-frame continuation a few contact particles then end several mm from the oracle (measured 4.8 mm on the 10k
@@ -133,7 +133,7 @@ def test_tube10k_from_settled_60_frames(gpu, oracle_mod, variant):
         _SETTLED_10K["start"] = o.snapshot()
     apart, rms, spread = expect_parity(gpu, oracle_mod, "tube10k", scene, variant, start=_SETTLED_10K["start"])
     assert rms < BAR_M, rms
-    if variant == 0:  # the parity path; the pipelined form's FP32 recurrences drift further
+    if variant != 1:  # the pipelined form's FP32 recurrences drift further
         assert apart <= max(BAR_M, 3.0 * spread), (apart, spread)
     else:
         assert apart <= PIPELINED_MAX_BAR_M, apart
@@ -159,12 +159,14 @@ def test_tube60k_from_settled_60_frames(gpu, variant):
     assert apart <= max(BAR_M, 3.0 * spread), (apart, spread)
 
 
-def test_pipelined_pcg_tracks_reference_order_one_frame(gpu):
-    """One frame of the 10k tube drop with each PCG form: the pipelined one is the reference-order PCG up to rounding
-    (same Newton iteration count, PCG counts within one per solve, positions within 1e-4 m: a solve that stops one
-    iteration apart at the 1e-2 tolerance moves the step by up to about 1 % of its length)."""
+@pytest.mark.parametrize("variant", [1, 2])
+def test_pcg_forms_track_reference_order_one_frame(gpu, variant):
+    """One frame of the 10k tube drop with each PCG form: the pipelined and Chronopoulos-Gear forms are the
+    reference-order PCG up to rounding (same Newton iteration count, PCG counts within one per solve, positions within
+    1e-4 m: a solve that stops one iteration apart at the 1e-2 tolerance moves the step by up to about 1 % of its
+    length)."""
     out = []
-    for variant in VARIANTS:
+    for variant in (0, variant):
         s = cuda_solver(gpu, variant)()
         s.build(S.tube_10k())
         s.set_phase("tube", 0)
