@@ -82,6 +82,7 @@ struct Control {
   int pad;
   long long learnedSolves, precondFallbacks;  // PCG solves with the learned preconditioner; of those, restarted
   long long pcgNs;  // %globaltimer nanoseconds inside the PCG solves (block 0's view: CG init to the last iteration)
+  unsigned long long frameBeginNs;  // %globaltimer at the current frame's first kernel (0: not started)
 };
 
 constexpr unsigned int kCgLogCapacity = 1u << 16;  // PCG iterations per Newton iteration, ring buffer
@@ -1389,6 +1390,7 @@ struct StatsOut {
   unsigned long long moving;
   int nonFinite;
   int pad;
+  unsigned long long beginNs, endNs;  // %globaltimer at the frame's first kernel and at its statistics' end
 };
 
 }  // namespace dcu

@@ -436,7 +436,7 @@ struct drape_solver {
     }
   }
 
-  // Frame graphs: one frame's launches (its substeps, then the statistics into slot f) captured once per slot and
+  // Frame graphs: one frame's launches (its substeps, then the statistics into device slot f) captured once per slot and
   // replayed, one graph launch a frame instead of a dozen kernel launches. A graph is recaptured when the device view
   // or a launch parameter it was captured with changes; profiling and the learned preconditioner launch directly.
   struct FrameGraph {
@@ -462,7 +462,7 @@ struct drape_solver {
       CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
       try {
         for (int k = 0; k < substeps; ++k) enqueueSubstep(h, iterations, false);
-        enqueueStats(slot);
+        enqueueStats(slot, false);
       } catch (...) {
         cudaStreamEndCapture(stream, &graph);
         if (graph) cudaGraphDestroy(graph);
@@ -489,7 +489,6 @@ struct drape_solver {
       g.barrierLimitNs = barrierLimitNs;
     }
     CK(cudaGraphLaunch(g.exec, stream));
-    d2hBytes += sizeof(dcu::StatsOut);
     for (int k = 0; k < substeps; ++k) advanceHostClock(h);
     return true;
   }
@@ -590,13 +589,18 @@ struct drape_solver {
     readControl();
   }
 
-  void enqueueStats(int slot = 0) {
+  // The statistics of the state after this frame into device slot `slot`; with `copy`, also to the host slot. A batch
+  // of frames copies its slots once at its end (advanceFrames), so the stream carries one small device-to-host copy
+  // per batch instead of one per frame.
+  void enqueueStats(int slot = 0, bool copy = true) {
     cudaEvent_t e = profStart(5);
     dcu::k_stats<<<statsGrid, 256, 0, stream>>>(dev, statsPartials.p, statsDone.p, statsOut.p + slot);
     CK(cudaGetLastError());
     profStop(e, 5);
-    CK(cudaMemcpyAsync(hStats.p + slot, statsOut.p + slot, sizeof(dcu::StatsOut), cudaMemcpyDeviceToHost, stream));
-    d2hBytes += sizeof(dcu::StatsOut);
+    if (copy) {
+      CK(cudaMemcpyAsync(hStats.p + slot, statsOut.p + slot, sizeof(dcu::StatsOut), cudaMemcpyDeviceToHost, stream));
+      d2hBytes += sizeof(dcu::StatsOut);
+    }
   }
 
   drape_stats stats() {
@@ -628,15 +632,26 @@ struct drape_solver {
     for (int f = 0; f < frames; ++f) {
       if (launchFrameGraph(h, sub, its, f)) continue;
       for (int k = 0; k < sub; ++k) enqueueSubstep(h, its);
-      enqueueStats(f);
+      enqueueStats(f, false);
     }
+    CK(cudaMemcpyAsync(hStats.p, statsOut.p, sizeof(dcu::StatsOut) * frames, cudaMemcpyDeviceToHost, stream));
+    d2hBytes += sizeof(dcu::StatsOut) * frames;
     CK(cudaMemcpyAsync(hCtl.p, ctl.p, sizeof(dcu::Control), cudaMemcpyDeviceToHost, stream));
     d2hBytes += sizeof(dcu::Control);
     waitStream();
     collectProfile();
     checkControl();
-    for (int f = 0; f < frames; ++f) out[f] = hostStats(f);
+    for (int f = 0; f < frames; ++f) {
+      out[f] = hostStats(f);
+      if (frameTimes.size() < kFrameTimeCapacity) frameTimes.push_back({hStats.p[f].beginNs, hStats.p[f].endNs});
+    }
   }
+
+  // Device timestamps (%globaltimer, ns) of the frames run in batches since the last read: the frame's first kernel
+  // and the end of its statistics. Consecutive frames show the device-side duration of each frame and the idle time
+  // between frames.
+  static constexpr size_t kFrameTimeCapacity = 1u << 16;
+  std::vector<std::pair<unsigned long long, unsigned long long>> frameTimes;
 
   drape_stats advanceWithStats(double dt, int substeps, int iterations) {
     drape_stats st{};
@@ -1570,6 +1585,20 @@ int drape_cuda_set_precond_schedule(drape_solver* s, int refresh_every, int jaco
     if (jacobi_first < 0) throw std::invalid_argument("jacobi_first must be >= 0");
     s->precondRefresh = refresh_every;
     s->precondSwitch = jacobi_first;
+  });
+}
+
+int drape_cuda_frame_times(drape_solver* s, uint64_t* begin_ns, uint64_t* end_ns, size_t capacity, size_t* count) {
+  return guarded(s, [&] {
+    need(s);
+    if (!count || (capacity && (!begin_ns || !end_ns))) throw std::invalid_argument("null argument");
+    const size_t k = std::min(capacity, s->frameTimes.size());
+    for (size_t i = 0; i < k; ++i) {
+      begin_ns[i] = s->frameTimes[i].first;
+      end_ns[i] = s->frameTimes[i].second;
+    }
+    *count = k;
+    s->frameTimes.clear();
   });
 }
 

@@ -6,7 +6,10 @@
 
 namespace dcu {
 
-__global__ void k_begin(Dev D) { beginRows(D, blockIdx.x, gridDim.x); }
+__global__ void k_begin(Dev D) {
+  if (blockIdx.x == 0 && threadIdx.x == 0 && D.ctl->frameBeginNs == 0ull) D.ctl->frameBeginNs = globalTimerNs();
+  beginRows(D, blockIdx.x, gridDim.x);
+}
 
 // Contact candidates for given positions (test entry point; same code as k_begin).
 __global__ void k_contact_candidates(Dev D, const float4* xs, Contact* out) {
@@ -140,6 +143,9 @@ __global__ void k_stats(Dev D, double* part, unsigned int* done, StatsOut* out) 
     s.maxSeamGap = tot2[0];
     s.maxPenetration = tot2[1];
     s.nonFinite = nonFinite != 0;
+    s.beginNs = D.ctl->frameBeginNs;
+    s.endNs = globalTimerNs();
+    D.ctl->frameBeginNs = 0ull;
     *out = s;
     *done = 0;
   }

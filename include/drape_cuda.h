@@ -212,6 +212,12 @@ int drape_cuda_pcg_noalloc(uint32_t n, uint32_t slots, const uint32_t* d_row_sta
                            const uint8_t* d_active, const void* d_normals, const void* d_grad, int max_iterations,
                            double tolerance, void* d_step, void* d_resid, int32_t* d_iterations, void* stream);
 
+/* Measurement hook (no reference counterpart): device timestamps (%globaltimer, ns) of the frames run in batches
+   (drape_cuda_drape_to_rest) since the last call: begin = the frame's first kernel, end = the end of its statistics
+   kernel. end - begin is the frame's device-side duration; the next frame's begin minus this end is the device's idle
+   time between them. Writes min(capacity, recorded) pairs, sets *count, and clears the record. */
+int drape_cuda_frame_times(drape_solver* s, uint64_t* begin_ns, uint64_t* end_ns, size_t capacity, size_t* count);
+
 /* How the host waits for the solver's stream (no reference counterpart): it polls for up to `spin_microseconds`, then
    sleeps 20 us between polls (default 200; UINT32_MAX polls without sleeping). Results do not depend on it. */
 int drape_cuda_set_host_wait(drape_solver* s, uint32_t spin_microseconds);
