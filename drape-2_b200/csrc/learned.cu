@@ -1495,9 +1495,9 @@ void Network::forwardOn(Graph& g, cudaStream_t st, bool training, int* error) {
   const int cap = 2 * numSMs_;
   const __nv_bfloat16* W = wBf16_;
   const float* M = master_;
-  k_encode<<<gridFor((g.n + 127) / 128, cap), kThreads, smemFor(sizeof(EncodeSmem)), st>>>(
+  k_encode<<<gridFor((g.n + 127) / 128, 4 * numSMs_), kThreads, smemFor(sizeof(EncodeSmem)), st>>>(
       g.n, g.f, W + Layout::kNe, M + Layout::kNeB, g.h[0], error_);
-  k_encode<<<gridFor((g.B + 127) / 128, cap), kThreads, smemFor(sizeof(EncodeSmem)), st>>>(
+  k_encode<<<gridFor((g.B + 127) / 128, 4 * numSMs_), kThreads, smemFor(sizeof(EncodeSmem)), st>>>(
       g.B, g.e, W + Layout::kEe, M + Layout::kEeB, g.eps, error_);
   for (int l = 0; l < kLayers; ++l) {
     const __nv_bfloat16* hin = training ? g.h[l] : g.h[l & 1];
@@ -1506,7 +1506,8 @@ void Network::forwardOn(Graph& g, cudaStream_t st, bool training, int* error) {
         g, W + Layout::m(l), W + Layout::u(l), M + Layout::mB(l), M + Layout::uB(l), hin, hout,
         training ? g.agg[l] : nullptr, error_);
   }
-  k_output<<<gridFor(g.nTiles, cap), kThreads, smemFor(sizeof(OutputSmem)), st>>>(
+  // k_output's 57 KB of shared memory fit three blocks on an SM (k_layer's 100 KB fit two: `cap`).
+  k_output<<<gridFor(g.nTiles, 3 * numSMs_), kThreads, smemFor(sizeof(OutputSmem)), st>>>(
       g, W + Layout::kO, M + Layout::kOB, training ? g.h[kLayers] : g.h[kLayers & 1], training ? 1 : 0, error_);
   NCK(cudaGetLastError());
 }
