@@ -652,6 +652,9 @@ struct drape_solver {
   // between frames.
   static constexpr size_t kFrameTimeCapacity = 1u << 16;
   std::vector<std::pair<unsigned long long, unsigned long long>> frameTimes;
+  // Host seconds of the last drape_to_rest: [0] set-up (phase change, first snapshot), [1] the frame loop, [2] the
+  // return (everything after the loop).
+  double runnerHostSeconds[3] = {0.0, 0.0, 0.0};
 
   drape_stats advanceWithStats(double dt, int substeps, int iterations) {
     drape_stats st{};
@@ -723,6 +726,9 @@ struct drape_solver {
     std::vector<double> assemblyTime;
     std::vector<float> seamStartGap;
   };
+  // The drape runner's snapshots (the retry snapshot and a batch's start), kept across drapes so that a drape
+  // allocates and frees no device memory (cudaFree synchronises the device, and either call can stall the host).
+  DeviceSnapshot runnerSaved, runnerBatchStart;
 
   void saveTo(DeviceSnapshot& s) {
     const size_t n = m.x.size();
@@ -763,13 +769,25 @@ struct drape_solver {
     CK(cudaStreamSynchronize(stream));
   }
 
-  // Phase change without a full host round trip: seam start gaps need the current positions.
+  // Phase change without a full host round trip. Model::setPhase reads positions (the seams' start gaps) and writes
+  // only the garment's phase and assembly time and its seams' start gaps, so Assembling downloads the positions and
+  // uploads the garment and seam tables; nothing else of the model changes.
   void setPhase(const std::string& id, int phase) {
     requireBuilt();
     if (phase == DRAPE_PHASE_ASSEMBLING) {
-      syncToModel();
+      use();
+      const size_t n = m.x.size();
+      std::vector<float4> xs(n);
+      if (n) {
+        CK(cudaMemcpyAsync(xs.data(), x.p, sizeof(float4) * n, cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        d2hBytes += sizeof(float4) * n;
+      }
+      for (size_t i = 0; i < n; ++i) m.x[i] = {xs[i].x, xs[i].y, xs[i].z};
       m.setPhase(id, phase);
-      syncFromModel();
+      garment.upload(garmentData(), stream);
+      seam.upload(seamData(), stream);
+      CK(cudaStreamSynchronize(stream));
     } else {
       m.setPhase(id, phase);
       use();
@@ -809,14 +827,16 @@ drape_drape_result drapeToRest(drape_solver& s, const std::vector<std::string>& 
   auto setAll = [&](int phase) {
     for (const auto& g : garments) s.setPhase(g, phase);
   };
+  const auto tStart = std::chrono::steady_clock::now();
   setAll(DRAPE_PHASE_ASSEMBLING);
   struct Saved {
-    drape_solver::DeviceSnapshot snap;
+    drape_solver::DeviceSnapshot& snap;
     double time = 0;
     int phase = DRAPE_PHASE_ASSEMBLING;
     double phaseTime = 0;
-  } saved;
+  } saved{s.runnerSaved};
   s.saveTo(saved.snap);
+  const auto tLoop = std::chrono::steady_clock::now();
   int state = DRAPE_STATE_ASSEMBLING, phase = DRAPE_PHASE_ASSEMBLING;
   double time = 0, phaseTime = 0, lastEnergy = INFINITY;
   int substeps = o.substeps, stillFrames = 0, riseFrames = 0, keptFrames = 0;
@@ -836,7 +856,7 @@ drape_drape_result drapeToRest(drape_solver& s, const std::vector<std::string>& 
   // the one-frame-per-wait runner's, frame for frame. The learned preconditioner refreshes on a Newton-iteration
   // count, which a replay would shift, so it keeps one frame per wait.
   const int perWait = s.learnedOn ? 1 : std::clamp(o.frames_per_wait, 1, drape_solver::kFrameSlots);
-  drape_solver::DeviceSnapshot batchStart;
+  drape_solver::DeviceSnapshot& batchStart = s.runnerBatchStart;
   drape_stats frameStats[drape_solver::kFrameSlots], replayStats[drape_solver::kFrameSlots];
   // The last two frames' seam gaps while Assembling: a batch stops at the frame where their trend meets
   // seam_gap_done, so the phase change seldom needs a replay.
@@ -945,6 +965,9 @@ drape_drape_result drapeToRest(drape_solver& s, const std::vector<std::string>& 
       state = phase == DRAPE_PHASE_ASSEMBLING ? DRAPE_STATE_ASSEMBLING : DRAPE_STATE_SETTLING;
     }
   }
+  const auto tEnd = std::chrono::steady_clock::now();
+  s.runnerHostSeconds[0] = std::chrono::duration<double>(tLoop - tStart).count();
+  s.runnerHostSeconds[1] = std::chrono::duration<double>(tEnd - tLoop).count();
   return result;
 }
 
@@ -1178,7 +1201,17 @@ int drape_cuda_drape_to_rest(drape_solver* s, const char* const* garments, uint3
     const drape_drape_options o = options ? *options : defaultOptions();
     if (!(o.frame_dt > 0) || o.snapshot_every < 1 || o.substeps < 1)
       throw std::invalid_argument("frame_dt, substeps and snapshot_every must be positive");
+    const auto t0 = std::chrono::steady_clock::now();
     *out = drapeToRest(*s, ids, o);
+    s->runnerHostSeconds[2] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() -
+                              s->runnerHostSeconds[0] - s->runnerHostSeconds[1];
+  });
+}
+
+int drape_cuda_runner_host_seconds(const drape_solver* s, double* out) {
+  return guarded(nullptr, [&] {
+    if (!s || !out) throw std::invalid_argument("null argument");
+    for (int k = 0; k < 3; ++k) out[k] = s->runnerHostSeconds[k];
   });
 }
 

@@ -85,6 +85,7 @@ def load(build_if_missing: bool = True):
     L.drape_cuda_inject_failure.argtypes = [C.c_void_p, C.c_int]
     L.drape_cuda_set_pcg_variant.argtypes = [C.c_void_p, C.c_int]
     L.drape_cuda_set_host_wait.argtypes = [C.c_void_p, C.c_uint32]
+    L.drape_cuda_runner_host_seconds.argtypes = [C.c_void_p, _P(_d)]
     L.drape_cuda_frame_times.argtypes = [C.c_void_p, _P(C.c_uint64), _P(C.c_uint64), C.c_size_t, _P(C.c_size_t)]
     L.drape_cuda_reduction_floor.argtypes = [C.c_int, C.c_int, C.c_int, _P(_d)]
     L.drape_cuda_cg_history.argtypes = [C.c_void_p, _P(_i32), C.c_size_t, _P(C.c_size_t)]
@@ -315,6 +316,12 @@ class CudaSolver:
 
     def set_precond_schedule(self, refresh_every: int = 1, jacobi_first: int = 0) -> None:
         self._check(self.L.drape_cuda_set_precond_schedule(self.h, int(refresh_every), int(jacobi_first)))
+
+    def runner_host_seconds(self):
+        """Host seconds of the last drape_to_rest: (set-up, frame loop, rest of the call)."""
+        out = (_d * 3)()
+        _raise(self.L.drape_cuda_runner_host_seconds(self.h, out), self.L.drape_cuda_last_error(None))
+        return tuple(out)
 
     def frame_times(self, capacity: int = 1 << 16):
         """(begin, end) device timestamps in ns of the frames run in batches since the last call, as an (n, 2) array."""

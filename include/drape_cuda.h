@@ -218,6 +218,10 @@ int drape_cuda_pcg_noalloc(uint32_t n, uint32_t slots, const uint32_t* d_row_sta
    time between them. Writes min(capacity, recorded) pairs, sets *count, and clears the record. */
 int drape_cuda_frame_times(drape_solver* s, uint64_t* begin_ns, uint64_t* end_ns, size_t capacity, size_t* count);
 
+/* Measurement hook (no reference counterpart): host seconds of the last drape_cuda_drape_to_rest, out[0] its set-up
+   (the phase change and the first snapshot), out[1] its frame loop, out[2] the rest of the call. */
+int drape_cuda_runner_host_seconds(const drape_solver* s, double* out);
+
 /* How the host waits for the solver's stream (no reference counterpart): it polls for up to `spin_microseconds`, then
    sleeps 20 us between polls (default 200; UINT32_MAX polls without sleeping). Results do not depend on it. */
 int drape_cuda_set_host_wait(drape_solver* s, uint32_t spin_microseconds);
