@@ -74,7 +74,8 @@ struct Garment {
 // Device control block: the PCG / Newton scalars every block of k_solve recomputes identically, plus counters.
 struct Control {
   int newtonDone;   // this substep's Newton loop has stopped (slope >= 0 or max move < 1e-9)
-  int error;        // 1: a grid barrier gave up waiting; 2: a row exceeded the assembly capacity
+  int error;        // 1: a grid barrier gave up waiting; 2: a row exceeded the assembly capacity; 4: a block's sliced
+                    // matrix exceeded its shared memory (k_solve_rows)
   unsigned long long barrierArrivals;
   long long cgIterations, newtonIterations, lineSearchHalvings, substeps, energyEvaluations;
   double lastAlpha, lastSlope, lastE0, lastMaxMove;
@@ -97,8 +98,10 @@ struct Params {
   uint32_t n, nStretch, nHinge, nSeam, nBlocks, nGarments, slotsPadded;
   uint32_t smemSlots;   // k_solve: block slots a block keeps in shared memory
   int learnedSwitch;    // k_solve<true>: block-Jacobi iterations before the learned preconditioner takes over
-  int pcgVariant;       // the solve kernel chosen for block-Jacobi: 0 reference order, 1 pipelined, 2 Chronopoulos-Gear (kept in the view
-                        // so that captured frame graphs are recaptured when it changes)
+  int pcgVariant;       // the solve kernel chosen for block-Jacobi: 0 reference order, 1 pipelined, 2 Chronopoulos-Gear,
+                        // 3 reference order with resident rows (kept in the view so that captured frame graphs are
+                        // recaptured when it changes)
+  uint32_t slicedSlots; // k_solve_rows: padded slots of the sliced layout a block may hold in shared memory
   unsigned long long barrierLimitNs;
 };
 
@@ -916,6 +919,206 @@ __device__ inline int pcgReferenceOrder(const Dev& D, GridSync& gs, const SmemMa
   return it;
 }
 
+// ---------------------------------------------------------------------------------------------------------------
+// Reference-order PCG with resident rows (k_solve_rows; pcgVariant 3). One thread owns one row of its block for the
+// whole solve and keeps the row's PCG state (p, A p and its filtered copy, r, step, resid, z, the contact plane and
+// the preconditioner block) in registers, so an iteration's only global traffic is the gather of z_j over the row's
+// columns and the store of the new z_i: the reference-order kernel re-reads the row vectors from L2 in both passes.
+// The block's slots sit in shared memory in a sliced layout: the rows in warps of 32, warp w's slots padded to its
+// longest row L_w, slot k of lane l at base_w + 32 k + l (nine planes, then the columns; padding holds kPinnedBit),
+// so a warp's 32 row threads read 32 consecutive words. The row's product keeps the two-lane order of
+// pcgReferenceOrder<2> (the even slots in one sum, the odd slots in another, added at the end), so the iterates are
+// that kernel's.
+constexpr int kRowThreads = 512;     // k_solve_rows block size: a block's rows must not exceed it
+constexpr int kSlicedDepth = 12;     // gathers a row thread has in flight (even, so k0 + k has the parity of k)
+
+struct SlicedMatrix {
+  const float* planes;   // 9 planes of `stride` floats
+  const uint32_t* cols;  // `stride` column indices (bit 31: pinned column or padding)
+  uint32_t stride;       // padded slots of the block
+  uint32_t base, len;    // this thread's warp: its first position and its padded row length
+};
+
+// Copies this block's rows [r0, r1) into the sliced layout (all threads; ends with a block barrier). Returns false,
+// after raising error 4, when the padded slots exceed P.slicedSlots (the host picks k_solve_rows only for scenes whose
+// every block fits, so this is a guard).
+__device__ inline bool stageSliced(const Dev& D, uint32_t r0, uint32_t r1, SlicedMatrix& A) {
+  constexpr int kWarps = kRowThreads / 32;
+  __shared__ uint32_t off[kRowThreads + 1];  // the rows' first slots, relative to the block's first
+  __shared__ uint32_t cnt[kRowThreads];      // the rows' slot counts (0 for pinned rows: they take no product)
+  __shared__ uint32_t warpLen[kWarps], warpBase[kWarps + 1];
+  const uint32_t t = threadIdx.x, lane = t & 31u, w = t >> 5;
+  const uint32_t R = r1 - r0;
+  if (R > static_cast<uint32_t>(kRowThreads) || blockDim.x != static_cast<unsigned>(kRowThreads)) {
+    if (t == 0) atomicExch(&D.ctl->error, 4);
+    return false;
+  }
+  const uint32_t first = __ldg(D.rowStart + r0);  // r0 <= n: rowStart has n + 1 entries
+  uint32_t c = 0;
+  if (t < R) {
+    const uint32_t rs = __ldg(D.rowStart + r0 + t);
+    off[t] = rs - first;
+    if (D.particle[r0 + t].pinned == 0u) c = __ldg(D.rowStart + r0 + t + 1) - rs;
+  }
+  if (t == 0) off[R] = __ldg(D.rowStart + r1) - first;
+  cnt[t] = c;
+  const uint32_t len = __reduce_max_sync(0xffffffffu, c);
+  if (lane == 0) warpLen[w] = len;
+  __syncthreads();
+  if (t == 0) {
+    uint32_t acc = 0;
+    for (int k = 0; k < kWarps; ++k) {
+      warpBase[k] = acc;
+      acc += 32u * warpLen[k];
+    }
+    warpBase[kWarps] = acc;
+  }
+  __syncthreads();
+  const uint32_t total = warpBase[kWarps];
+  if (total > D.P.slicedSlots) {
+    if (t == 0) atomicExch(&D.ctl->error, 4);
+    return false;
+  }
+  float* planes = reinterpret_cast<float*>(solveSmem);
+  uint32_t* cols = reinterpret_cast<uint32_t*>(planes + 9 * total);
+  A.planes = planes;
+  A.cols = cols;
+  A.stride = total;
+  A.base = warpBase[w];
+  A.len = warpLen[w];
+  // Padding of this thread's row: positions [c, len) of its lane.
+  for (uint32_t k = c; k < len; ++k) cols[A.base + 32u * k + lane] = kPinnedBit;
+  // The slots, read in slot order (coalesced); each finds its row by bisection over off[].
+  const uint32_t S = off[R];
+  const uint32_t SP = D.P.slotsPadded;
+  for (uint32_t k = t; k < S; k += blockDim.x) {
+    uint32_t lo = 0, hi = R;  // off[lo] <= k < off[hi]
+    while (hi - lo > 1) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (off[mid] <= k) lo = mid; else hi = mid;
+    }
+    const uint32_t j = k - off[lo];
+    if (j >= cnt[lo]) continue;  // a pinned row's slot
+    const uint32_t pos = warpBase[lo >> 5] + 32u * j + (lo & 31u);
+    const uint32_t s = first + k;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) planes[q * total + pos] = __ldg(D.blocks + q * SP + s);
+    cols[pos] = __ldg(D.colIndex + s);
+  }
+  __syncthreads();
+  return true;
+}
+
+// y_i (unfiltered) = sum over the row's unpinned columns j of A_ij x_j, for this thread's row, in pcgReferenceOrder<2>'s
+// order: slot k of the row into sum k mod 2, each sum in slot order, the odd sum added to the even one last.
+__device__ __forceinline__ float3 slicedProduct(const SlicedMatrix& A, const float4* x) {
+  float3 acc0 = mk(0, 0, 0), acc1 = mk(0, 0, 0);
+  const uint32_t lane = threadIdx.x & 31u;
+  for (uint32_t k0 = 0; k0 < A.len; k0 += kSlicedDepth) {
+    uint32_t col[kSlicedDepth];
+#pragma unroll
+    for (int k = 0; k < kSlicedDepth; ++k)
+      col[k] = k0 + k < A.len ? A.cols[A.base + 32u * (k0 + k) + lane] : kPinnedBit;
+    float3 v[kSlicedDepth];
+#pragma unroll
+    for (int k = 0; k < kSlicedDepth; ++k) v[k] = (col[k] & kPinnedBit) ? mk(0, 0, 0) : ld3(x, col[k]);
+#pragma unroll
+    for (int k = 0; k < kSlicedDepth; ++k) {
+      if (col[k] & kPinnedBit) continue;
+      const uint32_t pos = A.base + 32u * (k0 + k) + lane;
+      float a[9];
+#pragma unroll
+      for (int q = 0; q < 9; ++q) a[q] = A.planes[q * A.stride + pos];
+      float3& acc = (k & 1) ? acc1 : acc0;
+      acc.x += a[0] * v[k].x + a[1] * v[k].y + a[2] * v[k].z;
+      acc.y += a[3] * v[k].x + a[4] * v[k].y + a[5] * v[k].z;
+      acc.z += a[6] * v[k].x + a[7] * v[k].y + a[8] * v[k].z;
+    }
+  }
+  acc0.x += acc1.x;
+  acc0.y += acc1.y;
+  acc0.z += acc1.z;
+  return acc0;
+}
+
+// The reference-order PCG of pcgReferenceOrder (same recurrences, same stopping tests) over resident rows. Writes
+// step, resid, r and z of the block's rows; returns the iteration count, or -1 when a grid barrier gave up.
+__device__ inline int pcgResidentRows(const Dev& D, GridSync& gs, const SlicedMatrix& A) {
+  uint32_t r0i, r1i;
+  blockRange(D.P.n, gs.rank, gs.size, r0i, r1i);
+  const uint32_t i = r0i + threadIdx.x;
+  const bool own = i < r1i;
+  Contact c{};
+  M3 M{};
+  float3 step = mk(0, 0, 0), resid = mk(0, 0, 0), r = mk(0, 0, 0), z = mk(0, 0, 0);
+  float3 p = mk(0, 0, 0), apFull = mk(0, 0, 0), ap = mk(0, 0, 0);
+  // CG init (kernels.h:252-268): step = 0, resid = -grad, r = filter(resid), z = filter(M r).
+  double tot[2];
+  {
+    double v[2] = {0.0, 0.0};
+    if (own) {
+      c = D.contact[i];
+      M = loadPrecond(D, i);
+      resid = -ld3(D.grad, i);
+      r = filterContact(c, resid);
+      z = filterContact(c, mul(M, r));
+      D.z[i] = f4(z);
+      v[0] += dotd3(r, z);
+      v[1] += dotd3(r, r);
+    }
+    if (!gridReduce<2>(D, gs, v, tot)) return -1;
+  }
+  double rz = tot[0];
+  const double r0 = sqrt(tot[1]);
+  double beta = 0.0;
+  int it = 0;
+  const int maxCg = D.P.maxCg;
+  if (r0 > 0.0) {
+    while (it < maxCg) {
+      // A p = A z + beta A pPrev, p = z + beta pPrev (the direction update folded into the product).
+      const float fb = static_cast<float>(beta);
+      const bool firstIt = it == 0;
+      double vpap[1] = {0.0};
+      const float3 az = slicedProduct(A, D.z);
+      if (own) {
+        p = firstIt ? z : z + p * fb;
+        const float3 acc = firstIt ? az : az + apFull * fb;
+        ap = filterContact(c, acc);
+        apFull = acc;
+        vpap[0] += dotd3(p, ap);
+      }
+      double pAp[1];
+      if (!gridReduce<1>(D, gs, vpap, pAp)) return -1;
+      if (!(pAp[0] > 0.0)) break;
+      const double alpha = rz / pAp[0];
+      const float fa = static_cast<float>(alpha);
+      ++it;
+      // Update (kernels.h:304-315) fused with the preconditioner apply (kernels.h:324-332).
+      double v[2] = {0.0, 0.0};
+      if (own) {
+        step = step + p * fa;
+        r = r - ap * fa;
+        resid = resid - apFull * fa;
+        z = filterContact(c, mul(M, r));
+        D.z[i] = f4(z);
+        v[0] += dotd3(r, r);
+        v[1] += dotd3(r, z);
+      }
+      double t2[2];
+      if (!gridReduce<2>(D, gs, v, t2)) return -1;
+      if (sqrt(t2[0]) <= D.P.cgTolerance * r0) break;
+      beta = t2[1] / rz;
+      rz = t2[1];
+    }
+  }
+  if (own) {
+    D.step[i] = f4(step);
+    D.resid[i] = f4(resid);
+    D.r[i] = f4(r);
+  }
+  return it;
+}
+
 // Pipelined contact-filtered block-Jacobi PCG (Ghysels and Vanroose, "Hiding global synchronization latency in the
 // preconditioned conjugate gradient algorithm", Parallel Computing 40 (2014) 224-238, Alg. 3). In exact arithmetic
 // its iterates, iteration count and stopping tests are those of pcgReferenceOrder (operator F A F, preconditioner
@@ -1245,6 +1448,15 @@ template <bool Learned, int PL, int Variant = 0>
 __device__ inline int pcgSolve(const Dev& D, GridSync& gs) {
   uint32_t r0i, r1i;
   blockRange(D.P.n, gs.rank, gs.size, r0i, r1i);
+  if constexpr (Variant == 3) {
+    static_assert(!Learned, "resident rows: block-Jacobi only");
+    SlicedMatrix A;
+    if (!stageSliced(D, r0i, r1i, A)) return -1;
+    const unsigned long long t0 = globalTimerNs();
+    const int it = pcgResidentRows(D, gs, A);
+    if (gs.rank == 0 && threadIdx.x == 0) D.ctl->pcgNs += static_cast<long long>(globalTimerNs() - t0);
+    return it;
+  }
   const SmemMatrix A = stageMatrix(D, r0i, r1i);
   const unsigned long long t0 = globalTimerNs();
   const int it = pcgSolveStaged<Learned, PL, Variant>(D, gs, A);

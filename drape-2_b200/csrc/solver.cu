@@ -53,6 +53,27 @@ static uint32_t maxBlockSlots(const uint32_t* rowStart, uint32_t n, int grid) {
   return most;
 }
 
+// Padded slots of the sliced layout k_solve_rows stages for its largest block (the rows in warps of 32, each warp's
+// rows padded to its longest unpinned row; pinned rows take no slots), or UINT32_MAX when a block has more rows than
+// k_solve_rows has threads.
+static uint32_t maxSlicedSlots(const uint32_t* rowStart, const uint8_t* pinned, uint32_t n, int grid) {
+  const uint32_t per = (n + static_cast<uint32_t>(grid) - 1) / static_cast<uint32_t>(grid);
+  if (per > static_cast<uint32_t>(dcu::kRowThreads)) return UINT32_MAX;
+  uint32_t most = 0;
+  for (int b = 0; b < grid; ++b) {
+    const uint32_t r0 = std::min<uint32_t>(n, static_cast<uint32_t>(b) * per), r1 = std::min<uint32_t>(n, r0 + per);
+    uint32_t total = 0;
+    for (uint32_t w0 = r0; w0 < r1; w0 += 32) {
+      uint32_t len = 0;
+      for (uint32_t i = w0; i < std::min(r1, w0 + 32); ++i)
+        if (!pinned[i]) len = std::max(len, rowStart[i + 1] - rowStart[i]);
+      total += 32 * len;
+    }
+    most = std::max(most, total);
+  }
+  return most;
+}
+
 struct drape_solver {
   int device = 0;
   int numSMs = 0;
@@ -65,15 +86,17 @@ struct drape_solver {
   int failAfter = -1;
   static constexpr int kFrameSlots = 32;  // most frames one advanceFrames call runs before its host wait
   uint32_t solveSmemCap = 0;       // block slots one solve block can keep in shared memory
+  uint32_t rowsSmemCap = 0;        // padded slots one k_solve_rows block can keep in shared memory
   // Learned preconditioner: the solver's own copy of the network and its workspace on this solver's CSR.
   std::unique_ptr<net::Network> net;
   net::GraphHandle netGraph;
   bool learnedOn = false;
   int precondRefresh = 1;           // run the network on every precondRefresh-th Newton iteration
   int precondSwitch = 0;            // block-Jacobi iterations before the learned preconditioner takes over
-  int pcgVariant = 0;               // block-Jacobi PCG: 0 the reference's order, 1 pipelined (drape_cuda_set_pcg_variant)
+  int pcgVariant = 0;               // block-Jacobi PCG form (drape_cuda_set_pcg_variant)
   uint64_t netNewtonCounter = 0;
   size_t solveSmemBytes = 0;       // dynamic shared memory of the solve launch for the built scene
+  size_t rowsSmemBytes = 0;        // k_solve_rows's, when the built scene fits it (0: it does not)
 
   DBuf<dcu::Particle> particle;
   DBuf<dcu::Fabric> fabric;
@@ -177,6 +200,17 @@ struct drape_solver {
       CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k, dcu::kSolveThreads, dynMax));
       if (perSM < 1) throw std::runtime_error("cuda: the solve kernel does not fit on an SM");
     }
+    {
+      cudaFuncAttributes fa{};
+      CK(cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(dcu::k_solve_rows)));
+      rowsSmemCap = static_cast<uint32_t>((prop.sharedMemPerBlockOptin - fa.sharedSizeBytes) / dcu::kSmemSlotBytes);
+      const int rowsMax = static_cast<int>(rowsSmemCap * dcu::kSmemSlotBytes);
+      CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(dcu::k_solve_rows),
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, rowsMax));
+      int perSM = 0;
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, dcu::k_solve_rows, dcu::kRowThreads, rowsMax));
+      if (perSM < 1) throw std::runtime_error("cuda: the resident-row solve kernel does not fit on an SM");
+    }
     solveGrid = numSMs;  // one 1024-thread block per SM: fewest barrier arrivals
     pointGrid = numSMs * 8;
     statsGrid = numSMs * 2;
@@ -266,6 +300,12 @@ struct drape_solver {
     dmodel::params(m, SP, barrierLimitNs, d);
     d.P.smemSlots = std::min(solveSmemCap, maxBlockSlots(m.rowStart.data(), n, solveGrid));
     solveSmemBytes = static_cast<size_t>(d.P.smemSlots) * dcu::kSmemSlotBytes;
+    {
+      const uint32_t sliced = maxSlicedSlots(m.rowStart.data(), m.pinned.data(), n, solveGrid);
+      const bool fits = sliced <= rowsSmemCap;
+      d.P.slicedSlots = fits ? std::max<uint32_t>(sliced, 1u) : 0u;
+      rowsSmemBytes = fits ? static_cast<size_t>(d.P.slicedSlots) * dcu::kSmemSlotBytes : 0;
+    }
     d.fieldValues = fieldValues.p;
     d.particle = particle.p;
     d.fabric = fabric.p;
@@ -415,10 +455,11 @@ struct drape_solver {
   }
 
   void launchSolve(const dcu::Dev& d) {
+    const bool rows = d.P.pcgVariant == 3 && rowsSmemBytes > 0 && !(learnedOn && netGraph);
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(solveGrid);
-    cfg.blockDim = dim3(dcu::kSolveThreads);
-    cfg.dynamicSmemBytes = solveSmemBytes;
+    cfg.blockDim = dim3(rows ? dcu::kRowThreads : dcu::kSolveThreads);
+    cfg.dynamicSmemBytes = rows ? rowsSmemBytes : solveSmemBytes;
     cfg.stream = stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeCooperative;  // co-resident blocks for the grid barrier; capturable in a graph
@@ -427,6 +468,8 @@ struct drape_solver {
     cfg.numAttrs = 1;
     if (learnedOn && netGraph) {
       CK(cudaLaunchKernelEx(&cfg, dcu::k_solve<true, 0>, d));
+    } else if (rows) {
+      CK(cudaLaunchKernelEx(&cfg, dcu::k_solve_rows, d));
     } else if (d.P.pcgVariant == 1) {
       CK(cudaLaunchKernelEx(&cfg, dcu::k_solve<false, 1>, d));
     } else if (d.P.pcgVariant == 2) {
@@ -1645,8 +1688,9 @@ int drape_cuda_set_host_wait(drape_solver* s, uint32_t spin_microseconds) {
 int drape_cuda_set_pcg_variant(drape_solver* s, int variant) {
   return guarded(s, [&] {
     need(s);
-    if (variant < 0 || variant > 2)
-      throw std::invalid_argument("PCG variant must be 0 (reference order), 1 (pipelined) or 2 (Chronopoulos-Gear)");
+    if (variant < 0 || variant > 3)
+      throw std::invalid_argument(
+          "PCG variant must be 0 (reference order), 1 (pipelined), 2 (Chronopoulos-Gear) or 3 (resident rows)");
     s->pcgVariant = variant;
     s->dev.P.pcgVariant = variant;  // the frame graphs compare the device view and recapture
   });
@@ -1677,8 +1721,10 @@ int drape_cuda_test_barrier_timeout(int device, int blocks, uint64_t nanoseconds
 
 int drape_cuda_reduction_floor(int device, int mode, int iterations, double* ns_per_iteration) {
   return guarded(nullptr, [&] {
-    if (!ns_per_iteration || mode < 0 || mode > 3 || iterations < 1 || iterations > 1000000)
+    if (!ns_per_iteration || mode < 0 || mode > 7 || iterations < 1 || iterations > 1000000)
       throw std::invalid_argument("bad argument");
+    const bool rows = mode >= 4;  // modes 4-7: modes 0-3 on k_solve_rows's 512-thread blocks
+    mode &= 3;
     CK(cudaSetDevice(device));
     int sms = 0;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
@@ -1694,8 +1740,13 @@ int drape_cuda_reduction_floor(int device, int mode, int iterations, double* ns_
     d.P.barrierLimitNs = 2000000000ull;
     unsigned long long* o = out.p;
     void* args[] = {&d, &mode, &iterations, &o};
-    CK(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(dcu::k_reduction_floor), dim3(sms),
-                                   dim3(dcu::kSolveThreads), args, 0, nullptr));
+    if (rows) {
+      CK(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(dcu::k_reduction_floor<dcu::kRowThreads>), dim3(sms),
+                                     dim3(dcu::kRowThreads), args, 0, nullptr));
+    } else {
+      CK(cudaLaunchCooperativeKernel(reinterpret_cast<void*>(dcu::k_reduction_floor<dcu::kSolveThreads>), dim3(sms),
+                                     dim3(dcu::kSolveThreads), args, 0, nullptr));
+    }
     CK(cudaGetLastError());
     CK(cudaDeviceSynchronize());
     unsigned long long ns = 0;

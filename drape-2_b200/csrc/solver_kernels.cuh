@@ -41,6 +41,16 @@ __global__ void __launch_bounds__(kSolveThreads, 1) k_solve(Dev D) {
   solveGroup<Learned, kRowLanes, Variant>(D, gs);
 }
 
+// The same Newton iteration with the reference-order PCG over resident rows (pcgResidentRows): 512-thread blocks, so a
+// row thread has the registers to keep its row's PCG state; launched only for scenes whose blocks have at most 512
+// rows and whose sliced matrix fits in shared memory.
+__global__ void __launch_bounds__(kRowThreads, 1) k_solve_rows(Dev D) {
+  if (D.ctl->newtonDone) return;
+  GridSync gs;
+  gs.init(D.ctl, D.P.barrierLimitNs);
+  solveGroup<false, kRowLanes, 3>(D, gs);
+}
+
 __global__ void k_finish(Dev D) { finishRows(D, blockIdx.x, gridDim.x); }
 
 __global__ void k_advance_clock(Dev D) {
@@ -254,9 +264,11 @@ __global__ void k_barrier_probe(Control* ctl, unsigned long long limitNs, int* o
 //   mode 1: gridReduce<3> + a plain barrier (one merged reduction plus the direction's exchange before the next SpMV)
 //   mode 2: gridReduce<3> alone
 //   mode 3: two plain barriers
-// Each round feeds its result into the next, so no round can be skipped or overlapped.
-__global__ void __launch_bounds__(kSolveThreads, 1) k_reduction_floor(Dev D, int mode, int iterations,
-                                                                       unsigned long long* ns) {
+// Each round feeds its result into the next, so no round can be skipped or overlapped. Threads: the block size of the
+// solve kernel measured (k_solve 1024, k_solve_rows 512).
+template <int Threads>
+__global__ void __launch_bounds__(Threads, 1) k_reduction_floor(Dev D, int mode, int iterations,
+                                                                  unsigned long long* ns) {
   GridSync gs;
   gs.init(D.ctl, D.P.barrierLimitNs);
   double x = 1e-3 * threadIdx.x;

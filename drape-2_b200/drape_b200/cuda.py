@@ -320,7 +320,7 @@ class CudaSolver:
     def runner_host_seconds(self):
         """Host seconds of the last drape_to_rest: (set-up, frame loop, rest of the call)."""
         out = (_d * 3)()
-        _raise(self.L.drape_cuda_runner_host_seconds(self.h, out), self.L.drape_cuda_last_error(None))
+        self._check(self.L.drape_cuda_runner_host_seconds(self.h, out))
         return tuple(out)
 
     def frame_times(self, capacity: int = 1 << 16):
@@ -337,7 +337,9 @@ class CudaSolver:
         self._check(self.L.drape_cuda_set_host_wait(self.h, int(spin_microseconds)))
 
     def set_pcg_variant(self, variant: int) -> None:
-        """0: the reference-order block-Jacobi PCG (default); 1: pipelined, one grid exchange per iteration."""
+        """0: the reference-order block-Jacobi PCG (default); 1: pipelined, one grid exchange per iteration;
+        2: Chronopoulos-Gear, one reduction and one plain barrier per iteration; 3: the reference order over resident
+        rows (512-thread blocks, row state in registers; runs as 0 where the scene does not fit it)."""
         self._check(self.L.drape_cuda_set_pcg_variant(self.h, int(variant)))
 
     def inject_failure(self, steps: int) -> None:
@@ -376,7 +378,8 @@ def test_barrier_timeout(device: int = 0, blocks: int = 2, nanoseconds: int = 20
 def reduction_floor(device: int = 0, mode: int = 0, iterations: int = 2000) -> float:
     """Device microseconds per round of the persistent solve's grid-wide exchanges with no other work
     (drape_cuda_reduction_floor): mode 0 = the two FP64 reductions of a reference-order PCG iteration, 1 = one merged
-    reduction plus a plain barrier, 2 = one merged reduction, 3 = two plain barriers."""
+    reduction plus a plain barrier, 2 = one merged reduction, 3 = two plain barriers; 4-7 = modes 0-3 on the
+    resident-row solve's grid (one 512-thread block per SM)."""
     L = load()
     ns = C.c_double(0.0)
     _raise(L.drape_cuda_reduction_floor(device, mode, iterations, C.byref(ns)), L.drape_cuda_last_error(None))

@@ -230,8 +230,11 @@ int drape_cuda_set_host_wait(drape_solver* s, uint32_t spin_microseconds);
    stopping tests, cpu_solver.cpp:169-213): 0 (the default) the reference's order, two grid-wide reductions per
    iteration; 1 pipelined (Ghysels and Vanroose 2014), one reduction per iteration and three more work vectors, its
    FP32 recurrences drifting further from the products they stand for; 2 Chronopoulos-Gear, one reduction and one plain
-   barrier per iteration with the reference order's recurrences. All three give the same iterates in exact
-   arithmetic and round differently. The learned preconditioner always runs its own PCG. */
+   barrier per iteration with the reference order's recurrences; 3 the reference's order with resident rows: one
+   512-thread block per SM, each row's PCG state in its thread's registers and the block's matrix in a sliced layout in
+   shared memory, the same arithmetic as 0 in the same order (used where every block has at most 512 rows and its
+   sliced matrix fits in shared memory; elsewhere 3 runs as 0). Forms 0-2 give the same iterates in exact arithmetic
+   and round differently. The learned preconditioner always runs its own PCG. */
 int drape_cuda_set_pcg_variant(drape_solver* s, int variant);
 
 /* The bounded wait of the device grid barrier, in nanoseconds (0 restores the default of 2 s). A kernel whose barrier
@@ -242,7 +245,7 @@ int drape_cuda_set_barrier_limit(drape_solver* s, uint64_t nanoseconds);
    solve's grid (one 1024-thread block per SM, cooperative) runs `iterations` rounds of grid-wide exchanges with no
    other work and *ns_per_iteration gets the device time per round (%globaltimer, block 0). mode 0: the two FP64 grid
    reductions of a reference-order PCG iteration; 1: one three-value reduction plus a plain barrier; 2: one three-value
-   reduction; 3: two plain barriers. */
+   reduction; 3: two plain barriers; 4-7: modes 0-3 on one 512-thread block per SM (the resident-row form's grid). */
 int drape_cuda_reduction_floor(int device, int mode, int iterations, double* ns_per_iteration);
 /* Test hook: runs a grid barrier that can only end by its time limit (it waits for one more block than it has) on
    `blocks` blocks with the given limit, and returns the status the blocks read back in *status (0: released, which

@@ -95,7 +95,9 @@ def expect_parity(gpu, oracle_mod, key, scene, variant, start=None, informationa
     return apart, rms, spread
 
 
-VARIANTS = [0, 1, 2]  # the reference-order PCG (the parity path), the pipelined one, the Chronopoulos-Gear one
+# The reference-order PCG (the parity path), the pipelined one, the Chronopoulos-Gear one, the reference order over
+# resident rows.
+VARIANTS = [0, 1, 2, 3]
 # The pipelined PCG carries A p, M A p and A M A p by FP32 recurrences whose rounding drifts from the products they
 # stand for (its Newton steps take about 4x the reference order's line-search halvings on the 60k drape); on a settled
 # drape's 60-frame continuation a few contact particles then end several mm from the oracle (measured 4.8 mm on the 10k
@@ -178,6 +180,44 @@ def test_pcg_forms_track_reference_order_one_frame(gpu, variant):
     assert n0 == n1
     assert np.abs(np.asarray(h0) - np.asarray(h1)).max() <= 1, (h0, h1)
     assert np.abs(x0 - x1).max() < 1e-4
+
+
+@pytest.mark.parametrize("scene_name", ["tube10k", "tube60k"])
+def test_resident_rows_are_the_reference_order(gpu, scene_name):
+    """The resident-row form (variant 3: row state in registers, sliced matrix in shared memory) does the
+    reference-order PCG's arithmetic in the same order; only the grouping of the FP64 p.Ap partials differs. Three
+    frames of the drop: the same PCG iteration count in every solve and positions within 1e-6 m (bit-identical in
+    practice)."""
+    scene = S.tube_10k() if scene_name == "tube10k" else S.tube_60k()
+    out = []
+    for variant in (0, 3):
+        s = cuda_solver(gpu, variant)()
+        s.build(scene)
+        for _ in range(3):
+            s.step(1.0 / 60.0, 2, 2)
+        out.append((s.positions().astype(np.float64), np.asarray(s.cg_history())))
+        s.close()
+    (x0, h0), (x3, h3) = out
+    print(f"resident rows vs reference order ({scene_name}): max |dx| {np.abs(x0 - x3).max():.3e} m, "
+          f"{len(h0)} solves, PCG counts equal: {np.array_equal(h0, h3)}")
+    assert np.array_equal(h0, h3), (h0, h3)
+    assert np.abs(x0 - x3).max() < 1e-6
+
+
+def test_pcg_variant_range(gpu):
+    s = cuda_solver(gpu, 0)()
+    with pytest.raises(ValueError):
+        s.set_pcg_variant(4)
+    with pytest.raises(ValueError):
+        s.set_pcg_variant(-1)
+    s.close()
+
+
+def test_reduction_floor_modes(gpu):
+    """The exchange floors on both solve grids: positive, and two reductions cost more than one."""
+    f = {m: gpu.reduction_floor(0, m, 200) for m in (0, 2, 4, 6)}
+    assert all(v > 0 for v in f.values()), f
+    assert f[0] > f[2] and f[4] > f[6], f
 
 
 @pytest.mark.parametrize("name", ["c1", "c2"])
