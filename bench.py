@@ -685,9 +685,10 @@ def main():
     ap.add_argument("--refresh-every", type=int, default=1,
                     help="learned leg: run the network every this many Newton iterations")
     ap.add_argument("--no-deviation", action="store_true", help="skip the deviation-from-the-oracle leg")
-    ap.add_argument("--pcg-variant", type=int, choices=[0, 1, 2], default=0,
-                    help="block-Jacobi PCG form: 0 the reference's order, 1 pipelined (one grid exchange an iteration), "
-                         "2 Chronopoulos-Gear (one reduction and one plain barrier)")
+    ap.add_argument("--pcg-variant", type=int, choices=[0, 1, 2, 3], default=0,
+                    help="block-Jacobi PCG form: 0 the reference's order (resident rows where the scene fits), "
+                         "1 pipelined (one grid exchange an iteration), 2 Chronopoulos-Gear (one reduction and one "
+                         "plain barrier), 3 the reference's order on the 1024-thread kernel")
     ap.add_argument("--batch-garments", type=int, default=64, help="garments of the batched leg (0: skip it)")
     ap.add_argument("--profile-case", choices=["spmv", "batch", "bake", "drape", "learned"], default=None,
                     help="run one small case for a profiler capture instead of the benchmark")
@@ -802,7 +803,8 @@ def main():
     if os.path.exists(tfile):
         with open(tfile) as f:
             t = json.load(f)
-        if t.get("workload") == args.workload:
+        if t.get("workload") == args.workload and t.get("kernel") == ("k_solve_rows" if solver.solve_threads() == 512
+                                                                      else "k_solve"):
             traffic = t.get("dram_bytes_per_launch")
     # Kernel shares from one more drape (the workload's own start state) with every kernel timed, outside the timed
     # region (events around every launch cost about 6 % of the frame time).
@@ -819,9 +821,12 @@ def main():
     # per PCG iteration is set by the grid-wide exchanges. The PCG loop's own device time (%globaltimer, block 0) per
     # iteration is set beside the measured floor of the same exchanges on the same grid with no other work.
     pcg_us = counters.pcg_nanoseconds / 1000.0 / max(1, counters.cg_iterations)
-    floor_mode = {0: 0, 1: 2, 2: 1}[args.pcg_variant]
-    floor_us = statistics.median(CU.reduction_floor(local, floor_mode, 4000) for _ in range(3))
-    latency = {"kernel": "k_solve PCG loop", "us_per_pcg_iteration": pcg_us, "floor_us": floor_us,
+    solve_threads = solver.solve_threads()
+    floor_mode = {0: 0, 3: 0, 1: 2, 2: 1}[args.pcg_variant]
+    floor_us = statistics.median(CU.reduction_floor(local, floor_mode + (4 if solve_threads == 512 else 0), 4000)
+                                 for _ in range(3))
+    latency = {"kernel": ("k_solve_rows" if solve_threads == 512 else "k_solve") + " PCG loop",
+               "solve_threads": solve_threads, "us_per_pcg_iteration": pcg_us, "floor_us": floor_us,
                "floor": {0: "two FP64 grid reductions per iteration (reference-order PCG)",
                          2: "one three-value FP64 grid reduction per iteration (pipelined PCG)",
                          1: "one three-value FP64 grid reduction and one plain barrier per iteration "
@@ -829,7 +834,8 @@ def main():
                "frac_of_floor": floor_us / pcg_us if pcg_us else None,
                "onchip_bytes_per_iteration": ab["pcg_iter"],
                "onchip_gbs": ab["pcg_iter"] / (pcg_us * 1e-6) / 1e9 if pcg_us else None,
-               "note": "floor = drape_cuda_reduction_floor on the solve's grid (one 1024-thread block per SM), "
+               "note": f"floor = drape_cuda_reduction_floor on the solve's grid (one {solve_threads}-thread block per "
+                       "SM), "
                        "median of 3 x 4000 rounds; us_per_pcg_iteration = in-kernel PCG time / PCG iterations over "
                        "the timed drapes (CG init amortised); onchip_gbs = the iteration's algorithmic bytes over its "
                        "time, served from shared memory and L2"}
@@ -879,9 +885,11 @@ def main():
         "dtype": "f32+f64", "data": "synthetic",
         "config": {"workload": WORKLOADS[args.workload]["desc"], "precond": "block-Jacobi",
                    "pcg": {0: "reference order (two grid reductions per iteration)",
+                           3: "reference order (two grid reductions per iteration)",
                            1: "pipelined (one grid reduction per iteration)",
                            2: "Chronopoulos-Gear (one grid reduction and one plain barrier per iteration)"}[
-                               args.pcg_variant],
+                               args.pcg_variant] + (", resident rows (512-thread blocks)" if solve_threads == 512
+                                                    else ", 1024-thread blocks"),
                    "start_states": SEED_DESC,
                    "precision": "FP32 blocks/SpMV/vectors, FP64 dots, FP64 energy/slope/line search",
                    "l2": "256 MB buffer written between timed drapes (L2 flushed)",

@@ -98,9 +98,9 @@ struct Params {
   uint32_t n, nStretch, nHinge, nSeam, nBlocks, nGarments, slotsPadded;
   uint32_t smemSlots;   // k_solve: block slots a block keeps in shared memory
   int learnedSwitch;    // k_solve<true>: block-Jacobi iterations before the learned preconditioner takes over
-  int pcgVariant;       // the solve kernel chosen for block-Jacobi: 0 reference order, 1 pipelined, 2 Chronopoulos-Gear,
-                        // 3 reference order with resident rows (kept in the view so that captured frame graphs are
-                        // recaptured when it changes)
+  int pcgVariant;       // the block-Jacobi PCG form: 0 reference order (resident rows where the scene fits), 1 pipelined,
+                        // 2 Chronopoulos-Gear, 3 reference order on the 1024-thread kernel (kept in the view so that
+                        // captured frame graphs are recaptured when it changes)
   uint32_t slicedSlots; // k_solve_rows: padded slots of the sliced layout a block may hold in shared memory
   unsigned long long barrierLimitNs;
 };
@@ -264,31 +264,34 @@ __device__ __forceinline__ double combine(double a, double b) {
 // loads issued before the first add) and combines them in a fixed order; the other warps wait at one block barrier
 // meanwhile. Every block obtains bit-identical results and takes the same branches. Two block barriers per call: `red`
 // is rewritten only after the closing barrier, by which warp 0 has read it, and `res` only after the next call's first
-// barrier, by which every warp has read it. Returns false when the barrier gave up.
-template <int K, bool Max = false>
-__device__ inline bool gridReduce(const Dev& D, GridSync& gs, double (&v)[K], double (&out)[K]) {
+// barrier, by which every warp has read it; so every call shares one scratch. Returns false when the barrier gave up.
+struct ReduceScratch {
+  double red[3][32];  // per-warp sums (at most three values, 32 warps)
+  double res[3];
+  int ok;
+};
+
+__device__ __forceinline__ ReduceScratch& reduceScratch() {
+  __shared__ ReduceScratch r;
+  return r;
+}
+
+// The grid stage: the caller has put nw per-warp sums in red and passed a block barrier.
+template <int K, bool Max>
+__device__ inline bool gridCombine(const Dev& D, GridSync& gs, int nw, double (&out)[K]) {
+  static_assert(K >= 1 && K <= 3, "gridReduce: one to three values");
   constexpr int kLoads = 5;  // partials a lane loads at a time (160 blocks per round: one round for one block per SM)
-  __shared__ double red[K][32];
-  __shared__ double res[K];
-  __shared__ int ok;
   constexpr double kIdentity = Max ? -INFINITY : 0.0;
+  ReduceScratch& sc = reduceScratch();
   double* half = D.partials + static_cast<size_t>(gs.parity) * gs.size * kPartialStride;
   gs.parity ^= 1u;
   gs.target += gs.size;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-#pragma unroll
-  for (int k = 0; k < K; ++k)
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v[k] = combine<Max>(v[k], __shfl_down_sync(0xffffffffu, v[k], o));
-  if (lane == 0)
-#pragma unroll
-    for (int k = 0; k < K; ++k) red[k][w] = v[k];
-  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   if (w == 0) {
     double s[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      s[k] = lane < nw ? red[k][lane] : kIdentity;
+      s[k] = lane < nw ? sc.red[k][lane] : kIdentity;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) s[k] = combine<Max>(s[k], __shfl_down_sync(0xffffffffu, s[k], o));
     }
@@ -323,15 +326,60 @@ __device__ inline bool gridReduce(const Dev& D, GridSync& gs, double (&v)[K], do
         for (int o = 16; o > 0; o >>= 1) t[k] = combine<Max>(t[k], __shfl_down_sync(0xffffffffu, t[k], o));
       if (lane == 0)
 #pragma unroll
-        for (int k = 0; k < K; ++k) res[k] = t[k];
+        for (int k = 0; k < K; ++k) sc.res[k] = t[k];
     }
-    if (lane == 0) ok = good;
+    if (lane == 0) sc.ok = good;
   }
   __syncthreads();
-  if (!ok) return false;
+  if (!sc.ok) return false;
 #pragma unroll
-  for (int k = 0; k < K; ++k) out[k] = res[k];
+  for (int k = 0; k < K; ++k) out[k] = sc.res[k];
   return true;
+}
+
+// HalfWarps (blocks of at most 512 threads): each half-warp is summed on its own (a 16-lane tree) into its own entry
+// of `red`, so 16 rows per entry as in a 1024-thread block whose rows sit on even lanes (pcgReferenceOrder<2>'s p.Ap
+// partials): that block's tree with zeros on its odd lanes adds the same values in the same order.
+template <int K, bool Max = false, bool HalfWarps = false>
+__device__ inline bool gridReduce(const Dev& D, GridSync& gs, double (&v)[K], double (&out)[K]) {
+  ReduceScratch& sc = reduceScratch();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nw = HalfWarps ? 2 * ((blockDim.x + 31) >> 5) : (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+#pragma unroll
+    for (int o = HalfWarps ? 8 : 16; o > 0; o >>= 1)
+      v[k] = combine<Max>(v[k], __shfl_down_sync(0xffffffffu, v[k], o, HalfWarps ? 16 : 32));
+  if (HalfWarps ? (lane & 15) == 0 : lane == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k) sc.red[k][HalfWarps ? 2 * w + (lane >> 4) : w] = v[k];
+  __syncthreads();
+  return gridCombine<K, Max>(D, gs, nw, out);
+}
+
+// Sums for a block that stands for one twice its size (at most 512 threads for 1024): thread t carries virtual
+// threads t (lo) and t + blockDim.x (hi), so warp w's lo sums are virtual warp w's and its hi sums virtual warp
+// w + nw's, in the order a block of the virtual size adds them.
+template <int K>
+__device__ inline bool gridReducePairs(const Dev& D, GridSync& gs, double (&lo)[K], double (&hi)[K],
+                                       double (&out)[K]) {
+  ReduceScratch& sc = reduceScratch();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[k] += __shfl_down_sync(0xffffffffu, lo[k], o);
+      hi[k] += __shfl_down_sync(0xffffffffu, hi[k], o);
+    }
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      sc.red[k][w] = lo[k];
+      sc.red[k][w + nw] = hi[k];
+    }
+  __syncthreads();
+  return gridCombine<K, false>(D, gs, 2 * nw, out);
 }
 
 // Block `rank`'s contiguous share of [0, n) in a group of `size` blocks: the persistent kernels give each block one
@@ -347,6 +395,31 @@ __device__ __forceinline__ float3 filterContact(const Contact& c, float3 v) {
   if (c.active == 0u) return v;
   const float3 n = xyz(c.normal);
   return v - n * dot(n, v);
+}
+
+// The PCG's FP32 arithmetic with every rounding written out (products and sums fused or rounded explicitly, nothing
+// left to the compiler's contraction), so that the reference-order kernels (pcgReferenceOrder over 1024-thread blocks,
+// pcgResidentRows over 512-thread ones) round alike in whatever code surrounds them.
+__device__ __forceinline__ float3 axpyRn(float3 x, float s, float3 y) {  // y + s x, one rounding per component
+  return mk(__fmaf_rn(x.x, s, y.x), __fmaf_rn(x.y, s, y.y), __fmaf_rn(x.z, s, y.z));
+}
+__device__ __forceinline__ float dotRn(float a0, float a1, float a2, float3 b) {
+  return __fmaf_rn(a2, b.z, __fmaf_rn(a1, b.y, __fmul_rn(a0, b.x)));
+}
+__device__ __forceinline__ float3 mulRn(const M3& a, float3 v) {
+  return mk(dotRn(a.m[0], a.m[1], a.m[2], v), dotRn(a.m[3], a.m[4], a.m[5], v), dotRn(a.m[6], a.m[7], a.m[8], v));
+}
+// v - n (n . v) on active contact rows.
+__device__ __forceinline__ float3 filterRn(const Contact& c, float3 v) {
+  if (c.active == 0u) return v;
+  const float3 n = xyz(c.normal);
+  return axpyRn(n, -dotRn(n.x, n.y, n.z, v), v);
+}
+// acc += a v for a row-major 3x3 block a: each row's three products summed in order, then added to acc.
+__device__ __forceinline__ void blockMulAddRn(float3& acc, const float (&a)[9], float3 v) {
+  acc.x = __fadd_rn(acc.x, dotRn(a[0], a[1], a[2], v));
+  acc.y = __fadd_rn(acc.y, dotRn(a[3], a[4], a[5], v));
+  acc.z = __fadd_rn(acc.z, dotRn(a[6], a[7], a[8], v));
 }
 
 __device__ __forceinline__ float contactRadius(const Params& P, const Fabric& f) {
@@ -588,17 +661,19 @@ __device__ inline void assembleSlots(const Dev& D, uint32_t rank, uint32_t size)
 // ---------------------------------------------------------------------------------------------------------------
 // Energy at u + alpha * step, in FP64, summed per thread over particles (inertia + friction) and terms.
 
-__device__ inline double energyPartial(const Dev& D, const GridSync& gs, double alpha) {
+// Virtual thread vt of a block of vdim threads: the elements idx = rank * vdim + vt + k * size * vdim (a kernel whose
+// blocks stand for larger ones sums in the larger blocks' order).
+__device__ inline double energyPartial(const Dev& D, const GridSync& gs, double alpha, uint32_t vt, uint32_t vdim) {
   double e = 0.0;
   const uint32_t n = D.P.n, S = D.P.nStretch, H = D.P.nHinge, K = D.P.nSeam;
   const uint32_t total = n + S + H + K;
-  const uint32_t stride = gs.size * blockDim.x;
+  const uint32_t stride = gs.size * vdim;
   auto pos = [&](uint32_t v0, uint32_t vk) -> d3 {
     const d3 rel = toD(ld3(D.xStart, vk)) - toD(ld3(D.xStart, v0));
     return rel + (toD(ld3(D.u, vk)) + alpha * toD(ld3(D.step, vk)));
   };
   const double invH2 = 1.0 / (D.P.hD * D.P.hD);
-  for (uint32_t idx = gs.rank * blockDim.x + threadIdx.x; idx < total; idx += stride) {
+  for (uint32_t idx = gs.rank * vdim + vt; idx < total; idx += stride) {
     if (idx < n) {
       const uint32_t i = idx;
       const Particle pa = D.particle[i];
@@ -628,6 +703,10 @@ __device__ inline double energyPartial(const Dev& D, const GridSync& gs, double 
     }
   }
   return e;
+}
+
+__device__ inline double energyPartial(const Dev& D, const GridSync& gs, double alpha) {
+  return energyPartial(D, gs, alpha, threadIdx.x, blockDim.x);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -726,16 +805,14 @@ __device__ __forceinline__ float3 rowProduct(const SmemMatrix& A, uint32_t rs, u
       if (col[k] & kPinnedBit) continue;
       float a[9];
       A.block(s0 + k * RL, a);
-      acc.x += a[0] * v[k].x + a[1] * v[k].y + a[2] * v[k].z;
-      acc.y += a[3] * v[k].x + a[4] * v[k].y + a[5] * v[k].z;
-      acc.z += a[6] * v[k].x + a[7] * v[k].y + a[8] * v[k].z;
+      blockMulAddRn(acc, a, v[k]);
     }
   }
 #pragma unroll
   for (int o = RL / 2; o > 0; o >>= 1) {
-    acc.x += __shfl_xor_sync(mask, acc.x, o);
-    acc.y += __shfl_xor_sync(mask, acc.y, o);
-    acc.z += __shfl_xor_sync(mask, acc.z, o);
+    acc.x = __fadd_rn(acc.x, __shfl_xor_sync(mask, acc.x, o));
+    acc.y = __fadd_rn(acc.y, __shfl_xor_sync(mask, acc.y, o));
+    acc.z = __fadd_rn(acc.z, __shfl_xor_sync(mask, acc.z, o));
   }
   return acc;
 }
@@ -834,10 +911,10 @@ __device__ inline double directionStep(const Dev& D, const SmemMatrix& A, uint32
       D, A, r0, r1, [&](uint32_t j) { return ld3(D.z, j); },
       [&](uint32_t i, float3 zi, float3 az) {
         // A p = A z + beta A pPrev: the previous direction's product is this row's apFull.
-        const float3 pi = first ? zi : zi + ld3(pPrev, i) * fb;
-        const float3 acc = first ? az : az + ld3(D.apFull, i) * fb;
+        const float3 pi = first ? zi : axpyRn(ld3(pPrev, i), fb, zi);
+        const float3 acc = first ? az : axpyRn(ld3(D.apFull, i), fb, az);
         pCur[i] = f4(pi);
-        const float3 filtered = filterContact(D.contact[i], acc);
+        const float3 filtered = filterRn(D.contact[i], acc);
         D.apFull[i] = f4(acc);
         D.ap[i] = f4(filtered);
         vpap += dotd3(pi, filtered);
@@ -862,8 +939,8 @@ __device__ inline int pcgReferenceOrder(const Dev& D, GridSync& gs, const SmemMa
     for (uint32_t i = r0i + threadIdx.x; i < r1i; i += blockDim.x) {
       const Contact c = D.contact[i];
       const float3 res = -ld3(D.grad, i);
-      const float3 ri = filterContact(c, res);
-      const float3 zi = filterContact(c, mul(loadPrecond(D, i), ri));
+      const float3 ri = filterRn(c, res);
+      const float3 zi = filterRn(c, mulRn(loadPrecond(D, i), ri));
       D.step[i] = make_float4(0, 0, 0, 0);
       D.resid[i] = f4(res);
       D.r[i] = f4(ri);
@@ -897,11 +974,11 @@ __device__ inline int pcgReferenceOrder(const Dev& D, GridSync& gs, const SmemMa
     for (uint32_t i = r0i + threadIdx.x; i < r1i; i += blockDim.x) {
       const Contact c = D.contact[i];
       const float3 pi = ld3(pCur, i);
-      D.step[i] = f4(ld3(D.step, i) + pi * fa);
-      const float3 ri = ld3(D.r, i) - ld3(D.ap, i) * fa;
+      D.step[i] = f4(axpyRn(pi, fa, ld3(D.step, i)));
+      const float3 ri = axpyRn(ld3(D.ap, i), -fa, ld3(D.r, i));
       D.r[i] = f4(ri);
-      D.resid[i] = f4(ld3(D.resid, i) - ld3(D.apFull, i) * fa);
-      const float3 zi = filterContact(c, mul(loadPrecond(D, i), ri));
+      D.resid[i] = f4(axpyRn(ld3(D.apFull, i), -fa, ld3(D.resid, i)));
+      const float3 zi = filterRn(c, mulRn(loadPrecond(D, i), ri));
       D.z[i] = f4(zi);
       v[0] += dotd3(ri, ri);
       v[1] += dotd3(ri, zi);
@@ -920,16 +997,18 @@ __device__ inline int pcgReferenceOrder(const Dev& D, GridSync& gs, const SmemMa
 }
 
 // ---------------------------------------------------------------------------------------------------------------
-// Reference-order PCG with resident rows (k_solve_rows; pcgVariant 3). One thread owns one row of its block for the
+// Reference-order PCG with resident rows (k_solve_rows; the form pcgVariant 0 runs where a scene fits it). One thread owns one row of its block for the
 // whole solve and keeps the row's PCG state (p, A p and its filtered copy, r, step, resid, z, the contact plane and
 // the preconditioner block) in registers, so an iteration's only global traffic is the gather of z_j over the row's
 // columns and the store of the new z_i: the reference-order kernel re-reads the row vectors from L2 in both passes.
 // The block's slots sit in shared memory in a sliced layout: the rows in warps of 32, warp w's slots padded to its
 // longest row L_w, slot k of lane l at base_w + 32 k + l (nine planes, then the columns; padding holds kPinnedBit),
 // so a warp's 32 row threads read 32 consecutive words. The row's product keeps the two-lane order of
-// pcgReferenceOrder<2> (the even slots in one sum, the odd slots in another, added at the end), so the iterates are
-// that kernel's.
+// pcgReferenceOrder<2> (the even slots in one sum, the odd slots in another, added at the end) and the FP64 partials
+// are grouped as that kernel groups them (p.Ap by half-warps; the others fall on the same threads), so the iterates
+// are that kernel's bit for bit.
 constexpr int kRowThreads = 512;     // k_solve_rows block size: a block's rows must not exceed it
+constexpr int kResidentRows = 4;     // the solve templates' Variant value of this form
 constexpr int kSlicedDepth = 12;     // gathers a row thread has in flight (even, so k0 + k has the parity of k)
 
 struct SlicedMatrix {
@@ -944,8 +1023,8 @@ struct SlicedMatrix {
 // every block fits, so this is a guard).
 __device__ inline bool stageSliced(const Dev& D, uint32_t r0, uint32_t r1, SlicedMatrix& A) {
   constexpr int kWarps = kRowThreads / 32;
-  __shared__ uint32_t off[kRowThreads + 1];  // the rows' first slots, relative to the block's first
-  __shared__ uint32_t cnt[kRowThreads];      // the rows' slot counts (0 for pinned rows: they take no product)
+  // The rows' first slots relative to the block's first, bit 31 set for pinned rows (they take no product).
+  __shared__ uint32_t off[kRowThreads + 1];
   __shared__ uint32_t warpLen[kWarps], warpBase[kWarps + 1];
   const uint32_t t = threadIdx.x, lane = t & 31u, w = t >> 5;
   const uint32_t R = r1 - r0;
@@ -957,11 +1036,11 @@ __device__ inline bool stageSliced(const Dev& D, uint32_t r0, uint32_t r1, Slice
   uint32_t c = 0;
   if (t < R) {
     const uint32_t rs = __ldg(D.rowStart + r0 + t);
-    off[t] = rs - first;
-    if (D.particle[r0 + t].pinned == 0u) c = __ldg(D.rowStart + r0 + t + 1) - rs;
+    const bool pinned = D.particle[r0 + t].pinned != 0u;
+    off[t] = (rs - first) | (pinned ? kPinnedBit : 0u);
+    if (!pinned) c = __ldg(D.rowStart + r0 + t + 1) - rs;
   }
   if (t == 0) off[R] = __ldg(D.rowStart + r1) - first;
-  cnt[t] = c;
   const uint32_t len = __reduce_max_sync(0xffffffffu, c);
   if (lane == 0) warpLen[w] = len;
   __syncthreads();
@@ -992,13 +1071,13 @@ __device__ inline bool stageSliced(const Dev& D, uint32_t r0, uint32_t r1, Slice
   const uint32_t S = off[R];
   const uint32_t SP = D.P.slotsPadded;
   for (uint32_t k = t; k < S; k += blockDim.x) {
-    uint32_t lo = 0, hi = R;  // off[lo] <= k < off[hi]
+    uint32_t lo = 0, hi = R;  // row lo's first slot <= k < row hi's first slot
     while (hi - lo > 1) {
       const uint32_t mid = (lo + hi) >> 1;
-      if (off[mid] <= k) lo = mid; else hi = mid;
+      if ((off[mid] & ~kPinnedBit) <= k) lo = mid; else hi = mid;
     }
+    if (off[lo] & kPinnedBit) continue;  // a pinned row's slot
     const uint32_t j = k - off[lo];
-    if (j >= cnt[lo]) continue;  // a pinned row's slot
     const uint32_t pos = warpBase[lo >> 5] + 32u * j + (lo & 31u);
     const uint32_t s = first + k;
 #pragma unroll
@@ -1029,16 +1108,10 @@ __device__ __forceinline__ float3 slicedProduct(const SlicedMatrix& A, const flo
       float a[9];
 #pragma unroll
       for (int q = 0; q < 9; ++q) a[q] = A.planes[q * A.stride + pos];
-      float3& acc = (k & 1) ? acc1 : acc0;
-      acc.x += a[0] * v[k].x + a[1] * v[k].y + a[2] * v[k].z;
-      acc.y += a[3] * v[k].x + a[4] * v[k].y + a[5] * v[k].z;
-      acc.z += a[6] * v[k].x + a[7] * v[k].y + a[8] * v[k].z;
+      blockMulAddRn((k & 1) ? acc1 : acc0, a, v[k]);
     }
   }
-  acc0.x += acc1.x;
-  acc0.y += acc1.y;
-  acc0.z += acc1.z;
-  return acc0;
+  return mk(__fadd_rn(acc0.x, acc1.x), __fadd_rn(acc0.y, acc1.y), __fadd_rn(acc0.z, acc1.z));
 }
 
 // The reference-order PCG of pcgReferenceOrder (same recurrences, same stopping tests) over resident rows. Writes
@@ -1060,8 +1133,8 @@ __device__ inline int pcgResidentRows(const Dev& D, GridSync& gs, const SlicedMa
       c = D.contact[i];
       M = loadPrecond(D, i);
       resid = -ld3(D.grad, i);
-      r = filterContact(c, resid);
-      z = filterContact(c, mul(M, r));
+      r = filterRn(c, resid);
+      z = filterRn(c, mulRn(M, r));
       D.z[i] = f4(z);
       v[0] += dotd3(r, z);
       v[1] += dotd3(r, r);
@@ -1081,14 +1154,14 @@ __device__ inline int pcgResidentRows(const Dev& D, GridSync& gs, const SlicedMa
       double vpap[1] = {0.0};
       const float3 az = slicedProduct(A, D.z);
       if (own) {
-        p = firstIt ? z : z + p * fb;
-        const float3 acc = firstIt ? az : az + apFull * fb;
-        ap = filterContact(c, acc);
+        p = firstIt ? z : axpyRn(p, fb, z);
+        const float3 acc = firstIt ? az : axpyRn(apFull, fb, az);
+        ap = filterRn(c, acc);
         apFull = acc;
         vpap[0] += dotd3(p, ap);
       }
       double pAp[1];
-      if (!gridReduce<1>(D, gs, vpap, pAp)) return -1;
+      if (!gridReduce<1, false, true>(D, gs, vpap, pAp)) return -1;
       if (!(pAp[0] > 0.0)) break;
       const double alpha = rz / pAp[0];
       const float fa = static_cast<float>(alpha);
@@ -1096,10 +1169,10 @@ __device__ inline int pcgResidentRows(const Dev& D, GridSync& gs, const SlicedMa
       // Update (kernels.h:304-315) fused with the preconditioner apply (kernels.h:324-332).
       double v[2] = {0.0, 0.0};
       if (own) {
-        step = step + p * fa;
-        r = r - ap * fa;
-        resid = resid - apFull * fa;
-        z = filterContact(c, mul(M, r));
+        step = axpyRn(p, fa, step);
+        r = axpyRn(ap, -fa, r);
+        resid = axpyRn(apFull, -fa, resid);
+        z = filterRn(c, mulRn(M, r));
         D.z[i] = f4(z);
         v[0] += dotd3(r, r);
         v[1] += dotd3(r, z);
@@ -1448,7 +1521,7 @@ template <bool Learned, int PL, int Variant = 0>
 __device__ inline int pcgSolve(const Dev& D, GridSync& gs) {
   uint32_t r0i, r1i;
   blockRange(D.P.n, gs.rank, gs.size, r0i, r1i);
-  if constexpr (Variant == 3) {
+  if constexpr (Variant == kResidentRows) {
     static_assert(!Learned, "resident rows: block-Jacobi only");
     SlicedMatrix A;
     if (!stageSliced(D, r0i, r1i, A)) return -1;
@@ -1456,12 +1529,13 @@ __device__ inline int pcgSolve(const Dev& D, GridSync& gs) {
     const int it = pcgResidentRows(D, gs, A);
     if (gs.rank == 0 && threadIdx.x == 0) D.ctl->pcgNs += static_cast<long long>(globalTimerNs() - t0);
     return it;
+  } else {
+    const SmemMatrix A = stageMatrix(D, r0i, r1i);
+    const unsigned long long t0 = globalTimerNs();
+    const int it = pcgSolveStaged<Learned, PL, Variant>(D, gs, A);
+    if (gs.rank == 0 && threadIdx.x == 0) D.ctl->pcgNs += static_cast<long long>(globalTimerNs() - t0);
+    return it;
   }
-  const SmemMatrix A = stageMatrix(D, r0i, r1i);
-  const unsigned long long t0 = globalTimerNs();
-  const int it = pcgSolveStaged<Learned, PL, Variant>(D, gs, A);
-  if (gs.rank == 0 && threadIdx.x == 0) D.ctl->pcgNs += static_cast<long long>(globalTimerNs() - t0);
-  return it;
 }
 
 template <bool Learned, int PL, int Variant>
@@ -1510,6 +1584,10 @@ __device__ inline void solveGroup(const Dev& D, GridSync& gs) {
     ctl->energyEvaluations += 1;  // E(0) below
   }
 
+  // The resident-row kernel's 512-thread blocks stand for the reference-order kernel's 1024-thread ones: its energies
+  // are summed as two virtual threads per thread, in that kernel's order, so both kernels take the same line-search
+  // decisions (its rows, at most 512 per block, already sit on the same threads).
+  constexpr bool kVirtual = Variant == kResidentRows;
   // Contact normal force from the residual (kernels.h:391-396), Newton slope grad . step and E(0), in FP64.
   double se[2];
   {
@@ -1520,8 +1598,14 @@ __device__ inline void solveGroup(const Dev& D, GridSync& gs) {
       D.contact[i].force = c.active != 0u ? fmaxf(0.0f, -dot(res, xyz(c.normal))) : 0.0f;
       v[0] += dotd3(ld3(D.grad, i), ld3(D.step, i));
     }
-    v[1] = energyPartial(D, gs, 0.0);
-    if (!gridReduce<2>(D, gs, v, se)) return;
+    if constexpr (kVirtual) {
+      v[1] = energyPartial(D, gs, 0.0, threadIdx.x, 2 * blockDim.x);
+      double hi[2] = {0.0, energyPartial(D, gs, 0.0, threadIdx.x + blockDim.x, 2 * blockDim.x)};
+      if (!gridReducePairs<2>(D, gs, v, hi, se)) return;
+    } else {
+      v[1] = energyPartial(D, gs, 0.0);
+      if (!gridReduce<2>(D, gs, v, se)) return;
+    }
   }
   const double slope = se[0], e0 = se[1];
   if (!(slope < 0.0)) {
@@ -1535,9 +1619,15 @@ __device__ inline void solveGroup(const Dev& D, GridSync& gs) {
   double alpha = 1.0;
   for (int ls = 0; ls < 20; ++ls) {
     if (gs.rank == 0 && threadIdx.x == 0) ctl->energyEvaluations += 1;
-    double v[1] = {energyPartial(D, gs, alpha)};
     double e[1];
-    if (!gridReduce<1>(D, gs, v, e)) return;
+    if constexpr (kVirtual) {
+      double lo[1] = {energyPartial(D, gs, alpha, threadIdx.x, 2 * blockDim.x)};
+      double hi[1] = {energyPartial(D, gs, alpha, threadIdx.x + blockDim.x, 2 * blockDim.x)};
+      if (!gridReducePairs<1>(D, gs, lo, hi, e)) return;
+    } else {
+      double v[1] = {energyPartial(D, gs, alpha)};
+      if (!gridReduce<1>(D, gs, v, e)) return;
+    }
     if (e[0] <= e0 + 1e-4 * alpha * slope) break;
     alpha *= 0.5;
     if (gs.rank == 0 && threadIdx.x == 0) ctl->lineSearchHalvings += 1;

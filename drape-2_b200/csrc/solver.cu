@@ -454,8 +454,14 @@ struct drape_solver {
     CK(cudaMemcpy(ctl.p, &c, sizeof(c), cudaMemcpyHostToDevice));
   }
 
+  // The reference-order PCG runs over resident rows (k_solve_rows) where the built scene fits it; bit-identical to
+  // k_solve<false, 0>, which variant 3 forces.
+  bool usesResidentRows(const dcu::Dev& d) const {
+    return d.P.pcgVariant == 0 && rowsSmemBytes > 0 && !(learnedOn && netGraph);
+  }
+
   void launchSolve(const dcu::Dev& d) {
-    const bool rows = d.P.pcgVariant == 3 && rowsSmemBytes > 0 && !(learnedOn && netGraph);
+    const bool rows = usesResidentRows(d);
     cudaLaunchConfig_t cfg{};
     cfg.gridDim = dim3(solveGrid);
     cfg.blockDim = dim3(rows ? dcu::kRowThreads : dcu::kSolveThreads);
@@ -1689,10 +1695,19 @@ int drape_cuda_set_pcg_variant(drape_solver* s, int variant) {
   return guarded(s, [&] {
     need(s);
     if (variant < 0 || variant > 3)
-      throw std::invalid_argument(
-          "PCG variant must be 0 (reference order), 1 (pipelined), 2 (Chronopoulos-Gear) or 3 (resident rows)");
+      throw std::invalid_argument("PCG variant must be 0 (reference order), 1 (pipelined), 2 (Chronopoulos-Gear) or 3 "
+                                  "(reference order, 1024-thread kernel)");
     s->pcgVariant = variant;
     s->dev.P.pcgVariant = variant;  // the frame graphs compare the device view and recapture
+  });
+}
+
+int drape_cuda_solve_threads(const drape_solver* s, int* threads) {
+  return guarded(s, [&] {
+    need(s);
+    if (!threads) throw std::invalid_argument("null argument");
+    s->requireBuilt();
+    *threads = s->usesResidentRows(s->dev) ? dcu::kRowThreads : dcu::kSolveThreads;
   });
 }
 
@@ -1734,6 +1749,7 @@ int drape_cuda_reduction_floor(int device, int mode, int iterations, double* ns_
     c.alloc(1);
     partials.alloc(2 * static_cast<size_t>(sms) * dcu::kPartialStride);
     out.alloc(1);
+    CK(cudaMemset(c.p, 0, sizeof(dcu::Control)));
     dcu::Dev d{};
     d.ctl = c.p;
     d.partials = partials.p;

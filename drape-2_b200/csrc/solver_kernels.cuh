@@ -48,7 +48,7 @@ __global__ void __launch_bounds__(kRowThreads, 1) k_solve_rows(Dev D) {
   if (D.ctl->newtonDone) return;
   GridSync gs;
   gs.init(D.ctl, D.P.barrierLimitNs);
-  solveGroup<false, kRowLanes, 3>(D, gs);
+  solveGroup<false, kRowLanes, kResidentRows>(D, gs);
 }
 
 __global__ void k_finish(Dev D) { finishRows(D, blockIdx.x, gridDim.x); }

@@ -85,6 +85,7 @@ def load(build_if_missing: bool = True):
     L.drape_cuda_inject_failure.argtypes = [C.c_void_p, C.c_int]
     L.drape_cuda_set_pcg_variant.argtypes = [C.c_void_p, C.c_int]
     L.drape_cuda_set_host_wait.argtypes = [C.c_void_p, C.c_uint32]
+    L.drape_cuda_solve_threads.argtypes = [C.c_void_p, _P(C.c_int)]
     L.drape_cuda_runner_host_seconds.argtypes = [C.c_void_p, _P(_d)]
     L.drape_cuda_frame_times.argtypes = [C.c_void_p, _P(C.c_uint64), _P(C.c_uint64), C.c_size_t, _P(C.c_size_t)]
     L.drape_cuda_reduction_floor.argtypes = [C.c_int, C.c_int, C.c_int, _P(_d)]
@@ -337,10 +338,16 @@ class CudaSolver:
         self._check(self.L.drape_cuda_set_host_wait(self.h, int(spin_microseconds)))
 
     def set_pcg_variant(self, variant: int) -> None:
-        """0: the reference-order block-Jacobi PCG (default); 1: pipelined, one grid exchange per iteration;
-        2: Chronopoulos-Gear, one reduction and one plain barrier per iteration; 3: the reference order over resident
-        rows (512-thread blocks, row state in registers; runs as 0 where the scene does not fit it)."""
+        """0: the reference-order block-Jacobi PCG (default; resident rows where the scene fits); 1: pipelined, one
+        grid exchange per iteration; 2: Chronopoulos-Gear, one reduction and one plain barrier per iteration; 3: the
+        reference order on the 1024-thread kernel (bit-identical to 0)."""
         self._check(self.L.drape_cuda_set_pcg_variant(self.h, int(variant)))
+
+    def solve_threads(self) -> int:
+        """Threads per block of the built scene's solve kernel: 512 (resident rows) or 1024."""
+        t = C.c_int(0)
+        self._check(self.L.drape_cuda_solve_threads(self.h, C.byref(t)))
+        return t.value
 
     def inject_failure(self, steps: int) -> None:
         self._check(self.L.drape_cuda_inject_failure(self.h, int(steps)))

@@ -228,14 +228,18 @@ int drape_cuda_set_host_wait(drape_solver* s, uint32_t spin_microseconds);
 
 /* The block-Jacobi PCG's form (no reference counterpart; each solves the reference's contact-filtered system with its
    stopping tests, cpu_solver.cpp:169-213): 0 (the default) the reference's order, two grid-wide reductions per
-   iteration; 1 pipelined (Ghysels and Vanroose 2014), one reduction per iteration and three more work vectors, its
-   FP32 recurrences drifting further from the products they stand for; 2 Chronopoulos-Gear, one reduction and one plain
-   barrier per iteration with the reference order's recurrences; 3 the reference's order with resident rows: one
-   512-thread block per SM, each row's PCG state in its thread's registers and the block's matrix in a sliced layout in
-   shared memory, the same arithmetic as 0 in the same order (used where every block has at most 512 rows and its
-   sliced matrix fits in shared memory; elsewhere 3 runs as 0). Forms 0-2 give the same iterates in exact arithmetic
-   and round differently. The learned preconditioner always runs its own PCG. */
+   iteration, run over resident rows (one 512-thread block per SM, each row's PCG state in its thread's registers, the
+   block's matrix in a sliced layout in shared memory) where every block has at most 512 rows and its sliced matrix fits
+   in shared memory, else on one 1024-thread block per SM: the two kernels give bit-identical results; 1 pipelined
+   (Ghysels and Vanroose 2014), one reduction per iteration and three more work vectors, its FP32 recurrences drifting
+   further from the products they stand for; 2 Chronopoulos-Gear, one reduction and one plain barrier per iteration
+   with the reference order's recurrences; 3 the reference's order on the 1024-thread kernel whatever the scene (for
+   comparison). Forms 0-2 give the same iterates in exact arithmetic and round differently. The learned preconditioner
+   always runs its own PCG. */
 int drape_cuda_set_pcg_variant(drape_solver* s, int variant);
+/* Threads per block of the built scene's solve kernel under the current settings: 512 when the reference-order PCG runs
+   over resident rows, else 1024 (the grid has one block per SM either way). */
+int drape_cuda_solve_threads(const drape_solver* s, int* threads);
 
 /* The bounded wait of the device grid barrier, in nanoseconds (0 restores the default of 2 s). A kernel whose barrier
    waits longer sets the handle's error status and returns instead of hanging; the step then fails with
