@@ -228,6 +228,32 @@ def run_reference(args):
     return 0
 
 
+def network_forward(s, args, frames: int = 10) -> dict:
+    """Device time of the learned preconditioner's network forward inside the 60k drape (the inference path:
+    k_scale, k_features, k_slot_encode, k_node x 5, k_message x 4, k_output_rows), from `frames` more frames of the
+    learned solver `s` with every kernel timed by CUDA events, beside its algorithmic bytes: per block slot 108 B of
+    features (block 36, column 4, C_j 36, e 32), 608 B of slot encoding (e 32 read, E 512 and F 64 written), 388 B
+    per layer of messages (E 128, P_j 256, column 4) and 88 B of output (F 48, Q_j 36 on the lower half, L 36);
+    per particle 72 B of scaling (diagonal block, C), 32 B of node features and 416 B per node GEMM (h, a, h', P)."""
+    st = s.structure()
+    n, B = len(st["diag_slot"]), len(st["col_index"])
+    s.profile(True)
+    for _ in range(frames):
+        s.step(1.0 / 60.0, 1, 2)
+    p = s.profile_read()
+    s.profile(False)
+    launches = max(1, p["launches"]["net_forward"])
+    ms = p["milliseconds"]["net_forward"] / launches
+    algo = B * (108 + 608 + 4 * 388 + 88) + n * (72 + 32 + 5 * 416)
+    peak, kind = measured_peaks()
+    gbs = algo / (ms / 1e3) / 1e9 if ms > 0 else None
+    return {"ms_per_forward": ms, "forwards": launches, "particles": n, "block_slots": B,
+            "algorithmic_bytes": algo, "achieved_gbs": gbs, "peak_gbs": peak, "peak_source": kind,
+            "frac": gbs / peak if gbs else None,
+            "note": f"{frames} frames of the learned 60k solver (every Newton iteration runs the network), CUDA events "
+                    f"around each forward; the P_j gathers (4 x 256 B per slot) are served mostly from L2"}
+
+
 def precond_leg(CU, device, args, flush, max_over_ranks, cap: int = 1000, tol: float = 1e-2, window: int = 120):
     """Block-Jacobi against the learned preconditioner on the same GPU and the same 60k tube, in two parts.
     settle: each drapes the workload's own start state to rest at the reference's PCG settings (cap 50, tolerance
@@ -307,6 +333,7 @@ def precond_leg(CU, device, args, flush, max_over_ranks, cap: int = 1000, tol: f
         if name == "learned":
             out["convergence"][name].update({"learned_solves": int(c.learned_solves),
                                              "jacobi_fallbacks": int(c.precond_fallbacks)})
+            out["network_forward"] = network_forward(s, args)
         s.close()
         if net is not None:
             net.close()
@@ -629,6 +656,24 @@ def run_profile_case(args):
         print(json.dumps({"case": "learned", "particles": n, "block_slots": int(len(sysm["col_index"])),
                           "loss": float(loss), "grad_norm": float(np.linalg.norm(grad))}))
         return 0
+    if args.profile_case == "learned_inference":
+        # The network's inference path (the solver's forward) on a captured --workload system, three times.
+        from drape_b200 import learned as LR
+        s = CU.CudaSolver(0)
+        s.build(make_scene(args.workload))
+        for _ in range(20):
+            s.step(1.0 / 60.0, 1, 2)
+        sysm = s.capture_system(1.0 / 60.0)
+        n = len(sysm["diag_slot"])
+        s.close()
+        p = LR.LearnedPreconditioner(0, LR.load_weights("tube"))
+        sid = p.add_sample(sysm["row_start"], sysm["col_index"], sysm["blocks"], np.zeros(n, np.uint8),
+                           sysm["active"], np.zeros((1, n, 3), np.float32))
+        Ls = [p.forward_inference(sid) for _ in range(3)]
+        print(json.dumps({"case": "learned_inference", "workload": args.workload, "particles": n,
+                          "block_slots": int(len(sysm["col_index"])), "deterministic": bool(np.array_equal(Ls[0], Ls[2])),
+                          "l_norm": float(np.linalg.norm(Ls[0]))}))
+        return 0
     if args.profile_case == "drape":
         s = CU.CudaSolver(0)
         s.set_pcg_variant(args.pcg_variant)
@@ -690,7 +735,8 @@ def main():
                          "1 pipelined (one grid exchange an iteration), 2 Chronopoulos-Gear (one reduction and one "
                          "plain barrier), 3 the reference's order on the 1024-thread kernel")
     ap.add_argument("--batch-garments", type=int, default=64, help="garments of the batched leg (0: skip it)")
-    ap.add_argument("--profile-case", choices=["spmv", "batch", "bake", "drape", "learned"], default=None,
+    ap.add_argument("--profile-case", choices=["spmv", "batch", "bake", "drape", "learned", "learned_inference"],
+                    default=None,
                     help="run one small case for a profiler capture instead of the benchmark")
     ap.add_argument("--spmv-tiles", type=int, default=12)
     ap.add_argument("--batch-frames", type=int, default=6)

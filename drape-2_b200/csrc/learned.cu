@@ -195,7 +195,8 @@ __global__ void k_features(Graph g) {
     float fro = 0.0f;
     for (int k = 0; k < 9; ++k) fro += ah[k] * ah[k];
     fro = sqrtf(fro);
-    for (int k = 0; k < 9; ++k) g.Ahat[9 * static_cast<size_t>(s) + k] = ah[k];
+    if (g.Ahat)
+      for (int k = 0; k < 9; ++k) g.Ahat[9 * static_cast<size_t>(s) + k] = ah[k];
     float ev[16] = {0};
     for (int k = 0; k < 9; ++k) ev[k] = ah[k];
     ev[9] = fro;
@@ -527,6 +528,269 @@ __global__ void __launch_bounds__(kThreads) k_output(Graph g, const __nv_bfloat1
     __syncthreads();
   }
   T.done();
+}
+
+// ------------------------------------------------------------------------------------------------------------------
+// Inference path (the solver's forward; the same network as above, regrouped so that no tensor-core operand is
+// gathered). The message GEMM splits by its input halves, W_m [h_j; eps_s] = W_mh h_j + W_me eps_s, and the output
+// layer's likewise, W_o [h_i; h_j; eps_s] = W_oi h_i + W_oj h_j + W_oe eps_s:
+//   k_slot_encode   per 128 consecutive slots (contiguous tiles): eps = relu(W_ee e + b_ee), then in one MMA the
+//                   four layers' slot terms E^l = W_me^l eps + b_m^l (N = 256, stored BF16) and the output layer's
+//                   F = W_oe eps + b_o (FP32);
+//   k_node          per 128 consecutive rows: h' = relu(W_ne f + b_ne) (the node encoder) or h' = h + relu(W_u [h; a]
+//                   + b_u) (a layer's update), then from the same tile the next layer's node term P = W_mh h' or
+//                   the output layer's Q = [W_oi h'; W_oj h'] (FP32);
+//   k_message       one warp per row: a_i = (1/8) sum over the row's message slots, in slot order, of
+//                   relu(P_j + E^l_s), lane l holding features 2l and 2l + 1 (every gather is a 128- or 256-byte
+//                   coalesced row);
+//   k_output_rows   one warp per row, a lane per slot: o = F_s + Q_i + Q_j, G_s, L_s = C_i G_s.
+// The GEMMs stage only contiguous rows; every irregular access is a plain coalesced row gather on the CUDA cores.
+// Against the fused tile kernels the results differ by FP32 summation order and by one BF16 rounding of E.
+
+struct SlotEncSmem {
+  unsigned char x[128 * 16 * 2];
+  unsigned char wee[64 * 16 * 2];
+  unsigned char eps[128 * 64 * 2];
+  unsigned char wme[256 * 64 * 2];
+  unsigned char woe[16 * 64 * 2];
+  float bee[64], bm[256], bo[16];
+  uint64_t bar;
+  uint32_t tmem;
+};
+
+// Rows [r0, r0 + rows) of a K-major operand tile of K columns: row r0 + o = W[o * ld + col0 ... + K).
+__device__ __forceinline__ void stageSlice(unsigned char* tile, int K, int r0, const __nv_bfloat16* W, int rows, int ld,
+                                           int col0) {
+  const int chunks = K / 8;
+  for (int k = threadIdx.x; k < rows * chunks; k += blockDim.x) {
+    const int o = k / chunks, c = k % chunks;
+    st16(tile, r0 + o, c, K, *reinterpret_cast<const uint4*>(W + static_cast<size_t>(o) * ld + col0 + 8 * c));
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_slot_encode(Graph g, const __nv_bfloat16* __restrict__ W,
+                                                          const float* __restrict__ M, int* error) {
+  SlotEncSmem& S = *reinterpret_cast<SlotEncSmem*>(alignSmem(netSmem));
+  TileCtx T;
+  T.init(&S.bar, &S.tmem, 256, error);
+  const int t = threadIdx.x;
+  stageSlice(S.wee, 16, 0, W + Layout::kEe, 64, 16, 0);
+  for (int l = 0; l < kLayers; ++l) stageSlice(S.wme, 64, 64 * l, W + Layout::m(l), 64, 2 * kHidden, kHidden);
+  stageSlice(S.woe, 64, 0, W + Layout::kO, kOutputs, 3 * kHidden, 2 * kHidden);
+  for (int k = t; k < 64; k += kThreads) S.bee[k] = M[Layout::kEeB + k];
+  for (int k = t; k < 256; k += kThreads) S.bm[k] = M[Layout::mB(k / 64) + k % 64];
+  if (t < kOutputs) S.bo[t] = M[Layout::kOB + t];
+  const uint32_t tiles = (g.B + 127) / 128;
+  const size_t layerStride = 64 * static_cast<size_t>(g.B);
+  for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const uint32_t s0 = tile * 128;
+    for (int k = t; k < 128 * 2; k += kThreads) {
+      const uint32_t q = k / 2, c = k % 2, s = s0 + q;
+      st16(S.x, q, c, 16, s < g.B ? reinterpret_cast<const uint4*>(g.e + 16 * static_cast<size_t>(s))[c] : zero4());
+    }
+    if (!T.run([&] { umma::gemmIssue(T.tmem, S.x, S.wee, 128, 64, 16, false); })) break;
+    for (int c = 0; c < 4; ++c) {
+      float v[16];
+      T.load(16 * c, v);
+      for (int k = 0; k < 16; ++k) v[k] = fmaxf(v[k] + S.bee[16 * c + k], 0.0f);
+      st16(S.eps, t, 2 * c, 64, packBf16(v));
+      st16(S.eps, t, 2 * c + 1, 64, packBf16(v + 8));
+    }
+    if (!T.run([&] { umma::gemmIssue(T.tmem, S.eps, S.wme, 128, 256, 64, false); })) break;
+    const uint32_t s = s0 + t;
+    for (int c = 0; c < 16; ++c) {
+      float v[16];
+      T.load(16 * c, v);
+      if (s < g.B) {
+        for (int k = 0; k < 16; ++k) v[k] += S.bm[16 * c + k];
+        uint4* o = reinterpret_cast<uint4*>(g.E + (c / 4) * layerStride + 64 * static_cast<size_t>(s) + 16 * (c % 4));
+        o[0] = packBf16(v);
+        o[1] = packBf16(v + 8);
+      }
+    }
+    if (!T.run([&] { umma::gemmIssue(T.tmem, S.eps, S.woe, 128, kOutputs, 64, false); })) break;
+    {
+      float v[16];
+      T.load(0, v);
+      if (s < g.B) {
+        float4* o = reinterpret_cast<float4*>(g.F + kOutputs * static_cast<size_t>(s));
+        for (int k = 0; k < 4; ++k)
+          o[k] = make_float4(v[4 * k] + S.bo[4 * k], v[4 * k + 1] + S.bo[4 * k + 1], v[4 * k + 2] + S.bo[4 * k + 2],
+                             v[4 * k + 3] + S.bo[4 * k + 3]);
+      }
+    }
+    umma::fenceBeforeSync();
+    __syncthreads();
+  }
+  T.done();
+}
+
+struct NodeSmem {
+  unsigned char x[128 * 128 * 2];
+  unsigned char w1[64 * 128 * 2];
+  unsigned char hb[128 * 64 * 2];
+  unsigned char w2[64 * 64 * 2];
+  float b1[64];
+  uint64_t bar;
+  uint32_t tmem;
+};
+
+// K1 = 16: h' = relu(W1 f + b1) (node encoder; X = f). K1 = 128: h' = h + relu(W1 [h; a] + b1) (a layer's update).
+// Then Out = W2 h' (N2 rows of W2: rows 0..N2-1 of the tile from W2's columns col2a, or for N2 = 32 rows 0..15 from
+// col2a and 16..31 from col2b), FP32, N2 floats per row.
+template <int K1, int N2>
+__global__ void __launch_bounds__(kThreads) k_node(uint32_t n, const __nv_bfloat16* __restrict__ X,
+                                                   const __nv_bfloat16* __restrict__ A,
+                                                   const __nv_bfloat16* __restrict__ W1, const float* __restrict__ b1,
+                                                   const __nv_bfloat16* __restrict__ W2, int ld2, int col2a, int col2b,
+                                                   __nv_bfloat16* __restrict__ hout, float* __restrict__ out,
+                                                   int* error) {
+  NodeSmem& S = *reinterpret_cast<NodeSmem*>(alignSmem(netSmem));
+  TileCtx T;
+  T.init(&S.bar, &S.tmem, 128, error);
+  const int t = threadIdx.x;
+  stageSlice(S.w1, K1, 0, W1, 64, K1, 0);
+  if (N2 == 64) {
+    stageSlice(S.w2, 64, 0, W2, 64, ld2, col2a);
+  } else {
+    stageSlice(S.w2, 64, 0, W2, 16, ld2, col2a);
+    stageSlice(S.w2, 64, 16, W2, 16, ld2, col2b);
+  }
+  if (t < 64) S.b1[t] = b1[t];
+  const uint32_t tiles = (n + 127) / 128;
+  for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const uint32_t r0 = tile * 128;
+    if (K1 == 16) {
+      for (int k = t; k < 128 * 2; k += kThreads) {
+        const uint32_t q = k / 2, c = k % 2, r = r0 + q;
+        st16(S.x, q, c, 16, r < n ? reinterpret_cast<const uint4*>(X + 16 * static_cast<size_t>(r))[c] : zero4());
+      }
+    } else {
+      for (int k = t; k < 128 * 16; k += kThreads) {
+        const uint32_t q = k / 16, c = k % 16, r = r0 + q;
+        uint4 v = zero4();
+        if (r < n)
+          v = c < 8 ? reinterpret_cast<const uint4*>(X + 64 * static_cast<size_t>(r))[c]
+                    : reinterpret_cast<const uint4*>(A + 64 * static_cast<size_t>(r))[c - 8];
+        st16(S.x, q, c, 128, v);
+      }
+    }
+    if (!T.run([&] { umma::gemmIssue(T.tmem, S.x, S.w1, 128, 64, K1, false); })) break;
+    const uint32_t r = r0 + t;
+    for (int c = 0; c < 4; ++c) {
+      float v[16];
+      T.load(16 * c, v);
+      for (int k = 0; k < 16; ++k) v[k] = fmaxf(v[k] + S.b1[16 * c + k], 0.0f);
+      if (K1 == 128) {
+        float h[16];
+        unpackBf16(*reinterpret_cast<const uint4*>(S.x + umma::kmajorOffset(t, 16 * c, 128)), h);
+        unpackBf16(*reinterpret_cast<const uint4*>(S.x + umma::kmajorOffset(t, 16 * c + 8, 128)), h + 8);
+        for (int k = 0; k < 16; ++k) v[k] += h[k];
+      }
+      const uint4 lo = packBf16(v), hi = packBf16(v + 8);
+      st16(S.hb, t, 2 * c, 64, lo);
+      st16(S.hb, t, 2 * c + 1, 64, hi);
+      if (r < n) {
+        uint4* o = reinterpret_cast<uint4*>(hout + 64 * static_cast<size_t>(r));
+        o[2 * c] = lo;
+        o[2 * c + 1] = hi;
+      }
+    }
+    if (!T.run([&] { umma::gemmIssue(T.tmem + 64, S.hb, S.w2, 128, N2, 64, false); })) break;
+    for (int c = 0; c < N2 / 16; ++c) {
+      float v[16];
+      T.load(64 + 16 * c, v);
+      if (r < n) {
+        float4* o = reinterpret_cast<float4*>(out + N2 * static_cast<size_t>(r) + 16 * c);
+        for (int k = 0; k < 4; ++k) o[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+      }
+    }
+    umma::fenceBeforeSync();
+    __syncthreads();
+  }
+  T.done();
+}
+
+// One warp per row: a_i = (1/8) sum of relu(P_j + E_s) over the row's message slots (j != i, neither row pinned) in
+// slot order; lane l accumulates features 2l, 2l + 1. Slots are taken 32 at a time (a lane reads one slot's column);
+// each group of 8 issues its 16 row loads before the first add.
+__global__ void k_message(Graph g, const float* __restrict__ P, const __nv_bfloat16* __restrict__ E,
+                          __nv_bfloat16* __restrict__ aOut) {
+  const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) / 32u;
+  const int lane = threadIdx.x & 31;
+  if (i >= g.n) return;
+  const bool pi = pinnedRow(g, i);
+  const uint32_t rs = __ldg(g.rowStart + i), re = __ldg(g.rowStart + i + 1);
+  float ax = 0.0f, ay = 0.0f;
+  for (uint32_t base = rs; base < re; base += 32) {
+    const uint32_t s = base + lane;
+    uint32_t j = 0;
+    int keep = 0;
+    if (s < re && !pi) {
+      j = colOf(g, s);
+      keep = (j != i && !pinnedRow(g, j)) ? 1 : 0;
+    }
+    const uint32_t cnt = min(32u, re - base);
+    for (uint32_t k0 = 0; k0 < cnt; k0 += 8) {
+      float2 p[8];
+      __nv_bfloat162 e[8];
+      int kp[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const uint32_t k = k0 + u;
+        const uint32_t jk = __shfl_sync(0xffffffffu, j, k & 31u);
+        kp[u] = __shfl_sync(0xffffffffu, keep, k & 31u) && k < cnt;
+        p[u] = make_float2(0.0f, 0.0f);
+        e[u] = __floats2bfloat162_rn(0.0f, 0.0f);
+        if (kp[u]) {
+          p[u] = __ldg(reinterpret_cast<const float2*>(P + 64 * static_cast<size_t>(jk)) + lane);
+          e[u] = reinterpret_cast<const __nv_bfloat162*>(E + 64 * static_cast<size_t>(base + k))[lane];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        if (kp[u]) {
+          ax += fmaxf(p[u].x + __low2float(e[u]), 0.0f);
+          ay += fmaxf(p[u].y + __high2float(e[u]), 0.0f);
+        }
+      }
+    }
+  }
+  reinterpret_cast<__nv_bfloat162*>(aOut + 64 * static_cast<size_t>(i))[lane] =
+      __floats2bfloat162_rn(ax * kAggScale, ay * kAggScale);
+}
+
+// One warp per row, a lane per slot: L_s = C_i G_s on lower live slots (o = F_s + Q_i[0..15] + Q_j[16..31]), zero on
+// the others; every slot of the row is written.
+__global__ void k_output_rows(Graph g, const float* __restrict__ Q) {
+  const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) / 32u;
+  const int lane = threadIdx.x & 31;
+  if (i >= g.n) return;
+  const bool pi = pinnedRow(g, i);
+  const uint32_t rs = __ldg(g.rowStart + i), re = __ldg(g.rowStart + i + 1);
+  float C[9], qi[9];
+  for (int k = 0; k < 9; ++k) {
+    C[k] = __ldg(g.C + 9 * static_cast<size_t>(i) + k);
+    qi[k] = __ldg(Q + 32 * static_cast<size_t>(i) + k);
+  }
+  for (uint32_t s = rs + lane; s < re; s += 32) {
+    const uint32_t j = colOf(g, s);
+    float L[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    if (j <= i && !pi && !pinnedRow(g, j)) {
+      float o[9], G[9];
+      const float4* f = reinterpret_cast<const float4*>(g.F + kOutputs * static_cast<size_t>(s));
+      const float4* qj = reinterpret_cast<const float4*>(Q + 32 * static_cast<size_t>(j) + 16);
+      const float4 f0 = __ldg(f), f1 = __ldg(f + 1), f2 = __ldg(f + 2);
+      const float4 q0 = __ldg(qj), q1 = __ldg(qj + 1), q2 = __ldg(qj + 2);
+      const float fv[12] = {f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, f1.z, f1.w, f2.x, f2.y, f2.z, f2.w};
+      const float qv[12] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w};
+      for (int k = 0; k < 9; ++k) o[k] = fv[k] + qi[k] + qv[k];
+      outputToG(o, j == i, G);
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) L[3 * r + c] = C[3 * r] * G[c] + C[3 * r + 1] * G[3 + c] + C[3 * r + 2] * G[6 + c];
+    }
+    for (int k = 0; k < 9; ++k) g.L[k * g.SP + s] = L[k];
+  }
 }
 
 // ------------------------------------------------------------------------------------------------------------------
@@ -1247,6 +1511,9 @@ T* dalloc(size_t count) {
 }
 
 size_t smemFor(size_t bytes) { return bytes + 128; }
+// k_slot_encode holds 256 TMEM columns: its dynamic shared memory is padded so that at most two blocks share an SM
+// (3 x 77 KB > 228 KB) and a third never waits in tcgen05.alloc for a resident block's columns.
+constexpr size_t kSlotEncodeSmem = sizeof(SlotEncSmem) > 76 * 1024 ? sizeof(SlotEncSmem) : 76 * 1024;
 
 }  // namespace
 
@@ -1293,6 +1560,7 @@ struct GraphStore {
   double* partial = nullptr;
   int partialCount = 0;
   uint32_t liveUnknowns = 0;  // 3 x unpinned rows
+  bool inference = false;     // the inference workspace is allocated
   ~GraphStore() {
     for (void* p : owned) cudaFree(p);
   }
@@ -1306,17 +1574,31 @@ struct GraphStore {
 
 namespace {
 
+void allocInference(GraphStore& s) {
+  if (s.inference) return;
+  Graph& g = s.g;
+  g.E = s.own<__nv_bfloat16>(kLayers * 64 * static_cast<size_t>(g.B));
+  g.F = s.own<float>(kOutputs * static_cast<size_t>(g.B));
+  g.P = s.own<float>(64 * static_cast<size_t>(g.n));
+  g.Q = s.own<float>(32 * static_cast<size_t>(g.n));
+  g.a = s.own<__nv_bfloat16>(64 * static_cast<size_t>(g.n));
+  s.inference = true;
+}
+
+// training: every activation the backward pass reads (a training sample); otherwise the inference path's buffers
+// (a solver's bound graph).
 void allocWorkspace(GraphStore& s, bool training) {
   Graph& g = s.g;
   g.C = s.own<float>(9 * static_cast<size_t>(g.n));
-  g.Ahat = s.own<float>(9 * static_cast<size_t>(g.B));
   g.f = s.own<__nv_bfloat16>(16 * static_cast<size_t>(g.n));
   g.e = s.own<__nv_bfloat16>(16 * static_cast<size_t>(g.B));
-  g.eps = s.own<__nv_bfloat16>(64 * static_cast<size_t>(g.B));
   const int hs = training ? kLayers + 1 : 2;
   for (int l = 0; l < hs; ++l) g.h[l] = s.own<__nv_bfloat16>(64 * static_cast<size_t>(g.n));
   g.L = s.own<float>(9 * static_cast<size_t>(g.SP));
+  if (!training) allocInference(s);
   if (training) {
+    g.Ahat = s.own<float>(9 * static_cast<size_t>(g.B));
+    g.eps = s.own<__nv_bfloat16>(64 * static_cast<size_t>(g.B));
     for (int l = 0; l < kLayers; ++l) g.agg[l] = s.own<__nv_bfloat16>(64 * static_cast<size_t>(g.n));
     g.G = s.own<float>(9 * static_cast<size_t>(g.B));
     g.o = s.own<float>(16 * static_cast<size_t>(g.B));
@@ -1360,7 +1642,11 @@ Network::Network(int device) : device_(device) {
                  {reinterpret_cast<const void*>(k_output), sizeof(OutputSmem)},
                  {reinterpret_cast<const void*>(k_bw_output), sizeof(BwOutSmem)},
                  {reinterpret_cast<const void*>(k_bw_layer), sizeof(BwLayerSmem)},
-                 {reinterpret_cast<const void*>(k_bw_encode), sizeof(BwEncSmem)}};
+                 {reinterpret_cast<const void*>(k_bw_encode), sizeof(BwEncSmem)},
+                 {reinterpret_cast<const void*>(k_slot_encode), kSlotEncodeSmem},
+                 {reinterpret_cast<const void*>(k_node<16, 64>), sizeof(NodeSmem)},
+                 {reinterpret_cast<const void*>(k_node<128, 64>), sizeof(NodeSmem)},
+                 {reinterpret_cast<const void*>(k_node<128, 32>), sizeof(NodeSmem)}};
   for (const auto& k : kernels)
     NCK(cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smemFor(k.bytes))));
 }
@@ -1495,6 +1781,31 @@ void Network::forwardOn(Graph& g, cudaStream_t st, bool training, int* error) {
   const int cap = 2 * numSMs_;
   const __nv_bfloat16* W = wBf16_;
   const float* M = master_;
+  if (!training) {
+    if (!g.E) throw std::logic_error("forwardOn: the graph has no inference workspace");
+    const int rowWarps = static_cast<int>((g.n + 7) / 8);
+    const int nodeGrid = gridFor((g.n + 127) / 128, 3 * numSMs_);
+    const size_t nodeSmem = smemFor(sizeof(NodeSmem));
+    k_slot_encode<<<gridFor((g.B + 127) / 128, 2 * numSMs_), kThreads, smemFor(kSlotEncodeSmem), st>>>(g, W, M, error_);
+    k_node<16, 64><<<nodeGrid, kThreads, nodeSmem, st>>>(g.n, g.f, nullptr, W + Layout::kNe, M + Layout::kNeB,
+                                                         W + Layout::m(0), 2 * kHidden, 0, 0, g.h[0], g.P, error_);
+    for (int l = 0; l < kLayers; ++l) {
+      k_message<<<rowWarps, 256, 0, st>>>(g, g.P, g.E + l * 64 * static_cast<size_t>(g.B), g.a);
+      const __nv_bfloat16* hin = g.h[l & 1];
+      __nv_bfloat16* hout = g.h[(l + 1) & 1];
+      if (l + 1 < kLayers)
+        k_node<128, 64><<<nodeGrid, kThreads, nodeSmem, st>>>(g.n, hin, g.a, W + Layout::u(l), M + Layout::uB(l),
+                                                              W + Layout::m(l + 1), 2 * kHidden, 0, 0, hout, g.P,
+                                                              error_);
+      else
+        k_node<128, 32><<<nodeGrid, kThreads, nodeSmem, st>>>(g.n, hin, g.a, W + Layout::u(l), M + Layout::uB(l),
+                                                              W + Layout::kO, 3 * kHidden, 0, kHidden, hout, g.Q,
+                                                              error_);
+    }
+    k_output_rows<<<rowWarps, 256, 0, st>>>(g, g.Q);
+    NCK(cudaGetLastError());
+    return;
+  }
   k_encode<<<gridFor((g.n + 127) / 128, 4 * numSMs_), kThreads, smemFor(sizeof(EncodeSmem)), st>>>(
       g.n, g.f, W + Layout::kNe, M + Layout::kNeB, g.h[0], error_);
   k_encode<<<gridFor((g.B + 127) / 128, 4 * numSMs_), kThreads, smemFor(sizeof(EncodeSmem)), st>>>(
@@ -1610,6 +1921,23 @@ void Network::forward(int sample, float* Gout, float* Lout) {
   checkError(error_, stream_);
   const Graph& g = s.g;
   if (Gout) NCK(cudaMemcpyAsync(Gout, g.G, sizeof(float) * 9 * g.B, cudaMemcpyDeviceToHost, stream_));
+  if (Lout) {
+    std::vector<float> planes(9 * static_cast<size_t>(g.SP));
+    NCK(cudaMemcpyAsync(planes.data(), g.L, sizeof(float) * planes.size(), cudaMemcpyDeviceToHost, stream_));
+    NCK(cudaStreamSynchronize(stream_));
+    for (uint32_t k = 0; k < g.B; ++k)
+      for (int c = 0; c < 9; ++c) Lout[9 * static_cast<size_t>(k) + c] = planes[c * g.SP + k];
+  }
+  NCK(cudaStreamSynchronize(stream_));
+}
+
+void Network::forwardInference(int sample, float* Lout) {
+  if (sample < 0 || sample >= sampleCount()) throw std::out_of_range("no such sample");
+  GraphStore& s = *samples_[sample];
+  allocInference(s);
+  forwardOn(s.g, stream_, false);
+  checkError(error_, stream_);
+  const Graph& g = s.g;
   if (Lout) {
     std::vector<float> planes(9 * static_cast<size_t>(g.SP));
     NCK(cudaMemcpyAsync(planes.data(), g.L, sizeof(float) * planes.size(), cudaMemcpyDeviceToHost, stream_));
@@ -1857,6 +2185,13 @@ int drape_precond_forward(drape_precond* p, int sample, float* g_blocks, float* 
   return netGuarded(p, [&] {
     needNet(p);
     p->net->forward(sample, g_blocks, l_blocks);
+  });
+}
+
+int drape_precond_forward_inference(drape_precond* p, int sample, float* l_blocks) {
+  return netGuarded(p, [&] {
+    needNet(p);
+    p->net->forwardInference(sample, l_blocks);
   });
 }
 

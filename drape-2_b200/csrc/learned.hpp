@@ -30,10 +30,10 @@ struct Layout {
   static constexpr size_t kEe = kNeB + kHidden, kEeB = kEe + kHidden * kEdgeFeatures;
   static constexpr size_t kLayer0 = kEeB + kHidden;
   static constexpr size_t kLayerSize = 2 * (kHidden * 2 * kHidden + kHidden);
-  static constexpr size_t m(int l) { return kLayer0 + l * kLayerSize; }
-  static constexpr size_t mB(int l) { return m(l) + kHidden * 2 * kHidden; }
-  static constexpr size_t u(int l) { return mB(l) + kHidden; }
-  static constexpr size_t uB(int l) { return u(l) + kHidden * 2 * kHidden; }
+  __host__ __device__ static constexpr size_t m(int l) { return kLayer0 + l * kLayerSize; }
+  __host__ __device__ static constexpr size_t mB(int l) { return m(l) + kHidden * 2 * kHidden; }
+  __host__ __device__ static constexpr size_t u(int l) { return mB(l) + kHidden; }
+  __host__ __device__ static constexpr size_t uB(int l) { return u(l) + kHidden * 2 * kHidden; }
   static constexpr size_t kO = kLayer0 + kLayers * kLayerSize, kOB = kO + kOutputs * 3 * kHidden;
   static constexpr size_t kCount = kOB + kOutputs;
 };
@@ -61,6 +61,12 @@ struct Graph {
   float* G = nullptr;                // B x 9 (training only; lower live slots)
   float* o = nullptr;                // B x 16 (training only)
   float* L = nullptr;                // 9 planes of SP floats: the factor L = S G on lower live slots
+  // Inference workspace (forwardOn without training; eps, Ahat and the per-layer h are not kept).
+  __nv_bfloat16* E = nullptr;        // kLayers planes of B x 64: W_me^l eps_s + b_m^l
+  float* F = nullptr;                // B x 16: W_oe eps_s + b_o
+  float* P = nullptr;                // n x 64: W_mh^l h_j of the current layer
+  float* Q = nullptr;                // n x 32: W_oi h_i (0..15), W_oj h_j (16..31)
+  __nv_bfloat16* a = nullptr;        // n x 64: a_i of the current layer
 };
 
 // Host-owned device buffers of a graph built from host arrays (a training sample) or bound to a solver's arrays.
@@ -97,8 +103,11 @@ class Network {
   void setObjective(int objective) { objective_ = objective; }
 
   // Forward on a solver's system: writes g.L (and the workspace) on `st`. Params must be set. A tensor-core wait that
-  // gives up raises *error (the network's own flag when null).
+  // gives up raises *error (the network's own flag when null). training: the fused tile kernels, keeping every
+  // activation the backward pass reads; otherwise the inference path (needs the inference workspace).
   void forwardOn(Graph& g, cudaStream_t st, bool training, int* error = nullptr);
+  // The inference path on a training sample (its inference workspace is allocated on first use); L as in forward.
+  void forwardInference(int sample, float* Lout);
   // Builds a graph workspace for a solver's CSR (device arrays owned by the solver); returns the store to keep.
   GraphHandle bind(uint32_t n, uint32_t B, uint32_t SP, const uint32_t* hostRowStart,
                                    const uint32_t* hostColIndex, const uint32_t* dRowStart, const uint32_t* dColIndex,

@@ -40,6 +40,7 @@ def _lib():
                                            _u32, _P(C.c_int)]
     L.drape_precond_clear_samples.argtypes = [C.c_void_p]
     L.drape_precond_forward.argtypes = [C.c_void_p, C.c_int, _P(_f), _P(_f)]
+    L.drape_precond_forward_inference.argtypes = [C.c_void_p, C.c_int, _P(_f)]
     L.drape_precond_loss_grad.argtypes = [C.c_void_p, C.c_int, C.c_int, _P(_d), _P(_f)]
     L.drape_precond_apply.argtypes = [C.c_void_p, C.c_int, _P(_f), _P(_f)]
     L.drape_precond_train.argtypes = [C.c_void_p, C.c_int, C.c_float, C.c_int, C.c_uint64, _P(_f)]
@@ -140,6 +141,13 @@ class LearnedPreconditioner:
         Lb = np.zeros((B, 3, 3), np.float32)
         self._check(self.L.drape_precond_forward(self.h, sample, G.ctypes.data_as(_P(_f)), Lb.ctypes.data_as(_P(_f))))
         return G, Lb
+
+    def forward_inference(self, sample: int) -> np.ndarray:
+        """L per slot (B x 3 x 3) from the inference path the solver runs (drape_precond_forward_inference)."""
+        n, B = self.samples[sample]
+        Lb = np.zeros((B, 3, 3), np.float32)
+        self._check(self.L.drape_precond_forward_inference(self.h, sample, Lb.ctypes.data_as(_P(_f))))
+        return Lb
 
     def loss_grad(self, sample: int, residual: int = 0):
         loss = C.c_double()

@@ -43,6 +43,10 @@ int drape_precond_clear_samples(drape_precond* p);
 
 /* Network forward on a sample: G and L = S G per slot (9 floats each, row-major; zero off the lower live slots). */
 int drape_precond_forward(drape_precond* p, int sample, float* g_blocks, float* l_blocks);
+/* The same network on a sample through the inference path the solver runs (slot and node GEMMs on contiguous tiles,
+   message sums and the output layer as row gathers): L per slot as in drape_precond_forward, equal to it up to FP32
+   summation order and one more BF16 rounding. */
+int drape_precond_forward_inference(drape_precond* p, int sample, float* l_blocks);
 /* Evaluation PCG on a sample (no contact filter): solves S^T A S x = S^T r, r the sample's residual `rhs`, with the
    preconditioner G G^T (use_learned != 0) or the identity, which on the scaled system is block-Jacobi; stops at
    |r_k| <= tolerance |r_0| or max_iterations. Gives both preconditioners the same system for an ablation. */

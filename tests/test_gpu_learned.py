@@ -74,6 +74,27 @@ def test_forward_matches_oracle(gpu, sysm, pinned_rows):
     assert np.all(G[~g.lower] == 0) and np.all(L[~g.lower] == 0)
 
 
+@pytest.mark.parametrize("pinned_rows", [0, 7])
+def test_inference_path_matches_oracle_and_training_forward(gpu, sysm, pinned_rows):
+    """The solver's inference path (slot and node GEMMs on contiguous tiles, message sums and the output layer as
+    row gathers) computes the same L as the training forward and as the oracle, to the forward's bar."""
+    flat = _random_params(1)
+    n = len(sysm["diag_slot"])
+    pinned = np.zeros(n, bool)
+    pinned[:pinned_rows] = True
+    net = learned.LearnedPreconditioner(0, flat)
+    sid = _sample(net, sysm, pinned)
+    L_inf = net.forward_inference(sid)
+    _, L_train = net.forward(sid)
+    g = graph_of(sysm, pinned)
+    Gr, _, _ = mpnn.forward(g, flat.astype(np.float64))
+    Lr = mpnn.factor(g, Gr)
+    assert np.linalg.norm(L_inf - Lr) <= 1e-2 * np.linalg.norm(Lr)
+    assert np.linalg.norm(L_inf - L_train) <= 1e-2 * np.linalg.norm(L_train)
+    assert np.all(L_inf[~g.lower] == 0)
+    assert np.array_equal(net.forward_inference(sid), L_inf)  # deterministic
+
+
 def _groups_close(grad, grad_ref):
     assert np.linalg.norm(grad - grad_ref) <= 3e-2 * np.linalg.norm(grad_ref)
     k = 0

@@ -86,7 +86,8 @@ def test_learned_known_answers(gpu, case):
 
 def test_solver_factor_matches_network_on_the_same_system(gpu):
     """The factor the solver's network run produces (inference path, on the solver's own device arrays) equals the
-    sample path's (training forward) on the captured system that the next Newton iteration assembles."""
+    inference path run on the captured system that the next Newton iteration assembles, and the training forward
+    (the fused tile kernels) to the forward's 1e-2 bar."""
     p = learned.LearnedPreconditioner(0, learned.load_weights("tube"))
     s = gpu.CudaSolver(0)
     s.set_precond(p)
@@ -100,8 +101,10 @@ def test_solver_factor_matches_network_on_the_same_system(gpu):
     n = len(sysm["diag_slot"])
     sid = p.add_sample(sysm["row_start"], sysm["col_index"], sysm["blocks"], np.zeros(n, np.uint8), sysm["active"],
                        np.zeros((1, n, 3), np.float32))
+    Li = p.forward_inference(sid)
+    assert np.linalg.norm(Ls - Li) <= 1e-5 * np.linalg.norm(Li)
     _, Lp = p.forward(sid)
-    assert np.linalg.norm(Ls - Lp) <= 1e-5 * np.linalg.norm(Lp)
+    assert np.linalg.norm(Ls - Lp) <= 1e-2 * np.linalg.norm(Lp)
 
 
 def test_trained_network_needs_fewer_pcg_iterations_on_held_out_systems(gpu):
