@@ -167,17 +167,18 @@ __global__ void k_scale(Graph g) {
   for (int k = 0; k < 9; ++k) g.C[9 * static_cast<size_t>(i) + k] = c[k];
 }
 
-// Ahat_s = C_i^T A_s C_j, slot features e_s and node features f_i. One warp per row.
+// Ahat_s = C_i^T A_s C_j, slot features e_s and node features f_i. Sixteen lanes per row (two rows a warp).
 __global__ void k_features(Graph g) {
-  const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) / 32u;
-  const int lane = threadIdx.x & 31;
+  const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) / 16u;
+  const int lane = threadIdx.x & 15;
+  const unsigned mask = 0xFFFFu << (threadIdx.x & 16);
   if (i >= g.n) return;
   const bool pi = pinnedRow(g, i);
   float Ci[9];
   for (int k = 0; k < 9; ++k) Ci[k] = g.C[9 * static_cast<size_t>(i) + k];
   float deg = 0.0f, sumFro = 0.0f, maxFro = 0.0f, rd0 = 0.0f, rd1 = 0.0f, rd2 = 0.0f;
   const uint32_t rs = __ldg(g.rowStart + i), re = __ldg(g.rowStart + i + 1);
-  for (uint32_t s = rs + lane; s < re; s += 32) {
+  for (uint32_t s = rs + lane; s < re; s += 16) {
     const uint32_t j = colOf(g, s);
     const bool live = !pi && !pinnedRow(g, j);
     float ah[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -197,6 +198,7 @@ __global__ void k_features(Graph g) {
     fro = sqrtf(fro);
     if (g.Ahat)
       for (int k = 0; k < 9; ++k) g.Ahat[9 * static_cast<size_t>(s) + k] = ah[k];
+    if (g.code) g.code[s] = j | (live ? 0u : kPinBit);
     float ev[16] = {0};
     for (int k = 0; k < 9; ++k) ev[k] = ah[k];
     ev[9] = fro;
@@ -214,13 +216,13 @@ __global__ void k_features(Graph g) {
       rd2 += ah[8];
     }
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    deg += __shfl_xor_sync(0xffffffffu, deg, o);
-    sumFro += __shfl_xor_sync(0xffffffffu, sumFro, o);
-    maxFro = fmaxf(maxFro, __shfl_xor_sync(0xffffffffu, maxFro, o));
-    rd0 += __shfl_xor_sync(0xffffffffu, rd0, o);
-    rd1 += __shfl_xor_sync(0xffffffffu, rd1, o);
-    rd2 += __shfl_xor_sync(0xffffffffu, rd2, o);
+  for (int o = 8; o > 0; o >>= 1) {
+    deg += __shfl_xor_sync(mask, deg, o);
+    sumFro += __shfl_xor_sync(mask, sumFro, o);
+    maxFro = fmaxf(maxFro, __shfl_xor_sync(mask, maxFro, o));
+    rd0 += __shfl_xor_sync(mask, rd0, o);
+    rd1 += __shfl_xor_sync(mask, rd1, o);
+    rd2 += __shfl_xor_sync(mask, rd2, o);
   }
   if (lane == 0) {
     float fv[16] = {0};
@@ -536,16 +538,43 @@ __global__ void __launch_bounds__(kThreads) k_output(Graph g, const __nv_bfloat1
 // layer's likewise, W_o [h_i; h_j; eps_s] = W_oi h_i + W_oj h_j + W_oe eps_s:
 //   k_slot_encode   per 128 consecutive slots (contiguous tiles): eps = relu(W_ee e + b_ee), then in one MMA the
 //                   four layers' slot terms E^l = W_me^l eps + b_m^l (N = 256, stored BF16) and the output layer's
-//                   F = W_oe eps + b_o (FP32);
+//                   F = W_oe eps + b_o (FP32); results leave through a swizzled shared-memory tile as coalesced rows;
 //   k_node          per 128 consecutive rows: h' = relu(W_ne f + b_ne) (the node encoder) or h' = h + relu(W_u [h; a]
 //                   + b_u) (a layer's update), then from the same tile the next layer's node term P = W_mh h' or
 //                   the output layer's Q = [W_oi h'; W_oj h'] (FP32);
-//   k_message       one warp per row: a_i = (1/8) sum over the row's message slots, in slot order, of
-//                   relu(P_j + E^l_s), lane l holding features 2l and 2l + 1 (every gather is a 128- or 256-byte
-//                   coalesced row);
-//   k_output_rows   one warp per row, a lane per slot: o = F_s + Q_i + Q_j, G_s, L_s = C_i G_s.
-// The GEMMs stage only contiguous rows; every irregular access is a plain coalesced row gather on the CUDA cores.
-// Against the fused tile kernels the results differ by FP32 summation order and by one BF16 rounding of E.
+//   k_message       eight lanes per row (four rows a warp): a_i = (1/8) sum over the row's message slots, in slot
+//                   order, of relu(P_j + E^l_s), lane k holding features 8k..8k+7 (each slot's E and P_j are 128- and
+//                   256-byte coalesced rows);
+//   k_output_slots  one thread per slot: o = F_s + Q_i + Q_j, G_s, L_s = C_i G_s.
+// k_features writes each slot's code (column, bit 31 when the slot carries nothing: either row pinned), so the gathers
+// need no pinned-flag lookups. The GEMMs stage only contiguous rows; every irregular access is a plain coalesced row
+// gather on the CUDA cores. Against the fused tile kernels the results differ by FP32 summation order and by one
+// BF16 rounding of E.
+
+// Loads every 16-byte chunk this thread stages before its first store into the tile (all in flight together):
+// rows [r0, r0 + ROWS) of a K-major operand tile of K columns, row r0 + o = src(o, chunk c) for chunks of 8 BF16.
+template <int K, int ROWS, class Src>
+__device__ __forceinline__ void stageRows(unsigned char* tile, int r0, Src&& src) {
+  constexpr int kChunks = K / 8, kTotal = ROWS * kChunks, kPer = (kTotal + kThreads - 1) / kThreads;
+  uint4 v[kPer];
+#pragma unroll
+  for (int m = 0; m < kPer; ++m) {
+    const int k = threadIdx.x + kThreads * m;
+    v[m] = k < kTotal ? src(k / kChunks, k % kChunks) : zero4();
+  }
+#pragma unroll
+  for (int m = 0; m < kPer; ++m) {
+    const int k = threadIdx.x + kThreads * m;
+    if (k < kTotal) st16(tile, r0 + k / kChunks, k % kChunks, K, v[m]);
+  }
+}
+// Rows of W (row length ld) from column col0 as a K-major tile of K columns.
+template <int K, int ROWS>
+__device__ __forceinline__ void stageWeightRows(unsigned char* tile, int r0, const __nv_bfloat16* W, int ld, int col0) {
+  stageRows<K, ROWS>(tile, r0, [&](int o, int c) {
+    return *reinterpret_cast<const uint4*>(W + static_cast<size_t>(o) * ld + col0 + 8 * c);
+  });
+}
 
 struct SlotEncSmem {
   unsigned char x[128 * 16 * 2];
@@ -553,20 +582,11 @@ struct SlotEncSmem {
   unsigned char eps[128 * 64 * 2];
   unsigned char wme[256 * 64 * 2];
   unsigned char woe[16 * 64 * 2];
+  unsigned char out[2][128 * 128];  // results of one layer (128 slots x 128 B), swizzled; double-buffered
   float bee[64], bm[256], bo[16];
   uint64_t bar;
   uint32_t tmem;
 };
-
-// Rows [r0, r0 + rows) of a K-major operand tile of K columns: row r0 + o = W[o * ld + col0 ... + K).
-__device__ __forceinline__ void stageSlice(unsigned char* tile, int K, int r0, const __nv_bfloat16* W, int rows, int ld,
-                                           int col0) {
-  const int chunks = K / 8;
-  for (int k = threadIdx.x; k < rows * chunks; k += blockDim.x) {
-    const int o = k / chunks, c = k % chunks;
-    st16(tile, r0 + o, c, K, *reinterpret_cast<const uint4*>(W + static_cast<size_t>(o) * ld + col0 + 8 * c));
-  }
-}
 
 __global__ void __launch_bounds__(kThreads) k_slot_encode(Graph g, const __nv_bfloat16* __restrict__ W,
                                                           const float* __restrict__ M, int* error) {
@@ -574,9 +594,9 @@ __global__ void __launch_bounds__(kThreads) k_slot_encode(Graph g, const __nv_bf
   TileCtx T;
   T.init(&S.bar, &S.tmem, 256, error);
   const int t = threadIdx.x;
-  stageSlice(S.wee, 16, 0, W + Layout::kEe, 64, 16, 0);
-  for (int l = 0; l < kLayers; ++l) stageSlice(S.wme, 64, 64 * l, W + Layout::m(l), 64, 2 * kHidden, kHidden);
-  stageSlice(S.woe, 64, 0, W + Layout::kO, kOutputs, 3 * kHidden, 2 * kHidden);
+  stageWeightRows<16, 64>(S.wee, 0, W + Layout::kEe, 16, 0);
+  for (int l = 0; l < kLayers; ++l) stageWeightRows<64, 64>(S.wme, 64 * l, W + Layout::m(l), 2 * kHidden, kHidden);
+  stageWeightRows<64, kOutputs>(S.woe, 0, W + Layout::kO, 3 * kHidden, 2 * kHidden);
   for (int k = t; k < 64; k += kThreads) S.bee[k] = M[Layout::kEeB + k];
   for (int k = t; k < 256; k += kThreads) S.bm[k] = M[Layout::mB(k / 64) + k % 64];
   if (t < kOutputs) S.bo[t] = M[Layout::kOB + t];
@@ -584,10 +604,10 @@ __global__ void __launch_bounds__(kThreads) k_slot_encode(Graph g, const __nv_bf
   const size_t layerStride = 64 * static_cast<size_t>(g.B);
   for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
     const uint32_t s0 = tile * 128;
-    for (int k = t; k < 128 * 2; k += kThreads) {
-      const uint32_t q = k / 2, c = k % 2, s = s0 + q;
-      st16(S.x, q, c, 16, s < g.B ? reinterpret_cast<const uint4*>(g.e + 16 * static_cast<size_t>(s))[c] : zero4());
-    }
+    stageRows<16, 128>(S.x, 0, [&](int q, int c) {
+      const uint32_t s = s0 + q;
+      return s < g.B ? reinterpret_cast<const uint4*>(g.e + 16 * static_cast<size_t>(s))[c] : zero4();
+    });
     if (!T.run([&] { umma::gemmIssue(T.tmem, S.x, S.wee, 128, 64, 16, false); })) break;
     for (int c = 0; c < 4; ++c) {
       float v[16];
@@ -597,26 +617,44 @@ __global__ void __launch_bounds__(kThreads) k_slot_encode(Graph g, const __nv_bf
       st16(S.eps, t, 2 * c + 1, 64, packBf16(v + 8));
     }
     if (!T.run([&] { umma::gemmIssue(T.tmem, S.eps, S.wme, 128, 256, 64, false); })) break;
-    const uint32_t s = s0 + t;
-    for (int c = 0; c < 16; ++c) {
-      float v[16];
-      T.load(16 * c, v);
-      if (s < g.B) {
-        for (int k = 0; k < 16; ++k) v[k] += S.bm[16 * c + k];
-        uint4* o = reinterpret_cast<uint4*>(g.E + (c / 4) * layerStride + 64 * static_cast<size_t>(s) + 16 * (c % 4));
-        o[0] = packBf16(v);
-        o[1] = packBf16(v + 8);
+    // Layer l: thread t writes its slot's 8 chunks into row t of out[l & 1] (chunk c at position c ^ (t & 7): the
+    // eight lanes of a store phase hit eight different 16-byte bank groups), then the block copies the 128 rows out
+    // as 16 KB of consecutive bytes (lane k of a warp: chunk k of a row run), E's layout being [layer][slot][64].
+    for (int l = 0; l < kLayers; ++l) {
+      unsigned char* buf = S.out[l & 1];
+      for (int c = 0; c < 4; ++c) {
+        float v[16];
+        T.load(64 * l + 16 * c, v);
+        for (int k = 0; k < 16; ++k) v[k] += S.bm[64 * l + 16 * c + k];
+        *reinterpret_cast<uint4*>(buf + 128 * t + 16 * ((2 * c) ^ (t & 7))) = packBf16(v);
+        *reinterpret_cast<uint4*>(buf + 128 * t + 16 * ((2 * c + 1) ^ (t & 7))) = packBf16(v + 8);
+      }
+      __syncthreads();
+      __nv_bfloat16* dst = g.E + l * layerStride + 64 * static_cast<size_t>(s0);
+#pragma unroll
+      for (int m = 0; m < 8; ++m) {
+        const int k = t + kThreads * m, row = k >> 3, c = k & 7;
+        if (s0 + row < g.B)
+          reinterpret_cast<uint4*>(dst)[k] = *reinterpret_cast<const uint4*>(buf + 128 * row + 16 * (c ^ (row & 7)));
       }
     }
     if (!T.run([&] { umma::gemmIssue(T.tmem, S.eps, S.woe, 128, kOutputs, 64, false); })) break;
     {
+      // F: 64 B a slot, rows of 4 chunks (chunk c at c ^ ((t >> 1) & 3)), copied out as 8 KB of consecutive bytes.
+      // out[0] is free: the run above synchronised after its last copy-out read.
+      unsigned char* buf = S.out[0];
       float v[16];
       T.load(0, v);
-      if (s < g.B) {
-        float4* o = reinterpret_cast<float4*>(g.F + kOutputs * static_cast<size_t>(s));
-        for (int k = 0; k < 4; ++k)
-          o[k] = make_float4(v[4 * k] + S.bo[4 * k], v[4 * k + 1] + S.bo[4 * k + 1], v[4 * k + 2] + S.bo[4 * k + 2],
-                             v[4 * k + 3] + S.bo[4 * k + 3]);
+      for (int c = 0; c < 4; ++c)
+        *reinterpret_cast<float4*>(buf + 64 * t + 16 * (c ^ ((t >> 1) & 3))) =
+            make_float4(v[4 * c] + S.bo[4 * c], v[4 * c + 1] + S.bo[4 * c + 1], v[4 * c + 2] + S.bo[4 * c + 2],
+                        v[4 * c + 3] + S.bo[4 * c + 3]);
+      __syncthreads();
+      float4* dst = reinterpret_cast<float4*>(g.F + kOutputs * static_cast<size_t>(s0));
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        const int k = t + kThreads * m, row = k >> 2, c = k & 3;
+        if (s0 + row < g.B) dst[k] = *reinterpret_cast<const float4*>(buf + 64 * row + 16 * (c ^ ((row >> 1) & 3)));
       }
     }
     umma::fenceBeforeSync();
@@ -649,31 +687,29 @@ __global__ void __launch_bounds__(kThreads) k_node(uint32_t n, const __nv_bfloat
   TileCtx T;
   T.init(&S.bar, &S.tmem, 128, error);
   const int t = threadIdx.x;
-  stageSlice(S.w1, K1, 0, W1, 64, K1, 0);
+  stageWeightRows<K1, 64>(S.w1, 0, W1, K1, 0);
   if (N2 == 64) {
-    stageSlice(S.w2, 64, 0, W2, 64, ld2, col2a);
+    stageWeightRows<64, 64>(S.w2, 0, W2, ld2, col2a);
   } else {
-    stageSlice(S.w2, 64, 0, W2, 16, ld2, col2a);
-    stageSlice(S.w2, 64, 16, W2, 16, ld2, col2b);
+    stageWeightRows<64, 16>(S.w2, 0, W2, ld2, col2a);
+    stageWeightRows<64, 16>(S.w2, 16, W2, ld2, col2b);
   }
   if (t < 64) S.b1[t] = b1[t];
   const uint32_t tiles = (n + 127) / 128;
   for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
     const uint32_t r0 = tile * 128;
     if (K1 == 16) {
-      for (int k = t; k < 128 * 2; k += kThreads) {
-        const uint32_t q = k / 2, c = k % 2, r = r0 + q;
-        st16(S.x, q, c, 16, r < n ? reinterpret_cast<const uint4*>(X + 16 * static_cast<size_t>(r))[c] : zero4());
-      }
+      stageRows<16, 128>(S.x, 0, [&](int q, int c) {
+        const uint32_t r = r0 + q;
+        return r < n ? reinterpret_cast<const uint4*>(X + 16 * static_cast<size_t>(r))[c] : zero4();
+      });
     } else {
-      for (int k = t; k < 128 * 16; k += kThreads) {
-        const uint32_t q = k / 16, c = k % 16, r = r0 + q;
-        uint4 v = zero4();
-        if (r < n)
-          v = c < 8 ? reinterpret_cast<const uint4*>(X + 64 * static_cast<size_t>(r))[c]
-                    : reinterpret_cast<const uint4*>(A + 64 * static_cast<size_t>(r))[c - 8];
-        st16(S.x, q, c, 128, v);
-      }
+      stageRows<128, 128>(S.x, 0, [&](int q, int c) {
+        const uint32_t r = r0 + q;
+        if (r >= n) return zero4();
+        return c < 8 ? reinterpret_cast<const uint4*>(X + 64 * static_cast<size_t>(r))[c]
+                     : reinterpret_cast<const uint4*>(A + 64 * static_cast<size_t>(r))[c - 8];
+      });
     }
     if (!T.run([&] { umma::gemmIssue(T.tmem, S.x, S.w1, 128, 64, K1, false); })) break;
     const uint32_t r = r0 + t;
@@ -711,86 +747,95 @@ __global__ void __launch_bounds__(kThreads) k_node(uint32_t n, const __nv_bfloat
   T.done();
 }
 
-// One warp per row: a_i = (1/8) sum of relu(P_j + E_s) over the row's message slots (j != i, neither row pinned) in
-// slot order; lane l accumulates features 2l, 2l + 1. Slots are taken 32 at a time (a lane reads one slot's column);
-// each group of 8 issues its 16 row loads before the first add.
-__global__ void k_message(Graph g, const float* __restrict__ P, const __nv_bfloat16* __restrict__ E,
-                          __nv_bfloat16* __restrict__ aOut) {
-  const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) / 32u;
-  const int lane = threadIdx.x & 31;
+// slotRow[s] = the row of slot s. One thread per row; run once per graph.
+__global__ void k_slot_rows(Graph g) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.n) return;
-  const bool pi = pinnedRow(g, i);
-  const uint32_t rs = __ldg(g.rowStart + i), re = __ldg(g.rowStart + i + 1);
-  float ax = 0.0f, ay = 0.0f;
-  for (uint32_t base = rs; base < re; base += 32) {
-    const uint32_t s = base + lane;
-    uint32_t j = 0;
-    int keep = 0;
-    if (s < re && !pi) {
-      j = colOf(g, s);
-      keep = (j != i && !pinnedRow(g, j)) ? 1 : 0;
-    }
-    const uint32_t cnt = min(32u, re - base);
-    for (uint32_t k0 = 0; k0 < cnt; k0 += 8) {
-      float2 p[8];
-      __nv_bfloat162 e[8];
-      int kp[8];
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const uint32_t k = k0 + u;
-        const uint32_t jk = __shfl_sync(0xffffffffu, j, k & 31u);
-        kp[u] = __shfl_sync(0xffffffffu, keep, k & 31u) && k < cnt;
-        p[u] = make_float2(0.0f, 0.0f);
-        e[u] = __floats2bfloat162_rn(0.0f, 0.0f);
-        if (kp[u]) {
-          p[u] = __ldg(reinterpret_cast<const float2*>(P + 64 * static_cast<size_t>(jk)) + lane);
-          e[u] = reinterpret_cast<const __nv_bfloat162*>(E + 64 * static_cast<size_t>(base + k))[lane];
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        if (kp[u]) {
-          ax += fmaxf(p[u].x + __low2float(e[u]), 0.0f);
-          ay += fmaxf(p[u].y + __high2float(e[u]), 0.0f);
-        }
-      }
-    }
-  }
-  reinterpret_cast<__nv_bfloat162*>(aOut + 64 * static_cast<size_t>(i))[lane] =
-      __floats2bfloat162_rn(ax * kAggScale, ay * kAggScale);
+  for (uint32_t s = __ldg(g.rowStart + i); s < __ldg(g.rowStart + i + 1); ++s) g.slotRow[s] = i;
 }
 
-// One warp per row, a lane per slot: L_s = C_i G_s on lower live slots (o = F_s + Q_i[0..15] + Q_j[16..31]), zero on
-// the others; every slot of the row is written.
-__global__ void k_output_rows(Graph g, const float* __restrict__ Q) {
-  const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) / 32u;
-  const int lane = threadIdx.x & 31;
-  if (i >= g.n) return;
-  const bool pi = pinnedRow(g, i);
-  const uint32_t rs = __ldg(g.rowStart + i), re = __ldg(g.rowStart + i + 1);
-  float C[9], qi[9];
-  for (int k = 0; k < 9; ++k) {
-    C[k] = __ldg(g.C + 9 * static_cast<size_t>(i) + k);
-    qi[k] = __ldg(Q + 32 * static_cast<size_t>(i) + k);
-  }
-  for (uint32_t s = rs + lane; s < re; s += 32) {
-    const uint32_t j = colOf(g, s);
-    float L[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    if (j <= i && !pi && !pinnedRow(g, j)) {
-      float o[9], G[9];
-      const float4* f = reinterpret_cast<const float4*>(g.F + kOutputs * static_cast<size_t>(s));
-      const float4* qj = reinterpret_cast<const float4*>(Q + 32 * static_cast<size_t>(j) + 16);
-      const float4 f0 = __ldg(f), f1 = __ldg(f + 1), f2 = __ldg(f + 2);
-      const float4 q0 = __ldg(qj), q1 = __ldg(qj + 1), q2 = __ldg(qj + 2);
-      const float fv[12] = {f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, f1.z, f1.w, f2.x, f2.y, f2.z, f2.w};
-      const float qv[12] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w};
-      for (int k = 0; k < 9; ++k) o[k] = fv[k] + qi[k] + qv[k];
-      outputToG(o, j == i, G);
-      for (int r = 0; r < 3; ++r)
-        for (int c = 0; c < 3; ++c) L[3 * r + c] = C[3 * r] * G[c] + C[3 * r + 1] * G[3 + c] + C[3 * r + 2] * G[6 + c];
+// Eight lanes per row (four rows a warp): a_i = (1/8) sum of relu(P_j + E_s) over the row's message slots (code
+// without bit 31, j != i) in slot order; lane k of the row's eight accumulates features 8k..8k+7. The row's codes are
+// read eight at a time (one a lane) and shared by shuffles; four slots' E and P_j rows are loaded before the first add.
+__global__ void k_message(Graph g, const float* __restrict__ P, const __nv_bfloat16* __restrict__ E,
+                          __nv_bfloat16* __restrict__ aOut) {
+  const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t i = gt / 8u;
+  const int sub = threadIdx.x & 7;
+  const unsigned mask = 0xFFu << (threadIdx.x & 24);
+  const bool row = i < g.n;
+  const uint32_t rs = row ? __ldg(g.rowStart + i) : 0u, re = row ? __ldg(g.rowStart + i + 1) : 0u;
+  float acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  // Every lane of a row group loops the same number of times (the row's slot count).
+  for (uint32_t base = rs; base < re; base += 8) {
+    const uint32_t cnt = min(8u, re - base);
+    const uint32_t myCode = sub < static_cast<int>(cnt) ? __ldg(g.code + base + sub) : kPinBit;
+#pragma unroll
+    for (int k0 = 0; k0 < 8; k0 += 4) {
+      uint4 e[4];
+      float4 p0[4], p1[4];
+      bool kp[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const uint32_t code = __shfl_sync(mask, myCode, k0 + u, 8);
+        const uint32_t j = code & ~kPinBit;
+        kp[u] = !(code & kPinBit) && j != i;
+        e[u] = zero4();
+        p0[u] = p1[u] = make_float4(0, 0, 0, 0);
+        if (kp[u]) {
+          e[u] = __ldg(reinterpret_cast<const uint4*>(E + 64 * static_cast<size_t>(base + k0 + u)) + sub);
+          const float4* pj = reinterpret_cast<const float4*>(P + 64 * static_cast<size_t>(j) + 8 * sub);
+          p0[u] = __ldg(pj);
+          p1[u] = __ldg(pj + 1);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (!kp[u]) continue;
+        float ev[8];
+        unpackBf16(e[u], ev);
+        acc[0] += fmaxf(p0[u].x + ev[0], 0.0f);
+        acc[1] += fmaxf(p0[u].y + ev[1], 0.0f);
+        acc[2] += fmaxf(p0[u].z + ev[2], 0.0f);
+        acc[3] += fmaxf(p0[u].w + ev[3], 0.0f);
+        acc[4] += fmaxf(p1[u].x + ev[4], 0.0f);
+        acc[5] += fmaxf(p1[u].y + ev[5], 0.0f);
+        acc[6] += fmaxf(p1[u].z + ev[6], 0.0f);
+        acc[7] += fmaxf(p1[u].w + ev[7], 0.0f);
+      }
     }
-    for (int k = 0; k < 9; ++k) g.L[k * g.SP + s] = L[k];
   }
+  if (row) {
+    for (int k = 0; k < 8; ++k) acc[k] *= kAggScale;
+    reinterpret_cast<uint4*>(aOut + 64 * static_cast<size_t>(i))[sub] = packBf16(acc);
+  }
+}
+
+// One thread per slot: L_s = C_i G_s on lower live slots (o = F_s + Q_i[0..8] + Q_j[16..24]), zero on the others.
+__global__ void k_output_slots(Graph g, const float* __restrict__ Q) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= g.B) return;
+  const uint32_t code = __ldg(g.code + s), i = __ldg(g.slotRow + s), j = code & ~kPinBit;
+  float L[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (!(code & kPinBit) && j <= i) {
+    const float4* f = reinterpret_cast<const float4*>(g.F + kOutputs * static_cast<size_t>(s));
+    const float4* qi = reinterpret_cast<const float4*>(Q + 32 * static_cast<size_t>(i));
+    const float4* qj = reinterpret_cast<const float4*>(Q + 32 * static_cast<size_t>(j) + 16);
+    const float4 f0 = __ldg(f), f1 = __ldg(f + 1), f2 = __ldg(f + 2);
+    const float4 a0 = __ldg(qi), a1 = __ldg(qi + 1), a2 = __ldg(qi + 2);
+    const float4 b0 = __ldg(qj), b1 = __ldg(qj + 1), b2 = __ldg(qj + 2);
+    float C[9];
+    for (int k = 0; k < 9; ++k) C[k] = __ldg(g.C + 9 * static_cast<size_t>(i) + k);
+    const float fv[9] = {f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, f1.z, f1.w, f2.x};
+    const float av[9] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a2.x};
+    const float bv[9] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w, b2.x};
+    float o[9], G[9];
+    for (int k = 0; k < 9; ++k) o[k] = fv[k] + av[k] + bv[k];
+    outputToG(o, j == i, G);
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) L[3 * r + c] = C[3 * r] * G[c] + C[3 * r + 1] * G[3 + c] + C[3 * r + 2] * G[6 + c];
+  }
+  for (int k = 0; k < 9; ++k) g.L[k * g.SP + s] = L[k];
 }
 
 // ------------------------------------------------------------------------------------------------------------------
@@ -1512,7 +1557,8 @@ T* dalloc(size_t count) {
 
 size_t smemFor(size_t bytes) { return bytes + 128; }
 // k_slot_encode holds 256 TMEM columns: its dynamic shared memory is padded so that at most two blocks share an SM
-// (3 x 77 KB > 228 KB) and a third never waits in tcgen05.alloc for a resident block's columns.
+// (3 x 77 KB > 228 KB) and a third never waits in tcgen05.alloc for a resident block's columns (the grid is also
+// capped at two blocks per SM).
 constexpr size_t kSlotEncodeSmem = sizeof(SlotEncSmem) > 76 * 1024 ? sizeof(SlotEncSmem) : 76 * 1024;
 
 }  // namespace
@@ -1574,9 +1620,13 @@ struct GraphStore {
 
 namespace {
 
-void allocInference(GraphStore& s) {
+void allocInference(GraphStore& s, cudaStream_t st) {
   if (s.inference) return;
   Graph& g = s.g;
+  g.code = s.own<uint32_t>(g.B);
+  g.slotRow = s.own<uint32_t>(g.B);
+  k_slot_rows<<<static_cast<int>((g.n + 255) / 256), 256, 0, st>>>(g);
+  NCK(cudaGetLastError());
   g.E = s.own<__nv_bfloat16>(kLayers * 64 * static_cast<size_t>(g.B));
   g.F = s.own<float>(kOutputs * static_cast<size_t>(g.B));
   g.P = s.own<float>(64 * static_cast<size_t>(g.n));
@@ -1587,7 +1637,7 @@ void allocInference(GraphStore& s) {
 
 // training: every activation the backward pass reads (a training sample); otherwise the inference path's buffers
 // (a solver's bound graph).
-void allocWorkspace(GraphStore& s, bool training) {
+void allocWorkspace(GraphStore& s, bool training, cudaStream_t st) {
   Graph& g = s.g;
   g.C = s.own<float>(9 * static_cast<size_t>(g.n));
   g.f = s.own<__nv_bfloat16>(16 * static_cast<size_t>(g.n));
@@ -1595,7 +1645,7 @@ void allocWorkspace(GraphStore& s, bool training) {
   const int hs = training ? kLayers + 1 : 2;
   for (int l = 0; l < hs; ++l) g.h[l] = s.own<__nv_bfloat16>(64 * static_cast<size_t>(g.n));
   g.L = s.own<float>(9 * static_cast<size_t>(g.SP));
-  if (!training) allocInference(s);
+  if (!training) allocInference(s, st);
   if (training) {
     g.Ahat = s.own<float>(9 * static_cast<size_t>(g.B));
     g.eps = s.own<__nv_bfloat16>(64 * static_cast<size_t>(g.B));
@@ -1723,7 +1773,7 @@ int Network::addSample(uint32_t n, const uint32_t* rowStart, const uint32_t* col
   g.blocks = dbl;
   g.pinnedBase = dpin;
   g.activeBase = dact;
-  allocWorkspace(*s, true);
+  allocWorkspace(*s, true, stream_);
   s->residualCount = residualCount;
   for (uint32_t i = 0; i < n; ++i) s->liveUnknowns += pinned[i] ? 0u : 3u;
   s->residuals.resize(static_cast<size_t>(residualCount) * n);
@@ -1768,7 +1818,7 @@ GraphHandle Network::bind(uint32_t n, uint32_t B, uint32_t SP, const uint32_t* h
   g.pinnedStride = pinnedStride;
   g.activeBase = activeBase;
   g.activeStride = activeStride;
-  allocWorkspace(*s, false);
+  allocWorkspace(*s, false, st);
   NCK(cudaStreamSynchronize(st));
   return GraphHandle(s.release());
 }
@@ -1777,20 +1827,20 @@ void Network::forwardOn(Graph& g, cudaStream_t st, bool training, int* error) {
   int* error_ = error ? error : this->error_;
   const int rowBlocks = static_cast<int>((g.n + 127) / 128);
   k_scale<<<rowBlocks, 128, 0, st>>>(g);
-  k_features<<<static_cast<int>((g.n + 7) / 8), 256, 0, st>>>(g);
+  k_features<<<static_cast<int>((g.n + 15) / 16), 256, 0, st>>>(g);
   const int cap = 2 * numSMs_;
   const __nv_bfloat16* W = wBf16_;
   const float* M = master_;
   if (!training) {
     if (!g.E) throw std::logic_error("forwardOn: the graph has no inference workspace");
-    const int rowWarps = static_cast<int>((g.n + 7) / 8);
+    const int rowGroups = static_cast<int>((g.n + 31) / 32);  // eight lanes a row
     const int nodeGrid = gridFor((g.n + 127) / 128, 3 * numSMs_);
     const size_t nodeSmem = smemFor(sizeof(NodeSmem));
     k_slot_encode<<<gridFor((g.B + 127) / 128, 2 * numSMs_), kThreads, smemFor(kSlotEncodeSmem), st>>>(g, W, M, error_);
     k_node<16, 64><<<nodeGrid, kThreads, nodeSmem, st>>>(g.n, g.f, nullptr, W + Layout::kNe, M + Layout::kNeB,
                                                          W + Layout::m(0), 2 * kHidden, 0, 0, g.h[0], g.P, error_);
     for (int l = 0; l < kLayers; ++l) {
-      k_message<<<rowWarps, 256, 0, st>>>(g, g.P, g.E + l * 64 * static_cast<size_t>(g.B), g.a);
+      k_message<<<rowGroups, 256, 0, st>>>(g, g.P, g.E + l * 64 * static_cast<size_t>(g.B), g.a);
       const __nv_bfloat16* hin = g.h[l & 1];
       __nv_bfloat16* hout = g.h[(l + 1) & 1];
       if (l + 1 < kLayers)
@@ -1802,7 +1852,7 @@ void Network::forwardOn(Graph& g, cudaStream_t st, bool training, int* error) {
                                                               W + Layout::kO, 3 * kHidden, 0, kHidden, hout, g.Q,
                                                               error_);
     }
-    k_output_rows<<<rowWarps, 256, 0, st>>>(g, g.Q);
+    k_output_slots<<<static_cast<int>((g.B + 255) / 256), 256, 0, st>>>(g, g.Q);
     NCK(cudaGetLastError());
     return;
   }
@@ -1934,7 +1984,7 @@ void Network::forward(int sample, float* Gout, float* Lout) {
 void Network::forwardInference(int sample, float* Lout) {
   if (sample < 0 || sample >= sampleCount()) throw std::out_of_range("no such sample");
   GraphStore& s = *samples_[sample];
-  allocInference(s);
+  allocInference(s, stream_);
   forwardOn(s.g, stream_, false);
   checkError(error_, stream_);
   const Graph& g = s.g;

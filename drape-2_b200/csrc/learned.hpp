@@ -67,6 +67,8 @@ struct Graph {
   float* P = nullptr;                // n x 64: W_mh^l h_j of the current layer
   float* Q = nullptr;                // n x 32: W_oi h_i (0..15), W_oj h_j (16..31)
   __nv_bfloat16* a = nullptr;        // n x 64: a_i of the current layer
+  uint32_t* code = nullptr;          // B: column of the slot, bit 31 when either row is pinned (written by k_features)
+  uint32_t* slotRow = nullptr;       // B: row of the slot (fixed with the CSR)
 };
 
 // Host-owned device buffers of a graph built from host arrays (a training sample) or bound to a solver's arrays.
