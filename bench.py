@@ -231,10 +231,13 @@ def run_reference(args):
 def network_forward(s, args, frames: int = 10) -> dict:
     """Device time of the learned preconditioner's network forward inside the 60k drape (the inference path:
     k_scale, k_features, k_slot_encode, k_node x 5, k_message x 4, k_output_rows), from `frames` more frames of the
-    learned solver `s` with every kernel timed by CUDA events, beside its algorithmic bytes: per block slot 108 B of
-    features (block 36, column 4, C_j 36, e 32), 608 B of slot encoding (e 32 read, E 512 and F 64 written), 388 B
-    per layer of messages (E 128, P_j 256, column 4) and 88 B of output (F 48, Q_j 36 on the lower half, L 36);
-    per particle 72 B of scaling (diagonal block, C), 32 B of node features and 416 B per node GEMM (h, a, h', P)."""
+    learned solver `s` with every kernel timed by CUDA events, beside its algorithmic bytes: per block slot 112 B of
+    features (block 36, column 4, C_j 36, e 32, code 4), 608 B of slot encoding (e 32 read, E 512 and F 64 written),
+    260 B per layer of messages (E 128, P_j 128, code 4) and 130 B of output (code and row 8, L 36 written, F 48 and
+    Q_i, Q_j, C_i 108 on the lower live slots, about 55 %); per particle 72 B of scaling (diagonal block, C), 76 B of
+    node features (C_i, row bounds, f), 136 B per layer of messages (row bounds, a) and 2336 B of node GEMMs (the
+    encoder: f 32 read, h 128 and P 128 written; each layer's update: h 128 and a 128 read, h' 128 and P or Q 128
+    written)."""
     st = s.structure()
     n, B = len(st["diag_slot"]), len(st["col_index"])
     s.profile(True)
@@ -244,14 +247,14 @@ def network_forward(s, args, frames: int = 10) -> dict:
     s.profile(False)
     launches = max(1, p["launches"]["net_forward"])
     ms = p["milliseconds"]["net_forward"] / launches
-    algo = B * (108 + 608 + 4 * 388 + 88) + n * (72 + 32 + 5 * 416)
+    algo = B * (112 + 608 + 4 * 260 + 130) + n * (72 + 76 + 4 * 136 + 288 + 4 * 512)
     peak, kind = measured_peaks()
     gbs = algo / (ms / 1e3) / 1e9 if ms > 0 else None
     return {"ms_per_forward": ms, "forwards": launches, "particles": n, "block_slots": B,
             "algorithmic_bytes": algo, "achieved_gbs": gbs, "peak_gbs": peak, "peak_source": kind,
             "frac": gbs / peak if gbs else None,
             "note": f"{frames} frames of the learned 60k solver (every Newton iteration runs the network), CUDA events "
-                    f"around each forward; the P_j gathers (4 x 256 B per slot) are served mostly from L2"}
+                    f"around each forward; the P_j gathers (4 x 128 B per slot) are served mostly from L2"}
 
 
 def precond_leg(CU, device, args, flush, max_over_ranks, cap: int = 1000, tol: float = 1e-2, window: int = 120):

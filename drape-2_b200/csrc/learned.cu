@@ -13,6 +13,9 @@
 #include <random>
 #include <stdexcept>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "device_math.cuh"
 #include "learned.hpp"
 #include "umma.cuh"
@@ -539,17 +542,17 @@ __global__ void __launch_bounds__(kThreads) k_output(Graph g, const __nv_bfloat1
 //   k_slot_encode   per 128 consecutive slots (contiguous tiles): eps = relu(W_ee e + b_ee), then in one MMA the
 //                   four layers' slot terms E^l = W_me^l eps + b_m^l (N = 256, stored BF16) and the output layer's
 //                   F = W_oe eps + b_o (FP32); results leave through a swizzled shared-memory tile as coalesced rows;
-//   k_node          per 128 consecutive rows: h' = relu(W_ne f + b_ne) (the node encoder) or h' = h + relu(W_u [h; a]
-//                   + b_u) (a layer's update), then from the same tile the next layer's node term P = W_mh h' or
-//                   the output layer's Q = [W_oi h'; W_oj h'] (FP32);
+//   k_node          per 2 x 128 consecutive rows: h' = relu(W_ne f + b_ne) (the node encoder) or h' = h + relu(W_u
+//                   [h; a] + b_u) (a layer's update), then from the same tile the next layer's node term P = W_mh h'
+//                   (BF16) or the output layer's Q = [W_oi h'; W_oj h'] (FP32);
 //   k_message       eight lanes per row (four rows a warp): a_i = (1/8) sum over the row's message slots, in slot
-//                   order, of relu(P_j + E^l_s), lane k holding features 8k..8k+7 (each slot's E and P_j are 128- and
-//                   256-byte coalesced rows);
+//                   order, of relu(P_j + E^l_s), lane k holding features 8k..8k+7 (each slot's E and P_j are 128-byte
+//                   coalesced rows);
 //   k_output_slots  one thread per slot: o = F_s + Q_i + Q_j, G_s, L_s = C_i G_s.
 // k_features writes each slot's code (column, bit 31 when the slot carries nothing: either row pinned), so the gathers
 // need no pinned-flag lookups. The GEMMs stage only contiguous rows; every irregular access is a plain coalesced row
-// gather on the CUDA cores. Against the fused tile kernels the results differ by FP32 summation order and by one
-// BF16 rounding of E.
+// gather on the CUDA cores. Against the fused tile kernels the results differ by FP32 summation order and by the BF16
+// roundings of E and P.
 
 // Loads every 16-byte chunk this thread stages before its first store into the tile (all in flight together):
 // rows [r0, r0 + ROWS) of a K-major operand tile of K columns, row r0 + o = src(o, chunk c) for chunks of 8 BF16.
@@ -577,20 +580,48 @@ __device__ __forceinline__ void stageWeightRows(unsigned char* tile, int r0, con
 }
 
 struct SlotEncSmem {
+  unsigned char out[2][128 * 128];  // one layer's results (128 slots x 128 B, TMA 128-byte swizzle); 1024-B aligned
   unsigned char x[128 * 16 * 2];
   unsigned char wee[64 * 16 * 2];
   unsigned char eps[128 * 64 * 2];
   unsigned char wme[256 * 64 * 2];
   unsigned char woe[16 * 64 * 2];
-  unsigned char out[2][128 * 128];  // results of one layer (128 slots x 128 B), swizzled; double-buffered
   float bee[64], bm[256], bo[16];
   uint64_t bar;
   uint32_t tmem;
 };
 
-__global__ void __launch_bounds__(kThreads) k_slot_encode(Graph g, const __nv_bfloat16* __restrict__ W,
+// TMA tensor stores (cp.async.bulk.tensor, bulk-group completion) from a shared-memory tile: E^l rows [s0, s0 + 128)
+// of layer l through the 3-D map [layer][slot][64 BF16] (128-byte swizzle), F rows through the 2-D map [slot][16 FP32]
+// (64-byte swizzle); rows past B are clipped by the maps. The writing threads fence their shared-memory stores for the
+// async proxy and meet at a barrier before one thread issues.
+__device__ __forceinline__ void tmaStoreE(const CUtensorMap* map, const void* tile, int slot, int layer) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(map),
+               "r"(umma::smemAddr(tile)), "r"(0), "r"(slot), "r"(layer)
+               : "memory");
+}
+__device__ __forceinline__ void tmaStoreF(const CUtensorMap* map, const void* tile, int slot) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];" ::"l"(map),
+               "r"(umma::smemAddr(tile)), "r"(0), "r"(slot)
+               : "memory");
+}
+__device__ __forceinline__ void bulkCommit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// Waits until at most N of this thread's committed bulk groups still read their shared-memory source.
+template <int N>
+__device__ __forceinline__ void bulkWaitRead() {
+  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void bulkWaitAll() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+__device__ __forceinline__ unsigned char* alignSmem1024(unsigned char* p) {
+  return reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(p) + 1023u) & ~static_cast<uintptr_t>(1023u));
+}
+
+__global__ void __launch_bounds__(kThreads) k_slot_encode(Graph g, const __grid_constant__ CUtensorMap tmE,
+                                                          const __grid_constant__ CUtensorMap tmF,
+                                                          const __nv_bfloat16* __restrict__ W,
                                                           const float* __restrict__ M, int* error) {
-  SlotEncSmem& S = *reinterpret_cast<SlotEncSmem*>(alignSmem(netSmem));
+  SlotEncSmem& S = *reinterpret_cast<SlotEncSmem*>(alignSmem1024(netSmem));
   TileCtx T;
   T.init(&S.bar, &S.tmem, 256, error);
   const int t = threadIdx.x;
@@ -601,9 +632,11 @@ __global__ void __launch_bounds__(kThreads) k_slot_encode(Graph g, const __nv_bf
   for (int k = t; k < 256; k += kThreads) S.bm[k] = M[Layout::mB(k / 64) + k % 64];
   if (t < kOutputs) S.bo[t] = M[Layout::kOB + t];
   const uint32_t tiles = (g.B + 127) / 128;
-  const size_t layerStride = 64 * static_cast<size_t>(g.B);
   for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
     const uint32_t s0 = tile * 128;
+    // The previous tile's stores have read both staging tiles before this tile writes them (the next run's barrier
+    // carries the wait to every thread).
+    if (t == 0) bulkWaitRead<0>();
     stageRows<16, 128>(S.x, 0, [&](int q, int c) {
       const uint32_t s = s0 + q;
       return s < g.B ? reinterpret_cast<const uint4*>(g.e + 16 * static_cast<size_t>(s))[c] : zero4();
@@ -617,11 +650,14 @@ __global__ void __launch_bounds__(kThreads) k_slot_encode(Graph g, const __nv_bf
       st16(S.eps, t, 2 * c + 1, 64, packBf16(v + 8));
     }
     if (!T.run([&] { umma::gemmIssue(T.tmem, S.eps, S.wme, 128, 256, 64, false); })) break;
-    // Layer l: thread t writes its slot's 8 chunks into row t of out[l & 1] (chunk c at position c ^ (t & 7): the
-    // eight lanes of a store phase hit eight different 16-byte bank groups), then the block copies the 128 rows out
-    // as 16 KB of consecutive bytes (lane k of a warp: chunk k of a row run), E's layout being [layer][slot][64].
+    // Layer l: thread t writes its slot's 8 chunks into row t of out[l & 1] (chunk c at c ^ (t & 7), the TMA's
+    // 128-byte swizzle: the eight lanes of a store phase hit eight different bank groups); one thread stores the tile.
     for (int l = 0; l < kLayers; ++l) {
       unsigned char* buf = S.out[l & 1];
+      if (l >= 2) {
+        if (t == 0) bulkWaitRead<1>();  // layer l - 2's store has read buf
+        __syncthreads();
+      }
       for (int c = 0; c < 4; ++c) {
         float v[16];
         T.load(64 * l + 16 * c, v);
@@ -629,19 +665,19 @@ __global__ void __launch_bounds__(kThreads) k_slot_encode(Graph g, const __nv_bf
         *reinterpret_cast<uint4*>(buf + 128 * t + 16 * ((2 * c) ^ (t & 7))) = packBf16(v);
         *reinterpret_cast<uint4*>(buf + 128 * t + 16 * ((2 * c + 1) ^ (t & 7))) = packBf16(v + 8);
       }
+      umma::fenceSmemForMma();  // fence.proxy.async.shared::cta: the stores, for the TMA's reads
       __syncthreads();
-      __nv_bfloat16* dst = g.E + l * layerStride + 64 * static_cast<size_t>(s0);
-#pragma unroll
-      for (int m = 0; m < 8; ++m) {
-        const int k = t + kThreads * m, row = k >> 3, c = k & 7;
-        if (s0 + row < g.B)
-          reinterpret_cast<uint4*>(dst)[k] = *reinterpret_cast<const uint4*>(buf + 128 * row + 16 * (c ^ (row & 7)));
+      if (t == 0) {
+        tmaStoreE(&tmE, buf, static_cast<int>(s0), l);
+        bulkCommit();
       }
     }
     if (!T.run([&] { umma::gemmIssue(T.tmem, S.eps, S.woe, 128, kOutputs, 64, false); })) break;
     {
-      // F: 64 B a slot, rows of 4 chunks (chunk c at c ^ ((t >> 1) & 3)), copied out as 8 KB of consecutive bytes.
-      // out[0] is free: the run above synchronised after its last copy-out read.
+      // F: 64 B a slot, rows of 4 chunks (chunk c at c ^ ((t >> 1) & 3), the TMA's 64-byte swizzle), in out[0] once
+      // layer 2's store has read it.
+      if (t == 0) bulkWaitRead<1>();
+      __syncthreads();
       unsigned char* buf = S.out[0];
       float v[16];
       T.load(0, v);
@@ -649,97 +685,170 @@ __global__ void __launch_bounds__(kThreads) k_slot_encode(Graph g, const __nv_bf
         *reinterpret_cast<float4*>(buf + 64 * t + 16 * (c ^ ((t >> 1) & 3))) =
             make_float4(v[4 * c] + S.bo[4 * c], v[4 * c + 1] + S.bo[4 * c + 1], v[4 * c + 2] + S.bo[4 * c + 2],
                         v[4 * c + 3] + S.bo[4 * c + 3]);
+      umma::fenceSmemForMma();
       __syncthreads();
-      float4* dst = reinterpret_cast<float4*>(g.F + kOutputs * static_cast<size_t>(s0));
-#pragma unroll
-      for (int m = 0; m < 4; ++m) {
-        const int k = t + kThreads * m, row = k >> 2, c = k & 3;
-        if (s0 + row < g.B) dst[k] = *reinterpret_cast<const float4*>(buf + 64 * row + 16 * (c ^ ((row >> 1) & 3)));
+      if (t == 0) {
+        tmaStoreF(&tmF, buf, static_cast<int>(s0));
+        bulkCommit();
       }
     }
     umma::fenceBeforeSync();
     __syncthreads();
   }
+  if (t == 0) bulkWaitAll();  // every store has landed before the block's shared memory goes
   T.done();
 }
 
+// Two row tiles per block (256 threads: warps 0-3 take tile 0, warps 4-7 tile 1; TMEM columns [128 u, 128 u + 128)
+// hold tile u's accumulators), so that the n / 128 tiles of a graph run in one wave at two blocks per SM. Tile u's
+// operand x[u] is [h; a] (K = 128) or f (K = 16); h' goes back into x[u] as a K = 64 operand: into the a columns
+// (dead after the first MMA; start + 1024, 8-row groups 2048 B apart) for K = 128, behind the f tile (start + 16 KB,
+// the plain K = 64 layout) for K = 16.
 struct NodeSmem {
-  unsigned char x[128 * 128 * 2];
+  unsigned char x[2][128 * 128 * 2];
   unsigned char w1[64 * 128 * 2];
-  unsigned char hb[128 * 64 * 2];
   unsigned char w2[64 * 64 * 2];
   float b1[64];
   uint64_t bar;
   uint32_t tmem;
 };
+constexpr int kNodeThreads = 256;
+
+// Loads every 16-byte chunk of rows [r0, r0 + ROWS) of a K-major operand tile of K columns, src(o, c) for row r0 + o
+// chunk c, into registers before the first store into the tile (all in flight together), with `threads` threads.
+template <int K, int ROWS, int THREADS, class Src>
+__device__ __forceinline__ void stageRowsT(unsigned char* tile, int r0, Src&& src) {
+  constexpr int kChunks = K / 8, kTotal = ROWS * kChunks, kPer = (kTotal + THREADS - 1) / THREADS;
+  uint4 v[kPer];
+#pragma unroll
+  for (int m = 0; m < kPer; ++m) {
+    const int k = threadIdx.x + THREADS * m;
+    v[m] = k < kTotal ? src(k / kChunks, k % kChunks) : zero4();
+  }
+#pragma unroll
+  for (int m = 0; m < kPer; ++m) {
+    const int k = threadIdx.x + THREADS * m;
+    if (k < kTotal) st16(tile, r0 + k / kChunks, k % kChunks, K, v[m]);
+  }
+}
 
 // K1 = 16: h' = relu(W1 f + b1) (node encoder; X = f). K1 = 128: h' = h + relu(W1 [h; a] + b1) (a layer's update).
 // Then Out = W2 h' (N2 rows of W2: rows 0..N2-1 of the tile from W2's columns col2a, or for N2 = 32 rows 0..15 from
-// col2a and 16..31 from col2b), FP32, N2 floats per row.
+// col2a and 16..31 from col2b): N2 = 64, BF16 (the next layer's P); N2 = 32, FP32 (the output layer's Q); either way
+// 128 bytes a row. h' and Out leave through shared memory as coalesced 128-byte rows: h' read back from its operand
+// layout, Out from a swizzled staging tile in x[u] (16-byte chunk c of row q at c ^ (q & 7)).
 template <int K1, int N2>
-__global__ void __launch_bounds__(kThreads) k_node(uint32_t n, const __nv_bfloat16* __restrict__ X,
-                                                   const __nv_bfloat16* __restrict__ A,
-                                                   const __nv_bfloat16* __restrict__ W1, const float* __restrict__ b1,
-                                                   const __nv_bfloat16* __restrict__ W2, int ld2, int col2a, int col2b,
-                                                   __nv_bfloat16* __restrict__ hout, float* __restrict__ out,
-                                                   int* error) {
+__global__ void __launch_bounds__(kNodeThreads, 2) k_node(uint32_t n, const __nv_bfloat16* __restrict__ X,
+                                                       const __nv_bfloat16* __restrict__ A,
+                                                       const __nv_bfloat16* __restrict__ W1,
+                                                       const float* __restrict__ b1,
+                                                       const __nv_bfloat16* __restrict__ W2, int ld2, int col2a,
+                                                       int col2b, __nv_bfloat16* __restrict__ hout,
+                                                       void* __restrict__ out, int* error) {
   NodeSmem& S = *reinterpret_cast<NodeSmem*>(alignSmem(netSmem));
   TileCtx T;
-  T.init(&S.bar, &S.tmem, 128, error);
-  const int t = threadIdx.x;
-  stageWeightRows<K1, 64>(S.w1, 0, W1, K1, 0);
+  T.init(&S.bar, &S.tmem, 256, error);
+  const int t = threadIdx.x, u = t / 128, q = t % 128;  // tile u, row q of it
+  auto weights = [&](int o, int c, const __nv_bfloat16* W, int ld, int col0) {
+    return *reinterpret_cast<const uint4*>(W + static_cast<size_t>(o) * ld + col0 + 8 * c);
+  };
+  stageRowsT<K1, 64, kNodeThreads>(S.w1, 0, [&](int o, int c) { return weights(o, c, W1, K1, 0); });
   if (N2 == 64) {
-    stageWeightRows<64, 64>(S.w2, 0, W2, ld2, col2a);
+    stageRowsT<64, 64, kNodeThreads>(S.w2, 0, [&](int o, int c) { return weights(o, c, W2, ld2, col2a); });
   } else {
-    stageWeightRows<64, 16>(S.w2, 0, W2, ld2, col2a);
-    stageWeightRows<64, 16>(S.w2, 16, W2, ld2, col2b);
+    stageRowsT<64, 16, kNodeThreads>(S.w2, 0, [&](int o, int c) { return weights(o, c, W2, ld2, col2a); });
+    stageRowsT<64, 16, kNodeThreads>(S.w2, 16, [&](int o, int c) { return weights(o, c, W2, ld2, col2b); });
   }
   if (t < 64) S.b1[t] = b1[t];
-  const uint32_t tiles = (n + 127) / 128;
-  for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-    const uint32_t r0 = tile * 128;
+  constexpr uint32_t kHbOffset = K1 == 128 ? 1024u : 16384u, kHbSbo = K1 == 128 ? 2048u : 1024u;
+  const uint32_t tiles = (n + 127) / 128, pairs = (tiles + 1) / 2;
+  // This thread's TMEM lane group (warp % 4) and tile u's columns.
+  const uint32_t tm = umma::tmemAt(T.tmem, ((t / 32) % 4) * 32, 128 * u);
+  for (uint32_t pair = blockIdx.x; pair < pairs; pair += gridDim.x) {
+    const uint32_t rBase = pair * 256;  // tile u covers rows rBase + 128 u ...
     if (K1 == 16) {
-      stageRows<16, 128>(S.x, 0, [&](int q, int c) {
-        const uint32_t r = r0 + q;
-        return r < n ? reinterpret_cast<const uint4*>(X + 16 * static_cast<size_t>(r))[c] : zero4();
-      });
+      for (int v = 0; v < 2; ++v)
+        stageRowsT<16, 128, kNodeThreads>(S.x[v], 0, [&](int rr, int c) {
+          const uint32_t r = rBase + 128 * v + rr;
+          return r < n ? reinterpret_cast<const uint4*>(X + 16 * static_cast<size_t>(r))[c] : zero4();
+        });
     } else {
-      stageRows<128, 128>(S.x, 0, [&](int q, int c) {
-        const uint32_t r = r0 + q;
+      // 256 rows x 16 chunks as one K = 128 operand of 256 rows: rows 128..255 land in x[1] (x[0] is exactly 128 rows).
+      stageRowsT<128, 256, kNodeThreads>(S.x[0], 0, [&](int rr, int c) {
+        const uint32_t r = rBase + rr;
         if (r >= n) return zero4();
         return c < 8 ? reinterpret_cast<const uint4*>(X + 64 * static_cast<size_t>(r))[c]
                      : reinterpret_cast<const uint4*>(A + 64 * static_cast<size_t>(r))[c - 8];
       });
     }
-    if (!T.run([&] { umma::gemmIssue(T.tmem, S.x, S.w1, 128, 64, K1, false); })) break;
-    const uint32_t r = r0 + t;
+    if (!T.run([&] {
+          for (int v = 0; v < 2; ++v) umma::gemmIssue(T.tmem + 128 * v, S.x[v], S.w1, 128, 64, K1, false);
+        }))
+      break;
+    unsigned char* xu = S.x[u];
     for (int c = 0; c < 4; ++c) {
       float v[16];
-      T.load(16 * c, v);
+      umma::load16(tm + 16 * c, v);
       for (int k = 0; k < 16; ++k) v[k] = fmaxf(v[k] + S.b1[16 * c + k], 0.0f);
       if (K1 == 128) {
         float h[16];
-        unpackBf16(*reinterpret_cast<const uint4*>(S.x + umma::kmajorOffset(t, 16 * c, 128)), h);
-        unpackBf16(*reinterpret_cast<const uint4*>(S.x + umma::kmajorOffset(t, 16 * c + 8, 128)), h + 8);
+        unpackBf16(*reinterpret_cast<const uint4*>(xu + umma::kmajorOffset(q, 16 * c, 128)), h);
+        unpackBf16(*reinterpret_cast<const uint4*>(xu + umma::kmajorOffset(q, 16 * c + 8, 128)), h + 8);
         for (int k = 0; k < 16; ++k) v[k] += h[k];
       }
-      const uint4 lo = packBf16(v), hi = packBf16(v + 8);
-      st16(S.hb, t, 2 * c, 64, lo);
-      st16(S.hb, t, 2 * c + 1, 64, hi);
-      if (r < n) {
-        uint4* o = reinterpret_cast<uint4*>(hout + 64 * static_cast<size_t>(r));
-        o[2 * c] = lo;
-        o[2 * c + 1] = hi;
+      // h' chunks 2c, 2c + 1 of row q, in the operand layout described above.
+      if (K1 == 128) {
+        st16(xu, q, 8 + 2 * c, 128, packBf16(v));
+        st16(xu, q, 9 + 2 * c, 128, packBf16(v + 8));
+      } else {
+        st16(xu + kHbOffset, q, 2 * c, 64, packBf16(v));
+        st16(xu + kHbOffset, q, 2 * c + 1, 64, packBf16(v + 8));
       }
     }
-    if (!T.run([&] { umma::gemmIssue(T.tmem + 64, S.hb, S.w2, 128, N2, 64, false); })) break;
-    for (int c = 0; c < N2 / 16; ++c) {
-      float v[16];
-      T.load(64 + 16 * c, v);
-      if (r < n) {
-        float4* o = reinterpret_cast<float4*>(out + N2 * static_cast<size_t>(r) + 16 * c);
-        for (int k = 0; k < 4; ++k) o[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+    if (!T.run([&] {
+          const uint64_t bDesc = umma::smemDesc(S.w2, 64);
+          for (int v = 0; v < 2; ++v)
+            umma::gemmIssueDesc(T.tmem + 128 * v + 64, umma::smemDescSbo(S.x[v] + kHbOffset, kHbSbo), bDesc, 128,
+                                N2, 64, false);
+        }))
+      break;
+    // h' out: chunk k of the pair's 2 x 128 rows x 8 chunks (tile k / 1024), read from its operand layout.
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const int k = t + kNodeThreads * m, v = k >> 10, row = (k >> 3) & 127, c = k & 7;
+      const uint32_t r = rBase + 128 * v + row;
+      const unsigned char* src = K1 == 128 ? S.x[v] + umma::kmajorOffset(row, 64 + 8 * c, 128)
+                                           : S.x[v] + kHbOffset + umma::kmajorOffset(row, 8 * c, 64);
+      if (r < n) reinterpret_cast<uint4*>(hout + 64 * static_cast<size_t>(r))[c] = *reinterpret_cast<const uint4*>(src);
+    }
+    __syncthreads();  // x[u] is now free for the staging tile
+    {
+      uint4 w[8];
+      if (N2 == 64) {
+        for (int c = 0; c < 4; ++c) {
+          float v[16];
+          umma::load16(tm + 64 + 16 * c, v);
+          w[2 * c] = packBf16(v);
+          w[2 * c + 1] = packBf16(v + 8);
+        }
+      } else {
+        for (int c = 0; c < 2; ++c) {
+          float v[16];
+          umma::load16(tm + 64 + 16 * c, v);
+          for (int k = 0; k < 4; ++k) w[4 * c + k] = make_uint4(__float_as_uint(v[4 * k]), __float_as_uint(v[4 * k + 1]),
+                                                                 __float_as_uint(v[4 * k + 2]), __float_as_uint(v[4 * k + 3]));
+        }
       }
+      for (int c = 0; c < 8; ++c) *reinterpret_cast<uint4*>(xu + 128 * q + 16 * (c ^ (q & 7))) = w[c];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+      const int k = t + kNodeThreads * m, v = k >> 10, row = (k >> 3) & 127, c = k & 7;
+      const uint32_t r = rBase + 128 * v + row;
+      if (r < n)
+        reinterpret_cast<uint4*>(out)[8 * static_cast<size_t>(r) + c] =
+            *reinterpret_cast<const uint4*>(S.x[v] + 128 * row + 16 * (c ^ (row & 7)));
     }
     umma::fenceBeforeSync();
     __syncthreads();
@@ -757,7 +866,7 @@ __global__ void k_slot_rows(Graph g) {
 // Eight lanes per row (four rows a warp): a_i = (1/8) sum of relu(P_j + E_s) over the row's message slots (code
 // without bit 31, j != i) in slot order; lane k of the row's eight accumulates features 8k..8k+7. The row's codes are
 // read eight at a time (one a lane) and shared by shuffles; four slots' E and P_j rows are loaded before the first add.
-__global__ void k_message(Graph g, const float* __restrict__ P, const __nv_bfloat16* __restrict__ E,
+__global__ void k_message(Graph g, const __nv_bfloat16* __restrict__ P, const __nv_bfloat16* __restrict__ E,
                           __nv_bfloat16* __restrict__ aOut) {
   const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t i = gt / 8u;
@@ -772,36 +881,27 @@ __global__ void k_message(Graph g, const float* __restrict__ P, const __nv_bfloa
     const uint32_t myCode = sub < static_cast<int>(cnt) ? __ldg(g.code + base + sub) : kPinBit;
 #pragma unroll
     for (int k0 = 0; k0 < 8; k0 += 4) {
-      uint4 e[4];
-      float4 p0[4], p1[4];
+      uint4 e[4], pv[4];
       bool kp[4];
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
         const uint32_t code = __shfl_sync(mask, myCode, k0 + u, 8);
         const uint32_t j = code & ~kPinBit;
         kp[u] = !(code & kPinBit) && j != i;
-        e[u] = zero4();
-        p0[u] = p1[u] = make_float4(0, 0, 0, 0);
+        e[u] = pv[u] = zero4();
         if (kp[u]) {
           e[u] = __ldg(reinterpret_cast<const uint4*>(E + 64 * static_cast<size_t>(base + k0 + u)) + sub);
-          const float4* pj = reinterpret_cast<const float4*>(P + 64 * static_cast<size_t>(j) + 8 * sub);
-          p0[u] = __ldg(pj);
-          p1[u] = __ldg(pj + 1);
+          pv[u] = __ldg(reinterpret_cast<const uint4*>(P + 64 * static_cast<size_t>(j)) + sub);
         }
       }
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
         if (!kp[u]) continue;
-        float ev[8];
+        float ev[8], pf[8];
         unpackBf16(e[u], ev);
-        acc[0] += fmaxf(p0[u].x + ev[0], 0.0f);
-        acc[1] += fmaxf(p0[u].y + ev[1], 0.0f);
-        acc[2] += fmaxf(p0[u].z + ev[2], 0.0f);
-        acc[3] += fmaxf(p0[u].w + ev[3], 0.0f);
-        acc[4] += fmaxf(p1[u].x + ev[4], 0.0f);
-        acc[5] += fmaxf(p1[u].y + ev[5], 0.0f);
-        acc[6] += fmaxf(p1[u].z + ev[6], 0.0f);
-        acc[7] += fmaxf(p1[u].w + ev[7], 0.0f);
+        unpackBf16(pv[u], pf);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] += fmaxf(pf[k] + ev[k], 0.0f);
       }
     }
   }
@@ -1556,10 +1656,10 @@ T* dalloc(size_t count) {
 }
 
 size_t smemFor(size_t bytes) { return bytes + 128; }
-// k_slot_encode holds 256 TMEM columns: its dynamic shared memory is padded so that at most two blocks share an SM
-// (3 x 77 KB > 228 KB) and a third never waits in tcgen05.alloc for a resident block's columns (the grid is also
-// capped at two blocks per SM).
-constexpr size_t kSlotEncodeSmem = sizeof(SlotEncSmem) > 76 * 1024 ? sizeof(SlotEncSmem) : 76 * 1024;
+// k_slot_encode holds 256 TMEM columns: at most two of its blocks fit an SM's shared memory (3 x 91 KB > 228 KB), so a
+// third never waits in tcgen05.alloc for a resident block's columns (the grid is also capped at two blocks per SM).
+// Its tile needs 1024-byte alignment (the TMA swizzle), hence the extra 1 KB.
+constexpr size_t kSlotEncodeSmem = (sizeof(SlotEncSmem) > 76 * 1024 ? sizeof(SlotEncSmem) : 76 * 1024) + 1024 - 128;
 
 }  // namespace
 
@@ -1607,6 +1707,7 @@ struct GraphStore {
   int partialCount = 0;
   uint32_t liveUnknowns = 0;  // 3 x unpinned rows
   bool inference = false;     // the inference workspace is allocated
+  CUtensorMap maps[2];        // k_slot_encode's TMA store maps of E and F (inference)
   ~GraphStore() {
     for (void* p : owned) cudaFree(p);
   }
@@ -1620,6 +1721,19 @@ struct GraphStore {
 
 namespace {
 
+// The driver's cuTensorMapEncodeTiled, looked up once through the runtime (the library links the static runtime only).
+PFN_cuTensorMapEncodeTiled_v12000 tensorMapEncoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    NCK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || !p) throw std::runtime_error("cuda: cuTensorMapEncodeTiled unavailable");
+    fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
 void allocInference(GraphStore& s, cudaStream_t st) {
   if (s.inference) return;
   Graph& g = s.g;
@@ -1629,7 +1743,27 @@ void allocInference(GraphStore& s, cudaStream_t st) {
   NCK(cudaGetLastError());
   g.E = s.own<__nv_bfloat16>(kLayers * 64 * static_cast<size_t>(g.B));
   g.F = s.own<float>(kOutputs * static_cast<size_t>(g.B));
-  g.P = s.own<float>(64 * static_cast<size_t>(g.n));
+  {
+    // E: [layer][slot][64] BF16 as a 3-D tensor, boxes of 64 x 128 x 1 (one layer of one 128-slot tile), 128-byte
+    // swizzle; F: [slot][16] FP32, boxes of 16 x 128, 64-byte swizzle. Every stride is a multiple of 16 bytes.
+    auto encode = tensorMapEncoder();
+    const cuuint64_t eDim[3] = {64, g.B, static_cast<cuuint64_t>(kLayers)};
+    const cuuint64_t eStride[2] = {128, 128ull * g.B};
+    const cuuint32_t eBox[3] = {64, 128, 1}, one[3] = {1, 1, 1};
+    if (encode(&s.maps[0], CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, g.E, eDim, eStride, eBox, one,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      throw std::runtime_error("cuda: cuTensorMapEncodeTiled failed for the slot terms");
+    const cuuint64_t fDim[2] = {static_cast<cuuint64_t>(kOutputs), g.B};
+    const cuuint64_t fStride[1] = {64};
+    const cuuint32_t fBox[2] = {static_cast<cuuint32_t>(kOutputs), 128};
+    if (encode(&s.maps[1], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, g.F, fDim, fStride, fBox, one,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      throw std::runtime_error("cuda: cuTensorMapEncodeTiled failed for the output terms");
+    g.tmaps = s.maps;
+  }
+  g.P = s.own<__nv_bfloat16>(64 * static_cast<size_t>(g.n));
   g.Q = s.own<float>(32 * static_cast<size_t>(g.n));
   g.a = s.own<__nv_bfloat16>(64 * static_cast<size_t>(g.n));
   s.inference = true;
@@ -1834,21 +1968,23 @@ void Network::forwardOn(Graph& g, cudaStream_t st, bool training, int* error) {
   if (!training) {
     if (!g.E) throw std::logic_error("forwardOn: the graph has no inference workspace");
     const int rowGroups = static_cast<int>((g.n + 31) / 32);  // eight lanes a row
-    const int nodeGrid = gridFor((g.n + 127) / 128, 3 * numSMs_);
+    const int nodeGrid = gridFor((g.n + 255) / 256, 2 * numSMs_);  // two row tiles a block
     const size_t nodeSmem = smemFor(sizeof(NodeSmem));
-    k_slot_encode<<<gridFor((g.B + 127) / 128, 2 * numSMs_), kThreads, smemFor(kSlotEncodeSmem), st>>>(g, W, M, error_);
-    k_node<16, 64><<<nodeGrid, kThreads, nodeSmem, st>>>(g.n, g.f, nullptr, W + Layout::kNe, M + Layout::kNeB,
+    const CUtensorMap* maps = static_cast<const CUtensorMap*>(g.tmaps);
+    k_slot_encode<<<gridFor((g.B + 127) / 128, 2 * numSMs_), kThreads, smemFor(kSlotEncodeSmem), st>>>(
+        g, maps[0], maps[1], W, M, error_);
+    k_node<16, 64><<<nodeGrid, kNodeThreads, nodeSmem, st>>>(g.n, g.f, nullptr, W + Layout::kNe, M + Layout::kNeB,
                                                          W + Layout::m(0), 2 * kHidden, 0, 0, g.h[0], g.P, error_);
     for (int l = 0; l < kLayers; ++l) {
       k_message<<<rowGroups, 256, 0, st>>>(g, g.P, g.E + l * 64 * static_cast<size_t>(g.B), g.a);
       const __nv_bfloat16* hin = g.h[l & 1];
       __nv_bfloat16* hout = g.h[(l + 1) & 1];
       if (l + 1 < kLayers)
-        k_node<128, 64><<<nodeGrid, kThreads, nodeSmem, st>>>(g.n, hin, g.a, W + Layout::u(l), M + Layout::uB(l),
+        k_node<128, 64><<<nodeGrid, kNodeThreads, nodeSmem, st>>>(g.n, hin, g.a, W + Layout::u(l), M + Layout::uB(l),
                                                               W + Layout::m(l + 1), 2 * kHidden, 0, 0, hout, g.P,
                                                               error_);
       else
-        k_node<128, 32><<<nodeGrid, kThreads, nodeSmem, st>>>(g.n, hin, g.a, W + Layout::u(l), M + Layout::uB(l),
+        k_node<128, 32><<<nodeGrid, kNodeThreads, nodeSmem, st>>>(g.n, hin, g.a, W + Layout::u(l), M + Layout::uB(l),
                                                               W + Layout::kO, 3 * kHidden, 0, kHidden, hout, g.Q,
                                                               error_);
     }

@@ -64,11 +64,12 @@ struct Graph {
   // Inference workspace (forwardOn without training; eps, Ahat and the per-layer h are not kept).
   __nv_bfloat16* E = nullptr;        // kLayers planes of B x 64: W_me^l eps_s + b_m^l
   float* F = nullptr;                // B x 16: W_oe eps_s + b_o
-  float* P = nullptr;                // n x 64: W_mh^l h_j of the current layer
+  __nv_bfloat16* P = nullptr;        // n x 64: W_mh^l h_j of the current layer
   float* Q = nullptr;                // n x 32: W_oi h_i (0..15), W_oj h_j (16..31)
   __nv_bfloat16* a = nullptr;        // n x 64: a_i of the current layer
   uint32_t* code = nullptr;          // B: column of the slot, bit 31 when either row is pinned (written by k_features)
   uint32_t* slotRow = nullptr;       // B: row of the slot (fixed with the CSR)
+  const void* tmaps = nullptr;       // host memory: the TMA store maps of E and F (CUtensorMap[2])
 };
 
 // Host-owned device buffers of a graph built from host arrays (a training sample) or bound to a solver's arrays.

@@ -29,6 +29,14 @@ __device__ __forceinline__ uint64_t smemDesc(const void* tile, uint32_t K) {
          (static_cast<uint64_t>((16u * K) >> 4) << 32) | (1ull << 46);
 }
 
+// The same with an explicit stride-dimension byte offset (a K-major operand whose 8-row groups lie `sbo` bytes apart,
+// e.g. columns [64, 128) of a K = 128 tile read as a K = 64 operand: start + 1024, SBO = 2048).
+__device__ __forceinline__ uint64_t smemDescSbo(const void* tile, uint32_t sbo) {
+  const uint64_t addr = smemAddr(tile);
+  return ((addr & 0x3FFFFull) >> 4) | (static_cast<uint64_t>(128u >> 4) << 16) |
+         (static_cast<uint64_t>(sbo >> 4) << 32) | (1ull << 46);
+}
+
 // Instruction descriptor, kind::f16: D FP32, A and B BF16, both K-major, shape M x N.
 __host__ __device__ constexpr uint32_t instrDescBf16(uint32_t M, uint32_t N) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
@@ -127,6 +135,16 @@ __device__ __forceinline__ void gemmIssue(uint32_t dTmem, const void* a, const v
   const uint64_t aDesc = smemDesc(a, K), bDesc = smemDesc(b, K);
   for (uint32_t k = 0; k < K; k += 16) {
     // Advance the start address by 256 bytes per K step (address field is in 16-byte units).
+    const uint64_t step = static_cast<uint64_t>((k / 16) * 256u) >> 4;
+    mma(dTmem, aDesc + step, bDesc + step, idesc, accumulate || k > 0);
+  }
+}
+
+// gemmIssue with the operands' descriptors given (smemDesc / smemDescSbo).
+__device__ __forceinline__ void gemmIssueDesc(uint32_t dTmem, uint64_t aDesc, uint64_t bDesc, uint32_t M, uint32_t N,
+                                              uint32_t K, bool accumulate) {
+  const uint32_t idesc = instrDescBf16(M, N);
+  for (uint32_t k = 0; k < K; k += 16) {
     const uint64_t step = static_cast<uint64_t>((k / 16) * 256u) >> 4;
     mma(dTmem, aDesc + step, bDesc + step, idesc, accumulate || k > 0);
   }
