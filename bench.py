@@ -250,9 +250,24 @@ def network_forward(s, args, frames: int = 10) -> dict:
     algo = B * (112 + 608 + 4 * 260 + 130) + n * (72 + 76 + 4 * 136 + 288 + 4 * 512)
     peak, kind = measured_peaks()
     gbs = algo / (ms / 1e3) / 1e9 if ms > 0 else None
+    # Tensor-core work (BF16 MMAs, FP32 accumulation): per slot the edge encoder (16 -> 64), the four layers' slot terms
+    # and the output layer's (64 -> 256 + 16); per particle the node encoder and P^0 (16 -> 64 -> 64) and each layer's
+    # update and next node term (128 -> 64 -> 64, the last 128 -> 64 -> 32).
+    flops = 2 * B * (16 * 64 + 64 * 256 + 64 * 16) + 2 * n * (16 * 64 + 64 * 64 + 3 * (128 * 64 + 64 * 64)
+                                                                + 128 * 64 + 64 * 32)
+    tf = flops / (ms / 1e3) / 1e12 if ms > 0 else None
+    bf16_peak = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            bf16_peak = float(json.load(f)["bf16_tflops"])
+    except (OSError, KeyError, ValueError):
+        bf16_peak = 1590.0
     return {"ms_per_forward": ms, "forwards": launches, "particles": n, "block_slots": B,
             "algorithmic_bytes": algo, "achieved_gbs": gbs, "peak_gbs": peak, "peak_source": kind,
             "frac": gbs / peak if gbs else None,
+            "tensor": {"flops": flops, "achieved_tflops": tf, "peak_bf16_tflops": bf16_peak,
+                       "frac": tf / bf16_peak if tf else None,
+                       "note": "the GEMMs are small (hidden 64); the forward is bound by memory, not the tensor pipe"},
             "note": f"{frames} frames of the learned 60k solver (every Newton iteration runs the network), CUDA events "
                     f"around each forward; the P_j gathers (4 x 128 B per slot) are served mostly from L2"}
 
