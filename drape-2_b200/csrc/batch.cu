@@ -465,7 +465,7 @@ struct drape_batch {
   DBuf<dcu::Stretch> stretch;
   DBuf<dcu::Hinge> hinge;
   DBuf<dcu::Seam> seam, saveSeam;
-  DBuf<uint32_t> rowStart, colIndex, diagSlot, incStart, incEntry, offSlot, offStart, offContrib, tslot;
+  DBuf<uint32_t> rowStart, colIndex, diagSlot, incStart, incEntry, offSlot, offStart, offCode, tslot;
   DBuf<uint32_t> starts, bases;  // point and assembly prefixes; pBase and kBase
   DBuf<float> fieldValues, blocks, snapGap;
   DBuf<float4> x, v, xStart, yRel, u, grad, step, r, z, p0, p1, ap, apFull, resid, fExt, pinPos, precond;
@@ -617,7 +617,7 @@ struct drape_batch {
       append(hie, m.incEntry);
       append(hos, m.offSlot);
       append(hoS, m.offStart);
-      append(hoc, m.offContrib);
+      append(hoc, m.offCode);
       append(hts, net::transposedSlots(m.rowStart, cols));
       if (m.fieldValues.empty()) hfv.push_back(0.0f); else append(hfv, m.fieldValues);
       std::vector<float4> xs, vs, fe, pp;
@@ -641,7 +641,7 @@ struct drape_batch {
     incEntry.upload(hie, s);
     offSlot.upload(hos, s);
     offStart.upload(hoS, s);
-    offContrib.upload(hoc, s);
+    offCode.upload(hoc, s);
     tslot.upload(hts, s);
     fieldValues.upload(hfv, s);
     blocks.alloc(static_cast<size_t>(SP) * 9);
@@ -706,7 +706,7 @@ struct drape_batch {
       d.incEntry = incEntry.p + eBase[g];
       d.offSlot = offSlot.p + (sBase[g] - pBase[g]);
       d.offStart = offStart.p + (sBase[g] - pBase[g] + g);
-      d.offContrib = offContrib.p + cBase[g];
+      d.offCode = offCode.p + cBase[g];
       for (auto [dst, src] : {std::pair<float4**, float4*>{&d.x, x.p}, {&d.v, v.p}, {&d.xStart, xStart.p},
                               {&d.yRel, yRel.p}, {&d.u, u.p}, {&d.grad, grad.p}, {&d.step, step.p}, {&d.r, r.p},
                               {&d.z, z.p}, {&d.p0, p0.p}, {&d.p1, p1.p}, {&d.ap, ap.p}, {&d.apFull, apFull.p},

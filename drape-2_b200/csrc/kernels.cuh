@@ -122,8 +122,8 @@ struct Dev {
   const uint32_t* incStart;
   const uint32_t* incEntry;
   const uint32_t* offSlot;   // the off-diagonal slots in slot order: row << 6 | row-local position
-  const uint32_t* offStart;  // per off-diagonal slot: its contributions [offStart[k], offStart[k + 1]) of offContrib
-  const uint32_t* offContrib;  // incidence entry << 2 | block of the entry's term, in gather order
+  const uint32_t* offStart;  // per off-diagonal slot: its contributions [offStart[k], offStart[k + 1]) of offCode
+  const uint32_t* offCode;     // per contribution, in gather order: kind << 30 | term << 4 | vertex a << 2 | block b
   float4 *x, *v, *xStart, *yRel, *u, *grad, *step, *r, *z, *p0, *p1, *ap, *apFull, *resid;
   float4 *pm0, *pm1, *pz;  // pipelined PCG only: the two m = M w buffers and z = A q (null where not allocated)
   float4* stretchDer;      // per stretch term: its StretchDer record (6 float4), written by termsRows
@@ -634,10 +634,12 @@ __device__ inline void offDiagonalSlot(const Dev& D, uint32_t k, uint32_t SP) {
   zero(acc);
   const uint32_t ce = D.offStart[k + 1];
   for (uint32_t c = D.offStart[k]; c < ce; ++c) {
-    const uint32_t v = D.offContrib[c];
+    const uint32_t v = D.offCode[c];
     float3 g;
     M3 H;
-    entryBlock<false>(D, D.incEntry[v >> 2], static_cast<int>(v & 3u), g, H);
+    // The incidence-entry code (kind 2 bits, term 28, vertex 2) and the block.
+    entryBlock<false>(D, (v & 0xC0000000u) | (((v >> 4) & 0x03FFFFFFu) << 2) | ((v >> 2) & 3u), static_cast<int>(v & 3u),
+                      g, H);
 #pragma unroll
     for (int q = 0; q < 9; ++q) acc.m[q] += H.m[q];
   }

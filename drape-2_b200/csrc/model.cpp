@@ -486,6 +486,13 @@ void Model::buildStructure() {
       }
     }
   });
+  const std::size_t terms = std::max(stretch.size(), std::max(hinges.size(), seams.size()));
+  if (terms >= (1u << 26)) throw std::invalid_argument("too many terms for the contribution encoding");
+  offCode.resize(offContrib.size());
+  for (std::size_t c = 0; c < offContrib.size(); ++c) {
+    const uint32_t v = offContrib[c], code = incEntry[v >> 2];
+    offCode[c] = (code & 0xC0000000u) | (((code >> 2) & 0x03FFFFFFu) << 4) | ((code & 3u) << 2) | (v & 3u);
+  }
   contactForce.assign(n, 0.0);
 }
 

@@ -82,6 +82,9 @@ struct Model {
   // The off-diagonal slots in slot order (row << 6 | row-local position) and, per such slot k, the contributions
   // [offStart[k], offStart[k + 1]) of offContrib in gather order: incidence entry e << 2 | block b of its term.
   std::vector<uint32_t> offSlot, offStart, offContrib;
+  // offContrib resolved for the device: per contribution, kind << 30 | term << 4 | vertex a << 2 | block b (the term's
+  // entry and the block it adds), so the assembly reads the term's record without the incidence-entry indirection.
+  std::vector<uint32_t> offCode;
   std::vector<std::array<uint32_t, 9>> stretchSlots;
   std::vector<std::array<uint32_t, 16>> hingeSlots;
   std::vector<std::array<uint32_t, 4>> seamSlots;

@@ -104,7 +104,7 @@ struct drape_solver {
   DBuf<dcu::Stretch> stretch;
   DBuf<dcu::Hinge> hinge;
   DBuf<dcu::Seam> seam;
-  DBuf<uint32_t> rowStart, colIndex, diagSlot, incStart, incEntry, offSlot, offStart, offContrib;
+  DBuf<uint32_t> rowStart, colIndex, diagSlot, incStart, incEntry, offSlot, offStart, offCode;
   DBuf<float> fieldValues, blocks;
   DBuf<float4> x, v, xStart, yRel, u, grad, step, r, z, p0, p1, ap, apFull, resid, fExt, pinPos, precond;
   DBuf<float4> pm0, pm1, pz;  // the pipelined PCG's extra vectors
@@ -269,7 +269,7 @@ struct drape_solver {
     incEntry.upload(m.incEntry, s);
     offSlot.upload(m.offSlot, s);
     offStart.upload(m.offStart, s);
-    offContrib.upload(m.offContrib, s);
+    offCode.upload(m.offCode, s);
     if (m.fieldCount > 0) {
       fieldValues.upload(m.fieldData(), m.fieldCount, s);
       CK(cudaStreamSynchronize(s));  // the copy has read the caller's samples; the model keeps no pointer to them
@@ -320,7 +320,7 @@ struct drape_solver {
     d.incEntry = incEntry.p;
     d.offSlot = offSlot.p;
     d.offStart = offStart.p;
-    d.offContrib = offContrib.p;
+    d.offCode = offCode.p;
     d.x = x.p;
     d.v = v.p;
     d.xStart = xStart.p;
