@@ -184,13 +184,17 @@ template <bool Grad>
 __device__ inline void stretchBlockFrom(float4 d, const float4* __restrict__ rec, int a, int b, float3& g, M3& H) {
   zero(H);
   g = mk(0, 0, 0);
-  const float4 w1 = rec[1];
+  // The whole record in one round of loads (the flags in word 1 then select what is used).
+  float4 r[6];
+#pragma unroll
+  for (int k = 0; k < 6; ++k) r[k] = rec[k];
+  const float4 w1 = r[1];
   const uint32_t flags = __float_as_uint(w1.z);
 #pragma unroll
   for (int which = 0; which < 2; ++which) {
     if (!(flags & (which == 0 ? kStretchWarp : kStretchWeft))) continue;
-    const float4 wn = rec[2 * which];
-    const float4 ws = which == 0 ? w1 : rec[3];
+    const float4 wn = r[2 * which];
+    const float4 ws = which == 0 ? w1 : r[3];
     const float3 n = xyz(wn);
     const float gs = wn.w, hs = ws.x, ts = ws.y;
     const float ca = coef(d, which, a), cb = coef(d, which, b);
@@ -200,7 +204,7 @@ __device__ inline void stretchBlockFrom(float4 d, const float4* __restrict__ rec
     if (ts != 0.0f) addProjector(H, ts * ca * cb, n);
   }
   if (flags & kStretchBias) {
-    const float4 w4 = rec[4], w5 = rec[5];
+    const float4 w4 = r[4], w5 = r[5];
     const float3 dfu = xyz(w4), dfv = xyz(w5);
     const float3 gra = dfu * coef(d, 0, a) + dfv * coef(d, 1, a);
     const float3 grb = dfu * coef(d, 0, b) + dfv * coef(d, 1, b);

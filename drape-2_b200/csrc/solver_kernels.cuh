@@ -26,8 +26,10 @@ constexpr int kTermThreads = 256;  // k_terms block size
 
 __global__ void __launch_bounds__(kTermThreads) k_terms(Dev D) { termsRows(D, blockIdx.x, gridDim.x); }
 
-// Five 256-thread blocks per SM (48 registers): 3 % faster than four (59 registers); six or eight spill and are slower.
-__global__ void __launch_bounds__(kAssembleThreads, 5) k_assemble(Dev D) {
+// Four 256-thread blocks per SM (64 registers): with each stretch record loaded in one round (24 floats live), 1.9 %
+// faster per drape frame than five (48 registers, spilling); with the record read in two dependent rounds five had been
+// 3 % faster than four.
+__global__ void __launch_bounds__(kAssembleThreads, 4) k_assemble(Dev D) {
   assembleSlots(D, blockIdx.x, gridDim.x);
 }
 
