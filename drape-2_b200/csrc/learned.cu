@@ -554,22 +554,26 @@ __global__ void __launch_bounds__(kThreads) k_output(Graph g, const __nv_bfloat1
 // gather on the CUDA cores. Against the fused tile kernels the results differ by FP32 summation order and by the BF16
 // roundings of E and P.
 
-// Loads every 16-byte chunk this thread stages before its first store into the tile (all in flight together):
-// rows [r0, r0 + ROWS) of a K-major operand tile of K columns, row r0 + o = src(o, chunk c) for chunks of 8 BF16.
-template <int K, int ROWS, class Src>
-__device__ __forceinline__ void stageRows(unsigned char* tile, int r0, Src&& src) {
-  constexpr int kChunks = K / 8, kTotal = ROWS * kChunks, kPer = (kTotal + kThreads - 1) / kThreads;
+// Loads every 16-byte chunk of rows [r0, r0 + ROWS) of a K-major operand tile of K columns, src(o, c) for row r0 + o
+// chunk c (8 BF16), into registers before the first store into the tile (all in flight together), with THREADS threads.
+template <int K, int ROWS, int THREADS, class Src>
+__device__ __forceinline__ void stageRowsT(unsigned char* tile, int r0, Src&& src) {
+  constexpr int kChunks = K / 8, kTotal = ROWS * kChunks, kPer = (kTotal + THREADS - 1) / THREADS;
   uint4 v[kPer];
 #pragma unroll
   for (int m = 0; m < kPer; ++m) {
-    const int k = threadIdx.x + kThreads * m;
+    const int k = threadIdx.x + THREADS * m;
     v[m] = k < kTotal ? src(k / kChunks, k % kChunks) : zero4();
   }
 #pragma unroll
   for (int m = 0; m < kPer; ++m) {
-    const int k = threadIdx.x + kThreads * m;
+    const int k = threadIdx.x + THREADS * m;
     if (k < kTotal) st16(tile, r0 + k / kChunks, k % kChunks, K, v[m]);
   }
+}
+template <int K, int ROWS, class Src>
+__device__ __forceinline__ void stageRows(unsigned char* tile, int r0, Src&& src) {
+  stageRowsT<K, ROWS, kThreads>(tile, r0, static_cast<Src&&>(src));
 }
 // Rows of W (row length ld) from column col0 as a K-major tile of K columns.
 template <int K, int ROWS>
@@ -713,24 +717,6 @@ struct NodeSmem {
   uint32_t tmem;
 };
 constexpr int kNodeThreads = 256;
-
-// Loads every 16-byte chunk of rows [r0, r0 + ROWS) of a K-major operand tile of K columns, src(o, c) for row r0 + o
-// chunk c, into registers before the first store into the tile (all in flight together), with `threads` threads.
-template <int K, int ROWS, int THREADS, class Src>
-__device__ __forceinline__ void stageRowsT(unsigned char* tile, int r0, Src&& src) {
-  constexpr int kChunks = K / 8, kTotal = ROWS * kChunks, kPer = (kTotal + THREADS - 1) / THREADS;
-  uint4 v[kPer];
-#pragma unroll
-  for (int m = 0; m < kPer; ++m) {
-    const int k = threadIdx.x + THREADS * m;
-    v[m] = k < kTotal ? src(k / kChunks, k % kChunks) : zero4();
-  }
-#pragma unroll
-  for (int m = 0; m < kPer; ++m) {
-    const int k = threadIdx.x + THREADS * m;
-    if (k < kTotal) st16(tile, r0 + k / kChunks, k % kChunks, K, v[m]);
-  }
-}
 
 // K1 = 16: h' = relu(W1 f + b1) (node encoder; X = f). K1 = 128: h' = h + relu(W1 [h; a] + b1) (a layer's update).
 // Then Out = W2 h' (N2 rows of W2: rows 0..N2-1 of the tile from W2's columns col2a, or for N2 = 32 rows 0..15 from
@@ -1659,7 +1645,8 @@ size_t smemFor(size_t bytes) { return bytes + 128; }
 // k_slot_encode holds 256 TMEM columns: at most two of its blocks fit an SM's shared memory (3 x 91 KB > 228 KB), so a
 // third never waits in tcgen05.alloc for a resident block's columns (the grid is also capped at two blocks per SM).
 // Its tile needs 1024-byte alignment (the TMA swizzle), hence the extra 1 KB.
-constexpr size_t kSlotEncodeSmem = (sizeof(SlotEncSmem) > 76 * 1024 ? sizeof(SlotEncSmem) : 76 * 1024) + 1024 - 128;
+constexpr size_t kSlotEncodeSmem = sizeof(SlotEncSmem) + 1024 - 128;
+static_assert(3 * (kSlotEncodeSmem + 128 + 1024) > 228 * 1024, "k_slot_encode: three blocks would share an SM's TMEM");
 
 }  // namespace
 
