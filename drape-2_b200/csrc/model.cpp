@@ -35,6 +35,42 @@ inline uint64_t edgeKey(uint32_t a, uint32_t b) {
   return (static_cast<uint64_t>(lo) << 32) | hi;
 }
 
+// Runs f(c) for c in [0, chunks) on up to `chunks` threads (the calling thread takes chunk 0); the first exception a
+// chunk throws is rethrown after all have finished.
+template <class F>
+void parallelChunks(std::size_t chunks, F&& f) {
+  if (chunks <= 1) {
+    if (chunks == 1) f(0);
+    return;
+  }
+  std::vector<std::exception_ptr> errors(chunks);
+  std::vector<std::thread> pool;
+  for (std::size_t c = 1; c < chunks; ++c)
+    pool.emplace_back([&, c] {
+      try {
+        f(c);
+      } catch (...) {
+        errors[c] = std::current_exception();
+      }
+    });
+  try {
+    f(0);
+  } catch (...) {
+    errors[0] = std::current_exception();
+  }
+  for (auto& t : pool) t.join();
+  for (auto& e : errors)
+    if (e) std::rethrow_exception(e);
+}
+
+// Host threads for the build's parallel loops, and the chunk count for `items` items of at least `grain` each.
+std::size_t buildThreads() {
+  return std::max<std::size_t>(1, std::min<std::size_t>(16, std::thread::hardware_concurrency()));
+}
+std::size_t chunksFor(std::size_t items, std::size_t grain) {
+  return std::max<std::size_t>(1, std::min(buildThreads(), (items + grain - 1) / grain));
+}
+
 }  // namespace
 
 std::size_t Model::garmentIndex(const std::string& id) const {
@@ -118,30 +154,36 @@ Model Model::build(const drape_scene_desc& scene, bool copyField) {
       const double f0 = rest(c, 0) - rest(a, 0), f1 = rest(c, 1) - rest(a, 1);
       return 0.5 * std::abs(e0 * f1 - e1 * f0);
     };
-    next.stretch.reserve(next.stretch.size() + sg.triangle_count);
-    // Stretch terms: rest shape in the piece's grain frame, dmInv = Dm^-1, area = |det Dm| / 2 (sim_model.cpp:107-123).
-    for (uint32_t t = 0; t < sg.triangle_count; ++t) {
-      const uint32_t piece = sg.triangle_piece[t];
-      const double u0 = sg.piece_grain[2 * piece], u1 = sg.piece_grain[2 * piece + 1];
-      double r[3][2];
-      for (int k = 0; k < 3; ++k) {
-        const uint32_t v = T[3 * t + k];
-        r[k][0] = rest(v, 0) * u0 + rest(v, 1) * u1;
-        r[k][1] = rest(v, 0) * -u1 + rest(v, 1) * u0;
+    const std::size_t stretchBase = next.stretch.size();
+    next.stretch.resize(stretchBase + sg.triangle_count);
+    // Stretch terms: rest shape in the piece's grain frame, dmInv = Dm^-1, area = |det Dm| / 2 (sim_model.cpp:107-123);
+    // every triangle on its own, in parallel chunks.
+    const std::size_t triChunks = chunksFor(sg.triangle_count, 16384);
+    parallelChunks(triChunks, [&](std::size_t ch) {
+      for (uint32_t t = static_cast<uint32_t>(sg.triangle_count * ch / triChunks);
+           t < static_cast<uint32_t>(sg.triangle_count * (ch + 1) / triChunks); ++t) {
+        const uint32_t piece = sg.triangle_piece[t];
+        const double u0 = sg.piece_grain[2 * piece], u1 = sg.piece_grain[2 * piece + 1];
+        double r[3][2];
+        for (int k = 0; k < 3; ++k) {
+          const uint32_t v = T[3 * t + k];
+          r[k][0] = rest(v, 0) * u0 + rest(v, 1) * u1;
+          r[k][1] = rest(v, 0) * -u1 + rest(v, 1) * u0;
+        }
+        const double a = r[1][0] - r[0][0], b = r[2][0] - r[0][0], c = r[1][1] - r[0][1], d = r[2][1] - r[0][1];
+        const double det = a * d - c * b;
+        const double invdet = 1.0 / det;  // adjugate times 1 / det (the operation order of Eigen's 2x2 inverse)
+        Stretch st;
+        for (int k = 0; k < 3; ++k) st.v[k] = off + T[3 * t + k];
+        st.dmInv[0][0] = d * invdet;
+        st.dmInv[0][1] = -b * invdet;
+        st.dmInv[1][0] = -c * invdet;
+        st.dmInv[1][1] = a * invdet;
+        st.area = 0.5 * std::abs(det);
+        st.fabric = g.fabricOffset + piece;
+        next.stretch[stretchBase + t] = st;
       }
-      const double a = r[1][0] - r[0][0], b = r[2][0] - r[0][0], c = r[1][1] - r[0][1], d = r[2][1] - r[0][1];
-      const double det = a * d - c * b;
-      const double invdet = 1.0 / det;  // adjugate times 1 / det (the operation order of Eigen's 2x2 inverse)
-      Stretch st;
-      for (int k = 0; k < 3; ++k) st.v[k] = off + T[3 * t + k];
-      st.dmInv[0][0] = d * invdet;
-      st.dmInv[0][1] = -b * invdet;
-      st.dmInv[1][0] = -c * invdet;
-      st.dmInv[1][1] = a * invdet;
-      st.area = 0.5 * std::abs(det);
-      st.fabric = g.fabricOffset + piece;
-      next.stretch.push_back(st);
-    }
+    });
     // Edge occurrences in insertion order (triangle t, then k = 0, 1, 2), stably sorted by (min, max): the same
     // sequence a std::map<pair<min,max>, vector<tri>> iterates. Counting sort by the smaller vertex (stable), then a
     // stable insertion sort of each vertex's few edges by the larger one.
@@ -165,11 +207,25 @@ Model Model::build(const drape_scene_desc& scene, bool copyField) {
           occ[j] = item;
         }
     }
+    // Interior edges in occurrence order (the map order): the first occurrence of every edge shared by exactly two
+    // triangles of one piece, found by a serial scan; their hinges are then formed in parallel chunks.
+    std::vector<std::size_t> interior;
+    interior.reserve(occ.size() / 2);
+    for (std::size_t i = 0; i < occ.size();) {
+      std::size_t j = i;
+      while (j < occ.size() && occ[j].first == occ[i].first) ++j;
+      if (j - i == 2 && sg.triangle_piece[occ[i].second] == sg.triangle_piece[occ[i + 1].second]) interior.push_back(i);
+      i = j;
+    }
+    const std::size_t hingeBase = next.hinges.size();
     {
-      const std::size_t more = occ.size() / 2 + sg.seam_pair_count;
-      next.hinges.reserve(next.hinges.size() + more);
-      next.hingeSides.reserve(next.hingeSides.size() + more);
-      next.hingeGeom.reserve(next.hingeGeom.size() + more);
+      const std::size_t more = interior.size() + sg.seam_pair_count;
+      next.hinges.reserve(hingeBase + more);
+      next.hingeSides.reserve(hingeBase + more);
+      next.hingeGeom.reserve(hingeBase + more);
+      next.hinges.resize(hingeBase + interior.size());
+      next.hingeSides.resize(hingeBase + interior.size());
+      next.hingeGeom.resize(hingeBase + interior.size());
     }
     auto opposite = [&](uint32_t t, uint32_t e0, uint32_t e1) {
       for (int k = 0; k < 3; ++k) {
@@ -178,28 +234,27 @@ Model Model::build(const drape_scene_desc& scene, bool copyField) {
       }
       return e0;
     };
-    for (std::size_t i = 0; i < occ.size();) {
-      std::size_t j = i;
-      while (j < occ.size() && occ[j].first == occ[i].first) ++j;
-      if (j - i == 2 && sg.triangle_piece[occ[i].second] == sg.triangle_piece[occ[i + 1].second]) {
+    const std::size_t hingeChunks = chunksFor(interior.size(), 16384);
+    parallelChunks(hingeChunks, [&](std::size_t ch) {
+      for (std::size_t h = interior.size() * ch / hingeChunks; h < interior.size() * (ch + 1) / hingeChunks; ++h) {
+        const std::size_t i = interior[h];
         const uint32_t e0 = static_cast<uint32_t>(occ[i].first >> 32), e1 = static_cast<uint32_t>(occ[i].first);
         const uint32_t t0 = occ[i].second, t1 = occ[i + 1].second;
         const uint32_t piece = sg.triangle_piece[t0];
         Hinge hg;
         hg.v = {off + opposite(t0, e0, e1), off + opposite(t1, e0, e1), off + e0, off + e1};
-        next.hinges.push_back(hg);
+        next.hinges[hingeBase + h] = hg;
         HingeSide side;
         side.fabric = g.fabricOffset + piece;
         side.edgeDir[0] = rest(e1, 0) - rest(e0, 0);
         side.edgeDir[1] = rest(e1, 1) - rest(e0, 1);
         side.grain[0] = sg.piece_grain[2 * piece];
         side.grain[1] = sg.piece_grain[2 * piece + 1];
-        next.hingeSides.push_back({side, side});
-        next.hingeGeom.push_back((side.edgeDir[0] * side.edgeDir[0] + side.edgeDir[1] * side.edgeDir[1]) /
-                                 (triArea(t0) + triArea(t1)));
+        next.hingeSides[hingeBase + h] = {side, side};
+        next.hingeGeom[hingeBase + h] = (side.edgeDir[0] * side.edgeDir[0] + side.edgeDir[1] * side.edgeDir[1]) /
+                                        (triArea(t0) + triArea(t1));
       }
-      i = j;
-    }
+    });
     // The triangle of a boundary edge (an edge with exactly one triangle), or -1.
     auto triangleWithEdge = [&](uint32_t a, uint32_t b) -> int64_t {
       const uint64_t key = edgeKey(a, b);
@@ -269,7 +324,11 @@ Model Model::build(const drape_scene_desc& scene, bool copyField) {
     next.fExt[p].z += scene.forces[3 * k + 2];
   }
   for (uint32_t i = 0; i < n; ++i) next.updateMass(i);
-  for (std::size_t h = 0; h < next.hinges.size(); ++h) next.hinges[h].K = next.hingeStiffness(h);
+  const std::size_t kChunks = chunksFor(next.hinges.size(), 16384);
+  parallelChunks(kChunks, [&](std::size_t ch) {
+    for (std::size_t h = next.hinges.size() * ch / kChunks; h < next.hinges.size() * (ch + 1) / kChunks; ++h)
+      next.hinges[h].K = next.hingeStiffness(h);
+  });
   next.buildIncidence();
   next.buildStructure();
   return next;
@@ -335,38 +394,6 @@ void Model::buildIncidence() {
   for (std::size_t i = 0; i < n; ++i) maxRowEntries = std::max(maxRowEntries, incStart[i + 1] - incStart[i]);
 }
 
-namespace {
-
-// Runs f(c) for c in [0, chunks) on up to `chunks` threads (the calling thread takes chunk 0); the first exception a
-// chunk throws is rethrown after all have finished.
-template <class F>
-void parallelChunks(std::size_t chunks, F&& f) {
-  if (chunks <= 1) {
-    if (chunks == 1) f(0);
-    return;
-  }
-  std::vector<std::exception_ptr> errors(chunks);
-  std::vector<std::thread> pool;
-  for (std::size_t c = 1; c < chunks; ++c)
-    pool.emplace_back([&, c] {
-      try {
-        f(c);
-      } catch (...) {
-        errors[c] = std::current_exception();
-      }
-    });
-  try {
-    f(0);
-  } catch (...) {
-    errors[0] = std::current_exception();
-  }
-  for (auto& t : pool) t.join();
-  for (auto& e : errors)
-    if (e) std::rethrow_exception(e);
-}
-
-}  // namespace
-
 void Model::buildStructure() {
   const std::size_t n = x.size();
   // Row i's columns: i itself and every vertex of every term that contains i, deduplicated with a stamp array and
@@ -386,8 +413,7 @@ void Model::buildStructure() {
     std::vector<uint32_t> cols, offSlot, offStart, offContrib;
     uint32_t maxL = 0;
   };
-  const std::size_t threads = std::max<std::size_t>(1, std::min<std::size_t>(16, std::thread::hardware_concurrency()));
-  const std::size_t chunkCount = std::max<std::size_t>(1, std::min(threads, (n + 8191) / 8192));
+  const std::size_t chunkCount = chunksFor(n, 8192);
   std::vector<Chunk> chunks(chunkCount);
   for (std::size_t c = 0; c < chunkCount; ++c) {
     chunks[c].r0 = static_cast<uint32_t>(n * c / chunkCount);
@@ -489,10 +515,12 @@ void Model::buildStructure() {
   const std::size_t terms = std::max(stretch.size(), std::max(hinges.size(), seams.size()));
   if (terms >= (1u << 26)) throw std::invalid_argument("too many terms for the contribution encoding");
   offCode.resize(offContrib.size());
-  for (std::size_t c = 0; c < offContrib.size(); ++c) {
-    const uint32_t v = offContrib[c], code = incEntry[v >> 2];
-    offCode[c] = (code & 0xC0000000u) | (((code >> 2) & 0x03FFFFFFu) << 4) | ((code & 3u) << 2) | (v & 3u);
-  }
+  parallelChunks(chunkCount, [&](std::size_t c) {
+    for (std::size_t k = contribBase[c]; k < contribBase[c + 1]; ++k) {
+      const uint32_t v = offContrib[k], code = incEntry[v >> 2];
+      offCode[k] = (code & 0xC0000000u) | (((code >> 2) & 0x03FFFFFFu) << 4) | ((code & 3u) << 2) | (v & 3u);
+    }
+  });
   contactForce.assign(n, 0.0);
 }
 
