@@ -130,6 +130,7 @@ struct Dev {
   float4* hingeDer;        // per hinge term: its HingeDer record (4 float4)
   const float* Lf;         // learned factor L: 9 planes of slotsPadded floats on lower slots (k_solve<true>)
   const uint32_t* tslot;   // slot of (j, i) for slot (i, j)
+  const float4* LfRows;    // the factor by rows, three float4 a slot: L_ij at lower slots, L_ji at upper (i, j)
   const float4* fExt;
   const float4* pinPos;
   float* blocks;   // 9 planes of slotsPadded floats, component 3*row+col
@@ -1194,6 +1195,164 @@ __device__ inline int pcgResidentRows(const Dev& D, GridSync& gs, const SlicedMa
   return it;
 }
 
+constexpr int kLearnedDepth = 4;  // slots whose factor rows and gathered vector a row thread has in flight
+
+// acc += B x (Upper: B^T x) for this thread's row over its slots [k0, k1) of the block's sliced column layout (slot k
+// is global slot rs + k; the columns are sorted, so the lower part j <= i is [0, kd] and the upper part j >= i is
+// [kd, end) with kd the diagonal's position), the blocks from the factor by rows (D.LfRows); padding and pinned columns
+// carry bit 31 and are skipped. kLearnedDepth slots' loads are issued before their first FMA.
+template <bool Upper>
+__device__ __forceinline__ float3 factorProduct(const Dev& D, const SlicedMatrix& A, uint32_t rs, uint32_t kBegin,
+                                                uint32_t kEnd, const float4* x) {
+  const uint32_t lane = threadIdx.x & 31u;
+  float3 acc = mk(0, 0, 0);
+  for (uint32_t k0 = kBegin; k0 < kEnd; k0 += kLearnedDepth) {
+    bool use[kLearnedDepth];
+    float3 v[kLearnedDepth];
+    float4 m[kLearnedDepth][3];
+#pragma unroll
+    for (int u = 0; u < kLearnedDepth; ++u) {
+      const uint32_t k = k0 + u;
+      const uint32_t col = k < kEnd ? A.cols[A.base + 32u * k + lane] : kPinnedBit;
+      use[u] = !(col & kPinnedBit);
+      v[u] = mk(0, 0, 0);
+      m[u][0] = m[u][1] = m[u][2] = make_float4(0, 0, 0, 0);
+      if (use[u]) {
+        v[u] = ld3(x, col);
+        const float4* row = D.LfRows + 3 * static_cast<size_t>(rs + k);
+        m[u][0] = __ldg(row);
+        m[u][1] = __ldg(row + 1);
+        m[u][2] = __ldg(row + 2);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kLearnedDepth; ++u) {
+      if (!use[u]) continue;
+      const float4 a = m[u][0], b = m[u][1], c = m[u][2];
+      const float3 w = v[u];
+      if (Upper) {  // L_ji^T x_j
+        acc.x += a.x * w.x + b.x * w.y + c.x * w.z;
+        acc.y += a.y * w.x + b.y * w.y + c.y * w.z;
+        acc.z += a.z * w.x + b.z * w.y + c.z * w.z;
+      } else {  // L_ij x_j
+        acc.x += a.x * w.x + a.y * w.y + a.z * w.z;
+        acc.y += b.x * w.x + b.y * w.y + b.z * w.z;
+        acc.z += c.x * w.x + c.y * w.y + c.z * w.z;
+      }
+    }
+  }
+  return acc;
+}
+
+// z_i = F(L L^T r)_i for this thread's row over resident rows (pcgLearnedResident). y = L^T r goes through D.ap (r was
+// published by the caller's reduction; a grid barrier publishes y); returns false when the barrier gave up.
+__device__ inline bool applyLearnedResident(const Dev& D, GridSync& gs, const SlicedMatrix& A, uint32_t i, bool own,
+                                            uint32_t rs, uint32_t kd, uint32_t len, const Contact& c, float3& z) {
+  // y_i = sum over the row's slots (i, j), j >= i, of L_(j, i)^T r_j.
+  if (own) D.ap[i] = f4(factorProduct<true>(D, A, rs, kd, len, D.r));  // pinned rows: kd = len = 0
+  if (!gs.sync()) return false;
+  // z_i = F(sum over the row's slots (i, j), j <= i, of L_(i, j) y_j).
+  if (own) {
+    z = filterContact(c, factorProduct<false>(D, A, rs, 0, min(kd + 1, len), D.ap));
+    D.z[i] = f4(z);
+  }
+  return true;
+}
+
+// The learned-preconditioner PCG of pcgLearned (M^-1 = L L^T, contact-filtered, the same stopping tests and breakdown
+// rules) over resident rows: each thread keeps its row's step, resid, r, z, p, A p and its filtered copy in registers;
+// the matrix is the block's sliced shared-memory copy; r and z are published for the neighbours' gathers. Four grid
+// exchanges an iteration (p.Ap; r.r, which publishes r; y = L^T r; r.z, which publishes z), as in pcgLearned. Returns
+// the iteration count, -1 when a barrier gave up, or -2 - iterations on a breakdown (the caller then solves with
+// block-Jacobi).
+__device__ inline int pcgLearnedResident(const Dev& D, GridSync& gs, const SlicedMatrix& A) {
+  uint32_t r0i, r1i;
+  blockRange(D.P.n, gs.rank, gs.size, r0i, r1i);
+  const uint32_t i = r0i + threadIdx.x;
+  const bool own = i < r1i;
+  const uint32_t rs = own ? __ldg(D.rowStart + i) : 0u;
+  // The row's length and its diagonal's position (the factor's lower part is [0, kd], the upper [kd, len)); a pinned
+  // row has no slots in the sliced layout (its L is zero) and takes none, and no range passes the warp's length.
+  const bool live = own && D.particle[i].pinned == 0u;
+  const uint32_t len = live ? min(__ldg(D.rowStart + i + 1) - rs, A.len) : 0u;
+  const uint32_t kd = live ? min(__ldg(D.diagSlot + i) - rs, len) : 0u;
+  Contact c{};
+  float3 step = mk(0, 0, 0), resid = mk(0, 0, 0), r = mk(0, 0, 0), z = mk(0, 0, 0);
+  float3 p = mk(0, 0, 0), ap = mk(0, 0, 0), apFull = mk(0, 0, 0);
+  auto writeBack = [&] {
+    if (own) {
+      D.step[i] = f4(step);
+      D.resid[i] = f4(resid);
+      D.r[i] = f4(r);
+    }
+  };
+  double rr0;
+  {
+    double v[1] = {0.0}, t[1];
+    if (own) {
+      c = D.contact[i];
+      resid = -ld3(D.grad, i);
+      r = filterContact(c, resid);
+      D.r[i] = f4(r);
+      v[0] = dotd3(r, r);
+    }
+    if (!gridReduce<1>(D, gs, v, t)) return -1;
+    rr0 = t[0];
+  }
+  const double r0 = sqrt(rr0);
+  if (!(r0 > 0.0) || !(rr0 > 0.0)) {
+    writeBack();
+    return 0;
+  }
+  double rz;
+  {
+    if (!applyLearnedResident(D, gs, A, i, own, rs, kd, len, c, z)) return -1;
+    double v[1] = {own ? dotd3(r, z) : 0.0}, t[1];
+    if (!gridReduce<1>(D, gs, v, t)) return -1;
+    rz = t[0];
+  }
+  if (!isfinite(rz)) return -2;
+  double beta = 0.0;
+  int it = 0;
+  while (it < D.P.maxCg) {
+    // A p = A z + beta A pPrev, p = z + beta pPrev.
+    const float fb = static_cast<float>(beta);
+    const float3 az = slicedProduct(A, D.z);
+    double vpap[1] = {0.0}, pAp[1];
+    if (own) {
+      p = it == 0 ? z : z + p * fb;
+      apFull = it == 0 ? az : az + apFull * fb;
+      ap = filterContact(c, apFull);
+      vpap[0] = dotd3(p, ap);
+    }
+    if (!gridReduce<1>(D, gs, vpap, pAp)) return -1;
+    if (!isfinite(pAp[0])) return -2 - it;
+    if (!(pAp[0] > 0.0)) break;
+    const float fa = static_cast<float>(rz / pAp[0]);
+    ++it;
+    double v[1] = {0.0}, rr[1];
+    if (own) {
+      step = step + p * fa;
+      r = r - ap * fa;
+      resid = resid - apFull * fa;
+      D.r[i] = f4(r);
+      v[0] = dotd3(r, r);
+    }
+    if (!gridReduce<1>(D, gs, v, rr)) return -1;
+    if (!isfinite(rr[0])) return -2 - it;
+    if (sqrt(rr[0]) <= D.P.cgTolerance * r0) break;
+    if (rr[0] > 1e6 * rr0) return -2 - it;
+    if (!applyLearnedResident(D, gs, A, i, own, rs, kd, len, c, z)) return -1;
+    double vz[1] = {own ? dotd3(r, z) : 0.0}, rzNew[1];
+    if (!gridReduce<1>(D, gs, vz, rzNew)) return -1;
+    if (!isfinite(rzNew[0])) return -2 - it;
+    beta = rzNew[0] / rz;
+    rz = rzNew[0];
+  }
+  writeBack();
+  return it;
+}
+
 // Pipelined contact-filtered block-Jacobi PCG (Ghysels and Vanroose, "Hiding global synchronization latency in the
 // preconditioned conjugate gradient algorithm", Parallel Computing 40 (2014) 224-238, Alg. 3). In exact arithmetic
 // its iterates, iteration count and stopping tests are those of pcgReferenceOrder (operator F A F, preconditioner
@@ -1524,11 +1683,23 @@ __device__ inline int pcgSolve(const Dev& D, GridSync& gs) {
   uint32_t r0i, r1i;
   blockRange(D.P.n, gs.rank, gs.size, r0i, r1i);
   if constexpr (Variant == kResidentRows) {
-    static_assert(!Learned, "resident rows: block-Jacobi only");
     SlicedMatrix A;
     if (!stageSliced(D, r0i, r1i, A)) return -1;
     const unsigned long long t0 = globalTimerNs();
-    const int it = pcgResidentRows(D, gs, A);
+    int it;
+    if constexpr (Learned) {
+      // The learned schedule without block-Jacobi iterations first (the host picks this kernel only then): a learned
+      // solve that breaks down is followed by a full block-Jacobi solve, as in pcgSolveStaged.
+      it = pcgLearnedResident(D, gs, A);
+      if (gs.rank == 0 && threadIdx.x == 0) D.ctl->learnedSolves += 1;
+      if (it < -1) {
+        if (gs.rank == 0 && threadIdx.x == 0) D.ctl->precondFallbacks += 1;
+        const int jac = pcgResidentRows(D, gs, A);
+        it = jac < 0 ? jac : jac + (-2 - it);
+      }
+    } else {
+      it = pcgResidentRows(D, gs, A);
+    }
     if (gs.rank == 0 && threadIdx.x == 0) D.ctl->pcgNs += static_cast<long long>(globalTimerNs() - t0);
     return it;
   } else {

@@ -922,6 +922,22 @@ __global__ void k_output_slots(Graph g, const float* __restrict__ Q) {
       for (int c = 0; c < 3; ++c) L[3 * r + c] = C[3 * r] * G[c] + C[3 * r + 1] * G[3 + c] + C[3 * r + 2] * G[6 + c];
   }
   for (int k = 0; k < 9; ++k) g.L[k * g.SP + s] = L[k];
+  if (g.LF != nullptr && j <= i) {
+    // The block by rows at its own slot and, below the diagonal, at its transposed slot too (every upper slot has its
+    // lower counterpart, so every slot of LF is written).
+    const float4 r0 = make_float4(L[0], L[1], L[2], 0.0f), r1 = make_float4(L[3], L[4], L[5], 0.0f),
+                 r2 = make_float4(L[6], L[7], L[8], 0.0f);
+    float4* o = g.LF + 3 * static_cast<size_t>(s);
+    o[0] = r0;
+    o[1] = r1;
+    o[2] = r2;
+    if (j < i) {
+      float4* u = g.LF + 3 * static_cast<size_t>(__ldg(g.tslot + s));
+      u[0] = r0;
+      u[1] = r1;
+      u[2] = r2;
+    }
+  }
 }
 
 // ------------------------------------------------------------------------------------------------------------------
@@ -1940,6 +1956,7 @@ GraphHandle Network::bind(uint32_t n, uint32_t B, uint32_t SP, const uint32_t* h
   g.activeBase = activeBase;
   g.activeStride = activeStride;
   allocWorkspace(*s, false, st);
+  g.LF = s->own<float4>(3 * static_cast<size_t>(SP));
   NCK(cudaStreamSynchronize(st));
   return GraphHandle(s.release());
 }

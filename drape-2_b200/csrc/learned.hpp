@@ -70,6 +70,9 @@ struct Graph {
   uint32_t* code = nullptr;          // B: column of the slot, bit 31 when either row is pinned (written by k_features)
   uint32_t* slotRow = nullptr;       // B: row of the slot (fixed with the CSR)
   const void* tmaps = nullptr;       // host memory: the TMA store maps of E and F (CUtensorMap[2])
+  // A solver's bound graph only: per slot three float4 rows of a factor block for the solver's own products: L_ij at
+  // the lower slots (j <= i) and, at each upper slot (i, j), L_ji (the block of its transposed slot).
+  float4* LF = nullptr;
 };
 
 // Host-owned device buffers of a graph built from host arrays (a training sample) or bound to a solver's arrays.

@@ -201,15 +201,22 @@ struct drape_solver {
       if (perSM < 1) throw std::runtime_error("cuda: the solve kernel does not fit on an SM");
     }
     {
-      cudaFuncAttributes fa{};
-      CK(cudaFuncGetAttributes(&fa, reinterpret_cast<const void*>(dcu::k_solve_rows)));
-      rowsSmemCap = static_cast<uint32_t>((prop.sharedMemPerBlockOptin - fa.sharedSizeBytes) / dcu::kSmemSlotBytes);
+      const void* rowKernels[] = {reinterpret_cast<const void*>(dcu::k_solve_rows),
+                                  reinterpret_cast<const void*>(dcu::k_solve_rows_learned)};
+      size_t rowsStatic = 0;
+      for (const void* k : rowKernels) {
+        cudaFuncAttributes fa{};
+        CK(cudaFuncGetAttributes(&fa, k));
+        rowsStatic = std::max(rowsStatic, fa.sharedSizeBytes);
+      }
+      rowsSmemCap = static_cast<uint32_t>((prop.sharedMemPerBlockOptin - rowsStatic) / dcu::kSmemSlotBytes);
       const int rowsMax = static_cast<int>(rowsSmemCap * dcu::kSmemSlotBytes);
-      CK(cudaFuncSetAttribute(reinterpret_cast<const void*>(dcu::k_solve_rows),
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, rowsMax));
-      int perSM = 0;
-      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, dcu::k_solve_rows, dcu::kRowThreads, rowsMax));
-      if (perSM < 1) throw std::runtime_error("cuda: the resident-row solve kernel does not fit on an SM");
+      for (const void* k : rowKernels) {
+        CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, rowsMax));
+        int perSM = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, k, dcu::kRowThreads, rowsMax));
+        if (perSM < 1) throw std::runtime_error("cuda: the resident-row solve kernel does not fit on an SM");
+      }
     }
     solveGrid = numSMs;  // one 1024-thread block per SM: fewest barrier arrivals
     pointGrid = numSMs * 8;
@@ -372,6 +379,7 @@ struct drape_solver {
                          sizeof(dcu::Contact), stream);
     dev.Lf = net->graphOf(*netGraph).L;
     dev.tslot = net->graphOf(*netGraph).tslot;
+    dev.LfRows = net->graphOf(*netGraph).LF;
     netNewtonCounter = 0;
   }
 
@@ -381,6 +389,7 @@ struct drape_solver {
       netGraph.reset();
       dev.Lf = nullptr;
       dev.tslot = nullptr;
+      dev.LfRows = nullptr;
       return;
     }
     if (!p->net) throw std::invalid_argument("null preconditioner handle");
@@ -455,9 +464,10 @@ struct drape_solver {
   }
 
   // The reference-order PCG runs over resident rows (k_solve_rows) where the built scene fits it; bit-identical to
-  // k_solve<false, 0>, which variant 3 forces.
+  // k_solve<false, 0>, which variant 3 forces. The learned preconditioner runs over resident rows too
+  // (k_solve_rows_learned) unless block-Jacobi iterations come first (precondSwitch) or variant 3 forces k_solve<true>.
   bool usesResidentRows(const dcu::Dev& d) const {
-    return d.P.pcgVariant == 0 && rowsSmemBytes > 0 && !(learnedOn && netGraph);
+    return d.P.pcgVariant == 0 && rowsSmemBytes > 0 && (!(learnedOn && netGraph) || precondSwitch == 0);
   }
 
   void launchSolve(const dcu::Dev& d) {
@@ -473,7 +483,10 @@ struct drape_solver {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     if (learnedOn && netGraph) {
-      CK(cudaLaunchKernelEx(&cfg, dcu::k_solve<true, 0>, d));
+      if (rows)
+        CK(cudaLaunchKernelEx(&cfg, dcu::k_solve_rows_learned, d));
+      else
+        CK(cudaLaunchKernelEx(&cfg, dcu::k_solve<true, 0>, d));
     } else if (rows) {
       CK(cudaLaunchKernelEx(&cfg, dcu::k_solve_rows, d));
     } else if (d.P.pcgVariant == 1) {

@@ -53,6 +53,15 @@ __global__ void __launch_bounds__(kRowThreads, 1) k_solve_rows(Dev D) {
   solveGroup<false, kRowLanes, kResidentRows>(D, gs);
 }
 
+// The same with the learned preconditioner (pcgLearnedResident; block-Jacobi after a breakdown), for scenes that fit
+// resident rows and solves that start with the learned preconditioner.
+__global__ void __launch_bounds__(kRowThreads, 1) k_solve_rows_learned(Dev D) {
+  if (D.ctl->newtonDone) return;
+  GridSync gs;
+  gs.init(D.ctl, D.P.barrierLimitNs);
+  solveGroup<true, kRowLanes, kResidentRows>(D, gs);
+}
+
 __global__ void k_finish(Dev D) { finishRows(D, blockIdx.x, gridDim.x); }
 
 __global__ void k_advance_clock(Dev D) {
