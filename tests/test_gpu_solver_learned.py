@@ -60,6 +60,31 @@ def test_non_finite_network_falls_back_to_jacobi_bit_identically(gpu):
     assert a.counters().cg_iterations == cb.cg_iterations
 
 
+@pytest.mark.parametrize("iterations, bar", [(1, 1e-5), (2, 1e-3)])
+def test_resident_row_learned_pcg_tracks_the_1024_thread_kernel(gpu, iterations, bar):
+    """The learned PCG over resident rows (the default where the scene fits) against the 1024-thread learned kernel
+    (variant 3), trained network, the first frame of the assembling tube: the same PCG iteration counts, positions within
+    1e-5 m after one Newton iteration and 1e-3 m after two (their products sum in different orders; the capped solves
+    of the second system, assembled from the first step's slightly different positions, amplify that, and later frames
+    of this scene branch apart as any two FP32 orderings do)."""
+    p = learned.LearnedPreconditioner(0, learned.load_weights("tube"))
+    runs = []
+    for variant in (0, 3):
+        s = gpu.CudaSolver(0)
+        s.set_pcg_variant(variant)
+        s.set_precond(p)
+        s.build(_small_tube())
+        s.step(1 / 60, 1, iterations)
+        runs.append(s)
+    a, b = runs
+    assert a.solve_threads() == 512 and b.solve_threads() == 1024
+    ca, cb = a.counters(), b.counters()
+    assert ca.learned_solves == ca.newton_iterations == iterations and ca.precond_fallbacks == cb.precond_fallbacks == 0
+    assert np.array_equal(a.cg_history(), b.cg_history()), (a.cg_history(), b.cg_history())
+    dev = np.abs(a.positions().astype(np.float64) - b.positions()).max()
+    assert dev < bar, dev
+
+
 def test_switching_back_to_jacobi(gpu):
     p = learned.LearnedPreconditioner(0)
     s = gpu.CudaSolver(0)
