@@ -1932,7 +1932,8 @@ GraphHandle Network::bind(uint32_t n, uint32_t B, uint32_t SP, const uint32_t* h
                                           const uint32_t* hostColIndex, const uint32_t* dRowStart,
                                           const uint32_t* dColIndex, const float* dBlocks,
                                           const uint8_t* pinnedBase, uint32_t pinnedStride,
-                                          const uint8_t* activeBase, uint32_t activeStride, cudaStream_t st) {
+                                          const uint8_t* activeBase, uint32_t activeStride, cudaStream_t st,
+                                          bool factorRows) {
   auto s = std::make_unique<GraphStore>();
   std::vector<uint32_t> rs(hostRowStart, hostRowStart + n + 1), ci(hostColIndex, hostColIndex + B);
   const auto tiles = rowTiles(rs);
@@ -1956,7 +1957,7 @@ GraphHandle Network::bind(uint32_t n, uint32_t B, uint32_t SP, const uint32_t* h
   g.activeBase = activeBase;
   g.activeStride = activeStride;
   allocWorkspace(*s, false, st);
-  g.LF = s->own<float4>(3 * static_cast<size_t>(SP));
+  if (factorRows) g.LF = s->own<float4>(3 * static_cast<size_t>(SP));
   NCK(cudaStreamSynchronize(st));
   return GraphHandle(s.release());
 }

@@ -118,7 +118,8 @@ class Network {
   GraphHandle bind(uint32_t n, uint32_t B, uint32_t SP, const uint32_t* hostRowStart,
                                    const uint32_t* hostColIndex, const uint32_t* dRowStart, const uint32_t* dColIndex,
                                    const float* dBlocks, const uint8_t* pinnedBase, uint32_t pinnedStride,
-                                   const uint8_t* activeBase, uint32_t activeStride, cudaStream_t st);
+                                   const uint8_t* activeBase, uint32_t activeStride, cudaStream_t st,
+                                   bool factorRows = false);  // factorRows: also keep Graph::LF (a solver's graph)
   Graph& graphOf(GraphStore& s);
   const __nv_bfloat16* weights() const { return wBf16_; }
   const float* master() const { return master_; }

@@ -376,7 +376,7 @@ struct drape_solver {
                          reinterpret_cast<const uint8_t*>(particle.p) + offsetof(dcu::Particle, pinned),
                          sizeof(dcu::Particle),
                          reinterpret_cast<const uint8_t*>(contact.p) + offsetof(dcu::Contact, active),
-                         sizeof(dcu::Contact), stream);
+                         sizeof(dcu::Contact), stream, true);
     dev.Lf = net->graphOf(*netGraph).L;
     dev.tslot = net->graphOf(*netGraph).tslot;
     dev.LfRows = net->graphOf(*netGraph).LF;
