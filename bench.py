@@ -647,7 +647,8 @@ def run_profile_case(args):
     """One small case for an ncu capture (not a benchmark line): "spmv" times the standalone SpMV on the tiled tube
     system; "batch" builds the first --batch-garments tubes of the batched workload and runs --batch-frames frames
     (the first frame launches directly, the rest replay its CUDA graph); "bake" bakes the reference's test body;
-    "drape" runs --batch-frames frames of the --workload drape (direct launches, from its own start state)."""
+    "drape" runs --batch-frames frames of the --workload drape (direct launches, from its own start state), and
+    "drape_learned" the same with the learned preconditioner."""
     import torch
     from drape_b200 import cuda as CU
     torch.cuda.set_device(0)
@@ -692,14 +693,18 @@ def run_profile_case(args):
                           "block_slots": int(len(sysm["col_index"])), "deterministic": bool(np.array_equal(Ls[0], Ls[2])),
                           "l_norm": float(np.linalg.norm(Ls[0]))}))
         return 0
-    if args.profile_case == "drape":
+    if args.profile_case in ("drape", "drape_learned"):
         s = CU.CudaSolver(0)
         s.set_pcg_variant(args.pcg_variant)
+        if args.profile_case == "drape_learned":  # the shipped network every Newton iteration
+            from drape_b200 import learned as LR
+            net = LR.LearnedPreconditioner(0, LR.load_weights("tube"))
+            s.set_precond(net)
         s.build(make_scene(args.workload))
         for _ in range(args.batch_frames):
             s.step(1.0 / 60.0, 1, 2)
         c = s.counters()
-        print(json.dumps({"case": "drape", "workload": args.workload, "frames": args.batch_frames,
+        print(json.dumps({"case": args.profile_case, "workload": args.workload, "frames": args.batch_frames,
                           "newton_iterations": int(c.newton_iterations), "cg_iterations": int(c.cg_iterations)}))
         return 0
     if args.profile_case == "bake":
@@ -753,7 +758,8 @@ def main():
                          "1 pipelined (one grid exchange an iteration), 2 Chronopoulos-Gear (one reduction and one "
                          "plain barrier), 3 the reference's order on the 1024-thread kernel")
     ap.add_argument("--batch-garments", type=int, default=64, help="garments of the batched leg (0: skip it)")
-    ap.add_argument("--profile-case", choices=["spmv", "batch", "bake", "drape", "learned", "learned_inference"],
+    ap.add_argument("--profile-case", choices=["spmv", "batch", "bake", "drape", "drape_learned", "learned",
+                                               "learned_inference"],
                     default=None,
                     help="run one small case for a profiler capture instead of the benchmark")
     ap.add_argument("--spmv-tiles", type=int, default=12)
